@@ -1,0 +1,433 @@
+"""Benchmark: create/repair input GB/s on one B200, with the HBM roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Default workload (one step = one pass of the hot path over one job):
+  PAR2 create at scale, 32,768 input slices x 32 KiB (1 GiB) of seeded random
+  bytes, GF(2^16), 64 recovery slices with exponents 0..63.  Inputs are larger
+  than L2 (126 MB), so no L2 flush is needed between steps.
+Secondary lines (rank 0, a few steps each): PAR2 1,024 x 1 MiB R=8, PAR2
+plain 256 x 64 KiB R=8, PAR3 create 131,072 x 8 KiB R=8.
+
+JSON fields (one line on rank 0):
+  value          input GB/s with inputs resident in HBM (device-timed, CUDA
+                 events on the launching stream, max over ranks)
+  e2e            the same metric through the public API with pinned HOST
+                 buffers: H2D of the inputs and D2H of the recovery slices
+                 inside the timed region
+  roofline       the dominant kernel (region multiply-accumulate): algorithmic
+                 bytes (inputs read once + outputs written once) per launch /
+                 average launch time, against MEASURED_PEAKS.json hbm_gbs
+  cpu_baseline   the reference's own CPU code (oracle/_ref, compiled from its
+                 sources) on a bounded sample of the same workload
+Multi-GPU (torchrun): every rank runs its own job on its own GPU (weak
+scaling, no data-path collective); value = all ranks' input bytes / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GIB = 1 << 30
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(name):
+    """dram bytes per launch from a committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        try:
+            with open(p) as f:
+                return json.load(f).get(name)
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.lines = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={gpu_id}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+                power.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def gpu_uuid(dev: int) -> str:
+    import torch
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return str(dev)
+
+
+# ------------------------------------------------------------------ workloads
+WORKLOADS = {
+    "par2_create_32768x32KiB_R64": dict(field="gf16", n=32768, s=32 * 1024, r=64),
+    "par2_create_1024x1MiB_R8": dict(field="gf16", n=1024, s=1 << 20, r=8),
+    "par2_create_256x64KiB_R8": dict(field="gf16", n=256, s=64 * 1024, r=8),
+    "par3_create_131072x8KiB_R8": dict(field="gf64", n=131072, s=8 * 1024, r=8),
+}
+PRIMARY = "par2_create_32768x32KiB_R64"
+
+
+class Timer:
+    """CUDA-event timing on the stream the library launches on."""
+
+    def __init__(self, stream):
+        import torch
+        self.torch = torch
+        self.stream = stream
+
+    def run(self, fn, steps):
+        torch = self.torch
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(self.stream)
+        for _ in range(steps):
+            fn()
+        b.record(self.stream)
+        b.synchronize()
+        return a.elapsed_time(b) / steps  # ms
+
+
+def setup_job(name, dev, seed, ctx):
+    import torch
+    from parparpar_b200 import par2
+    w = WORKLOADS[name]
+    g = torch.Generator(device=f"cuda:{dev}")
+    g.manual_seed(seed)
+    job = dict(w)
+    if w["field"] == "gf16":
+        d_in = torch.randint(0, 256, (w["n"], w["s"]), dtype=torch.uint8, device=f"cuda:{dev}", generator=g)
+        d_out = torch.zeros((w["r"], w["s"]), dtype=torch.uint8, device=f"cuda:{dev}")
+        idx = np.arange(w["n"], dtype=np.uint16)
+        exps = np.arange(w["r"], dtype=np.uint16)
+        coeffs = torch.from_numpy(par2.coeff_matrix(idx, exps, ctx=ctx)).to(f"cuda:{dev}")
+        job.update(d_in=d_in, d_out=d_out, idx=idx, exps=exps, coeffs=coeffs)
+    else:
+        words = w["s"] // 8
+        d_in = torch.randint(-2**63, 2**63 - 1, (w["n"], words), dtype=torch.int64, device=f"cuda:{dev}",
+                             generator=g)
+        d_out = torch.zeros((w["r"], words), dtype=torch.int64, device=f"cuda:{dev}")
+        job.update(d_in=d_in, d_out=d_out, words=words)
+    return job
+
+
+def step_fn(job, ctx):
+    from parparpar_b200 import par2, par3
+    if job["field"] == "gf16":
+        return lambda: par2.par2_create(job["d_in"], job["idx"], job["exps"], out=job["d_out"], ctx=ctx)
+    par3.GF64Controller.ctx = ctx
+    return lambda: par3.GF64Controller.ComputeRecoveryBlocks(job["d_in"], job["n"], job["d_out"], job["r"],
+                                                             job["words"], 0, job["n"])
+
+
+def kernel_fn(job, ctx):
+    """The dominant kernel alone (coefficients already resident)."""
+    from parparpar_b200 import par2, par3
+    if job["field"] == "gf16":
+        return lambda: par2.gf16_muladd(job["d_in"], job["coeffs"], out=job["d_out"], ctx=ctx)
+    # the Cauchy matrix is cached on the device after the first call
+    return step_fn(job, ctx)
+
+
+def algo_bytes(job):
+    return (job["n"] + job["r"]) * job["s"]
+
+
+def measure(job, ctx, timer, steps, warmup, peak):
+    import parparpar_b200 as pp
+    f = step_fn(job, ctx)
+    for _ in range(warmup):
+        f()
+    ctx.synchronize()
+    l0 = pp.launch_count()
+    ms = timer.run(f, steps)
+    launches = pp.launch_count() - l0
+    kf = kernel_fn(job, ctx)
+    kf()
+    kms = timer.run(kf, max(3, min(steps, 20)))
+    achieved = algo_bytes(job) / (kms * 1e-3) / 1e9
+    return dict(ms=ms, launches=launches, kernel_ms=kms, achieved=achieved, frac=achieved / peak)
+
+
+def cpu_baseline_sample(name, budget_s=12.0, threads=0):
+    """Reference CPU code on a bounded sample of the workload: every slice,
+    a contiguous byte sub-range of each (cost is linear in the slice length)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    w = WORKLOADS[name]
+    rng = np.random.default_rng(99)
+    cores = os.cpu_count() or 1
+    if orc.Reference.available():
+        R = orc.Reference()
+        kind = "reference"
+        if w["field"] == "gf16":
+            sub = 2048
+            inp = rng.integers(0, 256, (w["n"], sub), dtype=np.uint8)
+            run = lambda: R.par2_create(inp, sub, np.arange(w["n"]), list(range(w["r"])), threads=threads)
+            sample = f"{w['n']} slices x {sub} B (a {sub}-byte sub-range of every slice), R={w['r']}"
+            nbytes = inp.nbytes
+        else:
+            sub = 256
+            inp = rng.integers(0, 2**64, (w["n"], sub // 8), dtype=np.uint64)
+            run = lambda: R.gf64_compute_recovery(0, inp, w["r"], 0, w["n"], threads=threads)
+            sample = f"{w['n']} blocks x {sub} B (a {sub}-byte sub-range of every block), R={w['r']}"
+            nbytes = inp.nbytes
+    else:
+        orc.build()
+        O = orc.Oracle()
+        kind = "port"
+        cores = 1
+        sub = 64
+        n = min(w["n"], 4096)
+        if w["field"] == "gf16":
+            inp = rng.integers(0, 256, (n, sub), dtype=np.uint8)
+            co = O.par2_coeff_matrix(np.arange(n), list(range(w["r"])))
+            run = lambda: O.par2_muladd(list(inp), sub, co)
+        else:
+            inp = rng.integers(0, 2**64, (n, sub // 8), dtype=np.uint64)
+            run = lambda: O.gf64_compute_recovery(inp, w["r"], 0, n)
+        sample = f"{n} slices x {sub} B, R={w['r']} (oracle C port, 1 thread)"
+        nbytes = inp.nbytes
+    times = []
+    t_end = time.time() + budget_s
+    while True:
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+        if time.time() > t_end or len(times) >= 5:
+            break
+    t = statistics.median(times)
+    return dict(value=nbytes / t / 1e9, unit="GB/s", cores=cores, kind=kind, sample=sample,
+                seconds_per_run=t, runs=len(times))
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's own CPU implementation on the host
+    cores, on the same workload/metric (bounded sample per step)."""
+    if rank != 0:
+        return
+    name = args.workload
+    w = WORKLOADS[name]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    times = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline_sample(name, budget_s=0.0)
+        if i >= args.warmup:
+            times.append(r)
+    val = statistics.median([t["value"] for t in times])
+    spr = statistics.median([t["seconds_per_run"] for t in times])
+    line = {
+        "impl": "reference", "metric": f"{name} input GB/s", "value": val, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": spr * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16" if w["field"] == "gf16" else "u64",
+        "data": "synthetic (seeded uniform random bytes)",
+        "config": {"workload": name, "num_inputs": w["n"], "slice_bytes": w["s"], "num_recovery": w["r"]},
+        "cpu_baseline": {"value": val, "unit": "GB/s", "cores": times[0]["cores"], "kind": times[0]["kind"],
+                         "sample": times[0]["sample"]},
+        "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=PRIMARY, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import parparpar_b200 as pp
+    ctx = pp.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    timer = Timer(stream)
+    peak, peak_kind = load_peaks()
+
+    job = setup_job(args.workload, local, 1234 + rank, ctx)
+    f = step_fn(job, ctx)
+    for _ in range(args.warmup):
+        f()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(gpu_uuid(local))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = pp.launch_count()
+    ms = timer.run(f, args.steps)
+    launches = pp.launch_count() - l0
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # dominant kernel alone, for the roofline
+    kf = kernel_fn(job, ctx)
+    kf()
+    kms = timer.run(kf, max(5, min(args.steps, 20)))
+    achieved = algo_bytes(job) / (kms * 1e-3) / 1e9
+
+    # end to end through the public API with pinned host buffers
+    w = WORKLOADS[args.workload]
+    from parparpar_b200 import par2, par3
+    if w["field"] == "gf16":
+        h_in = torch.empty((w["n"], w["s"]), dtype=torch.uint8).pin_memory()
+        h_in.copy_(job["d_in"])
+        h_out = torch.empty((w["r"], w["s"]), dtype=torch.uint8).pin_memory()
+        e2e_f = lambda: par2.par2_create(h_in, job["idx"], job["exps"], out=h_out, ctx=ctx)
+    else:
+        h_in = torch.empty((w["n"], w["s"] // 8), dtype=torch.int64).pin_memory()
+        h_in.copy_(job["d_in"])
+        h_out = torch.empty((w["r"], w["s"] // 8), dtype=torch.int64).pin_memory()
+        e2e_f = lambda: par3.GF64Controller.ComputeRecoveryBlocks(h_in, w["n"], h_out, w["r"], w["s"] // 8, 0, w["n"])
+    e2e_f()
+    torch.cuda.synchronize()
+    e2e_steps = max(2, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_f()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    ok = torch.equal(h_out.to(f"cuda:{local}"), job["d_out"])
+    del h_in, h_out
+
+    input_bytes = w["n"] * w["s"]
+    line = {
+        "metric": f"{args.workload} input GB/s", "value": input_bytes * world / (ms * 1e-3) / 1e9, "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16" if w["field"] == "gf16" else "u64",
+        "data": "synthetic (seeded uniform random bytes, generated on the device)",
+        "config": {"workload": args.workload, "num_inputs": w["n"], "slice_bytes": w["s"], "num_recovery": w["r"],
+                   "exponents": f"0..{w['r'] - 1}", "parallelism": f"replicas x{world} (one job per GPU)",
+                   "l2": "inputs (1 GiB) larger than L2; no flush needed"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s", "kernel": "k_gf16_muladd_lut" if w["field"] == "gf16"
+                     else "k_gf64_matvec_lut", "kernel_ms": kms,
+                     "traffic": load_traffic(args.workload)},
+        "e2e": {"value": input_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": input_bytes,
+                "d2h_bytes_per_step": w["r"] * w["s"], "host_buffers": "pinned", "matches_device_result": bool(ok)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+
+    if rank == 0 and world == 1 and not args.no_secondary:
+        sec = []
+        for name in WORKLOADS:
+            if name == args.workload:
+                continue
+            try:
+                j = setup_job(name, local, 77, ctx)
+                m = measure(j, ctx, timer, 5, 3, peak)
+                sec.append({"workload": name, "value": WORKLOADS[name]["n"] * WORKLOADS[name]["s"] / (m["ms"] * 1e-3)
+                            / 1e9, "unit": "GB/s", "ms_per_step": m["ms"], "kernel_ms": m["kernel_ms"],
+                            "roofline_frac": m["frac"]})
+                del j
+                torch.cuda.empty_cache()
+            except Exception as e:  # report, keep the primary line
+                sec.append({"workload": name, "error": str(e)[:200]})
+        line["secondary"] = sec
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline_sample(args.workload)
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,217 @@
+/*
+ * parpar_b200 — C ABI of the B200 (sm_100a) parity engine.
+ *
+ * This is the drop-in boundary for the two GF hot paths of ParParPar:
+ *   PAR2: the GF(2^16) region multiply-accumulate behind the gf16 controller
+ *         (gf16/controller.h:77-217, IPAR2ProcBackend) and the repair-matrix
+ *         inversion (gf16/gfmat_inv.h:16-50, Galois16RecMatrix);
+ *   PAR3: the GF(2^64) Cauchy-matrix engine behind the gf64_addon N-API entry
+ *         points (src/par3_engine.h:11-244, GF64Controller) and the gf64 region
+ *         dispatch table (gf64/gf64_global.h:23-37).
+ * All reference citations are path:line inside the ParParPar source tree.
+ *
+ * Conventions
+ *   - Every function returns an int status: PP_OK (0) or a negative PP_ERR_*
+ *     code; pp_ctx_last_error() gives the message of the last failure on that
+ *     context.  No C++ exception crosses this boundary.
+ *   - Buffer arguments may be HOST memory (pageable or pinned) or DEVICE
+ *     memory of the context's GPU; the library detects which.  Calls that take
+ *     host buffers are synchronous, like the reference: outputs are complete on
+ *     return.  Calls whose buffers are all device memory are enqueued on the
+ *     context's stream and return without waiting (pp_ctx_synchronize waits).
+ *   - Words are little-endian: u16 for GF(2^16), u64 for GF(2^64).
+ *   - No CPU fallback: without a usable CUDA device every compute entry point
+ *     fails with PP_ERR_NO_DEVICE.
+ */
+#ifndef PARPAR_B200_H
+#define PARPAR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define PP_API __declspec(dllexport)
+#else
+#define PP_API __attribute__((visibility("default")))
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define PP_OK 0
+#define PP_ERR_INVALID_ARG (-1)
+#define PP_ERR_CUDA (-2)
+#define PP_ERR_NO_MEMORY (-3)
+#define PP_ERR_SINGULAR (-4)      /* PAR3 solve: matrix singular (reference returns -1) */
+#define PP_ERR_NOT_INVERTIBLE (-5) /* PAR2 invert: not enough usable recovery (reference returns false) */
+#define PP_ERR_BUSY (-6)          /* PAR2 processor staging area full (reference PROC_ADD_FULL) */
+#define PP_ERR_NO_DEVICE (-7)
+#define PP_ERR_UNSUPPORTED (-8)
+
+/* reference PAR2ProcBackendAddResult (gf16/controller.h:38-43) */
+#define PP_PROC_ADD_OK 0
+#define PP_PROC_ADD_OK_BUSY 1
+#define PP_PROC_ADD_FULL 2
+
+/* kernel selection for pp_gf64_compute_recovery (the reference's entry points
+ * ComputeRecoveryBlocks / …Barycentric / …Fenger / …Full, src/par3_engine.h:23-243,
+ * all compute the same Cauchy product bit-for-bit) */
+#define PP_GF64_KERNEL_AUTO 0
+#define PP_GF64_KERNEL_MATVEC 1
+#define PP_GF64_KERNEL_BARYCENTRIC 2
+#define PP_GF64_KERNEL_FENGER 3
+
+typedef struct pp_ctx pp_ctx;
+typedef struct pp_par2_proc pp_par2_proc;
+
+/* ----------------------------------------------------------------- context */
+PP_API const char* pp_version(void);
+PP_API const char* pp_status_string(int status);
+/* Create a context on CUDA device `device` with its own stream. */
+PP_API int pp_ctx_create(int device, pp_ctx** out);
+PP_API void pp_ctx_destroy(pp_ctx* ctx);
+/* Use an external cudaStream_t (NULL restores the context's own stream). */
+PP_API int pp_ctx_set_stream(pp_ctx* ctx, void* cuda_stream);
+PP_API void* pp_ctx_get_stream(pp_ctx* ctx);
+PP_API int pp_ctx_synchronize(pp_ctx* ctx);
+PP_API const char* pp_ctx_last_error(pp_ctx* ctx);
+/* Number of kernels (and device memsets) this library has launched so far. */
+PP_API uint64_t pp_launch_count(void);
+/* Drop cached device buffers (scratch, coefficient matrices). */
+PP_API int pp_ctx_free_cache(pp_ctx* ctx);
+
+/* ============================================================ PAR2 / GF16 */
+
+/* Coefficient of input slice `input_block` for recovery exponent `exp`,
+ * 2^(L_i * exp mod 65535) with L_i the i-th log coprime to 65535
+ * (replaces gfmat_coeff, gf16/gfmat_coeff.c:99-101; host scalar helper). */
+PP_API uint16_t pp_par2_coeff(uint16_t input_block, uint16_t exp);
+PP_API uint16_t pp_par2_input_log(uint16_t input_block);
+
+/* coeffs[o * num_inputs + i] = coeff(input_idx[i], exps[o]), computed on the
+ * device (replaces the per-input set_coeffs loop, gf16/controller_cpu.cpp:372-378). */
+PP_API int pp_par2_coeff_matrix(pp_ctx* ctx, const uint16_t* input_idx, unsigned num_inputs,
+                                const uint16_t* exps, unsigned num_outputs, uint16_t* coeffs);
+
+/* Region multiply-accumulate (the work of Galois16Mul::mul_add_multi_packpf
+ * driven by PAR2ProcCPU::run_kernel/compute_worker, gf16/controller_cpu.cpp:463-624,
+ * gf16/gf16mul.h:360-412):
+ *   outputs[o] (^)= XOR_i coeffs[o * coeff_stride + i] * inputs[i]
+ * over the first slice_bytes bytes of each row; rows are input_stride /
+ * output_stride bytes apart.  An odd final byte is a word with a zero high
+ * byte.  accumulate=0 overwrites the outputs. */
+PP_API int pp_gf16_muladd(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
+                          size_t slice_bytes, const uint16_t* coeffs, size_t coeff_stride,
+                          unsigned num_outputs, void* outputs, size_t output_stride, int accumulate);
+
+/* PAR2 create in one call: recovery[o] = XOR_i coeff(input_idx[i], exps[o]) * inputs[i]. */
+PP_API int pp_par2_create(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
+                          size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps,
+                          unsigned num_outputs, void* outputs, size_t output_stride);
+
+/* PAR2 repair-matrix inversion (replaces Galois16RecMatrix::Compute +
+ * GetFactor, gf16/gfmat_inv.cpp:560-690, gf16/gfmat_inv.h:40-45).
+ *   valid[num_inputs]      nonzero = input slice present
+ *   recovery[*num_recovery] recovery exponents available; sorted on return and
+ *                          truncated to the rows used (a row whose pivot is
+ *                          zero is dropped and the inversion retried, as the
+ *                          reference does for the PAR2 flaw)
+ *   factors                num_missing x num_inputs, row k = missing slice k:
+ *                          columns [0, valid_count) weight the valid slices in
+ *                          index order, columns [valid_count, num_inputs) the
+ *                          recovery slices in the order of recovery[].
+ * Returns PP_ERR_NOT_INVERTIBLE where the reference returns false. */
+PP_API int pp_par2_invert(pp_ctx* ctx, const uint8_t* valid, unsigned num_inputs, uint16_t* recovery,
+                          unsigned* num_recovery, uint16_t* factors);
+
+/* ---- PAR2 processor: IPAR2ProcBackend for a CUDA device -----------------
+ * Mirrors gf16/controller.h:77-217 (and PAR2ProcCPU's behaviour,
+ * gf16/controller_cpu.cpp): staging areas of `input_batch` slices, inputs
+ * added one at a time (canAdd back-pressure), the kernel runs per full
+ * staging area, outputs read back per recovery slice. */
+PP_API int pp_par2_proc_create(pp_ctx* ctx, size_t slice_size, unsigned staging_areas, unsigned input_batch,
+                               pp_par2_proc** out);
+PP_API void pp_par2_proc_destroy(pp_par2_proc* proc);
+/* setCurrentSliceSize (may shrink; growing reallocates) */
+PP_API int pp_par2_proc_set_current_slice_size(pp_par2_proc* proc, size_t size);
+/* setRecoverySlices(n, exps); exps NULL -> every exponent 1 (custom-coefficient use) */
+PP_API int pp_par2_proc_set_recovery_slices(pp_par2_proc* proc, unsigned num, const uint16_t* exps);
+/* canAdd -> PP_PROC_ADD_OK / _OK_BUSY / _FULL */
+PP_API int pp_par2_proc_can_add(pp_par2_proc* proc);
+/* Block until an add is possible (waitForAdd). */
+PP_API int pp_par2_proc_wait_for_add(pp_par2_proc* proc);
+/* addInput(buffer, size, inputNum, flush): the buffer may be reused on return. */
+PP_API int pp_par2_proc_add_input(pp_par2_proc* proc, const void* buffer, size_t size, uint16_t input_num,
+                                  int flush);
+/* addInput(buffer, size, coeffs[num_recovery], flush) — decode overload. */
+PP_API int pp_par2_proc_add_input_coeffs(pp_par2_proc* proc, const void* buffer, size_t size,
+                                         const uint16_t* coeffs, int flush);
+PP_API int pp_par2_proc_flush(pp_par2_proc* proc);
+/* endInput: flush and wait for all processing. */
+PP_API int pp_par2_proc_end_input(pp_par2_proc* proc);
+/* getOutput(index, output) -> *valid (1 = output passed the integrity check). */
+PP_API int pp_par2_proc_get_output(pp_par2_proc* proc, unsigned index, void* output, int* valid);
+PP_API int pp_par2_proc_discard_output(pp_par2_proc* proc);
+PP_API int pp_par2_proc_free_processing_mem(pp_par2_proc* proc);
+PP_API unsigned pp_par2_proc_input_batch_size(pp_par2_proc* proc);
+PP_API unsigned pp_par2_proc_batches_started(pp_par2_proc* proc);
+
+/* ============================================================ PAR3 / GF64 */
+
+/* Cauchy matrix M[r][c] = inv((first_input + c) XOR (first_recovery + r)),
+ * zero denominators mapped to 1, row-major num_recovery x num_inputs
+ * (replaces GF64Controller::BuildCauchyMatrix, src/par3_engine.cc:358-425). */
+PP_API int pp_gf64_build_cauchy(pp_ctx* ctx, uint64_t* coeff, size_t num_inputs, size_t num_recovery,
+                                uint64_t first_input, uint64_t first_recovery);
+
+/* Recovery blocks from the Cauchy product (replaces
+ * GF64Controller::ComputeRecoveryBlocks / …Full / …Barycentric / …Fenger,
+ * src/par3_engine.h:23-243; N-API compute_recovery*, src/gf64_addon.cc:1266-1434).
+ *   recovery[r][w] (^)= XOR_c inputs[c][w] * M[r][c]
+ * inputs: num_inputs blocks of block_size64 words; recovery: num_recovery
+ * blocks.  accumulate=0 overwrites.  Empty problems return PP_OK untouched. */
+PP_API int pp_gf64_compute_recovery(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs, uint64_t* recovery,
+                                    size_t num_recovery, size_t block_size64, uint64_t first_input,
+                                    uint64_t first_recovery, int accumulate, int kernel);
+
+/* Same with a caller-supplied coefficient matrix (num_recovery x num_inputs)
+ * (replaces ComputeRecoveryBlocksWithCoeff, src/par3_engine.h:61-68). */
+PP_API int pp_gf64_compute_recovery_with_coeff(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs,
+                                               uint64_t* recovery, size_t num_recovery, size_t block_size64,
+                                               const uint64_t* coeff, int accumulate);
+
+/* Gauss-Jordan solve of A (n x n, modified) with the same row operations on
+ * rhs (n blocks of block_size64 words, becomes the solution)
+ * (replaces GF64Controller::SolveAndReconstruct, src/par3_engine.cc:980-1053).
+ * Returns PP_ERR_SINGULAR where the reference returns -1; on that error the
+ * contents of A and rhs are unspecified. */
+PP_API int pp_gf64_solve_and_reconstruct(pp_ctx* ctx, uint64_t* A, uint64_t* rhs, size_t n, size_t block_size64);
+
+/* Region primitives (replace the gf64_region_* dispatch pointers,
+ * gf64/gf64_global.h:23-37; semantics gf64/gf64_region_scalar.c:8-91). */
+PP_API int pp_gf64_region_mul(pp_ctx* ctx, uint64_t* out, const uint64_t* in, size_t len, uint64_t constant);
+/* out[i] = in[i] * coeff[i % n_coeff] */
+PP_API int pp_gf64_region_mul_arr(pp_ctx* ctx, uint64_t* out, const uint64_t* in, const uint64_t* coeff, size_t len,
+                                  size_t n_coeff);
+/* out[i] ^= XOR_c in[i] * coeff[c] */
+PP_API int pp_gf64_region_muladd_arr(pp_ctx* ctx, uint64_t* out, const uint64_t* in, const uint64_t* coeff,
+                                     size_t len, size_t n_coeff);
+/* out[w] ^= XOR_g in_blocks[g][w] * coeff_blocks[g] */
+PP_API int pp_gf64_region_coupled_muladd_arr(pp_ctx* ctx, uint64_t* out, const uint64_t* const* in_blocks,
+                                             const uint64_t* coeff_blocks, size_t len, size_t G);
+/* outs[k][w] ^= in[w] * coeff_block_starts[k][0] */
+PP_API int pp_gf64_region_fused_output_muladd_arr(pp_ctx* ctx, uint64_t* const* outs, const uint64_t* in,
+                                                  const uint64_t* const* coeff_block_starts, size_t len, size_t K);
+/* outs[k][w] ^= XOR_g in_blocks[g][w] * coeff_block_2d[k * K_stride + g] */
+PP_API int pp_gf64_region_2d_muladd_arr(pp_ctx* ctx, uint64_t* const* outs, size_t K, const uint64_t* const* in_blocks,
+                                        size_t G, const uint64_t* coeff_block_2d, size_t K_stride, size_t len);
+/* out[i] = inverse(in[i]), inverse(0) = 0 (replaces gf64_inverse_batch,
+ * gf64/gf64_invert.c:71-75). */
+PP_API int pp_gf64_inverse_batch(pp_ctx* ctx, uint64_t* out, const uint64_t* in, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARPAR_B200_H */

@@ -1,0 +1,305 @@
+/* Test infrastructure only: the oracle (see gf_oracle.h).
+ *
+ * Plain C, written from the field definitions and the reference's documented
+ * semantics; no SIMD, no reference code.  Never linked into the product.
+ */
+#include "gf_oracle.h"
+#include <stdlib.h>
+#include <string.h>
+
+/* ======================================================================= */
+/* GF(2^16)                                                                 */
+/* ======================================================================= */
+/* Field: GF(2)[x]/(x^16+x^12+x^3+x+1), the PAR2 field (gf16/gfmat_coeff.c:28,
+ * polynomial 0x1100B), generator 2 (= x).  Log/antilog tables are built by
+ * repeated doubling, as the PAR2 specification defines the field. */
+static uint16_t g16_exp[65535 * 2];
+static uint16_t g16_log[65536];
+static int g16_ready = 0;
+
+static void g16_init(void) {
+	if (g16_ready) return;
+	uint32_t n = 1;
+	for (uint32_t e = 0; e < 65535; e++) {
+		g16_exp[e] = (uint16_t)n;
+		g16_exp[e + 65535] = (uint16_t)n;
+		g16_log[n] = (uint16_t)e;
+		n <<= 1;
+		if (n & 0x10000) n ^= 0x1100B;
+	}
+	g16_log[0] = 0;
+	g16_ready = 1;
+}
+
+uint16_t or_gf16_mul(uint16_t a, uint16_t b) {
+	g16_init();
+	if (!a || !b) return 0;
+	return g16_exp[(uint32_t)g16_log[a] + g16_log[b]];
+}
+
+uint16_t or_gf16_exp(uint32_t e) {
+	g16_init();
+	return g16_exp[e % 65535];
+}
+
+uint16_t or_gf16_inv(uint16_t a) {
+	g16_init();
+	if (!a) return 0;
+	return g16_exp[(65535 - g16_log[a]) % 65535];
+}
+
+/* PAR2 input constant log: the (i+1)-th positive integer coprime to 65535
+ * (= 3*5*17*257).  Restates gfmat_init's table walk (gf16/gfmat_coeff.c:21-32)
+ * and gfmat_input_log (gf16/gfmat_coeff.c:80-82). */
+static uint16_t g16_ilog[32768];
+static int g16_ilog_ready = 0;
+uint16_t or_par2_input_log(uint16_t inputBlock) {
+	if (!g16_ilog_ready) {
+		uint32_t e = 0;
+		for (uint32_t i = 0; i < 32768; i++) {
+			do { e++; } while (!(e % 3) || !(e % 5) || !(e % 17) || !(e % 257));
+			g16_ilog[i] = (uint16_t)e;
+		}
+		g16_ilog_ready = 1;
+	}
+	return g16_ilog[inputBlock & 32767];
+}
+
+/* coeff(i, e) = 2^(L_i * e mod 65535) (gf16/gfmat_coeff.c:84-101). */
+uint16_t or_par2_coeff(uint16_t inputBlock, uint16_t recoveryExp) {
+	uint32_t l = or_par2_input_log(inputBlock);
+	return or_gf16_exp((uint32_t)(((uint64_t)l * recoveryExp) % 65535));
+}
+
+/* Region multiply-accumulate of the PAR2 controller, as its tests define the
+ * result (test/gf16/test-ctrl.cpp:185-199): words are little-endian u16; a
+ * source shorter than the slice contributes zeros past its end; an odd final
+ * byte is a word whose high byte is zero. */
+void or_par2_muladd(const uint8_t* const* src, const size_t* sizes, unsigned numInputs,
+                    size_t sliceSize, const uint16_t* coeffs, unsigned numOutputs,
+                    uint8_t* dst) {
+	g16_init();
+	size_t words = (sliceSize + 1) / 2;
+	uint16_t* acc = (uint16_t*)calloc(words ? words : 1, sizeof(uint16_t));
+	uint16_t* x = (uint16_t*)calloc(words ? words : 1, sizeof(uint16_t));
+	for (unsigned o = 0; o < numOutputs; o++) {
+		memset(acc, 0, words * sizeof(uint16_t));
+		for (unsigned i = 0; i < numInputs; i++) {
+			uint16_t c = coeffs[(size_t)o * numInputs + i];
+			if (!c) continue;
+			size_t sz = sizes[i] < sliceSize ? sizes[i] : sliceSize;
+			size_t nw = (sz + 1) / 2;
+			for (size_t w = 0; w < nw; w++) {
+				uint16_t lo = src[i][2 * w];
+				uint16_t hi = (2 * w + 1 < sz) ? src[i][2 * w + 1] : 0;
+				x[w] = (uint16_t)(lo | (hi << 8));
+			}
+			if (c == 1) {
+				for (size_t w = 0; w < nw; w++) acc[w] ^= x[w];
+			} else {
+				uint32_t lc = g16_log[c];
+				for (size_t w = 0; w < nw; w++)
+					if (x[w]) acc[w] ^= g16_exp[lc + g16_log[x[w]]];
+			}
+		}
+		uint8_t* d = dst + (size_t)o * sliceSize;
+		for (size_t b = 0; b < sliceSize; b++)
+			d[b] = (uint8_t)(b & 1 ? acc[b / 2] >> 8 : acc[b / 2] & 0xff);
+	}
+	free(acc);
+	free(x);
+}
+
+static int cmp_u16(const void* a, const void* b) {
+	return (int)*(const uint16_t*)a - (int)*(const uint16_t*)b;
+}
+
+/* PAR2 repair matrix inversion, restating Galois16RecMatrix::Compute
+ * (gf16/gfmat_inv.cpp:560-690) and Construct (:462-558):
+ *   - recovery exponents are sorted; the first m = #missing are the rows;
+ *   - columns: valid inputs in index order, then missing inputs in index order;
+ *   - Gauss-Jordan WITHOUT pivoting, row k pivots on column (validCount + k);
+ *     the eliminated column is replaced in place by the identity column, so the
+ *     result row k is GetFactor(col, k) (gf16/gfmat_inv.h:40-45);
+ *   - a zero pivot drops that recovery row and restarts (:631-668, "PAR2 flaw");
+ *     too few rows left -> not invertible. */
+int or_par2_invert(const uint8_t* valid, unsigned numInputs, uint16_t* recovery,
+                   unsigned* numRec, uint16_t* factors) {
+	g16_init();
+	unsigned validCount = 0;
+	for (unsigned i = 0; i < numInputs; i++) validCount += valid[i] ? 1 : 0;
+	unsigned m = numInputs - validCount;
+	unsigned nrec = *numRec;
+	if (m == 0 || m > nrec) return 0;
+	uint16_t* rec = (uint16_t*)malloc(nrec * sizeof(uint16_t));
+	memcpy(rec, recovery, nrec * sizeof(uint16_t));
+	qsort(rec, nrec, sizeof(uint16_t), cmp_u16);
+	unsigned* colOf = (unsigned*)malloc(numInputs * sizeof(unsigned));
+	unsigned vc = 0, mc = validCount;
+	for (unsigned i = 0; i < numInputs; i++) colOf[i] = valid[i] ? vc++ : mc++;
+	uint16_t* M = factors; /* m x numInputs, row-major */
+	int ok = 0;
+	for (;;) {
+		if (nrec < m) break;
+		for (unsigned r = 0; r < m; r++)
+			for (unsigned i = 0; i < numInputs; i++)
+				M[(size_t)r * numInputs + colOf[i]] = or_par2_coeff((uint16_t)i, rec[r]);
+		int bad = -1;
+		for (unsigned k = 0; k < m && bad < 0; k++) {
+			uint16_t* rowk = M + (size_t)k * numInputs;
+			uint16_t p = rowk[validCount + k];
+			rowk[validCount + k] = 1;
+			if (!p) { bad = (int)k; break; }
+			if (p != 1) {
+				uint16_t ip = or_gf16_inv(p);
+				for (unsigned c = 0; c < numInputs; c++) rowk[c] = or_gf16_mul(rowk[c], ip);
+			}
+			for (unsigned r = 0; r < m; r++) {
+				if (r == k) continue;
+				uint16_t* rowr = M + (size_t)r * numInputs;
+				uint16_t f = rowr[validCount + k];
+				rowr[validCount + k] = 0;
+				if (!f) continue;
+				for (unsigned c = 0; c < numInputs; c++) rowr[c] ^= or_gf16_mul(f, rowk[c]);
+			}
+		}
+		if (bad < 0) { ok = 1; break; }
+		memmove(rec + bad, rec + bad + 1, (nrec - bad - 1) * sizeof(uint16_t));
+		nrec--;
+	}
+	if (ok) {
+		memcpy(recovery, rec, m * sizeof(uint16_t));
+		*numRec = m;
+	}
+	free(rec);
+	free(colOf);
+	return ok;
+}
+
+/* ======================================================================= */
+/* GF(2^64)                                                                 */
+/* ======================================================================= */
+/* Field: GF(2)[x]/(x^64+x^4+x^3+x+1) (gf64/gf64_global.h:8), multiplication
+ * as gf64_mul_reference defines it (gf64/gf64_single.c:6-53): the 128-bit
+ * carry-less product reduced modulo the polynomial.  Written here as a plain
+ * shift-and-add carry-less multiply followed by a two-step fold. */
+uint64_t or_gf64_mul(uint64_t a, uint64_t b) {
+	uint64_t lo = 0, hi = 0;
+	for (int i = 0; i < 64; i++) {
+		if ((b >> i) & 1) {
+			lo ^= a << i;
+			if (i) hi ^= a >> (64 - i);
+		}
+	}
+	/* x^64 == x^4+x^3+x+1 (0x1B): fold hi twice. */
+	uint64_t t = hi ^ (hi >> 60) ^ (hi >> 61) ^ (hi >> 63);
+	return lo ^ t ^ (t << 1) ^ (t << 3) ^ (t << 4);
+}
+
+/* Multiplicative inverse, inverse(0) = 0 (gf64/gf64_invert.c:29-67 computes
+ * it by the extended Euclidean algorithm; the inverse is unique, so it is
+ * restated here as a^(2^64-2) by square-and-multiply). */
+uint64_t or_gf64_inv(uint64_t a) {
+	if (a == 0) return 0;
+	uint64_t r = 1, s = a;
+	/* exponent 2^64 - 2 = 0xFFFF...FE: bits 1..63 set */
+	for (int i = 1; i < 64; i++) {
+		s = or_gf64_mul(s, s);
+		r = or_gf64_mul(r, s);
+	}
+	return r;
+}
+
+/* Cauchy matrix (src/par3_engine.cc:358-425):
+ * M[r][c] = inv((firstInput + c) XOR (firstRecovery + r)), with a zero
+ * denominator replaced by 1; row-major numRecovery x numInputs. */
+void or_gf64_build_cauchy(uint64_t* m, size_t numInputs, size_t numRecovery,
+                          uint64_t firstInput, uint64_t firstRecovery) {
+	for (size_t r = 0; r < numRecovery; r++) {
+		uint64_t y = firstRecovery + r;
+		for (size_t c = 0; c < numInputs; c++) {
+			uint64_t d = (firstInput + c) ^ y;
+			m[r * numInputs + c] = or_gf64_inv(d ? d : 1);
+		}
+	}
+}
+
+/* out[r][w] (^)= XOR_c coeff[r][c] * in[c][w]
+ * (ComputeRecoveryBlocksWithCoeff, src/par3_engine.cc:1165-1387; zero-init
+ * unless accumulate). */
+void or_gf64_matvec(const uint64_t* in, size_t numInputs, uint64_t* out, size_t numRecovery,
+                    size_t blockSize64, const uint64_t* coeff, int accumulate) {
+	for (size_t r = 0; r < numRecovery; r++) {
+		uint64_t* o = out + r * blockSize64;
+		if (!accumulate) memset(o, 0, blockSize64 * sizeof(uint64_t));
+		for (size_t c = 0; c < numInputs; c++) {
+			uint64_t k = coeff[r * numInputs + c];
+			const uint64_t* x = in + c * blockSize64;
+			for (size_t w = 0; w < blockSize64; w++) o[w] ^= or_gf64_mul(x[w], k);
+		}
+	}
+}
+
+/* ComputeRecoveryBlocks (src/par3_engine.cc:1061-1114): Cauchy build + matvec.
+ * Empty problems return without touching the output. */
+void or_gf64_compute_recovery(const uint64_t* in, size_t numInputs, uint64_t* out,
+                              size_t numRecovery, size_t blockSize64, uint64_t firstInput,
+                              uint64_t firstRecovery, int accumulate) {
+	if (!numInputs || !numRecovery) return;
+	uint64_t* m = (uint64_t*)malloc(numInputs * numRecovery * sizeof(uint64_t));
+	or_gf64_build_cauchy(m, numInputs, numRecovery, firstInput, firstRecovery);
+	or_gf64_matvec(in, numInputs, out, numRecovery, blockSize64, m, accumulate);
+	free(m);
+}
+
+/* SolveAndReconstruct (src/par3_engine.cc:980-1053): in-place Gauss-Jordan
+ * on A (n x n) with the same row operations applied to the RHS blocks;
+ * pivot = first nonzero at or below the diagonal; returns -1 if singular. */
+int or_gf64_solve_and_reconstruct(uint64_t* A, uint64_t* rhs, size_t n, size_t B) {
+	for (size_t col = 0; col < n; col++) {
+		size_t piv = col;
+		while (piv < n && A[piv * n + col] == 0) piv++;
+		if (piv == n) return -1;
+		if (piv != col) {
+			for (size_t j = 0; j < n; j++) {
+				uint64_t t = A[col * n + j]; A[col * n + j] = A[piv * n + j]; A[piv * n + j] = t;
+			}
+			for (size_t w = 0; w < B; w++) {
+				uint64_t t = rhs[col * B + w]; rhs[col * B + w] = rhs[piv * B + w]; rhs[piv * B + w] = t;
+			}
+		}
+		uint64_t pv = A[col * n + col];
+		if (pv != 1) {
+			uint64_t pi = or_gf64_inv(pv);
+			for (size_t j = 0; j < n; j++) A[col * n + j] = or_gf64_mul(A[col * n + j], pi);
+			for (size_t w = 0; w < B; w++) rhs[col * B + w] = or_gf64_mul(rhs[col * B + w], pi);
+		}
+		for (size_t row = 0; row < n; row++) {
+			if (row == col) continue;
+			uint64_t f = A[row * n + col];
+			if (!f) continue;
+			for (size_t j = 0; j < n; j++) A[row * n + j] ^= or_gf64_mul(f, A[col * n + j]);
+			for (size_t w = 0; w < B; w++) rhs[row * B + w] ^= or_gf64_mul(rhs[col * B + w], f);
+		}
+	}
+	return 0;
+}
+
+/* Region primitives (gf64/gf64_region_scalar.c:8-28). */
+void or_gf64_region_mul(uint64_t* out, const uint64_t* in, size_t len, uint64_t c) {
+	for (size_t i = 0; i < len; i++) out[i] = or_gf64_mul(in[i], c);
+}
+/* mul_arr cycles the coefficients: out[i] = in[i] * coeff[i % nCoeff]. */
+void or_gf64_region_mul_arr(uint64_t* out, const uint64_t* in, const uint64_t* coeff,
+                            size_t len, size_t nCoeff) {
+	for (size_t i = 0; i < len; i++) out[i] = or_gf64_mul(in[i], coeff[i % nCoeff]);
+}
+/* muladd_arr XORs the products of ALL coefficients into every word. */
+void or_gf64_region_muladd_arr(uint64_t* out, const uint64_t* in, const uint64_t* coeff,
+                               size_t len, size_t nCoeff) {
+	for (size_t i = 0; i < len; i++) {
+		uint64_t s = 0;
+		for (size_t c = 0; c < nCoeff; c++) s ^= or_gf64_mul(in[i], coeff[c]);
+		out[i] ^= s;
+	}
+}

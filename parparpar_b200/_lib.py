@@ -1,0 +1,195 @@
+"""ctypes binding of libparpar_b200.so (the C ABI declared in include/parpar_b200.h).
+
+The library is the product: there is no Python or CPU implementation behind
+these calls.  If the shared library is missing or cannot be loaded, importing
+this module raises; if no CUDA device is present, creating a context raises
+``PPError(PP_ERR_NO_DEVICE)``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libparpar_b200.so")
+
+PP_OK = 0
+PP_ERR_INVALID_ARG = -1
+PP_ERR_CUDA = -2
+PP_ERR_NO_MEMORY = -3
+PP_ERR_SINGULAR = -4
+PP_ERR_NOT_INVERTIBLE = -5
+PP_ERR_BUSY = -6
+PP_ERR_NO_DEVICE = -7
+PP_ERR_UNSUPPORTED = -8
+
+PP_PROC_ADD_OK = 0
+PP_PROC_ADD_OK_BUSY = 1
+PP_PROC_ADD_FULL = 2
+
+PP_GF64_KERNEL_AUTO = 0
+PP_GF64_KERNEL_MATVEC = 1
+PP_GF64_KERNEL_BARYCENTRIC = 2
+PP_GF64_KERNEL_FENGER = 3
+
+# every symbol declared in include/parpar_b200.h
+EXPORTS = [
+    "pp_version", "pp_status_string", "pp_ctx_create", "pp_ctx_destroy", "pp_ctx_set_stream",
+    "pp_ctx_get_stream", "pp_ctx_synchronize", "pp_ctx_last_error", "pp_launch_count", "pp_ctx_free_cache",
+    "pp_par2_coeff", "pp_par2_input_log", "pp_par2_coeff_matrix", "pp_gf16_muladd", "pp_par2_create",
+    "pp_par2_invert", "pp_par2_proc_create", "pp_par2_proc_destroy", "pp_par2_proc_set_current_slice_size",
+    "pp_par2_proc_set_recovery_slices", "pp_par2_proc_can_add", "pp_par2_proc_wait_for_add",
+    "pp_par2_proc_add_input", "pp_par2_proc_add_input_coeffs", "pp_par2_proc_flush", "pp_par2_proc_end_input",
+    "pp_par2_proc_get_output", "pp_par2_proc_discard_output", "pp_par2_proc_free_processing_mem",
+    "pp_par2_proc_input_batch_size", "pp_par2_proc_batches_started", "pp_gf64_build_cauchy",
+    "pp_gf64_compute_recovery", "pp_gf64_compute_recovery_with_coeff", "pp_gf64_solve_and_reconstruct",
+    "pp_gf64_region_mul", "pp_gf64_region_mul_arr", "pp_gf64_region_muladd_arr",
+    "pp_gf64_region_coupled_muladd_arr", "pp_gf64_region_fused_output_muladd_arr",
+    "pp_gf64_region_2d_muladd_arr", "pp_gf64_inverse_batch",
+]
+
+
+class PPError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        super().__init__(f"parpar_b200 error {status}: {msg}")
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m parparpar_b200.build` "
+            "(the CUDA engine has no CPU fallback)")
+    return ctypes.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+_P = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+_U = ctypes.c_uint
+_I = ctypes.c_int
+_U16 = ctypes.c_uint16
+_U64 = ctypes.c_uint64
+
+
+def _sig(name, res, *args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+
+
+_sig("pp_version", ctypes.c_char_p)
+_sig("pp_status_string", ctypes.c_char_p, _I)
+_sig("pp_ctx_create", _I, _I, ctypes.POINTER(_P))
+_sig("pp_ctx_destroy", None, _P)
+_sig("pp_ctx_set_stream", _I, _P, _P)
+_sig("pp_ctx_get_stream", _P, _P)
+_sig("pp_ctx_synchronize", _I, _P)
+_sig("pp_ctx_last_error", ctypes.c_char_p, _P)
+_sig("pp_launch_count", _U64)
+_sig("pp_ctx_free_cache", _I, _P)
+_sig("pp_par2_coeff", _U16, _U16, _U16)
+_sig("pp_par2_input_log", _U16, _U16)
+_sig("pp_par2_coeff_matrix", _I, _P, _P, _U, _P, _U, _P)
+_sig("pp_gf16_muladd", _I, _P, _P, _SZ, _U, _SZ, _P, _SZ, _U, _P, _SZ, _I)
+_sig("pp_par2_create", _I, _P, _P, _SZ, _U, _SZ, _P, _P, _U, _P, _SZ)
+_sig("pp_par2_invert", _I, _P, _P, _U, _P, ctypes.POINTER(_U), _P)
+_sig("pp_par2_proc_create", _I, _P, _SZ, _U, _U, ctypes.POINTER(_P))
+_sig("pp_par2_proc_destroy", None, _P)
+_sig("pp_par2_proc_set_current_slice_size", _I, _P, _SZ)
+_sig("pp_par2_proc_set_recovery_slices", _I, _P, _U, _P)
+_sig("pp_par2_proc_can_add", _I, _P)
+_sig("pp_par2_proc_wait_for_add", _I, _P)
+_sig("pp_par2_proc_add_input", _I, _P, _P, _SZ, _U16, _I)
+_sig("pp_par2_proc_add_input_coeffs", _I, _P, _P, _SZ, _P, _I)
+_sig("pp_par2_proc_flush", _I, _P)
+_sig("pp_par2_proc_end_input", _I, _P)
+_sig("pp_par2_proc_get_output", _I, _P, _U, _P, ctypes.POINTER(_I))
+_sig("pp_par2_proc_discard_output", _I, _P)
+_sig("pp_par2_proc_free_processing_mem", _I, _P)
+_sig("pp_par2_proc_input_batch_size", _U, _P)
+_sig("pp_par2_proc_batches_started", _U, _P)
+_sig("pp_gf64_build_cauchy", _I, _P, _P, _SZ, _SZ, _U64, _U64)
+_sig("pp_gf64_compute_recovery", _I, _P, _P, _SZ, _P, _SZ, _SZ, _U64, _U64, _I, _I)
+_sig("pp_gf64_compute_recovery_with_coeff", _I, _P, _P, _SZ, _P, _SZ, _SZ, _P, _I)
+_sig("pp_gf64_solve_and_reconstruct", _I, _P, _P, _P, _SZ, _SZ)
+_sig("pp_gf64_region_mul", _I, _P, _P, _P, _SZ, _U64)
+_sig("pp_gf64_region_mul_arr", _I, _P, _P, _P, _P, _SZ, _SZ)
+_sig("pp_gf64_region_muladd_arr", _I, _P, _P, _P, _P, _SZ, _SZ)
+_sig("pp_gf64_region_coupled_muladd_arr", _I, _P, _P, _P, _P, _SZ, _SZ)
+_sig("pp_gf64_region_fused_output_muladd_arr", _I, _P, _P, _P, _P, _SZ, _SZ)
+_sig("pp_gf64_region_2d_muladd_arr", _I, _P, _P, _SZ, _P, _SZ, _P, _SZ, _SZ)
+_sig("pp_gf64_inverse_batch", _I, _P, _P, _P, _SZ)
+
+
+def status_string(s: int) -> str:
+    return lib.pp_status_string(s).decode()
+
+
+class Context:
+    """One device + stream.  ``check`` turns statuses into ``PPError``."""
+
+    def __init__(self, device: int = 0):
+        h = _P()
+        st = lib.pp_ctx_create(device, ctypes.byref(h))
+        if st != PP_OK:
+            raise PPError(st, status_string(st))
+        self.h = h
+        self.device = device
+
+    def check(self, st: int) -> int:
+        if st != PP_OK:
+            raise PPError(st, f"{status_string(st)}: {lib.pp_ctx_last_error(self.h).decode()}")
+        return st
+
+    def synchronize(self):
+        self.check(lib.pp_ctx_synchronize(self.h))
+
+    def set_stream(self, stream_ptr: int | None):
+        self.check(lib.pp_ctx_set_stream(self.h, _P(stream_ptr or 0)))
+
+    def free_cache(self):
+        self.check(lib.pp_ctx_free_cache(self.h))
+
+    def close(self):
+        if self.h:
+            lib.pp_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_ctx_lock = threading.Lock()
+_ctxs: dict[int, Context] = {}
+
+
+def default_context(device: int = 0) -> Context:
+    with _ctx_lock:
+        c = _ctxs.get(device)
+        if c is None:
+            c = Context(device)
+            _ctxs[device] = c
+        return c
+
+
+def launch_count() -> int:
+    return int(lib.pp_launch_count())
+
+
+def ptr(buf) -> int:
+    """Address of a numpy array or torch tensor (host or device)."""
+    if buf is None:
+        return 0
+    if hasattr(buf, "data_ptr"):
+        return int(buf.data_ptr())
+    if hasattr(buf, "ctypes"):
+        return int(buf.ctypes.data)
+    if isinstance(buf, int):
+        return buf
+    raise TypeError(f"unsupported buffer type {type(buf)}")

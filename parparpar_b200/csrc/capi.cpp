@@ -1,0 +1,1047 @@
+// C ABI implementation (include/parpar_b200.h): contexts, host/device buffer
+// staging, the PAR2 processor and the PAR3 engine entry points.  All GF
+// arithmetic on data runs in the CUDA kernels (gf16_kernels.cu,
+// gf64_kernels.cu); the host side does argument checking, layout, and the
+// scalar bookkeeping the reference also does on its host threads
+// (coefficient columns, permutations, retry of a dropped recovery row).
+#include "../../include/parpar_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <list>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pp_internal.h"
+
+namespace pp {
+static std::atomic<uint64_t> g_launches{0};
+void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+uint64_t launches() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace pp
+
+using namespace pp;
+
+// ------------------------------------------------------------- host GF(2^16)
+// Log/antilog tables of the PAR2 field with generator 2, and the table of
+// input-constant logs (the i-th positive integer coprime to 65535).  These
+// serve the scalar host bookkeeping only (coefficient columns of the
+// processor, the permutation of the repair matrix); region data never goes
+// through them.
+namespace {
+struct Gf16Host {
+  uint16_t exp[65535 * 2];
+  uint16_t log[65536];
+  uint16_t ilog[32768];
+  Gf16Host() {
+    uint32_t n = 1;
+    for (uint32_t e = 0; e < 65535; e++) {
+      exp[e] = exp[e + 65535] = (uint16_t)n;
+      log[n] = (uint16_t)e;
+      n <<= 1;
+      if (n & 0x10000) n ^= 0x1100B;
+    }
+    log[0] = 0;
+    uint32_t e = 0;
+    for (uint32_t i = 0; i < 32768; i++) {
+      do {
+        e++;
+      } while (!(e % 3) || !(e % 5) || !(e % 17) || !(e % 257));
+      ilog[i] = (uint16_t)e;
+    }
+  }
+  uint16_t coeff(uint16_t idx, uint16_t ex) const {
+    uint32_t l = ilog[idx & 32767];
+    return exp[(uint32_t)(((uint64_t)l * ex) % 65535)];
+  }
+};
+const Gf16Host& gf16h() {
+  static Gf16Host* t = new Gf16Host();
+  return *t;
+}
+}  // namespace
+
+// -------------------------------------------------------------------- ctx
+enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_NSLOTS };
+
+struct CauchyEntry {
+  size_t n_in, n_rec;
+  uint64_t fI, fR;
+  uint64_t* d;
+};
+
+struct pp_ctx {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  void* slot_p[S_NSLOTS] = {};
+  size_t slot_n[S_NSLOTS] = {};
+  std::list<CauchyEntry> cauchy;  // LRU, front = most recent
+  std::mutex mu;
+};
+
+static int set_err(pp_ctx* ctx, int code, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                                          \
+  do {                                                                                               \
+    cudaError_t _e = (expr);                                                                         \
+    if (_e != cudaSuccess) {                                                                         \
+      return set_err(ctx, PP_ERR_CUDA, "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, \
+                     __LINE__);                                                                      \
+    }                                                                                                \
+  } while (0)
+
+static int bind(pp_ctx* ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return set_err(ctx, PP_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return PP_OK;
+}
+
+static void* scratch(pp_ctx* ctx, Slot s, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (ctx->slot_n[s] >= bytes) return ctx->slot_p[s];
+  if (ctx->slot_p[s]) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->slot_p[s]);
+    ctx->slot_p[s] = nullptr;
+    ctx->slot_n[s] = 0;
+  }
+  size_t n = bytes + bytes / 8;  // some headroom against regrowth
+  n = (n + 255) & ~(size_t)255;
+  void* p = nullptr;
+  if (cudaMalloc(&p, n) != cudaSuccess) {
+    cudaGetLastError();
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    n = bytes;
+  }
+  ctx->slot_p[s] = p;
+  ctx->slot_n[s] = n;
+  return p;
+}
+
+static bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static inline size_t round16(size_t v) { return (v + 15) & ~(size_t)15; }
+static inline bool aligned16(const void* p, size_t stride) {
+  return ((uintptr_t)p % 16) == 0 && (stride % 16) == 0;
+}
+
+// Upload a small host array into a scratch slot (pageable source: safe to
+// reuse on return).  Device arrays are returned as is.
+template <class T>
+static const T* to_device(pp_ctx* ctx, Slot s, const T* p, size_t n, int* status) {
+  *status = PP_OK;
+  if (n == 0) return p;
+  if (is_device_ptr(p)) return p;
+  T* d = (T*)scratch(ctx, s, n * sizeof(T));
+  if (!d) {
+    *status = set_err(ctx, PP_ERR_NO_MEMORY, "device allocation of %zu bytes failed", n * sizeof(T));
+    return nullptr;
+  }
+  cudaError_t e = cudaMemcpyAsync(d, p, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) {
+    *status = set_err(ctx, PP_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+    return nullptr;
+  }
+  return d;
+}
+
+extern "C" {
+
+PP_API const char* pp_version(void) { return "parpar_b200 0.1 (sm_100a)"; }
+
+PP_API const char* pp_status_string(int s) {
+  switch (s) {
+    case PP_OK: return "ok";
+    case PP_ERR_INVALID_ARG: return "invalid argument";
+    case PP_ERR_CUDA: return "CUDA error";
+    case PP_ERR_NO_MEMORY: return "out of device memory";
+    case PP_ERR_SINGULAR: return "singular matrix";
+    case PP_ERR_NOT_INVERTIBLE: return "recovery matrix not invertible";
+    case PP_ERR_BUSY: return "staging area busy";
+    case PP_ERR_NO_DEVICE: return "no CUDA device";
+    case PP_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+PP_API uint64_t pp_launch_count(void) { return launches(); }
+
+PP_API int pp_ctx_create(int device, pp_ctx** out) {
+  if (!out) return PP_ERR_INVALID_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return PP_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) return PP_ERR_INVALID_ARG;
+  pp_ctx* ctx = new pp_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete ctx;
+    return PP_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return PP_ERR_CUDA;
+  }
+  ctx->stream = ctx->own;
+  *out = ctx;
+  return PP_OK;
+}
+
+PP_API int pp_ctx_free_cache(pp_ctx* ctx) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  bind(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  for (int s = 0; s < S_NSLOTS; s++) {
+    if (ctx->slot_p[s]) cudaFree(ctx->slot_p[s]);
+    ctx->slot_p[s] = nullptr;
+    ctx->slot_n[s] = 0;
+  }
+  for (auto& e : ctx->cauchy) cudaFree(e.d);
+  ctx->cauchy.clear();
+  return PP_OK;
+}
+
+PP_API void pp_ctx_destroy(pp_ctx* ctx) {
+  if (!ctx) return;
+  pp_ctx_free_cache(ctx);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+}
+
+PP_API int pp_ctx_set_stream(pp_ctx* ctx, void* s) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  ctx->stream = s ? (cudaStream_t)s : ctx->own;
+  return PP_OK;
+}
+PP_API void* pp_ctx_get_stream(pp_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+PP_API int pp_ctx_synchronize(pp_ctx* ctx) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  bind(ctx);
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+PP_API const char* pp_ctx_last_error(pp_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+// ============================================================ PAR2 / GF16
+PP_API uint16_t pp_par2_coeff(uint16_t input_block, uint16_t exp) { return gf16h().coeff(input_block, exp); }
+PP_API uint16_t pp_par2_input_log(uint16_t input_block) { return gf16h().ilog[input_block & 32767]; }
+
+static int par2_coeff_matrix_dev(pp_ctx* ctx, const uint16_t* input_idx, unsigned n_in, const uint16_t* exps,
+                                 unsigned n_out, uint16_t* d_coeffs) {
+  // per-input logs (host bookkeeping: a table lookup per input) -> device
+  std::vector<uint16_t> logs(n_in);
+  std::vector<uint16_t> hidx(n_in);
+  if (is_device_ptr(input_idx)) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(hidx.data(), input_idx, n_in * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  } else {
+    memcpy(hidx.data(), input_idx, n_in * 2);
+  }
+  for (unsigned i = 0; i < n_in; i++) {
+    if (hidx[i] >= 32768) return set_err(ctx, PP_ERR_INVALID_ARG, "input index %u >= 32768", hidx[i]);
+    logs[i] = gf16h().ilog[hidx[i]];
+  }
+  int st;
+  const uint16_t* d_logs = to_device(ctx, S_A, logs.data(), n_in, &st);
+  if (st) return st;
+  const uint16_t* d_exps = to_device(ctx, S_B, exps, n_out, &st);
+  if (st) return st;
+  CUDA_TRY(ctx, launch_gf16_coeff_matrix(d_logs, n_in, d_exps, n_out, d_coeffs, ctx->stream));
+  return PP_OK;
+}
+
+PP_API int pp_par2_coeff_matrix(pp_ctx* ctx, const uint16_t* input_idx, unsigned num_inputs, const uint16_t* exps,
+                                unsigned num_outputs, uint16_t* coeffs) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if ((num_inputs && !input_idx) || (num_outputs && !exps) || !coeffs) return PP_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  size_t n = (size_t)num_inputs * num_outputs;
+  if (!n) return PP_OK;
+  bool dev = is_device_ptr(coeffs);
+  uint16_t* d = dev ? coeffs : (uint16_t*)scratch(ctx, S_COEF, n * 2);
+  if (!d) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficient buffer");
+  if (int r = par2_coeff_matrix_dev(ctx, input_idx, num_inputs, exps, num_outputs, d)) return r;
+  if (!dev) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(coeffs, d, n * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return PP_OK;
+}
+
+// Region muladd with staging of host / unaligned buffers.
+static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, unsigned n_in, size_t slice,
+                            const uint16_t* d_coeffs, size_t ldc, unsigned n_out, void* outputs, size_t out_stride,
+                            bool accumulate) {
+  const bool in_dev = is_device_ptr(inputs);
+  const bool out_dev = is_device_ptr(outputs);
+  const size_t row = round16(slice);
+  const uint8_t* din = (const uint8_t*)inputs;
+  size_t dstride = in_stride;
+  if (n_in && (!in_dev || !aligned16(inputs, in_stride))) {
+    uint8_t* s = (uint8_t*)scratch(ctx, S_IN, row * n_in);
+    if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", row * n_in);
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(s, row, inputs, in_stride, slice, n_in,
+                                    in_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    din = s;
+    dstride = row;
+  }
+  uint8_t* dout = (uint8_t*)outputs;
+  size_t ostride = out_stride;
+  const bool stage_out = !out_dev || !aligned16(outputs, out_stride);
+  if (stage_out) {
+    dout = (uint8_t*)scratch(ctx, S_OUT, row * n_out);
+    if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "output staging (%zu bytes)", row * n_out);
+    ostride = row;
+    if (accumulate)
+      CUDA_TRY(ctx, cudaMemcpy2DAsync(dout, row, outputs, out_stride, slice, n_out,
+                                      out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CUDA_TRY(ctx, launch_gf16_muladd(din, dstride, n_in, slice, d_coeffs, ldc, n_out, dout, ostride, accumulate,
+                                   ctx->sms, ctx->stream));
+  if (stage_out) {
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,
+                                    out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (!in_dev || !out_dev) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+PP_API int pp_gf16_muladd(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
+                          size_t slice_bytes, const uint16_t* coeffs, size_t coeff_stride, unsigned num_outputs,
+                          void* outputs, size_t output_stride, int accumulate) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!outputs || (num_inputs && (!inputs || !coeffs))) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if (num_inputs && input_stride < slice_bytes) return set_err(ctx, PP_ERR_INVALID_ARG, "input_stride < slice_bytes");
+  if (num_outputs > 1 && output_stride < slice_bytes)
+    return set_err(ctx, PP_ERR_INVALID_ARG, "output_stride < slice_bytes");
+  if (num_outputs && coeff_stride < num_inputs) return set_err(ctx, PP_ERR_INVALID_ARG, "coeff_stride < num_inputs");
+  if (!num_outputs || !slice_bytes) return PP_OK;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  if (output_stride < slice_bytes) output_stride = round16(slice_bytes);
+  int st = PP_OK;
+  const uint16_t* dc = coeffs;
+  if (num_inputs) {
+    // pack coefficients densely on the device
+    std::vector<uint16_t> hc;
+    if (!is_device_ptr(coeffs)) {
+      hc.resize((size_t)num_outputs * num_inputs);
+      for (unsigned o = 0; o < num_outputs; o++)
+        memcpy(&hc[(size_t)o * num_inputs], coeffs + (size_t)o * coeff_stride, num_inputs * 2);
+      dc = to_device(ctx, S_COEF, hc.data(), hc.size(), &st);
+      if (st) return st;
+      coeff_stride = num_inputs;
+    }
+  }
+  return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, dc, coeff_stride, num_outputs, outputs,
+                          output_stride, accumulate != 0);
+}
+
+PP_API int pp_par2_create(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
+                          size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps, unsigned num_outputs,
+                          void* outputs, size_t output_stride) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!outputs || (num_inputs && (!inputs || !input_idx)) || (num_outputs && !exps))
+    return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if (num_inputs && input_stride < slice_bytes) return set_err(ctx, PP_ERR_INVALID_ARG, "input_stride < slice_bytes");
+  if (num_inputs > 32768) return set_err(ctx, PP_ERR_INVALID_ARG, "PAR2 allows at most 32768 input slices");
+  if (!num_outputs || !slice_bytes) return PP_OK;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  if (output_stride < slice_bytes) output_stride = round16(slice_bytes);
+  uint16_t* dc = nullptr;
+  if (num_inputs) {
+    dc = (uint16_t*)scratch(ctx, S_COEF, (size_t)num_inputs * num_outputs * 2);
+    if (!dc) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficients");
+    if (int r = par2_coeff_matrix_dev(ctx, input_idx, num_inputs, exps, num_outputs, dc)) return r;
+  }
+  return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, dc, num_inputs, num_outputs, outputs,
+                          output_stride, false);
+}
+
+PP_API int pp_par2_invert(pp_ctx* ctx, const uint8_t* valid, unsigned num_inputs, uint16_t* recovery,
+                          unsigned* num_recovery, uint16_t* factors) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!valid || !recovery || !num_recovery || !factors) return set_err(ctx, PP_ERR_INVALID_ARG, "null argument");
+  if (num_inputs == 0 || num_inputs > 32768) return set_err(ctx, PP_ERR_INVALID_ARG, "num_inputs out of range");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  // host bookkeeping: column permutation, row list (Construct, gfmat_inv.cpp:462-558)
+  std::vector<uint32_t> col_of(num_inputs);
+  unsigned vc = 0;
+  for (unsigned i = 0; i < num_inputs; i++) vc += valid[i] ? 1 : 0;
+  const unsigned m = num_inputs - vc;
+  if (m == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "no missing input slices");
+  {
+    unsigned a = 0, b = vc;
+    for (unsigned i = 0; i < num_inputs; i++) col_of[i] = valid[i] ? a++ : b++;
+  }
+  std::vector<uint16_t> rec(recovery, recovery + *num_recovery);
+  std::sort(rec.begin(), rec.end());
+  std::vector<uint16_t> logs(num_inputs);
+  for (unsigned i = 0; i < num_inputs; i++) logs[i] = gf16h().ilog[i];
+  const size_t ld = (num_inputs + 7) & ~(size_t)7;
+  uint16_t* d_mat = (uint16_t*)scratch(ctx, S_D, (size_t)m * ld * 2);
+  uint16_t* d_fcol = (uint16_t*)scratch(ctx, S_E, (size_t)m * 2 + 64);
+  if (!d_mat || !d_fcol) return set_err(ctx, PP_ERR_NO_MEMORY, "inversion matrix");
+  int* d_status = (int*)((char*)d_fcol + (((size_t)m * 2 + 15) & ~(size_t)15));
+  int st;
+  const uint16_t* d_logs = to_device(ctx, S_A, logs.data(), num_inputs, &st);
+  if (st) return st;
+  const uint32_t* d_col = to_device(ctx, S_B, col_of.data(), num_inputs, &st);
+  if (st) return st;
+  for (;;) {
+    if (rec.size() < m) return set_err(ctx, PP_ERR_NOT_INVERTIBLE, "not enough recovery slices to invert");
+    const uint16_t* d_rec = to_device(ctx, S_C, rec.data(), m, &st);
+    if (st) return st;
+    CUDA_TRY(ctx, cudaMemsetAsync(d_mat, 0, (size_t)m * ld * 2, ctx->stream));
+    CUDA_TRY(ctx, launch_gf16_build_rec_matrix(d_logs, d_col, num_inputs, d_rec, m, d_mat, ld, ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(d_status, 0xFF, sizeof(int), ctx->stream));
+    CUDA_TRY(ctx, launch_gf16_invert(d_mat, m, num_inputs, ld, vc, d_fcol, d_status, ctx->stream));
+    int hs = -1;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&hs, d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (hs < 0) break;
+    rec.erase(rec.begin() + hs);  // PAR2 flaw: drop the recovery row and retry
+  }
+  if (is_device_ptr(factors)) {
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(factors, (size_t)num_inputs * 2, d_mat, ld * 2, (size_t)num_inputs * 2, m,
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+  } else {
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(factors, (size_t)num_inputs * 2, d_mat, ld * 2, (size_t)num_inputs * 2, m,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  memcpy(recovery, rec.data(), m * 2);
+  *num_recovery = m;
+  return PP_OK;
+}
+
+// ------------------------------------------------------------ PAR2 processor
+struct pp_par2_proc {
+  pp_ctx* ctx = nullptr;
+  size_t alloc_size = 0, cur_size = 0, row = 0;
+  unsigned batch = 12, n_areas = 2;
+  struct Area {
+    uint8_t* d_in = nullptr;
+    uint16_t* d_coeff = nullptr;  // [n_out][batch]
+    std::vector<uint16_t> h_coeff;
+    unsigned count = 0;
+    cudaEvent_t done = nullptr;
+    bool active = false;
+  };
+  std::vector<Area> areas;
+  unsigned cur = 0;
+  std::vector<uint16_t> exps;
+  uint8_t* d_out = nullptr;
+  size_t d_out_n = 0;
+  bool has_output = false;
+  unsigned batches_started = 0;
+  cudaStream_t s_copy = nullptr, s_comp = nullptr;
+  cudaEvent_t copied = nullptr;
+};
+
+static int proc_alloc_inputs(pp_par2_proc* p) {
+  for (auto& a : p->areas) {
+    if (a.d_in) cudaFree(a.d_in);
+    a.d_in = nullptr;
+    if (cudaMalloc(&a.d_in, p->row * p->batch) != cudaSuccess) {
+      cudaGetLastError();
+      return PP_ERR_NO_MEMORY;
+    }
+  }
+  return PP_OK;
+}
+
+PP_API int pp_par2_proc_create(pp_ctx* ctx, size_t slice_size, unsigned staging_areas, unsigned input_batch,
+                               pp_par2_proc** out) {
+  if (!ctx || !out || slice_size == 0) return PP_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (int r = bind(ctx)) return r;
+  auto* p = new pp_par2_proc();
+  p->ctx = ctx;
+  p->alloc_size = p->cur_size = slice_size;
+  p->row = round16(slice_size);
+  p->n_areas = staging_areas ? staging_areas : 2;
+  // A GPU batch amortises launch latency; the default keeps a staging area
+  // at ~32 MiB of input or 64 slices, whichever is fewer (at least 12).
+  if (input_batch) {
+    p->batch = input_batch;
+  } else {
+    size_t b = (32u << 20) / p->row;
+    p->batch = (unsigned)std::max<size_t>(12, std::min<size_t>(64, b));
+  }
+  p->areas.resize(p->n_areas);
+  if (cudaStreamCreateWithFlags(&p->s_copy, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&p->s_comp, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->copied, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    pp_par2_proc_destroy(p);
+    return PP_ERR_CUDA;
+  }
+  for (auto& a : p->areas) {
+    if (cudaEventCreateWithFlags(&a.done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      pp_par2_proc_destroy(p);
+      return PP_ERR_CUDA;
+    }
+  }
+  if (proc_alloc_inputs(p) != PP_OK) {
+    pp_par2_proc_destroy(p);
+    return PP_ERR_NO_MEMORY;
+  }
+  *out = p;
+  return PP_OK;
+}
+
+PP_API void pp_par2_proc_destroy(pp_par2_proc* p) {
+  if (!p) return;
+  bind(p->ctx);
+  if (p->s_comp) cudaStreamSynchronize(p->s_comp);
+  if (p->s_copy) cudaStreamSynchronize(p->s_copy);
+  for (auto& a : p->areas) {
+    if (a.d_in) cudaFree(a.d_in);
+    if (a.d_coeff) cudaFree(a.d_coeff);
+    if (a.done) cudaEventDestroy(a.done);
+  }
+  if (p->d_out) cudaFree(p->d_out);
+  if (p->copied) cudaEventDestroy(p->copied);
+  if (p->s_copy) cudaStreamDestroy(p->s_copy);
+  if (p->s_comp) cudaStreamDestroy(p->s_comp);
+  delete p;
+}
+
+static bool area_busy(pp_par2_proc::Area& a) {
+  if (!a.active) return false;
+  cudaError_t e = cudaEventQuery(a.done);
+  if (e == cudaSuccess) {
+    a.active = false;
+    return false;
+  }
+  if (e != cudaErrorNotReady) cudaGetLastError();
+  return true;
+}
+
+PP_API int pp_par2_proc_set_current_slice_size(pp_par2_proc* p, size_t size) {
+  if (!p || size == 0) return PP_ERR_INVALID_ARG;
+  bind(p->ctx);
+  if (size > p->alloc_size) {
+    cudaStreamSynchronize(p->s_comp);
+    p->alloc_size = size;
+    p->row = round16(size);
+    if (proc_alloc_inputs(p) != PP_OK) return set_err(p->ctx, PP_ERR_NO_MEMORY, "staging realloc");
+    if (p->d_out) {
+      cudaFree(p->d_out);
+      p->d_out = nullptr;
+      p->d_out_n = 0;
+    }
+  }
+  p->cur_size = size;
+  return PP_OK;
+}
+
+static int proc_ensure_out(pp_par2_proc* p) {
+  size_t need = p->row * std::max<size_t>(1, p->exps.size());
+  if (p->d_out_n >= need) return PP_OK;
+  if (p->d_out) cudaFree(p->d_out);
+  p->d_out = nullptr;
+  if (cudaMalloc(&p->d_out, need) != cudaSuccess) {
+    cudaGetLastError();
+    p->d_out_n = 0;
+    return set_err(p->ctx, PP_ERR_NO_MEMORY, "processing buffer");
+  }
+  p->d_out_n = need;
+  return PP_OK;
+}
+
+PP_API int pp_par2_proc_set_recovery_slices(pp_par2_proc* p, unsigned num, const uint16_t* exps) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  bind(p->ctx);
+  cudaStreamSynchronize(p->s_comp);
+  p->exps.assign(num, 1);  // default 1 (custom-coefficient use), as gf16/controller_cpu.cpp:176
+  if (exps) memcpy(p->exps.data(), exps, num * 2);
+  for (auto& a : p->areas) {
+    a.h_coeff.assign((size_t)num * p->batch, 0);
+    if (a.d_coeff) cudaFree(a.d_coeff);
+    a.d_coeff = nullptr;
+    if (num && cudaMalloc(&a.d_coeff, (size_t)num * p->batch * 2) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(p->ctx, PP_ERR_NO_MEMORY, "coefficient buffer");
+    }
+  }
+  p->has_output = false;
+  return num ? proc_ensure_out(p) : PP_OK;
+}
+
+PP_API int pp_par2_proc_can_add(pp_par2_proc* p) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  bind(p->ctx);
+  if (area_busy(p->areas[p->cur])) return PP_PROC_ADD_FULL;
+  unsigned prev = (p->cur == 0 ? p->n_areas : p->cur) - 1;
+  return area_busy(p->areas[prev]) ? PP_PROC_ADD_OK_BUSY : PP_PROC_ADD_OK;
+}
+
+PP_API int pp_par2_proc_wait_for_add(pp_par2_proc* p) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  bind(p->ctx);
+  auto& a = p->areas[p->cur];
+  if (a.active) {
+    CUDA_TRY(p->ctx, cudaEventSynchronize(a.done));
+    a.active = false;
+  }
+  return PP_OK;
+}
+
+static int proc_submit(pp_par2_proc* p) {
+  auto& a = p->areas[p->cur];
+  if (!a.count) return PP_OK;
+  const unsigned n_out = (unsigned)p->exps.size();
+  // coefficient block [n_out][batch] (only the first `count` columns are used)
+  CUDA_TRY(p->ctx, cudaMemcpyAsync(a.d_coeff, a.h_coeff.data(), (size_t)n_out * p->batch * 2,
+                                   cudaMemcpyHostToDevice, p->s_copy));
+  CUDA_TRY(p->ctx, cudaEventRecord(p->copied, p->s_copy));
+  CUDA_TRY(p->ctx, cudaStreamWaitEvent(p->s_comp, p->copied, 0));
+  CUDA_TRY(p->ctx, launch_gf16_muladd(a.d_in, p->row, a.count, p->cur_size, a.d_coeff, p->batch, n_out, p->d_out,
+                                      p->row, p->has_output, p->ctx->sms, p->s_comp));
+  CUDA_TRY(p->ctx, cudaEventRecord(a.done, p->s_comp));
+  a.active = true;
+  a.count = 0;
+  p->has_output = true;
+  p->batches_started++;
+  p->cur = (p->cur + 1) % p->n_areas;
+  return PP_OK;
+}
+
+static int proc_add(pp_par2_proc* p, const void* buf, size_t size, const uint16_t* coeffs, uint16_t input_num,
+                    bool flush) {
+  if (!buf && size) return PP_ERR_INVALID_ARG;
+  if (p->exps.empty()) return set_err(p->ctx, PP_ERR_INVALID_ARG, "setRecoverySlices not called");
+  if (size > p->cur_size) return set_err(p->ctx, PP_ERR_INVALID_ARG, "input larger than the current slice size");
+  bind(p->ctx);
+  auto& a = p->areas[p->cur];
+  if (area_busy(a)) return set_err(p->ctx, PP_ERR_BUSY, "staging area busy");
+  const unsigned n_out = (unsigned)p->exps.size();
+  const unsigned idx = a.count;
+  for (unsigned o = 0; o < n_out; o++)
+    a.h_coeff[(size_t)o * p->batch + idx] = coeffs ? coeffs[o] : gf16h().coeff(input_num, p->exps[o]);
+  uint8_t* dst = a.d_in + (size_t)idx * p->row;
+  if (size) CUDA_TRY(p->ctx, cudaMemcpyAsync(dst, buf, size, cudaMemcpyDefault, p->s_copy));
+  if (size < p->row) CUDA_TRY(p->ctx, cudaMemsetAsync(dst + size, 0, p->row - size, p->s_copy));
+  // the caller may reuse the buffer once the copy has consumed it
+  CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_copy));
+  a.count++;
+  if (flush || a.count == p->batch) return proc_submit(p);
+  return PP_OK;
+}
+
+PP_API int pp_par2_proc_add_input(pp_par2_proc* p, const void* buffer, size_t size, uint16_t input_num, int flush) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  if (input_num >= 32768) return set_err(p->ctx, PP_ERR_INVALID_ARG, "input index >= 32768");
+  return proc_add(p, buffer, size, nullptr, input_num, flush != 0);
+}
+
+PP_API int pp_par2_proc_add_input_coeffs(pp_par2_proc* p, const void* buffer, size_t size, const uint16_t* coeffs,
+                                         int flush) {
+  if (!p || !coeffs) return PP_ERR_INVALID_ARG;
+  return proc_add(p, buffer, size, coeffs, 0, flush != 0);
+}
+
+PP_API int pp_par2_proc_flush(pp_par2_proc* p) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  bind(p->ctx);
+  return proc_submit(p);
+}
+
+PP_API int pp_par2_proc_end_input(pp_par2_proc* p) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  bind(p->ctx);
+  if (int r = proc_submit(p)) return r;
+  CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_comp));
+  for (auto& a : p->areas) a.active = false;
+  return PP_OK;
+}
+
+PP_API int pp_par2_proc_get_output(pp_par2_proc* p, unsigned index, void* output, int* valid) {
+  if (!p || !output) return PP_ERR_INVALID_ARG;
+  if (index >= p->exps.size()) return set_err(p->ctx, PP_ERR_INVALID_ARG, "output index out of range");
+  bind(p->ctx);
+  if (valid) *valid = 0;
+  CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_comp));
+  if (!p->has_output) {
+    // no input was added: the recovery data is all zero
+    CUDA_TRY(p->ctx, cudaMemsetAsync(p->d_out + (size_t)index * p->row, 0, p->cur_size, p->s_copy));
+  }
+  CUDA_TRY(p->ctx, cudaMemcpyAsync(output, p->d_out + (size_t)index * p->row, p->cur_size, cudaMemcpyDefault,
+                                   p->s_copy));
+  CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_copy));
+  if (valid) *valid = 1;
+  return PP_OK;
+}
+
+PP_API int pp_par2_proc_discard_output(pp_par2_proc* p) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  p->has_output = false;
+  return PP_OK;
+}
+
+PP_API int pp_par2_proc_free_processing_mem(pp_par2_proc* p) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  bind(p->ctx);
+  cudaStreamSynchronize(p->s_comp);
+  if (p->d_out) cudaFree(p->d_out);
+  p->d_out = nullptr;
+  p->d_out_n = 0;
+  p->has_output = false;
+  return PP_OK;
+}
+
+PP_API unsigned pp_par2_proc_input_batch_size(pp_par2_proc* p) { return p ? p->batch : 0; }
+PP_API unsigned pp_par2_proc_batches_started(pp_par2_proc* p) { return p ? p->batches_started : 0; }
+
+// ============================================================ PAR3 / GF64
+static uint64_t* cauchy_get(pp_ctx* ctx, size_t n_in, size_t n_rec, uint64_t fI, uint64_t fR, int* st) {
+  *st = PP_OK;
+  for (auto it = ctx->cauchy.begin(); it != ctx->cauchy.end(); ++it) {
+    if (it->n_in == n_in && it->n_rec == n_rec && it->fI == fI && it->fR == fR) {
+      ctx->cauchy.splice(ctx->cauchy.begin(), ctx->cauchy, it);
+      return ctx->cauchy.front().d;
+    }
+  }
+  // LRU of 8 matrices, as the reference's coefficient cache (src/par3_engine.cc:451-482)
+  if (ctx->cauchy.size() >= 8) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->cauchy.back().d);
+    ctx->cauchy.pop_back();
+  }
+  void* d = nullptr;
+  if (cudaMalloc(&d, n_in * n_rec * 8) != cudaSuccess) {
+    cudaGetLastError();
+    // make room: drop every cached matrix and retry once
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& e : ctx->cauchy) cudaFree(e.d);
+    ctx->cauchy.clear();
+    if (cudaMalloc(&d, n_in * n_rec * 8) != cudaSuccess) {
+      cudaGetLastError();
+      *st = set_err(ctx, PP_ERR_NO_MEMORY, "Cauchy matrix %zu x %zu", n_rec, n_in);
+      return nullptr;
+    }
+  }
+  cudaError_t e = launch_gf64_cauchy((uint64_t*)d, n_in, n_rec, fI, fR, n_in, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    *st = set_err(ctx, PP_ERR_CUDA, "Cauchy build: %s", cudaGetErrorString(e));
+    return nullptr;
+  }
+  ctx->cauchy.push_front({n_in, n_rec, fI, fR, (uint64_t*)d});
+  return (uint64_t*)d;
+}
+
+PP_API int pp_gf64_build_cauchy(pp_ctx* ctx, uint64_t* coeff, size_t num_inputs, size_t num_recovery,
+                                uint64_t first_input, uint64_t first_recovery) {
+  if (!ctx || !coeff) return PP_ERR_INVALID_ARG;
+  if (!num_inputs || !num_recovery) return PP_OK;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  if (is_device_ptr(coeff)) {
+    CUDA_TRY(ctx, launch_gf64_cauchy(coeff, num_inputs, num_recovery, first_input, first_recovery, num_inputs,
+                                     ctx->stream));
+    return PP_OK;
+  }
+  uint64_t* d = (uint64_t*)scratch(ctx, S_COEF, num_inputs * num_recovery * 8);
+  if (!d) return set_err(ctx, PP_ERR_NO_MEMORY, "Cauchy matrix");
+  CUDA_TRY(ctx, launch_gf64_cauchy(d, num_inputs, num_recovery, first_input, first_recovery, num_inputs,
+                                   ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpyAsync(coeff, d, num_inputs * num_recovery * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, uint64_t* recovery, size_t n_rec,
+                            size_t B, const uint64_t* d_coeff, bool accumulate) {
+  const bool in_dev = is_device_ptr(inputs);
+  const bool out_dev = is_device_ptr(recovery);
+  const uint64_t* din = inputs;
+  if (!in_dev) {
+    uint64_t* s = (uint64_t*)scratch(ctx, S_IN, n_in * B * 8);
+    if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", n_in * B * 8);
+    CUDA_TRY(ctx, cudaMemcpyAsync(s, inputs, n_in * B * 8, cudaMemcpyHostToDevice, ctx->stream));
+    din = s;
+  }
+  uint64_t* dout = recovery;
+  if (!out_dev) {
+    dout = (uint64_t*)scratch(ctx, S_OUT, n_rec * B * 8);
+    if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "output staging");
+    if (accumulate)
+      CUDA_TRY(ctx, cudaMemcpyAsync(dout, recovery, n_rec * B * 8, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CUDA_TRY(ctx, launch_gf64_matvec(din, B, n_in, B, d_coeff, n_in, n_rec, dout, B, accumulate, ctx->sms,
+                                   ctx->stream));
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(recovery, dout, n_rec * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!in_dev || !out_dev) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+PP_API int pp_gf64_compute_recovery(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs, uint64_t* recovery,
+                                    size_t num_recovery, size_t block_size64, uint64_t first_input,
+                                    uint64_t first_recovery, int accumulate, int kernel) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_inputs == 0 || num_recovery == 0 || block_size64 == 0) return PP_OK;
+  if (!inputs || !recovery) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if (kernel < PP_GF64_KERNEL_AUTO || kernel > PP_GF64_KERNEL_FENGER)
+    return set_err(ctx, PP_ERR_INVALID_ARG, "unknown kernel %d", kernel);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  int st;
+  uint64_t* M = cauchy_get(ctx, num_inputs, num_recovery, first_input, first_recovery, &st);
+  if (!M) return st;
+  return gf64_matvec_impl(ctx, inputs, num_inputs, recovery, num_recovery, block_size64, M, accumulate != 0);
+}
+
+PP_API int pp_gf64_compute_recovery_with_coeff(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs,
+                                               uint64_t* recovery, size_t num_recovery, size_t block_size64,
+                                               const uint64_t* coeff, int accumulate) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_inputs == 0 || num_recovery == 0 || block_size64 == 0) return PP_OK;
+  if (!inputs || !recovery || !coeff) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  int st;
+  const uint64_t* dc = to_device(ctx, S_COEF, coeff, num_inputs * num_recovery, &st);
+  if (st) return st;
+  return gf64_matvec_impl(ctx, inputs, num_inputs, recovery, num_recovery, block_size64, dc, accumulate != 0);
+}
+
+PP_API int pp_gf64_solve_and_reconstruct(pp_ctx* ctx, uint64_t* A, uint64_t* rhs, size_t n, size_t B) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (n == 0) return PP_OK;
+  if (!A || (!rhs && B)) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const bool a_dev = is_device_ptr(A), r_dev = rhs ? is_device_ptr(rhs) : true;
+  uint64_t* dA = A;
+  uint64_t* dR = rhs;
+  if (!a_dev) {
+    dA = (uint64_t*)scratch(ctx, S_D, n * n * 8);
+    if (!dA) return set_err(ctx, PP_ERR_NO_MEMORY, "solve matrix");
+    CUDA_TRY(ctx, cudaMemcpyAsync(dA, A, n * n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (!r_dev) {
+    dR = (uint64_t*)scratch(ctx, S_IN, n * B * 8);
+    if (!dR) return set_err(ctx, PP_ERR_NO_MEMORY, "solve rhs");
+    CUDA_TRY(ctx, cudaMemcpyAsync(dR, rhs, n * B * 8, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  uint64_t* dF = (uint64_t*)scratch(ctx, S_E, (n + 2) * 8 + 64);
+  if (!dF) return set_err(ctx, PP_ERR_NO_MEMORY, "solve scratch");
+  int* dS = (int*)(dF + n + 2);
+  CUDA_TRY(ctx, cudaMemsetAsync(dS, 0, sizeof(int), ctx->stream));
+  CUDA_TRY(ctx, launch_gf64_solve(dA, dR, n, B, dF, dS, ctx->stream));
+  int hs = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&hs, dS, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  if (!a_dev) CUDA_TRY(ctx, cudaMemcpyAsync(A, dA, n * n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!r_dev) CUDA_TRY(ctx, cudaMemcpyAsync(rhs, dR, n * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (hs != 0) return set_err(ctx, PP_ERR_SINGULAR, "matrix is singular");
+  return PP_OK;
+}
+
+// element-wise region ops ---------------------------------------------------
+static int region_elem(pp_ctx* ctx, uint64_t* out, const uint64_t* in, const uint64_t* coeff, size_t len,
+                       size_t n_coeff, bool add) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!len) return PP_OK;
+  if (!out || !in || !coeff || !n_coeff) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const bool in_dev = is_device_ptr(in), out_dev = is_device_ptr(out);
+  int st;
+  const uint64_t* dc = to_device(ctx, S_COEF, coeff, n_coeff, &st);
+  if (st) return st;
+  const uint64_t* din = in;
+  if (!in_dev) {
+    uint64_t* s = (uint64_t*)scratch(ctx, S_IN, len * 8);
+    if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "staging");
+    CUDA_TRY(ctx, cudaMemcpyAsync(s, in, len * 8, cudaMemcpyHostToDevice, ctx->stream));
+    din = s;
+  }
+  uint64_t* dout = out;
+  if (!out_dev) {
+    dout = (uint64_t*)scratch(ctx, S_OUT, len * 8);
+    if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "staging");
+    if (add) CUDA_TRY(ctx, cudaMemcpyAsync(dout, out, len * 8, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (add)
+    CUDA_TRY(ctx, launch_gf64_region_muladd_arr(dout, din, dc, len, n_coeff, ctx->stream));
+  else
+    CUDA_TRY(ctx, launch_gf64_region_mul_arr(dout, din, dc, len, n_coeff, ctx->stream));
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(out, dout, len * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!in_dev || !out_dev || !is_device_ptr(coeff)) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+PP_API int pp_gf64_region_mul(pp_ctx* ctx, uint64_t* out, const uint64_t* in, size_t len, uint64_t constant) {
+  return region_elem(ctx, out, in, &constant, len, 1, false);
+}
+PP_API int pp_gf64_region_mul_arr(pp_ctx* ctx, uint64_t* out, const uint64_t* in, const uint64_t* coeff, size_t len,
+                                  size_t n_coeff) {
+  return region_elem(ctx, out, in, coeff, len, n_coeff, false);
+}
+PP_API int pp_gf64_region_muladd_arr(pp_ctx* ctx, uint64_t* out, const uint64_t* in, const uint64_t* coeff,
+                                     size_t len, size_t n_coeff) {
+  return region_elem(ctx, out, in, coeff, len, n_coeff, true);
+}
+
+// 2-D gather form: all three pointer-table entry points reduce to
+//   outs[k][w] ^= XOR_g ins[g][w] * C[k][g]
+static int region_2d(pp_ctx* ctx, uint64_t* const* outs, size_t K, const uint64_t* const* ins, size_t G,
+                     const std::vector<uint64_t>& C, size_t len) {
+  if (!K || !G || !len) return PP_OK;
+  bool all_dev = true;
+  for (size_t k = 0; k < K && all_dev; k++) all_dev = is_device_ptr(outs[k]);
+  for (size_t g = 0; g < G && all_dev; g++) all_dev = is_device_ptr(ins[g]);
+  int st;
+  const uint64_t* dC = to_device(ctx, S_COEF, C.data(), C.size(), &st);
+  if (st) return st;
+  std::vector<const uint64_t*> din(G);
+  std::vector<uint64_t*> dout(K);
+  uint64_t *sin = nullptr, *sout = nullptr;
+  if (all_dev) {
+    for (size_t g = 0; g < G; g++) din[g] = ins[g];
+    for (size_t k = 0; k < K; k++) dout[k] = outs[k];
+  } else {
+    sin = (uint64_t*)scratch(ctx, S_IN, G * len * 8);
+    sout = (uint64_t*)scratch(ctx, S_OUT, K * len * 8);
+    if (!sin || !sout) return set_err(ctx, PP_ERR_NO_MEMORY, "staging");
+    for (size_t g = 0; g < G; g++) {
+      CUDA_TRY(ctx, cudaMemcpyAsync(sin + g * len, ins[g], len * 8, cudaMemcpyDefault, ctx->stream));
+      din[g] = sin + g * len;
+    }
+    for (size_t k = 0; k < K; k++) {
+      CUDA_TRY(ctx, cudaMemcpyAsync(sout + k * len, outs[k], len * 8, cudaMemcpyDefault, ctx->stream));
+      dout[k] = sout + k * len;
+    }
+  }
+  const uint64_t* const* dpin = to_device(ctx, S_A, din.data(), G, &st);
+  if (st) return st;
+  uint64_t* const* dpout = (uint64_t* const*)to_device(ctx, S_B, (const uint64_t* const*)dout.data(), K, &st);
+  if (st) return st;
+  CUDA_TRY(ctx, launch_gf64_2d_gather(dpout, K, dpin, G, dC, G, len, ctx->sms, ctx->stream));
+  if (!all_dev) {
+    for (size_t k = 0; k < K; k++)
+      CUDA_TRY(ctx, cudaMemcpyAsync(outs[k], sout + k * len, len * 8, cudaMemcpyDefault, ctx->stream));
+  }
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+PP_API int pp_gf64_region_coupled_muladd_arr(pp_ctx* ctx, uint64_t* out, const uint64_t* const* in_blocks,
+                                             const uint64_t* coeff_blocks, size_t len, size_t G) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!G || !len) return PP_OK;
+  if (!out || !in_blocks || !coeff_blocks) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  std::vector<uint64_t> C(G);
+  if (is_device_ptr(coeff_blocks))
+    CUDA_TRY(ctx, cudaMemcpy(C.data(), coeff_blocks, G * 8, cudaMemcpyDeviceToHost));
+  else
+    memcpy(C.data(), coeff_blocks, G * 8);
+  uint64_t* outs[1] = {out};
+  return region_2d(ctx, outs, 1, in_blocks, G, C, len);
+}
+
+PP_API int pp_gf64_region_fused_output_muladd_arr(pp_ctx* ctx, uint64_t* const* outs, const uint64_t* in,
+                                                  const uint64_t* const* coeff_block_starts, size_t len, size_t K) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!K || !len) return PP_OK;
+  if (!outs || !in || !coeff_block_starts) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  std::vector<uint64_t> C(K);
+  for (size_t k = 0; k < K; k++) {
+    if (is_device_ptr(coeff_block_starts[k]))
+      CUDA_TRY(ctx, cudaMemcpy(&C[k], coeff_block_starts[k], 8, cudaMemcpyDeviceToHost));
+    else
+      C[k] = coeff_block_starts[k][0];
+  }
+  const uint64_t* ins[1] = {in};
+  return region_2d(ctx, outs, K, ins, 1, C, len);
+}
+
+PP_API int pp_gf64_region_2d_muladd_arr(pp_ctx* ctx, uint64_t* const* outs, size_t K, const uint64_t* const* in_blocks,
+                                        size_t G, const uint64_t* coeff_block_2d, size_t K_stride, size_t len) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!K || !G || !len) return PP_OK;
+  if (!outs || !in_blocks || !coeff_block_2d || K_stride < G)
+    return set_err(ctx, PP_ERR_INVALID_ARG, "bad arguments");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  std::vector<uint64_t> C(K * G);
+  std::vector<uint64_t> raw((K - 1) * K_stride + G);
+  if (is_device_ptr(coeff_block_2d))
+    CUDA_TRY(ctx, cudaMemcpy(raw.data(), coeff_block_2d, raw.size() * 8, cudaMemcpyDeviceToHost));
+  else
+    memcpy(raw.data(), coeff_block_2d, raw.size() * 8);
+  for (size_t k = 0; k < K; k++)
+    for (size_t gg = 0; gg < G; gg++) C[k * G + gg] = raw[k * K_stride + gg];
+  return region_2d(ctx, outs, K, in_blocks, G, C, len);
+}
+
+PP_API int pp_gf64_inverse_batch(pp_ctx* ctx, uint64_t* out, const uint64_t* in, size_t n) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!n) return PP_OK;
+  if (!out || !in) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const bool in_dev = is_device_ptr(in), out_dev = is_device_ptr(out);
+  const uint64_t* din = in;
+  if (!in_dev) {
+    uint64_t* s = (uint64_t*)scratch(ctx, S_IN, n * 8);
+    if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "staging");
+    CUDA_TRY(ctx, cudaMemcpyAsync(s, in, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    din = s;
+  }
+  uint64_t* dout = out_dev ? out : (uint64_t*)scratch(ctx, S_OUT, n * 8);
+  if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "staging");
+  CUDA_TRY(ctx, launch_gf64_inverse_batch(dout, din, n, ctx->stream));
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(out, dout, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!in_dev || !out_dev) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+}  // extern "C"

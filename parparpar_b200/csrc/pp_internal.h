@@ -1,0 +1,72 @@
+// Internal host-side declarations shared by the C-ABI layer and the kernel
+// translation units.  Not part of the public interface (include/parpar_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+namespace pp {
+
+// Launch counter: every kernel launch issued by this library increments it
+// (reported by pp_ctx_launch_count so callers can account for native work).
+void note_launch(int n = 1);
+uint64_t launches();
+
+// ------------------------------------------------------------ GF(2^16)
+// coeffs[o*N + i] = 2^(logs[i] * exps[o] mod 65535)   (device buffers)
+cudaError_t launch_gf16_coeff_matrix(const uint16_t* d_logs, unsigned n_in, const uint16_t* d_exps,
+                                     unsigned n_out, uint16_t* d_coeffs, cudaStream_t s);
+
+// Region multiply-accumulate over 16-byte-aligned rows:
+//   out[o] (^)= XOR_i coeffs[o*N + i] * in[i]   for the first slice_bytes bytes
+// in/out rows are in_stride/out_stride bytes apart (multiples of 16).
+// Bytes past slice_bytes are neither read as data nor written.
+// If !accumulate the outputs are overwritten.
+// coeffs rows are ldc elements apart.
+cudaError_t launch_gf16_muladd(const uint8_t* d_in, size_t in_stride, unsigned n_in, size_t slice_bytes,
+                               const uint16_t* d_coeffs, size_t ldc, unsigned n_out, uint8_t* d_out,
+                               size_t out_stride, bool accumulate, int sms, cudaStream_t s);
+
+// PAR2 inversion (Gauss-Jordan without pivoting, identity columns in place).
+// d_mat: m rows x ncols (row stride ld elements).  Runs all m pivot steps;
+// d_status[0] receives -1 on success or the first row whose pivot was zero.
+cudaError_t launch_gf16_invert(uint16_t* d_mat, unsigned m, unsigned ncols, size_t ld, unsigned pivot_col0,
+                               uint16_t* d_fcol, int* d_status, cudaStream_t s);
+
+// Build the PAR2 repair matrix: mat[r][col_of[i]] = coeff(logs[i], rec[r]).
+cudaError_t launch_gf16_build_rec_matrix(const uint16_t* d_logs, const uint32_t* d_col_of, unsigned n_in,
+                                         const uint16_t* d_rec, unsigned m, uint16_t* d_mat, size_t ld,
+                                         cudaStream_t s);
+
+// ------------------------------------------------------------ GF(2^64)
+cudaError_t launch_gf64_cauchy(uint64_t* d_m, size_t n_in, size_t n_rec, uint64_t first_in, uint64_t first_rec,
+                               size_t ld, cudaStream_t s);
+cudaError_t launch_gf64_inverse_batch(uint64_t* d_out, const uint64_t* d_in, size_t n, cudaStream_t s);
+
+// out[r][w] (^)= XOR_c coeff[r*ldc + c] * in[c][w]
+// in rows in_stride words apart, out rows out_stride words apart.
+cudaError_t launch_gf64_matvec(const uint64_t* d_in, size_t in_stride, size_t n_in, size_t words,
+                               const uint64_t* d_coeff, size_t ldc, size_t n_out, uint64_t* d_out,
+                               size_t out_stride, bool accumulate, int sms, cudaStream_t s);
+
+// Gather form used by the region entry points: pointer tables on the device.
+//   outs[k][w] ^= XOR_g in_blocks[g][w] * coeff[k*kstride + g]
+cudaError_t launch_gf64_2d_gather(uint64_t* const* d_outs, size_t K, const uint64_t* const* d_ins, size_t G,
+                                  const uint64_t* d_coeff, size_t kstride, size_t len, int sms,
+                                  cudaStream_t s);
+
+// Element-wise region ops (n_coeff cycling / summing semantics of the
+// reference's gf64_region_mul_arr / gf64_region_muladd_arr).
+cudaError_t launch_gf64_region_mul_arr(uint64_t* d_out, const uint64_t* d_in, const uint64_t* d_coeff, size_t len,
+                                       size_t n_coeff, cudaStream_t s);
+cudaError_t launch_gf64_region_muladd_arr(uint64_t* d_out, const uint64_t* d_in, const uint64_t* d_coeff,
+                                          size_t len, size_t n_coeff, cudaStream_t s);
+
+// SolveAndReconstruct: Gauss-Jordan on A (n x n) with the RHS (n x B words).
+// d_status[0] = 0 on success, -1 if singular.
+cudaError_t launch_gf64_solve(uint64_t* d_A, uint64_t* d_rhs, size_t n, size_t B, uint64_t* d_fcol,
+                              int* d_status, cudaStream_t s);
+
+}  // namespace pp

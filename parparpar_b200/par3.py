@@ -1,0 +1,264 @@
+"""PAR3 (GF(2^64)) host interface over the CUDA engine.
+
+Mirrors the reference's PAR3 operator surface:
+
+* ``GF64Controller``  — static engine entry points with the reference's names
+                         and argument meaning (src/par3_engine.h:11-244).
+* ``compute_recovery*``, ``build_coefficient_matrix``, ``solve_and_reconstruct``,
+  ``Gf64Encoder`` — the gf64_addon N-API functions (src/gf64_addon.cc:3271-3612)
+  with the same argument checks (TypeError / RangeError become Python
+  ``TypeError`` / ``ValueError``).
+* ``gf64_region_*`` / ``gf64_inverse_batch`` — the region dispatch table
+  (gf64/gf64_global.h:23-37).
+
+Buffers: numpy uint64 arrays (host) or torch int64/uint64 tensors (host or
+CUDA).  numThreads arguments are accepted for interface parity; the device
+schedules itself.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import PP_OK, PPError, default_context, lib, ptr
+
+
+def _ctx(ctx):
+    return ctx if ctx is not None else default_context()
+
+
+def _u64(x) -> int:
+    return int(x) & 0xFFFFFFFFFFFFFFFF
+
+
+class GF64Controller:
+    """Static GF(2^64) engine entry points (reference src/par3_engine.h:11-244)."""
+
+    ctx = None
+
+    @classmethod
+    def _c(cls):
+        return _ctx(cls.ctx)
+
+    @classmethod
+    def ComputeRecoveryBlocks(cls, inputs, numInputs, recovery, numRecovery, blockSize64, firstInput, firstRecovery,
+                              numThreads=0, accumulate=False, kernel=_lib.PP_GF64_KERNEL_MATVEC):
+        c = cls._c()
+        c.check(lib.pp_gf64_compute_recovery(c.h, ptr(inputs), numInputs, ptr(recovery), numRecovery, blockSize64,
+                                             _u64(firstInput), _u64(firstRecovery), 1 if accumulate else 0, kernel))
+
+    @classmethod
+    def ComputeRecoveryBlocksFull(cls, inputs, numInputs, recovery, numRecovery, blockSize64, firstInput,
+                                  firstRecovery, numThreads=0, accumulate=False):
+        cls.ComputeRecoveryBlocks(inputs, numInputs, recovery, numRecovery, blockSize64, firstInput, firstRecovery,
+                                  numThreads, accumulate, _lib.PP_GF64_KERNEL_AUTO)
+
+    @classmethod
+    def ComputeRecoveryBlocksBarycentric(cls, inputs, numInputs, recovery, numRecovery, blockSize64, firstInput,
+                                         firstRecovery, numThreads=0, accumulate=False):
+        cls.ComputeRecoveryBlocks(inputs, numInputs, recovery, numRecovery, blockSize64, firstInput, firstRecovery,
+                                  numThreads, accumulate, _lib.PP_GF64_KERNEL_BARYCENTRIC)
+
+    @classmethod
+    def ComputeRecoveryBlocksFenger(cls, inputs, numInputs, recovery, numRecovery, blockSize64, firstInput,
+                                    firstRecovery, numThreads=0):
+        cls.ComputeRecoveryBlocks(inputs, numInputs, recovery, numRecovery, blockSize64, firstInput, firstRecovery,
+                                  numThreads, False, _lib.PP_GF64_KERNEL_FENGER)
+
+    @classmethod
+    def ComputeRecoveryBlocksWithCoeff(cls, inputs, numInputs, recovery, numRecovery, blockSize64, coeff,
+                                       numThreads=0, accumulate=False):
+        c = cls._c()
+        c.check(lib.pp_gf64_compute_recovery_with_coeff(c.h, ptr(inputs), numInputs, ptr(recovery), numRecovery,
+                                                        blockSize64, ptr(coeff), 1 if accumulate else 0))
+
+    @classmethod
+    def BuildCauchyMatrix(cls, coeffMatrix, numInputs, numRecovery, firstInput, firstRecovery):
+        c = cls._c()
+        c.check(lib.pp_gf64_build_cauchy(c.h, ptr(coeffMatrix), numInputs, numRecovery, _u64(firstInput),
+                                         _u64(firstRecovery)))
+
+    @classmethod
+    def BuildCauchyMatrixAlloc(cls, numInputs, numRecovery, firstInput, firstRecovery):
+        if numInputs == 0 or numRecovery == 0:
+            return None
+        m = np.zeros((numRecovery, numInputs), dtype=np.uint64)
+        cls.BuildCauchyMatrix(m, numInputs, numRecovery, firstInput, firstRecovery)
+        return m
+
+    @classmethod
+    def MultiplyAccumulate(cls, out, numOut, inp, numIn, coeffMatrix, blockSize64):
+        """out[i] ^= sum_j in[j] * coeffMatrix[i*numIn + j] (accumulating form)."""
+        cls.ComputeRecoveryBlocksWithCoeff(inp, numIn, out, numOut, blockSize64, coeffMatrix, 0, True)
+
+    @classmethod
+    def SolveAndReconstruct(cls, A, rhsBlocks, n, blockSize64, numThreads=0) -> int:
+        """0 on success, -1 if the matrix is singular (reference return codes)."""
+        c = cls._c()
+        st = lib.pp_gf64_solve_and_reconstruct(c.h, ptr(A), ptr(rhsBlocks), n, blockSize64)
+        if st == _lib.PP_ERR_SINGULAR:
+            return -1
+        c.check(st)
+        return 0
+
+
+# ------------------------------------------------------------- N-API mirror
+def _buf_words(buf, name):
+    if buf is None or not (hasattr(buf, "data_ptr") or hasattr(buf, "ctypes")):
+        raise TypeError(f"{name} must be a Buffer")
+    nbytes = buf.numel() * buf.element_size() if hasattr(buf, "numel") else buf.nbytes
+    return nbytes
+
+
+def _check_int(v, name):
+    if isinstance(v, bool) or not isinstance(v, (int, np.integer)):
+        raise TypeError(f"{name} must be an integer")
+    return int(v)
+
+
+def compute_recovery(inputs, outputs, numInputs, numRecovery, blockSize, firstInput, firstRecovery, numThreads=0,
+                     accumulate=False, _kernel=_lib.PP_GF64_KERNEL_MATVEC):
+    """gf64_addon compute_recovery (src/gf64_addon.cc:1266-1434): blockSize in
+    BYTES, a positive multiple of 8."""
+    in_bytes = _buf_words(inputs, "inputs")
+    out_bytes = _buf_words(outputs, "outputs")
+    numInputs = _check_int(numInputs, "numInputs")
+    numRecovery = _check_int(numRecovery, "numRecovery")
+    blockSize = _check_int(blockSize, "blockSize")
+    if not isinstance(firstInput, (int, np.integer)) or isinstance(firstInput, bool):
+        raise TypeError("firstInput must be a Number or BigInt")
+    if not isinstance(firstRecovery, (int, np.integer)) or isinstance(firstRecovery, bool):
+        raise TypeError("firstRecovery must be a Number or BigInt")
+    if not isinstance(accumulate, bool):
+        raise TypeError("accumulate must be a boolean")
+    if numInputs <= 0:
+        raise ValueError("numInputs must be positive")
+    if numRecovery <= 0:
+        raise ValueError("numRecovery must be positive")
+    if blockSize <= 0 or blockSize % 8:
+        raise ValueError("blockSize must be positive and a multiple of 8")
+    if in_bytes < numInputs * blockSize:
+        raise ValueError("inputs buffer too small for numInputs * blockSize")
+    if out_bytes < numRecovery * blockSize:
+        raise ValueError("outputs buffer too small for numRecovery * blockSize")
+    GF64Controller.ComputeRecoveryBlocks(inputs, numInputs, outputs, numRecovery, blockSize // 8, firstInput,
+                                         firstRecovery, numThreads, accumulate, _kernel)
+
+
+def compute_recovery_full(*a, **k):
+    compute_recovery(*a, _kernel=_lib.PP_GF64_KERNEL_AUTO, **k)
+
+
+def compute_recovery_barycentric(*a, **k):
+    compute_recovery(*a, _kernel=_lib.PP_GF64_KERNEL_BARYCENTRIC, **k)
+
+
+def compute_recovery_fenger(inputs, outputs, numInputs, numRecovery, blockSize, firstInput, firstRecovery,
+                            numThreads=0):
+    compute_recovery(inputs, outputs, numInputs, numRecovery, blockSize, firstInput, firstRecovery, numThreads,
+                     False, _kernel=_lib.PP_GF64_KERNEL_FENGER)
+
+
+def compute_recovery_accumulate(inputs, outputs, numInputs, numRecovery, blockSize, firstInput, firstRecovery,
+                                numThreads=0):
+    compute_recovery(inputs, outputs, numInputs, numRecovery, blockSize, firstInput, firstRecovery, numThreads, True)
+
+
+def build_coefficient_matrix(numInputs, numRecovery, firstInput, firstRecovery):
+    m = GF64Controller.BuildCauchyMatrixAlloc(numInputs, numRecovery, firstInput, firstRecovery)
+    return m
+
+
+def compute_recovery_with_coeff(inputs, outputs, numInputs, numRecovery, blockSize, coeff, numThreads=0,
+                                accumulate=False):
+    if blockSize <= 0 or blockSize % 8:
+        raise ValueError("blockSize must be positive and a multiple of 8")
+    GF64Controller.ComputeRecoveryBlocksWithCoeff(inputs, numInputs, outputs, numRecovery, blockSize // 8, coeff,
+                                                  numThreads, accumulate)
+
+
+def solve_and_reconstruct(A, rhs, n, blockSize):
+    """Returns the solved RHS (in place); raises on a singular matrix like the
+    N-API wrapper does."""
+    if blockSize <= 0 or blockSize % 8:
+        raise ValueError("blockSize must be positive and a multiple of 8")
+    if GF64Controller.SolveAndReconstruct(A, rhs, n, blockSize // 8) != 0:
+        raise PPError(_lib.PP_ERR_SINGULAR, "singular matrix")
+    return rhs
+
+
+# ------------------------------------------------------------- region table
+def gf64_region_mul(out, inp, length, constant, ctx=None):
+    c = _ctx(ctx)
+    c.check(lib.pp_gf64_region_mul(c.h, ptr(out), ptr(inp), length, _u64(constant)))
+
+
+def gf64_region_mul_arr(out, inp, coeff, length, n_coeff, ctx=None):
+    c = _ctx(ctx)
+    c.check(lib.pp_gf64_region_mul_arr(c.h, ptr(out), ptr(inp), ptr(coeff), length, n_coeff))
+
+
+def gf64_region_muladd_arr(out, inp, coeff, length, n_coeff, ctx=None):
+    c = _ctx(ctx)
+    c.check(lib.pp_gf64_region_muladd_arr(c.h, ptr(out), ptr(inp), ptr(coeff), length, n_coeff))
+
+
+def _ptr_array(bufs):
+    arr = (ctypes.c_void_p * len(bufs))(*[ptr(b) for b in bufs])
+    return arr
+
+
+def gf64_region_coupled_muladd_arr(out, in_blocks, coeff_blocks, length, G, ctx=None):
+    c = _ctx(ctx)
+    pa = _ptr_array(in_blocks)
+    c.check(lib.pp_gf64_region_coupled_muladd_arr(c.h, ptr(out), ctypes.cast(pa, ctypes.c_void_p), ptr(coeff_blocks),
+                                                  length, G))
+
+
+def gf64_region_fused_output_muladd_arr(outs, inp, coeff_block_starts, length, K, ctx=None):
+    c = _ctx(ctx)
+    po = _ptr_array(outs)
+    pc = _ptr_array(coeff_block_starts)
+    c.check(lib.pp_gf64_region_fused_output_muladd_arr(c.h, ctypes.cast(po, ctypes.c_void_p), ptr(inp),
+                                                       ctypes.cast(pc, ctypes.c_void_p), length, K))
+
+
+def gf64_region_2d_muladd_arr(outs, K, in_blocks, G, coeff_block_2d, K_stride, length, ctx=None):
+    c = _ctx(ctx)
+    po = _ptr_array(outs)
+    pi = _ptr_array(in_blocks)
+    c.check(lib.pp_gf64_region_2d_muladd_arr(c.h, ctypes.cast(po, ctypes.c_void_p), K,
+                                             ctypes.cast(pi, ctypes.c_void_p), G, ptr(coeff_block_2d), K_stride,
+                                             length))
+
+
+def gf64_inverse_batch(out, inp, n, ctx=None):
+    c = _ctx(ctx)
+    c.check(lib.pp_gf64_inverse_batch(c.h, ptr(out), ptr(inp), n))
+
+
+class Gf64Encoder:
+    """gf64_addon Gf64Encoder (src/gf64_addon.cc:446,835 and export table)."""
+
+    def __init__(self, ctx=None):
+        self.ctx = _ctx(ctx)
+
+    def mul(self, a: int, b: int) -> int:
+        x = np.array([a], dtype=np.uint64)
+        o = np.zeros(1, dtype=np.uint64)
+        gf64_region_mul(o, x, 1, b, self.ctx)
+        return int(o[0])
+
+    def mul_arr(self, out, inp, coeff, length, n_coeff):
+        gf64_region_mul_arr(out, inp, coeff, length, n_coeff, self.ctx)
+
+    def coupled_muladd_arr(self, out, in_blocks, coeff_blocks, G, length):
+        gf64_region_coupled_muladd_arr(out, in_blocks, coeff_blocks, length, G, self.ctx)
+
+    def fused_output_muladd_arr(self, outs, inp, coeffs, K, length):
+        gf64_region_fused_output_muladd_arr(outs, inp, coeffs, length, K, self.ctx)
+
+    def two_d_muladd_arr(self, outs, K, in_blocks, G, coeff2d, K_stride, length):
+        gf64_region_2d_muladd_arr(outs, K, in_blocks, G, coeff2d, K_stride, length, self.ctx)

@@ -1,0 +1,115 @@
+"""Pin the oracle (the C restatement in oracle/) to the reference.
+
+1. Golden fixtures generated from the reference's own build
+   (tests/golden/make_golden.py) and the reference's frozen PAR3 golden
+   vector (test/par3-golden.js: CRC32 6A941C15).
+2. Where the reference build (oracle/_ref) is present, direct randomized
+   cross-checks against it.
+"""
+import zlib
+
+import numpy as np
+import pytest
+
+
+def test_par3_golden_crc(oracle, golden):
+    g = golden("par3_golden.npz")
+    assert int(g["crc32"]) == 0x6A941C15
+    out = oracle.gf64_compute_recovery(g["inputs"], 2, int(g["first_input"]), int(g["first_recovery"]))
+    assert np.array_equal(out, g["recovery"])
+    assert zlib.crc32(out.tobytes()) == 0x6A941C15
+
+
+def test_gf64_mul_inv(oracle, golden):
+    g = golden("gf64_ops.npz")
+    for a, b, p, i in zip(g["a"], g["b"], g["prod"], g["inv"]):
+        assert oracle.gf64_mul(int(a), int(b)) == int(p)
+        assert oracle.gf64_inv(int(a)) == int(i)
+
+
+def test_gf64_cauchy_matvec_solve(oracle, golden):
+    g = golden("gf64_ops.npz")
+    assert np.array_equal(oracle.gf64_build_cauchy(37, 9, 3, 40), g["cauchy"])
+    assert np.array_equal(oracle.gf64_build_cauchy(8, 4, 0, 2), g["cauchy_clash"])
+    assert np.array_equal(oracle.gf64_compute_recovery(g["inp"], 7, 0, 33), g["matvec"])
+    out = g["acc0"].copy()
+    oracle.gf64_compute_recovery(g["inp"], 7, 0, 33, out=out, accumulate=True)
+    assert np.array_equal(out, g["matvec_acc"])
+    A, rhs = g["A"].copy(), g["rhs"].copy()
+    assert oracle.gf64_solve_and_reconstruct(A, rhs) == int(g["rc"]) == 0
+    assert np.array_equal(rhs, g["solved"])
+    assert oracle.gf64_solve_and_reconstruct(g["sing"].copy(), g["sing_rhs"].copy()) == int(g["sing_rc"]) == -1
+
+
+def test_par2_create_golden(oracle, golden):
+    g = golden("par2_create.npz")
+    for k in range(int(g["ncases"])):
+        inp, idx, exps, last, out = (g[f"c{k}_inputs"], g[f"c{k}_idx"], g[f"c{k}_exps"], int(g[f"c{k}_last"]),
+                                     g[f"c{k}_out"])
+        n, s = inp.shape
+        srcs = [inp[i] if i < n - 1 else inp[i][:last] for i in range(n)]
+        c = oracle.par2_coeff_matrix(idx, exps)
+        assert np.array_equal(oracle.par2_muladd(srcs, s, c), out), f"case {k}"
+    got = oracle.par2_muladd(list(g["coef_inputs"]), g["coef_inputs"].shape[1], g["coef_coeffs"])
+    assert np.array_equal(got, g["coef_out"])
+
+
+def test_par2_invert_golden(oracle, golden):
+    g = golden("par2_invert.npz")
+    for k in range(int(g["ncases"])):
+        ok, f, used = oracle.par2_invert(g[f"c{k}_valid"], g[f"c{k}_rec"])
+        assert ok == bool(g[f"c{k}_ok"]), f"case {k}"
+        if ok:
+            assert used == [int(x) for x in g[f"c{k}_used"]], f"case {k}"
+            assert np.array_equal(f, g[f"c{k}_factors"]), f"case {k}"
+
+
+def test_par2_invert_flaw_drops_a_row(oracle):
+    # test/gf16/test-inv.cpp:115-139: recovery {0,5,6} over the flawed input set
+    valid = np.ones(6555, dtype=np.uint8)
+    valid[0] = valid[6554] = 0
+    ok, _, used = oracle.par2_invert(valid, [0, 5, 6])
+    assert ok and len(used) == 2 and used[1] == 6 and used[0] in (0, 5)
+    ok, _, _ = oracle.par2_invert(valid, [0, 5])
+    assert not ok
+
+
+def test_gf16_field_axioms(oracle):
+    rng = np.random.default_rng(3)
+    for a, b, c in rng.integers(1, 65536, (200, 3)):
+        a, b, c = int(a), int(b), int(c)
+        assert oracle.gf16_mul(a, b) == oracle.gf16_mul(b, a)
+        assert oracle.gf16_mul(a, b ^ c) == oracle.gf16_mul(a, b) ^ oracle.gf16_mul(a, c)
+        assert oracle.gf16_mul(a, oracle.L.or_gf16_inv(a)) == 1
+
+
+# ---------------------------------------------------------------- vs _ref
+def test_oracle_vs_reference_par2(oracle, reference):
+    rng = np.random.default_rng(11)
+    for n, s, r in [(13, 1000, 5), (40, 4096, 16), (1, 2, 1), (7, 998, 3)]:
+        idx = rng.integers(0, 32768, n)
+        exps = rng.integers(0, 65535, r)
+        inp = rng.integers(0, 256, (n, s), dtype=np.uint8)
+        ref, _ = reference.par2_create(inp, s, idx, exps)
+        got = oracle.par2_muladd(list(inp), s, oracle.par2_coeff_matrix(idx, exps))
+        assert np.array_equal(got, ref)
+
+
+def test_oracle_vs_reference_par3(oracle, reference):
+    rng = np.random.default_rng(12)
+    for n, r, b, fi, fr in [(64, 8, 64, 0, 64), (17, 33, 40, 5, 100), (100, 1, 8, 0, 100), (16, 40, 24, 3, 7)]:
+        inp = rng.integers(0, 2**64, (n, b), dtype=np.uint64)
+        for kind in (0, 1, 2):
+            ref = reference.gf64_compute_recovery(kind, inp, r, fi, fr)
+            assert np.array_equal(oracle.gf64_compute_recovery(inp, r, fi, fr), ref), (n, r, kind)
+
+
+def test_oracle_vs_reference_par2_invert(oracle, reference):
+    rng = np.random.default_rng(13)
+    for n, miss, extra in [(50, 5, 2), (300, 30, 0), (12, 12, 3)]:
+        v = np.ones(n, dtype=np.uint8)
+        v[rng.choice(n, miss, replace=False)] = 0
+        rec = rng.choice(65535, miss + extra, replace=False).tolist()
+        a = oracle.par2_invert(v, rec)
+        b = reference.par2_invert(v, rec)
+        assert a[0] == b[0] and a[2] == b[2] and np.array_equal(a[1], b[1])

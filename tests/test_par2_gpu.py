@@ -1,0 +1,204 @@
+"""PAR2 / GF(2^16) parity on the GPU: the CUDA kernels through the C ABI
+against the golden fixtures and the oracle, bit-exact."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _host(t):
+    return t.cpu().numpy()
+
+
+def test_par2_create_golden(ctx, golden):
+    from parparpar_b200 import par2
+    g = golden("par2_create.npz")
+    for k in range(int(g["ncases"])):
+        inp, idx, exps, out = g[f"c{k}_inputs"], g[f"c{k}_idx"], g[f"c{k}_exps"], g[f"c{k}_out"]
+        got = par2.par2_create(inp, idx, exps, ctx=ctx)
+        assert np.array_equal(got, out), f"case {k}"
+        # same through device buffers
+        dout = _dev(np.zeros_like(out))
+        par2.par2_create(_dev(inp), idx, exps, out=dout, ctx=ctx)
+        ctx.synchronize()
+        assert np.array_equal(_host(dout), out), f"case {k} (device)"
+    got = par2.gf16_muladd(g["coef_inputs"], g["coef_coeffs"], ctx=ctx)
+    assert np.array_equal(got, g["coef_out"])
+
+
+@pytest.mark.parametrize("n,r,s", [
+    (1, 1, 2), (1, 3, 3), (7, 1, 16), (8, 4, 17), (9, 5, 1000), (33, 8, 8192), (33, 9, 8193),
+    (300, 17, 40000), (16, 16, 20000), (15, 15, 19998), (64, 2, 64 * 1024 + 6),
+])
+def test_gf16_muladd_vs_oracle(ctx, oracle, n, r, s):
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(n * 1000 + r * 10 + s)
+    inp = rng.integers(0, 256, (n, s), dtype=np.uint8)
+    co = rng.integers(0, 65536, (r, n)).astype(np.uint16)
+    co[:, 0] = 1  # exponent-0 style columns
+    if r > 1:
+        co[1, :] = 0
+    exp = oracle.par2_muladd(list(inp), s, co)
+    assert np.array_equal(par2.gf16_muladd(inp, co, ctx=ctx), exp)
+    # accumulate into existing contents
+    base = rng.integers(0, 256, (r, s), dtype=np.uint8)
+    out = base.copy()
+    par2.gf16_muladd(inp, co, out=out, accumulate=True, ctx=ctx)
+    assert np.array_equal(out, exp ^ base)
+
+
+def test_gf16_muladd_device_strided(ctx, oracle):
+    """Device rows with padding between them; bytes outside the slices are
+    neither read as data nor written."""
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(9)
+    n, r, s, stride = 20, 6, 1001, 1040
+    big = rng.integers(0, 256, (n, stride), dtype=np.uint8)
+    co = rng.integers(0, 65536, (r, n)).astype(np.uint16)
+    exp = oracle.par2_muladd([big[i, :s] for i in range(n)], s, co)
+    dout_np = rng.integers(0, 256, (r, stride), dtype=np.uint8)
+    dout = _dev(dout_np)
+    par2.gf16_muladd(_dev(big)[:, :s], co, out=dout[:, :s], slice_bytes=s, ctx=ctx)
+    ctx.synchronize()
+    got = _host(dout)
+    assert np.array_equal(got[:, :s], exp)
+    assert np.array_equal(got[:, s:], dout_np[:, s:]), "wrote past the slice"
+
+
+def test_gf16_muladd_split_inputs(ctx, oracle):
+    """Many inputs and a small slice: the launcher splits the input range
+    across blocks and combines with atomic XOR."""
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(10)
+    n, r, s = 2000, 8, 4096
+    inp = rng.integers(0, 256, (n, s), dtype=np.uint8)
+    co = rng.integers(0, 65536, (r, n)).astype(np.uint16)
+    exp = oracle.par2_muladd(list(inp), s, co)
+    assert np.array_equal(par2.gf16_muladd(inp, co, ctx=ctx), exp)
+    out = _dev(np.zeros((r, s), dtype=np.uint8))
+    par2.gf16_muladd(_dev(inp), _dev(co), out=out, ctx=ctx)
+    ctx.synchronize()
+    assert np.array_equal(_host(out), exp)
+
+
+def _ctrl_case(ctx, oracle, slice_size, last, n_in, n_out, seed, batch=0, areas=2):
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(seed)
+    idx = rng.integers(0, 0x8000, n_in).astype(np.uint16)
+    exps = rng.integers(0, 0xFFFF, n_out).astype(np.uint16)
+    exps[0] = 0
+    src = [rng.integers(0, 256, slice_size if i < n_in - 1 else last, dtype=np.uint8) for i in range(n_in)]
+    proc = par2.PAR2ProcCUDA(slice_size, areas, batch, ctx=ctx)
+    assert proc.setRecoverySlices(n_out, exps)
+    for i in range(n_in):
+        proc.waitForAdd()
+        proc.addInput(src[i], src[i].size, int(idx[i]))
+    proc.endInput()
+    exp = oracle.par2_muladd(src, slice_size, oracle.par2_coeff_matrix(idx, exps))
+    for o in range(n_out):
+        buf = np.zeros(slice_size, dtype=np.uint8)
+        assert proc.getOutput(o, buf)
+        assert np.array_equal(buf, exp[o]), (slice_size, last, n_in, n_out, o)
+    proc.deinit()
+
+
+def test_proc_test_ctrl_grid(ctx, oracle):
+    """The grid of test/gf16/test-ctrl.cpp:281-306: slice sizes {2, 19998,
+    20000}, last-slice sizes {1, 2, S-1, S}, 1/15/16 inputs x 1/15/16 outputs."""
+    seed = 0x01020304
+    for s in (2, 19998, 20000):
+        lasts = [1, 2] + ([s - 1, s] if s > 2 else [])
+        for last in lasts:
+            for n_out in (1, 15, 16):
+                for n_in in (1, 15, 16):
+                    if n_in == 1 and last != s:
+                        continue
+                    if last != s and last != 1 and (n_in > 15 or n_out > 2):
+                        continue
+                    seed += 1
+                    _ctrl_case(ctx, oracle, s, last, n_in, n_out, seed)
+
+
+def test_proc_batches_and_reuse(ctx, oracle):
+    from parparpar_b200 import par2
+    # small batch to exercise several staging areas, flush, and a second pass
+    _ctrl_case(ctx, oracle, 4096, 4096, 50, 5, 77, batch=4, areas=3)
+    rng = np.random.default_rng(78)
+    proc = par2.PAR2ProcCUDA(2048, 2, 3, ctx=ctx)
+    proc.setRecoverySlices(3, [0, 1, 2])
+    data = rng.integers(0, 256, (7, 2048), dtype=np.uint8)
+    for rnd in range(2):
+        for i in range(7):
+            proc.waitForAdd()
+            proc.addInput(data[i], 2048, i, flush=(i == 3))
+        proc.endInput()
+        exp = oracle.par2_muladd(list(data), 2048, oracle.par2_coeff_matrix(range(7), [0, 1, 2]))
+        for o in range(3):
+            buf = np.zeros(2048, dtype=np.uint8)
+            proc.getOutput(o, buf)
+            assert np.array_equal(buf, exp[o])
+        proc.discardOutput()
+    # decode overload: explicit coefficients per input
+    co = rng.integers(0, 65536, (7, 3)).astype(np.uint16)
+    for i in range(7):
+        proc.waitForAdd()
+        proc.addInput(data[i], 2048, co[i])
+    proc.endInput()
+    exp = oracle.par2_muladd(list(data), 2048, co.T.copy())
+    for o in range(3):
+        buf = np.zeros(2048, dtype=np.uint8)
+        proc.getOutput(o, buf)
+        assert np.array_equal(buf, exp[o])
+    proc.deinit()
+
+
+def test_par2_invert_golden(ctx, golden):
+    from parparpar_b200 import par2
+    g = golden("par2_invert.npz")
+    for k in range(int(g["ncases"])):
+        valid = [bool(x) for x in g[f"c{k}_valid"]]
+        rec = [int(x) for x in g[f"c{k}_rec"]]
+        m = par2.Galois16RecMatrix(ctx=ctx)
+        ok = m.Compute(valid, sum(valid), rec)
+        assert ok == bool(g[f"c{k}_ok"]), f"case {k}"
+        if ok:
+            assert rec == [int(x) for x in g[f"c{k}_used"]]
+            assert np.array_equal(m.factors, g[f"c{k}_factors"]), f"case {k}"
+
+
+def test_par2_invert_vs_oracle(ctx, oracle):
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(21)
+    for n, miss, extra in [(1000, 40, 3), (32768, 8, 0), (257, 257, 1)]:
+        v = np.ones(n, dtype=np.uint8)
+        v[rng.choice(n, miss, replace=False)] = 0
+        rec = sorted(rng.choice(65535, miss + extra, replace=False).tolist())
+        ok, f, used = oracle.par2_invert(v, rec)
+        m = par2.Galois16RecMatrix(ctx=ctx)
+        r2 = list(rec)
+        assert m.Compute([bool(x) for x in v], int(v.sum()), r2) == ok
+        assert r2 == used and np.array_equal(m.factors, f)
+
+
+def test_par2_repair_roundtrip(ctx):
+    """create -> erase -> invert -> decode restores the erased slices."""
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(31)
+    n, s, r = 500, 8192, 12
+    data = rng.integers(0, 256, (n, s), dtype=np.uint8)
+    exps = list(range(r))
+    rec = par2.par2_create(data, np.arange(n), exps, ctx=ctx)
+    lost = sorted(rng.choice(n, 10, replace=False).tolist())
+    valid = np.ones(n, dtype=bool)
+    valid[lost] = False
+    m = par2.Galois16RecMatrix(ctx=ctx)
+    used = list(exps)
+    assert m.Compute(list(valid), int(valid.sum()), used)
+    srcs = np.concatenate([data[valid], rec[[exps.index(e) for e in used]]], axis=0)
+    restored = par2.gf16_muladd(srcs, m.factors, ctx=ctx)
+    assert np.array_equal(restored, data[lost])

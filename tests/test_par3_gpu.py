@@ -1,0 +1,185 @@
+"""PAR3 / GF(2^64) parity on the GPU: the CUDA kernels through the C ABI
+against the golden fixtures and the oracle, bit-exact."""
+import zlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+
+
+def _host(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
+def test_par3_golden_all_kernels(ctx, golden):
+    from parparpar_b200 import par3
+    g = golden("par3_golden.npz")
+    inp = g["inputs"]
+    for fn in (par3.compute_recovery, par3.compute_recovery_full, par3.compute_recovery_barycentric,
+               par3.compute_recovery_fenger):
+        out = np.zeros((2, 128), dtype=np.uint64)
+        fn(inp, out, 5, 2, 1024, 0, 5)
+        assert zlib.crc32(out.tobytes()) == 0x6A941C15, fn.__name__
+
+
+def test_gf64_ops_golden(ctx, golden):
+    from parparpar_b200 import par3
+    g = golden("gf64_ops.npz")
+    a, b = g["a"], g["b"]
+    out = np.zeros_like(a)
+    for i in range(0, 64):
+        par3.gf64_region_mul(out[i:i + 1], a[i:i + 1], 1, int(b[i]), ctx)
+    assert np.array_equal(out[:64], g["prod"][:64])
+    par3.gf64_region_mul_arr(out, a, b, a.size, 1)  # n_coeff=1: all by b[0]
+    inv = np.zeros_like(a)
+    par3.gf64_inverse_batch(inv, a, a.size, ctx)
+    assert np.array_equal(inv, g["inv"])
+    assert np.array_equal(par3.GF64Controller.BuildCauchyMatrixAlloc(37, 9, 3, 40), g["cauchy"])
+    assert np.array_equal(par3.GF64Controller.BuildCauchyMatrixAlloc(8, 4, 0, 2), g["cauchy_clash"])
+    out = np.zeros((7, 96), dtype=np.uint64)
+    par3.GF64Controller.ComputeRecoveryBlocks(g["inp"], 33, out, 7, 96, 0, 33)
+    assert np.array_equal(out, g["matvec"])
+    out = g["acc0"].copy()
+    par3.GF64Controller.ComputeRecoveryBlocks(g["inp"], 33, out, 7, 96, 0, 33, accumulate=True)
+    assert np.array_equal(out, g["matvec_acc"])
+    A, rhs = g["A"].copy(), g["rhs"].copy()
+    assert par3.GF64Controller.SolveAndReconstruct(A, rhs, A.shape[0], rhs.shape[1]) == 0
+    assert np.array_equal(rhs, g["solved"])
+    assert par3.GF64Controller.SolveAndReconstruct(g["sing"].copy(), g["sing_rhs"].copy(), 3, 4) == -1
+
+
+def test_region_elementwise_vs_oracle(ctx, oracle):
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(40)
+    for n in (1, 7, 1000, 4097):
+        x = rng.integers(0, 2**64, n, dtype=np.uint64)
+        for nc in (1, 3, 8):
+            c = rng.integers(0, 2**64, nc, dtype=np.uint64)
+            out = np.zeros(n, dtype=np.uint64)
+            par3.gf64_region_mul_arr(out, x, c, n, nc)
+            assert np.array_equal(out, oracle.gf64_region("mul_arr", x, c, np.zeros(n, dtype=np.uint64)))
+            base = rng.integers(0, 2**64, n, dtype=np.uint64)
+            out = base.copy()
+            par3.gf64_region_muladd_arr(out, x, c, n, nc)
+            assert np.array_equal(out, oracle.gf64_region("muladd_arr", x, c, base.copy()))
+        out = np.zeros(n, dtype=np.uint64)
+        par3.gf64_region_mul(out, x, n, 0xDEADBEEFCAFEBABE)
+        assert np.array_equal(out, oracle.gf64_region("mul", x, 0xDEADBEEFCAFEBABE, np.zeros(n, dtype=np.uint64)))
+
+
+@pytest.mark.parametrize("n,r,b,fi,fr", [
+    (1, 1, 1, 0, 1), (2, 7, 3, 0, 2), (5, 8, 128, 0, 5), (64, 9, 1000, 0, 64), (257, 33, 1025, 0, 257),
+    (300, 8, 1024, 0, 300), (40, 17, 64, 5, 3), (1024, 1, 2048, 0, 1024), (3000, 8, 16, 0, 3000),
+])
+def test_compute_recovery_vs_oracle(ctx, oracle, n, r, b, fi, fr):
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(n + r * 7 + b * 13)
+    inp = rng.integers(0, 2**64, (n, b), dtype=np.uint64)
+    exp = oracle.gf64_compute_recovery(inp, r, fi, fr)
+    out = np.zeros((r, b), dtype=np.uint64)
+    par3.GF64Controller.ComputeRecoveryBlocks(inp, n, out, r, b, fi, fr)
+    assert np.array_equal(out, exp)
+    base = rng.integers(0, 2**64, (r, b), dtype=np.uint64)
+    out = base.copy()
+    par3.GF64Controller.ComputeRecoveryBlocks(inp, n, out, r, b, fi, fr, accumulate=True)
+    assert np.array_equal(out, exp ^ base)
+    # device-resident buffers
+    dout = _dev(np.zeros((r, b), dtype=np.uint64))
+    par3.GF64Controller.ComputeRecoveryBlocks(_dev(inp), n, dout, r, b, fi, fr)
+    ctx.synchronize()
+    assert np.array_equal(_host(dout), exp)
+
+
+def test_with_coeff_and_build(ctx, oracle):
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(41)
+    n, r, b = 70, 11, 300
+    coeff = rng.integers(0, 2**64, (r, n), dtype=np.uint64)
+    inp = rng.integers(0, 2**64, (n, b), dtype=np.uint64)
+    out = np.zeros((r, b), dtype=np.uint64)
+    par3.GF64Controller.ComputeRecoveryBlocksWithCoeff(inp, n, out, r, b, coeff)
+    assert np.array_equal(out, oracle.gf64_matvec(inp, coeff))
+    m = np.zeros((r, n), dtype=np.uint64)
+    par3.GF64Controller.BuildCauchyMatrix(m, n, r, 2**40 + 3, 2**41 + 5)
+    assert np.array_equal(m, oracle.gf64_build_cauchy(n, r, 2**40 + 3, 2**41 + 5))
+    dm = _dev(np.zeros((r, n), dtype=np.uint64))
+    par3.GF64Controller.BuildCauchyMatrix(dm, n, r, 7, 1000)
+    ctx.synchronize()
+    assert np.array_equal(_host(dm), oracle.gf64_build_cauchy(n, r, 7, 1000))
+
+
+def test_pointer_table_region_ops(ctx, oracle):
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(42)
+    L, K, G = 777, 5, 9
+    ins = [rng.integers(0, 2**64, L, dtype=np.uint64) for _ in range(G)]
+    C = rng.integers(0, 2**64, (K, 12), dtype=np.uint64)  # K_stride 12 > G
+    outs = [rng.integers(0, 2**64, L, dtype=np.uint64) for _ in range(K)]
+    exp = [o.copy() for o in outs]
+    for k in range(K):
+        for g in range(G):
+            oracle.gf64_region("muladd_arr", ins[g], C[k, g], exp[k])
+    par3.gf64_region_2d_muladd_arr(outs, K, ins, G, C, 12, L)
+    for k in range(K):
+        assert np.array_equal(outs[k], exp[k])
+    # coupled: G inputs -> 1 output
+    out = rng.integers(0, 2**64, L, dtype=np.uint64)
+    e = out.copy()
+    cb = C[0, :G].copy()
+    for g in range(G):
+        oracle.gf64_region("muladd_arr", ins[g], cb[g], e)
+    par3.gf64_region_coupled_muladd_arr(out, ins, cb, L, G)
+    assert np.array_equal(out, e)
+    # fused output: 1 input -> K outputs, device buffers
+    douts = [_dev(o) for o in outs]
+    starts = [C[k, 3:4].copy() for k in range(K)]
+    e = [o.copy() for o in outs]
+    for k in range(K):
+        oracle.gf64_region("muladd_arr", ins[0], starts[k][0], e[k])
+    par3.gf64_region_fused_output_muladd_arr(douts, _dev(ins[0]), starts, L, K)
+    for k in range(K):
+        assert np.array_equal(_host(douts[k]), e[k])
+
+
+def test_solve_vs_oracle(ctx, oracle):
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(43)
+    for n, b in [(1, 5), (2, 1), (17, 33), (120, 64)]:
+        # a Cauchy submatrix with one zero forcing a row swap
+        A = oracle.gf64_build_cauchy(400, n, 0, 400)[:, rng.choice(400, n, replace=False)].copy()
+        if n > 1:
+            A[0, 0] = 0
+        rhs = rng.integers(0, 2**64, (n, b), dtype=np.uint64)
+        A1, r1 = A.copy(), rhs.copy()
+        rc = oracle.gf64_solve_and_reconstruct(A1, r1)
+        A2, r2 = A.copy(), rhs.copy()
+        assert par3.GF64Controller.SolveAndReconstruct(A2, r2, n, b) == rc
+        if rc == 0:
+            assert np.array_equal(r2, r1)
+            assert np.array_equal(A2, A1)
+
+
+def test_par3_repair_roundtrip(ctx):
+    """create -> erase -> (RHS via with_coeff) -> solve restores the blocks."""
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(44)
+    N, R, B = 400, 16, 256
+    data = rng.integers(0, 2**64, (N, B), dtype=np.uint64)
+    rec = np.zeros((R, B), dtype=np.uint64)
+    par3.GF64Controller.ComputeRecoveryBlocks(data, N, rec, R, B, 0, N)
+    lost = np.sort(rng.choice(N, 10, replace=False))
+    n = lost.size
+    M = par3.GF64Controller.BuildCauchyMatrixAlloc(N, n, 0, N)
+    known = np.setdiff1d(np.arange(N), lost)
+    A = np.ascontiguousarray(M[:, lost])
+    rhs = rec[:n].copy()
+    par3.GF64Controller.ComputeRecoveryBlocksWithCoeff(np.ascontiguousarray(data[known]), known.size, rhs, n, B,
+                                                       np.ascontiguousarray(M[:, known]), accumulate=True)
+    assert par3.GF64Controller.SolveAndReconstruct(A, rhs, n, B) == 0
+    assert np.array_equal(rhs, data[lost])
