@@ -79,6 +79,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t_end = time.time() + 3.0
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
@@ -325,17 +328,20 @@ def main():
 
     import parparpar_b200 as pp
     ctx = pp.Context(local)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream shared by the library's launches and
+    # the timing events
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     timer = Timer(stream)
     peak, peak_kind = load_peaks()
 
     job = setup_job(args.workload, local, 1234 + rank, ctx)
     f = step_fn(job, ctx)
+    sampler = ClockSampler(gpu_uuid(local))
     for _ in range(args.warmup):
         f()
     torch.cuda.synchronize()
-    sampler = ClockSampler(gpu_uuid(local))
     if dist:
         dist.barrier()
     torch.cuda.synchronize()

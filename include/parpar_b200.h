@@ -211,6 +211,16 @@ PP_API int pp_gf64_region_2d_muladd_arr(pp_ctx* ctx, uint64_t* const* outs, size
  * gf64/gf64_invert.c:71-75). */
 PP_API int pp_gf64_inverse_batch(pp_ctx* ctx, uint64_t* out, const uint64_t* in, size_t n);
 
+/* Additive FFT over GF(2^64), novel-polynomial basis on the Cantor basis
+ * (replaces gf64_addfft64_fwd_recursive_scratch / _inv_recursive_scratch,
+ * gf64/gf64_additive_fft_hqc2026.c:1656-1705).  Batched: `batch` polynomials
+ * of n coefficients, coefficient c of polynomial b at data[c * ld + b]
+ * (batch = ld = 1 is the reference's single-array call).  n must be a power
+ * of two <= 2^20; n <= 1 is a no-op.  The inverse is not normalised, as in the
+ * reference. */
+PP_API int pp_gf64_fft_fwd(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld);
+PP_API int pp_gf64_fft_inv(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld);
+
 #ifdef __cplusplus
 }
 #endif

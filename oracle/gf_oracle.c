@@ -303,3 +303,144 @@ void or_gf64_region_muladd_arr(uint64_t* out, const uint64_t* in, const uint64_t
 		out[i] ^= s;
 	}
 }
+
+/* ======================================================================= */
+/* Additive FFT over GF(2^64), novel-polynomial basis on the Cantor basis   */
+/* ======================================================================= */
+/* Restates gf64_addfft64_{fwd,inv}_recursive_scratch
+ * (gf64/gf64_additive_fft_hqc2026.c:1656-1705):
+ *   forward = monomial -> novel-polynomial basis conversion (hqc_cvt,
+ *             :1011-1017, an XOR-only network), then the radix-2 butterflies
+ *             (butterfly_fwd, :1068-1086) with affine shift v_{n/2};
+ *   inverse = inverse butterflies (:1088-1108), then the inverse conversion.
+ * The Cantor basis v_0..v_19 (gf64/gf64_cantor_basis.h:20-44) satisfies
+ * v_0 = 1 and v_{i+1}^2 + v_{i+1} = v_i; it is regenerated here from that
+ * recurrence (below) and checked against the reference's fixtures.  With
+ * v_j = XOR of basis vectors at the set bits of j, the butterfly twiddle of
+ * block t at depth d (block size n >> d) is v_{2^d XOR 2t}: the recursion's
+ * s_{logn-1}(v_j) = v_{j >> (logn-1)} evaluated on the shift index
+ * 2^(L-1) XOR (t << (L-d)). */
+static uint64_t cantor[20];
+static int cantor_ready = 0;
+
+/* Solve y^2 + y = c over GF(2^64): the map y -> y^2 + y is GF(2)-linear with
+ * kernel {0, 1}; solve by Gaussian elimination over GF(2) and return the
+ * solution with bit 0 clear.  Returns 0 when c has no solution. */
+static int solve_artin_schreier(uint64_t c, uint64_t* out) {
+	uint64_t col[64];
+	for (int j = 0; j < 64; j++) {
+		uint64_t e = 1ull << j;
+		col[j] = or_gf64_mul(e, e) ^ e; /* image of basis vector x^j */
+	}
+	/* augmented system rows: row i = bit i of the images; solve L y = c */
+	uint64_t rows[64];
+	uint64_t rhs = 0;
+	for (int i = 0; i < 64; i++) {
+		uint64_t r = 0;
+		for (int j = 0; j < 64; j++) r |= ((col[j] >> i) & 1ull) << j;
+		rows[i] = r;
+		rhs |= ((c >> i) & 1ull) << i;
+	}
+	int pivcol[64];
+	int rank = 0;
+	for (int j = 0; j < 64 && rank < 64; j++) {
+		int p = -1;
+		for (int i = rank; i < 64; i++) if ((rows[i] >> j) & 1) { p = i; break; }
+		if (p < 0) continue;
+		uint64_t t = rows[p]; rows[p] = rows[rank]; rows[rank] = t;
+		uint64_t b1 = (rhs >> p) & 1, b2 = (rhs >> rank) & 1;
+		rhs &= ~((1ull << p) | (1ull << rank));
+		rhs |= (b1 << rank) | (b2 << p);
+		for (int i = 0; i < 64; i++) {
+			if (i != rank && ((rows[i] >> j) & 1)) {
+				rows[i] ^= rows[rank];
+				rhs ^= ((rhs >> rank) & 1ull) << i;
+			}
+		}
+		pivcol[rank++] = j;
+	}
+	for (int i = rank; i < 64; i++) if ((rhs >> i) & 1) return 0;
+	uint64_t y = 0;
+	for (int i = 0; i < rank; i++) if ((rhs >> i) & 1) y |= 1ull << pivcol[i];
+	if (y & 1) y ^= 1; /* pick the root with bit 0 clear (y and y+1 both solve) */
+	*out = y;
+	return 1;
+}
+
+uint64_t or_gf64_cantor(int i) {
+	if (!cantor_ready) {
+		cantor[0] = 1;
+		for (int k = 1; k < 20; k++) solve_artin_schreier(cantor[k - 1], &cantor[k]);
+		cantor_ready = 1;
+	}
+	return cantor[i];
+}
+
+static uint64_t vj(uint64_t j) {
+	uint64_t v = 0;
+	for (int k = 0; k < 20; k++) if ((j >> k) & 1) v ^= or_gf64_cantor(k);
+	return v;
+}
+
+static int ilog2(size_t n) { int l = 0; while (((size_t)1 << l) < n) l++; return l; }
+
+/* hqc_cvt: recursive XOR network, monomial -> novel polynomial basis */
+static int choose_si(int n) { int si = 1; for (int i = 1; (1 << i) < n; i++) si = 1 << i; return si; }
+static void cvt(uint64_t* d, int len, int lb, int pl) {
+	if (pl <= 1) return;
+	int si = choose_si(pl);
+	for (int i = pl - 1; i >= si; i--) {
+		int polylen = 1 << (i + lb + 1), sh = 1 << (i + lb), sl = 1 << (i + lb - si), dd = sh - sl;
+		for (int j = 0; j < len; j += polylen)
+			for (int k = polylen - 1; k >= sh; k--) d[j + k - dd] ^= d[j + k];
+	}
+	cvt(d, len, lb, si);
+	cvt(d, len, lb + si, pl - si);
+}
+static void icvt(uint64_t* d, int len, int lb, int pl) {
+	if (pl <= 1) return;
+	int si = choose_si(pl);
+	icvt(d, len, lb, si);
+	icvt(d, len, lb + si, pl - si);
+	for (int i = si; i < pl; i++) {
+		int polylen = 1 << (i + lb + 1), sh = 1 << (i + lb), sl = 1 << (i + lb - si), dd = sh - sl;
+		for (int j = 0; j < len; j += polylen)
+			for (int k = sh; k < polylen; k++) d[j + k - dd] ^= d[j + k];
+	}
+}
+
+void or_gf64_fft_fwd(uint64_t* a, size_t n) {
+	if (n <= 1) return;
+	int L = ilog2(n);
+	cvt(a, (int)n, 0, L);
+	for (int d = 0; d < L; d++) {
+		size_t h = n >> (d + 1);
+		for (size_t t = 0; t < ((size_t)1 << d); t++) {
+			uint64_t w = vj(((uint64_t)1 << d) ^ (2 * t));
+			uint64_t* f = a + t * 2 * h;
+			for (size_t k = 0; k < h; k++) {
+				uint64_t lo = f[k] ^ or_gf64_mul(w, f[k + h]);
+				f[k + h] ^= lo;
+				f[k] = lo;
+			}
+		}
+	}
+}
+
+void or_gf64_fft_inv(uint64_t* a, size_t n) {
+	if (n <= 1) return;
+	int L = ilog2(n);
+	for (int d = L - 1; d >= 0; d--) {
+		size_t h = n >> (d + 1);
+		for (size_t t = 0; t < ((size_t)1 << d); t++) {
+			uint64_t w = vj(((uint64_t)1 << d) ^ (2 * t));
+			uint64_t* f = a + t * 2 * h;
+			for (size_t k = 0; k < h; k++) {
+				uint64_t fh = f[k] ^ f[k + h];
+				f[k] ^= or_gf64_mul(w, fh);
+				f[k + h] = fh;
+			}
+		}
+	}
+	icvt(a, (int)n, 0, L);
+}

@@ -53,6 +53,11 @@ void or_gf64_region_mul_arr(uint64_t* out, const uint64_t* in, const uint64_t* c
 void or_gf64_region_muladd_arr(uint64_t* out, const uint64_t* in, const uint64_t* coeff,
                                size_t len, size_t nCoeff);
 
+/* additive FFT, novel-polynomial basis on the Cantor basis; n a power of 2 */
+uint64_t or_gf64_cantor(int i);
+void or_gf64_fft_fwd(uint64_t* a, size_t n);
+void or_gf64_fft_inv(uint64_t* a, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -137,6 +137,11 @@ class Oracle:
         b = rhs.shape[1] if rhs.ndim == 2 else 0
         return self.L.or_gf64_solve_and_reconstruct(_ptr(A), _ptr(rhs), _SZ(n), _SZ(b))
 
+    def gf64_fft(self, a: np.ndarray, inverse: bool = False) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.uint64).copy()
+        (self.L.or_gf64_fft_inv if inverse else self.L.or_gf64_fft_fwd)(_ptr(a), _SZ(a.size))
+        return a
+
     def gf64_region(self, op: str, inp: np.ndarray, coeff, out: np.ndarray) -> np.ndarray:
         c = np.ascontiguousarray(np.atleast_1d(np.asarray(coeff, dtype=np.uint64)))
         if op == "mul":

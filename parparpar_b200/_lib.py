@@ -46,7 +46,7 @@ EXPORTS = [
     "pp_gf64_compute_recovery", "pp_gf64_compute_recovery_with_coeff", "pp_gf64_solve_and_reconstruct",
     "pp_gf64_region_mul", "pp_gf64_region_mul_arr", "pp_gf64_region_muladd_arr",
     "pp_gf64_region_coupled_muladd_arr", "pp_gf64_region_fused_output_muladd_arr",
-    "pp_gf64_region_2d_muladd_arr", "pp_gf64_inverse_batch",
+    "pp_gf64_region_2d_muladd_arr", "pp_gf64_inverse_batch", "pp_gf64_fft_fwd", "pp_gf64_fft_inv",
 ]
 
 
@@ -122,6 +122,8 @@ _sig("pp_gf64_region_coupled_muladd_arr", _I, _P, _P, _P, _P, _SZ, _SZ)
 _sig("pp_gf64_region_fused_output_muladd_arr", _I, _P, _P, _P, _P, _SZ, _SZ)
 _sig("pp_gf64_region_2d_muladd_arr", _I, _P, _P, _SZ, _P, _SZ, _P, _SZ, _SZ)
 _sig("pp_gf64_inverse_batch", _I, _P, _P, _P, _SZ)
+_sig("pp_gf64_fft_fwd", _I, _P, _P, _SZ, _SZ, _SZ)
+_sig("pp_gf64_fft_inv", _I, _P, _P, _SZ, _SZ, _SZ)
 
 
 def status_string(s: int) -> str:

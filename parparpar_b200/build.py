@@ -21,6 +21,7 @@ OBJ_DIR = os.path.join(HERE, "_build")
 SOURCES = [
     "gf16_kernels.cu",
     "gf64_kernels.cu",
+    "gf64_fft.cu",
     "capi.cpp",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -1044,4 +1044,39 @@ PP_API int pp_gf64_inverse_batch(pp_ctx* ctx, uint64_t* out, const uint64_t* in,
   return PP_OK;
 }
 
+static int gf64_fft_common(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld, bool inverse) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (n <= 1 || batch == 0) return PP_OK;
+  if (!data) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if ((n & (n - 1)) != 0 || n > ((size_t)1 << 20))
+    return set_err(ctx, PP_ERR_INVALID_ARG, "n must be a power of two <= 2^20");
+  if (ld < batch) return set_err(ctx, PP_ERR_INVALID_ARG, "ld < batch");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const bool dev = is_device_ptr(data);
+  uint64_t* d = data;
+  size_t dld = ld;
+  if (!dev) {
+    dld = batch;
+    d = (uint64_t*)scratch(ctx, S_IN, n * batch * 8);
+    if (!d) return set_err(ctx, PP_ERR_NO_MEMORY, "fft staging");
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(d, dld * 8, data, ld * 8, batch * 8, n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  uint64_t* tmp = (uint64_t*)scratch(ctx, S_OUT, n * dld * 8);
+  if (!tmp) return set_err(ctx, PP_ERR_NO_MEMORY, "fft scratch");
+  CUDA_TRY(ctx, launch_gf64_fft(d, tmp, n, batch, dld, inverse, ctx->stream));
+  if (!dev) {
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(data, ld * 8, d, dld * 8, batch * 8, n, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return PP_OK;
+}
+
+PP_API int pp_gf64_fft_fwd(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld) {
+  return gf64_fft_common(ctx, data, n, batch, ld, false);
+}
+PP_API int pp_gf64_fft_inv(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld) {
+  return gf64_fft_common(ctx, data, n, batch, ld, true);
+}
+
 }  // extern "C"

@@ -239,6 +239,37 @@ def gf64_inverse_batch(out, inp, n, ctx=None):
     c.check(lib.pp_gf64_inverse_batch(c.h, ptr(out), ptr(inp), n))
 
 
+def gf64_addfft64_fwd(arr, n=None, batch=1, ld=None, ctx=None):
+    """Forward additive FFT (gf64_addfft64_fwd_recursive_scratch), in place.
+    1-D: one polynomial; 2-D (n, batch): one polynomial per column."""
+    c = _ctx(ctx)
+    n, batch, ld = _fft_shape(arr, n, batch, ld)
+    c.check(lib.pp_gf64_fft_fwd(c.h, ptr(arr), n, batch, ld))
+    return arr
+
+
+def gf64_addfft64_inv(arr, n=None, batch=1, ld=None, ctx=None):
+    """Inverse additive FFT (gf64_addfft64_inv_recursive_scratch), in place,
+    not normalised."""
+    c = _ctx(ctx)
+    n, batch, ld = _fft_shape(arr, n, batch, ld)
+    c.check(lib.pp_gf64_fft_inv(c.h, ptr(arr), n, batch, ld))
+    return arr
+
+
+def _fft_shape(arr, n, batch, ld):
+    shape = tuple(arr.shape)
+    if len(shape) == 2:
+        n = shape[0] if n is None else n
+        batch = shape[1]
+        ld = (arr.stride(0) if hasattr(arr, "stride") and callable(arr.stride) else arr.strides[0] // 8) \
+            if ld is None else ld
+    else:
+        n = shape[0] if n is None else n
+        ld = 1 if ld is None else ld
+    return n, batch, ld
+
+
 class Gf64Encoder:
     """gf64_addon Gf64Encoder (src/gf64_addon.cc:446,835 and export table)."""
 

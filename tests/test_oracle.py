@@ -113,3 +113,31 @@ def test_oracle_vs_reference_par2_invert(oracle, reference):
         a = oracle.par2_invert(v, rec)
         b = reference.par2_invert(v, rec)
         assert a[0] == b[0] and a[2] == b[2] and np.array_equal(a[1], b[1])
+
+
+def test_gf64_fft_golden(oracle, golden):
+    """Additive FFT forward/inverse vs the reference's
+    gf64_addfft64_{fwd,inv}_recursive_scratch outputs."""
+    g = golden("gf64_fft.npz")
+    for n in g["sizes"]:
+        n = int(n)
+        assert np.array_equal(oracle.gf64_fft(g[f"x{n}"]), g[f"fwd{n}"]), n
+        assert np.array_equal(oracle.gf64_fft(g[f"x{n}"], inverse=True), g[f"inv{n}"]), n
+
+
+def test_gf64_fft_cantor_basis(oracle):
+    # v_0 = 1 and v_{i+1}^2 + v_{i+1} = v_i (gf64/gf64_cantor_basis.h:8-13)
+    import ctypes
+    oracle.L.or_gf64_cantor.restype = ctypes.c_uint64
+    v = [oracle.L.or_gf64_cantor(i) for i in range(20)]
+    assert v[0] == 1 and v[19] == 0x4A8DCF8BD7EDE826
+    for i in range(19):
+        assert oracle.gf64_mul(v[i + 1], v[i + 1]) ^ v[i + 1] == v[i]
+
+
+def test_oracle_vs_reference_fft(oracle, reference):
+    rng = np.random.default_rng(14)
+    for n in (2, 32, 512, 8192, 65536):
+        x = rng.integers(0, 2**64, n, dtype=np.uint64)
+        assert np.array_equal(oracle.gf64_fft(x), reference.gf64_fft_fwd(x)), n
+        assert np.array_equal(oracle.gf64_fft(x, True), reference.gf64_fft_inv(x)), n
