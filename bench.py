@@ -307,6 +307,7 @@ def main():
     ap.add_argument("--workload", default=PRIMARY, choices=sorted(WORKLOADS))
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gf16-kernel", default="auto", choices=["auto", "lut", "tensor"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -333,6 +334,7 @@ def main():
     stream = torch.cuda.Stream(device=local)
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
+    ctx.set_gf16_kernel({"auto": 0, "lut": 1, "tensor": 2}[args.gf16_kernel])
     timer = Timer(stream)
     peak, peak_kind = load_peaks()
 

@@ -49,6 +49,7 @@ extern "C" {
 #define PP_ERR_BUSY (-6)          /* PAR2 processor staging area full (reference PROC_ADD_FULL) */
 #define PP_ERR_NO_DEVICE (-7)
 #define PP_ERR_UNSUPPORTED (-8)
+#define PP_ERR_TIMEOUT (-9)       /* a bounded device-side wait gave up (kernel returned early) */
 
 /* reference PAR2ProcBackendAddResult (gf16/controller.h:38-43) */
 #define PP_PROC_ADD_OK 0
@@ -62,6 +63,11 @@ extern "C" {
 #define PP_GF64_KERNEL_MATVEC 1
 #define PP_GF64_KERNEL_BARYCENTRIC 2
 #define PP_GF64_KERNEL_FENGER 3
+
+/* GF(2^16) region kernel selection (pp_ctx_set_gf16_kernel) */
+#define PP_GF16_KERNEL_AUTO 0
+#define PP_GF16_KERNEL_LUT 1      /* shared-memory 4-bit split tables */
+#define PP_GF16_KERNEL_TENSOR 2   /* tcgen05 u8 MMA over the GF(2) bit matrices */
 
 typedef struct pp_ctx pp_ctx;
 typedef struct pp_par2_proc pp_par2_proc;
@@ -81,6 +87,8 @@ PP_API const char* pp_ctx_last_error(pp_ctx* ctx);
 PP_API uint64_t pp_launch_count(void);
 /* Drop cached device buffers (scratch, coefficient matrices). */
 PP_API int pp_ctx_free_cache(pp_ctx* ctx);
+/* Choose the GF(2^16) region kernel used by this context (PP_GF16_KERNEL_*). */
+PP_API int pp_ctx_set_gf16_kernel(pp_ctx* ctx, int kernel);
 
 /* ============================================================ PAR2 / GF16 */
 

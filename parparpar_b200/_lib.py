@@ -23,6 +23,11 @@ PP_ERR_NOT_INVERTIBLE = -5
 PP_ERR_BUSY = -6
 PP_ERR_NO_DEVICE = -7
 PP_ERR_UNSUPPORTED = -8
+PP_ERR_TIMEOUT = -9
+
+PP_GF16_KERNEL_AUTO = 0
+PP_GF16_KERNEL_LUT = 1
+PP_GF16_KERNEL_TENSOR = 2
 
 PP_PROC_ADD_OK = 0
 PP_PROC_ADD_OK_BUSY = 1
@@ -37,6 +42,7 @@ PP_GF64_KERNEL_FENGER = 3
 EXPORTS = [
     "pp_version", "pp_status_string", "pp_ctx_create", "pp_ctx_destroy", "pp_ctx_set_stream",
     "pp_ctx_get_stream", "pp_ctx_synchronize", "pp_ctx_last_error", "pp_launch_count", "pp_ctx_free_cache",
+    "pp_ctx_set_gf16_kernel",
     "pp_par2_coeff", "pp_par2_input_log", "pp_par2_coeff_matrix", "pp_gf16_muladd", "pp_par2_create",
     "pp_par2_invert", "pp_par2_proc_create", "pp_par2_proc_destroy", "pp_par2_proc_set_current_slice_size",
     "pp_par2_proc_set_recovery_slices", "pp_par2_proc_can_add", "pp_par2_proc_wait_for_add",
@@ -90,6 +96,7 @@ _sig("pp_ctx_synchronize", _I, _P)
 _sig("pp_ctx_last_error", ctypes.c_char_p, _P)
 _sig("pp_launch_count", _U64)
 _sig("pp_ctx_free_cache", _I, _P)
+_sig("pp_ctx_set_gf16_kernel", _I, _P, _I)
 _sig("pp_par2_coeff", _U16, _U16, _U16)
 _sig("pp_par2_input_log", _U16, _U16)
 _sig("pp_par2_coeff_matrix", _I, _P, _P, _U, _P, _U, _P)
@@ -151,6 +158,10 @@ class Context:
 
     def set_stream(self, stream_ptr: int | None):
         self.check(lib.pp_ctx_set_stream(self.h, _P(stream_ptr or 0)))
+
+    def set_gf16_kernel(self, kernel: int):
+        """PP_GF16_KERNEL_AUTO / _LUT / _TENSOR"""
+        self.check(lib.pp_ctx_set_gf16_kernel(self.h, kernel))
 
     def free_cache(self):
         self.check(lib.pp_ctx_free_cache(self.h))

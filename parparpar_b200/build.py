@@ -20,6 +20,7 @@ OBJ_DIR = os.path.join(HERE, "_build")
 
 SOURCES = [
     "gf16_kernels.cu",
+    "gf16_tc.cu",
     "gf64_kernels.cu",
     "gf64_fft.cu",
     "capi.cpp",

@@ -12,6 +12,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <list>
 #include <mutex>
@@ -68,7 +69,7 @@ const Gf16Host& gf16h() {
 }  // namespace
 
 // -------------------------------------------------------------------- ctx
-enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_NSLOTS };
+enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_AEXP, S_NSLOTS };
 
 struct CauchyEntry {
   size_t n_in, n_rec;
@@ -85,6 +86,8 @@ struct pp_ctx {
   void* slot_p[S_NSLOTS] = {};
   size_t slot_n[S_NSLOTS] = {};
   std::list<CauchyEntry> cauchy;  // LRU, front = most recent
+  int gf16_kernel = PP_GF16_KERNEL_AUTO;
+  int* d_status = nullptr;  // set nonzero by a kernel whose bounded wait gave up
   std::mutex mu;
 };
 
@@ -112,6 +115,20 @@ static int set_err(pp_ctx* ctx, int code, const char* fmt, ...) {
 static int bind(pp_ctx* ctx) {
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return set_err(ctx, PP_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return PP_OK;
+}
+
+// Read and clear the device status word (after a synchronize).
+static int device_status(pp_ctx* ctx) {
+  int h = 0;
+  if (cudaMemcpy(&h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, PP_ERR_CUDA, "status read failed");
+  }
+  if (h) {
+    cudaMemset(ctx->d_status, 0, sizeof(int));
+    return set_err(ctx, PP_ERR_TIMEOUT, "a device-side wait timed out; the kernel returned early");
+  }
   return PP_OK;
 }
 
@@ -216,7 +233,17 @@ PP_API int pp_ctx_create(int device, pp_ctx** out) {
     delete ctx;
     return PP_ERR_CUDA;
   }
+  if (cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess || cudaMemset(ctx->d_status, 0, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return PP_ERR_CUDA;
+  }
   ctx->stream = ctx->own;
+  if (const char* k = getenv("PP_GF16_KERNEL")) {
+    if (!strcmp(k, "lut")) ctx->gf16_kernel = PP_GF16_KERNEL_LUT;
+    else if (!strcmp(k, "tensor")) ctx->gf16_kernel = PP_GF16_KERNEL_TENSOR;
+  }
   *out = ctx;
   return PP_OK;
 }
@@ -239,6 +266,7 @@ PP_API int pp_ctx_free_cache(pp_ctx* ctx) {
 PP_API void pp_ctx_destroy(pp_ctx* ctx) {
   if (!ctx) return;
   pp_ctx_free_cache(ctx);
+  if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
 }
@@ -253,6 +281,12 @@ PP_API int pp_ctx_synchronize(pp_ctx* ctx) {
   if (!ctx) return PP_ERR_INVALID_ARG;
   bind(ctx);
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return device_status(ctx);
+}
+
+PP_API int pp_ctx_set_gf16_kernel(pp_ctx* ctx, int kernel) {
+  if (!ctx || kernel < PP_GF16_KERNEL_AUTO || kernel > PP_GF16_KERNEL_TENSOR) return PP_ERR_INVALID_ARG;
+  ctx->gf16_kernel = kernel;
   return PP_OK;
 }
 PP_API const char* pp_ctx_last_error(pp_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
@@ -304,6 +338,25 @@ PP_API int pp_par2_coeff_matrix(pp_ctx* ctx, const uint16_t* input_idx, unsigned
   return PP_OK;
 }
 
+// GF(2^16) region kernel dispatch.  The tensor-core kernel needs its
+// coefficient bit-matrix tiles, expanded into `aexp` (device scratch of
+// gf16_tc_coeff_bytes bytes).
+static bool use_tensor(int sel, unsigned n_in, unsigned n_out) {
+  if (sel == PP_GF16_KERNEL_LUT) return false;
+  if (sel == PP_GF16_KERNEL_TENSOR) return true;
+  return n_in >= 8 && n_out >= 1;
+}
+static cudaError_t gf16_region(int sel, const uint8_t* din, size_t dstride, unsigned n_in, size_t slice,
+                               const uint16_t* d_coeffs, size_t ldc, unsigned n_out, uint8_t* dout, size_t ostride,
+                               bool accumulate, int sms, uint8_t* aexp, int* d_status, cudaStream_t s) {
+  if (use_tensor(sel, n_in, n_out) && aexp) {
+    cudaError_t e = launch_gf16_tc_expand(d_coeffs, ldc, n_in, n_out, aexp, s);
+    if (e != cudaSuccess) return e;
+    return launch_gf16_muladd_tc(din, dstride, n_in, slice, aexp, n_out, dout, ostride, accumulate, sms, d_status, s);
+  }
+  return launch_gf16_muladd(din, dstride, n_in, slice, d_coeffs, ldc, n_out, dout, ostride, accumulate, sms, s);
+}
+
 // Region muladd with staging of host / unaligned buffers.
 static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, unsigned n_in, size_t slice,
                             const uint16_t* d_coeffs, size_t ldc, unsigned n_out, void* outputs, size_t out_stride,
@@ -332,13 +385,21 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
       CUDA_TRY(ctx, cudaMemcpy2DAsync(dout, row, outputs, out_stride, slice, n_out,
                                       out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
   }
-  CUDA_TRY(ctx, launch_gf16_muladd(din, dstride, n_in, slice, d_coeffs, ldc, n_out, dout, ostride, accumulate,
-                                   ctx->sms, ctx->stream));
+  uint8_t* aexp = nullptr;
+  if (use_tensor(ctx->gf16_kernel, n_in, n_out)) {
+    aexp = (uint8_t*)scratch(ctx, S_AEXP, gf16_tc_coeff_bytes(n_in, n_out));
+    if (!aexp) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficient tiles");
+  }
+  CUDA_TRY(ctx, gf16_region(ctx->gf16_kernel, din, dstride, n_in, slice, d_coeffs, ldc, n_out, dout, ostride,
+                            accumulate, ctx->sms, aexp, ctx->d_status, ctx->stream));
   if (stage_out) {
     CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,
                                     out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
   }
-  if (!in_dev || !out_dev) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!in_dev || !out_dev) {
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return device_status(ctx);
+  }
   return PP_OK;
 }
 
@@ -461,6 +522,7 @@ struct pp_par2_proc {
   struct Area {
     uint8_t* d_in = nullptr;
     uint16_t* d_coeff = nullptr;  // [n_out][batch]
+    uint8_t* d_aexp = nullptr;    // tensor-core coefficient tiles
     std::vector<uint16_t> h_coeff;
     unsigned count = 0;
     cudaEvent_t done = nullptr;
@@ -538,6 +600,7 @@ PP_API void pp_par2_proc_destroy(pp_par2_proc* p) {
   for (auto& a : p->areas) {
     if (a.d_in) cudaFree(a.d_in);
     if (a.d_coeff) cudaFree(a.d_coeff);
+    if (a.d_aexp) cudaFree(a.d_aexp);
     if (a.done) cudaEventDestroy(a.done);
   }
   if (p->d_out) cudaFree(p->d_out);
@@ -600,9 +663,15 @@ PP_API int pp_par2_proc_set_recovery_slices(pp_par2_proc* p, unsigned num, const
     a.h_coeff.assign((size_t)num * p->batch, 0);
     if (a.d_coeff) cudaFree(a.d_coeff);
     a.d_coeff = nullptr;
+    if (a.d_aexp) cudaFree(a.d_aexp);
+    a.d_aexp = nullptr;
     if (num && cudaMalloc(&a.d_coeff, (size_t)num * p->batch * 2) != cudaSuccess) {
       cudaGetLastError();
       return set_err(p->ctx, PP_ERR_NO_MEMORY, "coefficient buffer");
+    }
+    if (num && cudaMalloc(&a.d_aexp, gf16_tc_coeff_bytes(p->batch, num)) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(p->ctx, PP_ERR_NO_MEMORY, "coefficient tiles");
     }
   }
   p->has_output = false;
@@ -637,8 +706,9 @@ static int proc_submit(pp_par2_proc* p) {
                                    cudaMemcpyHostToDevice, p->s_copy));
   CUDA_TRY(p->ctx, cudaEventRecord(p->copied, p->s_copy));
   CUDA_TRY(p->ctx, cudaStreamWaitEvent(p->s_comp, p->copied, 0));
-  CUDA_TRY(p->ctx, launch_gf16_muladd(a.d_in, p->row, a.count, p->cur_size, a.d_coeff, p->batch, n_out, p->d_out,
-                                      p->row, p->has_output, p->ctx->sms, p->s_comp));
+  CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_in, p->row, a.count, p->cur_size, a.d_coeff, p->batch,
+                               n_out, p->d_out, p->row, p->has_output, p->ctx->sms, a.d_aexp, p->ctx->d_status,
+                               p->s_comp));
   CUDA_TRY(p->ctx, cudaEventRecord(a.done, p->s_comp));
   a.active = true;
   a.count = 0;
@@ -694,7 +764,7 @@ PP_API int pp_par2_proc_end_input(pp_par2_proc* p) {
   if (int r = proc_submit(p)) return r;
   CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_comp));
   for (auto& a : p->areas) a.active = false;
-  return PP_OK;
+  return device_status(p->ctx);
 }
 
 PP_API int pp_par2_proc_get_output(pp_par2_proc* p, unsigned index, void* output, int* valid) {

@@ -1,0 +1,478 @@
+// GF(2^16) region multiply-accumulate on the 5th-generation tensor cores
+// (tcgen05, kind::i8), sm_100a.
+//
+// Multiplication by a constant c in GF(2^16) is a 16x16 matrix over GF(2):
+// bit b of c*x = XOR_e bit_e(x) * bit_b(c * x^e).  The whole region product
+//   out[o][w] = XOR_i c[o][i] * in_i[w]
+// is therefore one GF(2) matrix product; here it is computed as the parity
+// of an exact integer u8 MMA.
+//
+// Shift trick: with A entries in {0,1}, sum_k A_k * B_k is congruent mod 2 to
+// sum_k A_k * (B_k mod 2), so only the lowest bit of each B byte matters.
+// Feeding the RAW input bytes shifted right by j (a plain 32-bit shift: the
+// bits that slide in from the neighbouring byte only add even amounts) makes
+// the low bit of byte beta equal bit 8*beta + j of the word.  With
+//   A[(o,b)][(j, i, beta)] = bit_b(c[o][i] * x^(8*beta + j))
+//   B[w][(j, i, beta)]     = byte_beta(in_i[w]) >> j        (j = 0..7)
+// the count D[(o,b)][w] = sum A*B has parity = bit b of out[o][w].  Counts
+// stay below 255 * 16 * num_inputs < 2^31.
+//
+// CTA tile: 8 outputs (M = 128 rows = 8 x 16 bits) x 512 words (two MMAs of
+// N = 256), looping over the inputs 8 at a time.  A stage's K is 128 bytes:
+// eight 16-byte chunks j = 0..7, each holding the 2 bytes of the 8 inputs'
+// words shifted right by j; four K = 32 MMA steps per stage.  The
+// accumulator fills TMEM (128 lanes x 512 columns of int32).
+//
+//   warp 0      producer: cp.async.bulk of the stage's A tile (pre-expanded
+//               coefficient bits, already in the swizzled smem layout) and
+//               of the 8 raw input rows of the word tile
+//   warp 1      TMEM allocation + one thread issuing tcgen05.mma
+//   warps 2-9   build the B tile (byte-permute the 8 inputs' words of a word
+//               pair into one 16-byte row, shift by j, 128-byte swizzle),
+//               then the epilogue: tcgen05.ld of the counts, parity, warp
+//               ballot -> two u16 outputs per lane
+//
+// Every mbarrier wait is bounded (about one second of %globaltimer); on a
+// timeout the CTA records an error in *status, drains what it issued, frees
+// TMEM and returns.
+#include "pp_common.cuh"
+#include "pp_internal.h"
+
+#include <algorithm>
+
+namespace pp {
+namespace tc16 {
+
+constexpr int kWords = 512;                 // words per CTA
+constexpr int kStageIn = 8;                 // inputs per stage
+constexpr int kABytes = 128 * 128;          // A tile: 128 rows x 128 B
+constexpr int kBBytes = kWords * 128;       // B tile: 512 rows x 128 B
+constexpr int kRawBytes = kStageIn * kWords * 2;
+constexpr int kThreads = 320;
+constexpr int kExp = 256;  // expander / epilogue threads (warps 2-9)
+constexpr int kOffA = 0;
+constexpr int kOffB = 2 * kABytes;                 // 32 KiB
+constexpr int kOffRaw = kOffB + 2 * kBBytes;       // 160 KiB
+constexpr int kOffBar = kOffRaw + 2 * kRawBytes;   // 176 KiB
+constexpr int kSmemBytes = kOffBar + 256 + 1024;   // + barriers + alignment slack
+constexpr uint64_t kWaitNs = 1000000000ull;        // bounded waits: 1 s
+
+// instruction descriptor: D int32, A/B unsigned 8-bit, both K-major,
+// N = 256, M = 128
+constexpr uint32_t kIdesc = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+
+PP_D uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+PP_D uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+PP_D void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+PP_D void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+PP_D void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+PP_D bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; false on timeout
+PP_D bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = gtimer();
+  while (!mbar_try(bar, parity)) {
+    if (gtimer() - t0 > kWaitNs) return false;
+  }
+  return true;
+}
+PP_D void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+PP_D uint64_t sw128_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
+}
+PP_D void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+PP_D void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+PP_D void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+PP_D void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+PP_D void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+PP_D void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 4 bits -> 4 bytes of 0/1 (bit k of n lands in byte k)
+PP_D uint32_t spread4(uint32_t n) { return (n * 0x00204081u) & 0x01010101u; }
+
+// ----------------------------------------------------------------------------
+// A tiles: for output group g (outputs 8g..8g+7) and input stage s (inputs
+// 8s..8s+7) a 16 KiB tile in the smem canonical layout (K-major, 128-byte
+// swizzle): row m = 16*oo + b; chunk j (shift); byte 2*ii + beta within the
+// chunk holds bit b of c[8g+oo][8s+ii] * x^(8*beta + j).
+__global__ void __launch_bounds__(128)
+k_gf16_tc_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigned n_in, unsigned n_out,
+                        unsigned n_stages, uint8_t* __restrict__ a_exp) {
+  const size_t total = (size_t)((n_out + 7) / 8) * n_stages * 8;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const unsigned oo = t & 7;
+    const size_t gs = t >> 3;  // g * n_stages + s
+    const unsigned s = (unsigned)(gs % n_stages), g = (unsigned)(gs / n_stages);
+    const unsigned o = 8 * g + oo;
+    uint16_t y[8][16];  // y[ii][e] = c_ii * x^e
+#pragma unroll
+    for (int ii = 0; ii < 8; ii++) {
+      const unsigned i = 8 * s + ii;
+      uint32_t c = (o < n_out && i < n_in) ? coeffs[(size_t)o * ldc + i] : 0;
+#pragma unroll
+      for (int e = 0; e < 16; e++) {
+        y[ii][e] = (uint16_t)c;
+        c = gf16_dbl(c);
+      }
+    }
+    uint8_t* tile = a_exp + gs * kABytes;
+#pragma unroll 1
+    for (int b = 0; b < 16; b++) {
+      const unsigned m = 16 * oo + b;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        uint32_t w4[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          // bytes 4q..4q+3 = (ii = 2q, beta 0), (2q, 1), (2q+1, 0), (2q+1, 1)
+          uint32_t v = 0;
+#pragma unroll
+          for (int t4 = 0; t4 < 4; t4++) {
+            const int ii = 2 * q + (t4 >> 1), beta = t4 & 1;
+            v |= (uint32_t)((y[ii][8 * beta + j] >> b) & 1u) << (8 * t4);
+          }
+          w4[q] = v;
+        }
+        *reinterpret_cast<uint4*>(tile + (m >> 3) * 1024 + (m & 7) * 128 + ((j ^ (m & 7)) << 4)) =
+            make_uint4(w4[0], w4[1], w4[2], w4[3]);
+      }
+    }
+  }
+}
+
+// mode: 0 overwrite, 1 xor into existing, 2 atomic xor (inputs split across CTAs)
+__global__ void __launch_bounds__(kThreads, 1)
+k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in, size_t slice_bytes,
+                 const uint8_t* __restrict__ a_exp, unsigned n_stages_total, unsigned n_out, uint8_t* __restrict__ out,
+                 size_t out_stride, unsigned stages_per_split, int mode, int* __restrict__ status) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t base_s = smem_addr(smem_raw);
+  const uint32_t pad = ((base_s + 1023) & ~1023u) - base_s;
+  uint8_t* smem = smem_raw + pad;
+  const uint32_t sA = base_s + pad + kOffA, sB = base_s + pad + kOffB, sRaw = base_s + pad + kOffRaw;
+  uint8_t* raw_p = smem + kOffRaw;
+  uint8_t* b_p = smem + kOffB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+  // barriers: a_full[2], raw_full[2], b_full[2], stage_empty[2], raw_empty[2], d_full, done
+  const uint32_t bar0 = smem_addr(bars);
+  auto BAR = [&](int k) { return bar0 + 8u * (uint32_t)k; };
+  enum { A_FULL = 0, RAW_FULL = 2, B_FULL = 4, ST_EMPTY = 6, RAW_EMPTY = 8, D_FULL = 10, DONE = 11 };
+  volatile uint32_t* tmem_holder = reinterpret_cast<volatile uint32_t*>(smem + kOffBar + 128);
+  volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 136);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned g = blockIdx.x;  // output group
+  const size_t w0 = (size_t)blockIdx.y * kWords;
+  const unsigned st_begin = blockIdx.z * stages_per_split;
+  const unsigned st_end = min(n_stages_total, st_begin + stages_per_split);
+  const unsigned nst = st_end > st_begin ? st_end - st_begin : 0;
+  const size_t total_words = (slice_bytes + 1) / 2;
+  const unsigned words_valid = (unsigned)min((size_t)kWords, total_words - w0);
+  // raw bytes copied per input row (16-byte multiple, inside the padded row)
+  const size_t tile_bytes_valid = min((size_t)kWords * 2, slice_bytes - 2 * w0);
+  const uint32_t raw_copy = (uint32_t)((tile_bytes_valid + 15) & ~(size_t)15);
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 10; k++) mbar_init(BAR(k), (k >= B_FULL && k < ST_EMPTY) || (k >= RAW_EMPTY && k < D_FULL)
+                                                          ? (uint32_t)kExp : 1u);
+    mbar_init(BAR(D_FULL), 1);
+    mbar_init(BAR(DONE), 1);
+    *err = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr((const void*)tmem_holder)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_holder;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      unsigned issued = 0;
+      for (unsigned k = 0; k < nst && !*err; k++) {
+        const unsigned s = k & 1, use = k >> 1;
+        if (k >= 2) {
+          if (!mbar_wait(BAR(ST_EMPTY + s), (use - 1) & 1) || !mbar_wait(BAR(RAW_EMPTY + s), (use - 1) & 1)) {
+            *err = 1;
+            break;
+          }
+        }
+        const unsigned st = st_begin + k;
+        mbar_expect_tx(BAR(A_FULL + s), kABytes);
+        bulk_g2s(sA + s * kABytes, a_exp + ((size_t)g * n_stages_total + st) * kABytes, kABytes, BAR(A_FULL + s));
+        const unsigned i0 = st * kStageIn;
+        const unsigned ni = min((unsigned)kStageIn, n_in - i0);
+        mbar_expect_tx(BAR(RAW_FULL + s), raw_copy * ni);
+        for (unsigned ii = 0; ii < ni; ii++)
+          bulk_g2s(sRaw + s * kRawBytes + ii * (kWords * 2), in + (size_t)(i0 + ii) * in_stride + 2 * w0, raw_copy,
+                   BAR(RAW_FULL + s));
+        issued = k + 1;
+      }
+      // drain: the last stages' copies must land before the CTA exits
+      if (*err) {
+        for (unsigned k = issued >= 2 ? issued - 2 : 0; k < issued; k++) {
+          mbar_wait(BAR(A_FULL + (k & 1)), (k >> 1) & 1);
+          mbar_wait(BAR(RAW_FULL + (k & 1)), (k >> 1) & 1);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      unsigned k = 0;
+      for (; k < nst; k++) {
+        const unsigned s = k & 1, use = k >> 1;
+        if (*err || !mbar_wait(BAR(A_FULL + s), use & 1) || !mbar_wait(BAR(B_FULL + s), use & 1)) {
+          *err = 1;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+#pragma unroll
+          for (int nn = 0; nn < 2; nn++) {
+            mma_i8(tmem + nn * 256, sw128_desc(sA + s * kABytes + 32 * kk),
+                   sw128_desc(sB + s * kBBytes + nn * (256 * 128) + 32 * kk), kIdesc, (k > 0 || kk > 0) ? 1u : 0u);
+          }
+        }
+        mma_commit(BAR(ST_EMPTY + s));
+      }
+      if (!*err) mma_commit(BAR(D_FULL));
+      // all MMAs issued by this thread complete before TMEM is released
+      mma_commit(BAR(DONE));
+      if (!mbar_wait(BAR(DONE), 0)) *err = 1;
+    }
+  } else {
+    // ------------------------------------------------------------ expanders
+    const int e = threadIdx.x - 64;  // 0..255: word pair n = 2e, 2e+1 of the tile
+    const unsigned n = 2 * e;
+    const bool odd_tail = (slice_bytes & 1) && (w0 + kWords >= total_words);
+    const unsigned last_word = (unsigned)(total_words - 1 - w0);
+    uint32_t mask = 0;
+    if (n < words_valid) mask = 0xFFFFu;
+    if (n + 1 < words_valid) mask |= 0xFFFF0000u;
+    if (odd_tail) {
+      if (n == last_word) mask &= 0xFFFF00FFu;
+      else if (n + 1 == last_word) mask &= 0x00FFFFFFu;
+    }
+    const uint32_t row0 = (n >> 3) * 1024 + (n & 7) * 128, r0 = n & 7;
+    const uint32_t row1 = ((n + 1) >> 3) * 1024 + ((n + 1) & 7) * 128, r1 = (n + 1) & 7;
+    for (unsigned k = 0; k < nst; k++) {
+      const unsigned s = k & 1, use = k >> 1;
+      if (*err || !mbar_wait(BAR(RAW_FULL + s), use & 1)) {
+        *err = 1;
+        break;
+      }
+      if (k >= 2 && !mbar_wait(BAR(ST_EMPTY + s), (use - 1) & 1)) {
+        *err = 1;
+        break;
+      }
+      const unsigned i0 = (st_begin + k) * kStageIn;
+      const unsigned ni = min((unsigned)kStageIn, n_in - i0);
+      const uint8_t* raw = raw_p + s * kRawBytes;
+      uint8_t* bt = b_p + s * kBBytes;
+      uint32_t v[kStageIn];
+#pragma unroll
+      for (int ii = 0; ii < kStageIn; ii++)
+        v[ii] = (unsigned)ii < ni ? (*reinterpret_cast<const uint32_t*>(raw + ii * (kWords * 2) + 2 * n) & mask) : 0u;
+      // row of word n: low halves of the 8 inputs; word n+1: high halves
+      uint32_t p0[4], p1[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        p0[q] = __byte_perm(v[2 * q], v[2 * q + 1], 0x5410);
+        p1[q] = __byte_perm(v[2 * q], v[2 * q + 1], 0x7632);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        *reinterpret_cast<uint4*>(bt + row0 + ((j ^ r0) << 4)) =
+            make_uint4(p0[0] >> j, p0[1] >> j, p0[2] >> j, p0[3] >> j);
+        *reinterpret_cast<uint4*>(bt + row1 + ((j ^ r1) << 4)) =
+            make_uint4(p1[0] >> j, p1[1] >> j, p1[2] >> j, p1[3] >> j);
+      }
+      fence_async_smem();
+      mbar_arrive(BAR(RAW_EMPTY + s));
+      mbar_arrive(BAR(B_FULL + s));
+    }
+    // ------------------------------------------------------------ epilogue
+    const bool have = nst > 0 && !*err && mbar_wait(BAR(D_FULL), 0);
+    if (nst > 0 && !have) *err = 1;
+    tc_fence_after();
+    const int q = warp & 3;               // TMEM lane quarter of this warp
+    const int chalf = (warp - 2) >> 2;    // columns [256*chalf, 256*chalf + 256)
+    const unsigned o_lo = 8 * g + 2 * q, o_hi = o_lo + 1;
+    for (int c = 8 * chalf; c < 8 * chalf + 8; c++) {
+      uint32_t r[32];
+      if (have) {
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + 32 * c, r);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++) r[j] = 0;
+      }
+      uint32_t mine = 0;
+#pragma unroll
+      for (int j = 0; j < 32; j++) {
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, r[j] & 1u);
+        if (lane == j) mine = bal;
+      }
+      if (!have) continue;
+      const unsigned widx = 32 * c + lane;  // word within the tile
+      // pair lanes into 32-bit words: even lane holds words widx, widx+1
+      const uint32_t nb = __shfl_down_sync(0xFFFFFFFFu, mine, 1);
+      if ((lane & 1) || widx >= words_valid) continue;
+      const size_t wbyte = 2 * (w0 + widx);
+      const size_t nbytes = min((size_t)4, slice_bytes - wbyte);
+#pragma unroll
+      for (int hsel = 0; hsel < 2; hsel++) {
+        const unsigned o = hsel ? o_hi : o_lo;
+        if (o >= n_out) continue;
+        uint32_t val = hsel ? ((mine >> 16) | (nb & 0xFFFF0000u)) : ((mine & 0xFFFFu) | (nb << 16));
+        uint8_t* dst = out + (size_t)o * out_stride + wbyte;
+        if (nbytes >= 4) {
+          if (mode == 2) {
+            if (val) atomicXor(reinterpret_cast<uint32_t*>(dst), val);
+          } else if (mode == 1) {
+            *reinterpret_cast<uint32_t*>(dst) ^= val;
+          } else {
+            *reinterpret_cast<uint32_t*>(dst) = val;
+          }
+        } else {
+          if (mode == 2) {
+            uint32_t m = nbytes >= 4 ? 0xFFFFFFFFu : ((1u << (8 * nbytes)) - 1u);
+            if (val & m) atomicXor(reinterpret_cast<uint32_t*>(dst), val & m);
+          } else {
+            for (size_t bb = 0; bb < nbytes; bb++) {
+              uint8_t nbv = (uint8_t)(val >> (8 * bb));
+              dst[bb] = mode == 1 ? (uint8_t)(dst[bb] ^ nbv) : nbv;
+            }
+          }
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+  if (threadIdx.x == 0 && *err) atomicOr(status, 1);
+}
+
+}  // namespace tc16
+
+size_t gf16_tc_coeff_bytes(unsigned n_in, unsigned n_out) {
+  return (size_t)((n_out + 7) / 8) * ((n_in + 7) / 8) * tc16::kABytes;
+}
+
+cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned n_in, unsigned n_out,
+                                  uint8_t* d_aexp, cudaStream_t s) {
+  const unsigned n_stages = (n_in + 7) / 8;
+  const size_t total = (size_t)((n_out + 7) / 8) * n_stages * 8;
+  if (!total) return cudaSuccess;
+  unsigned blocks = (unsigned)std::min<size_t>(ceil_div(total, 128), 148 * 16);
+  tc16::k_gf16_tc_expand_coeffs<<<blocks, 128, 0, s>>>(d_coeffs, ldc, n_in, n_out, n_stages, d_aexp);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigned n_in, size_t slice_bytes,
+                                  const uint8_t* d_aexp, unsigned n_out, uint8_t* d_out, size_t out_stride,
+                                  bool accumulate, int sms, int* d_status, cudaStream_t s) {
+  if (!n_out || !slice_bytes) return cudaSuccess;
+  if (!n_in) {
+    if (accumulate) return cudaSuccess;
+    note_launch();
+    return cudaMemset2DAsync(d_out, out_stride, 0, slice_bytes, n_out, s);
+  }
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tc16::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const unsigned groups = (n_out + 7) / 8;
+  const size_t words = (slice_bytes + 1) / 2;
+  const unsigned wt = (unsigned)ceil_div(words, tc16::kWords);
+  const unsigned n_stages = (n_in + 7) / 8;
+  const unsigned base = groups * wt;
+  const unsigned target = (unsigned)(sms > 0 ? sms : 148);
+  unsigned splits = base >= target ? 1 : (unsigned)ceil_div(target, base);
+  // keep at least 8 stages per split so the pipeline fills
+  unsigned max_splits = (unsigned)std::max<size_t>(1, n_stages / 8);
+  if (splits > max_splits) splits = max_splits;
+  unsigned per = (unsigned)ceil_div(n_stages, splits);
+  splits = (unsigned)ceil_div(n_stages, per);
+  int mode;
+  if (splits == 1) {
+    mode = accumulate ? 1 : 0;
+  } else {
+    mode = 2;
+    if (!accumulate) {
+      cudaError_t e = cudaMemset2DAsync(d_out, out_stride, 0, slice_bytes, n_out, s);
+      note_launch();
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (groups > 65535 || wt > 65535 || splits > 65535) return cudaErrorInvalidConfiguration;
+  dim3 grid(groups, wt, splits);
+  tc16::k_gf16_muladd_tc<<<grid, tc16::kThreads, tc16::kSmemBytes, s>>>(
+      d_in, in_stride, n_in, slice_bytes, d_aexp, n_stages, n_out, d_out, out_stride, per, mode, d_status);
+  note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace pp

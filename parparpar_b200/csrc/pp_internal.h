@@ -29,6 +29,17 @@ cudaError_t launch_gf16_muladd(const uint8_t* d_in, size_t in_stride, unsigned n
                                const uint16_t* d_coeffs, size_t ldc, unsigned n_out, uint8_t* d_out,
                                size_t out_stride, bool accumulate, int sms, cudaStream_t s);
 
+// Tensor-core (tcgen05, kind::i8) variant.  launch_gf16_tc_expand builds
+// the coefficient bit-matrix tiles (gf16_tc_coeff_bytes(n_in, n_out) bytes)
+// that launch_gf16_muladd_tc consumes; *d_status is set nonzero if a bounded
+// device wait timed out.
+size_t gf16_tc_coeff_bytes(unsigned n_in, unsigned n_out);
+cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned n_in, unsigned n_out,
+                                  uint8_t* d_aexp, cudaStream_t s);
+cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigned n_in, size_t slice_bytes,
+                                  const uint8_t* d_aexp, unsigned n_out, uint8_t* d_out, size_t out_stride,
+                                  bool accumulate, int sms, int* d_status, cudaStream_t s);
+
 // PAR2 inversion (Gauss-Jordan without pivoting, identity columns in place).
 // d_mat: m rows x ncols (row stride ld elements).  Runs all m pivot steps;
 // d_status[0] receives -1 on success or the first row whose pivot was zero.

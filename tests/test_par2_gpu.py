@@ -6,6 +6,16 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=["lut", "tensor"])
+def kctx(ctx, request):
+    """The default context with the GF(2^16) region kernel forced to one
+    implementation; every parity test below runs against both."""
+    import parparpar_b200._lib as L
+    ctx.set_gf16_kernel(L.PP_GF16_KERNEL_LUT if request.param == "lut" else L.PP_GF16_KERNEL_TENSOR)
+    yield ctx
+    ctx.set_gf16_kernel(L.PP_GF16_KERNEL_AUTO)
+
+
 def _dev(a):
     import torch
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
@@ -15,19 +25,19 @@ def _host(t):
     return t.cpu().numpy()
 
 
-def test_par2_create_golden(ctx, golden):
+def test_par2_create_golden(kctx, golden):
     from parparpar_b200 import par2
     g = golden("par2_create.npz")
     for k in range(int(g["ncases"])):
         inp, idx, exps, out = g[f"c{k}_inputs"], g[f"c{k}_idx"], g[f"c{k}_exps"], g[f"c{k}_out"]
-        got = par2.par2_create(inp, idx, exps, ctx=ctx)
+        got = par2.par2_create(inp, idx, exps, ctx=kctx)
         assert np.array_equal(got, out), f"case {k}"
         # same through device buffers
         dout = _dev(np.zeros_like(out))
-        par2.par2_create(_dev(inp), idx, exps, out=dout, ctx=ctx)
-        ctx.synchronize()
+        par2.par2_create(_dev(inp), idx, exps, out=dout, ctx=kctx)
+        kctx.synchronize()
         assert np.array_equal(_host(dout), out), f"case {k} (device)"
-    got = par2.gf16_muladd(g["coef_inputs"], g["coef_coeffs"], ctx=ctx)
+    got = par2.gf16_muladd(g["coef_inputs"], g["coef_coeffs"], ctx=kctx)
     assert np.array_equal(got, g["coef_out"])
 
 
@@ -35,7 +45,7 @@ def test_par2_create_golden(ctx, golden):
     (1, 1, 2), (1, 3, 3), (7, 1, 16), (8, 4, 17), (9, 5, 1000), (33, 8, 8192), (33, 9, 8193),
     (300, 17, 40000), (16, 16, 20000), (15, 15, 19998), (64, 2, 64 * 1024 + 6),
 ])
-def test_gf16_muladd_vs_oracle(ctx, oracle, n, r, s):
+def test_gf16_muladd_vs_oracle(kctx, oracle, n, r, s):
     from parparpar_b200 import par2
     rng = np.random.default_rng(n * 1000 + r * 10 + s)
     inp = rng.integers(0, 256, (n, s), dtype=np.uint8)
@@ -44,15 +54,15 @@ def test_gf16_muladd_vs_oracle(ctx, oracle, n, r, s):
     if r > 1:
         co[1, :] = 0
     exp = oracle.par2_muladd(list(inp), s, co)
-    assert np.array_equal(par2.gf16_muladd(inp, co, ctx=ctx), exp)
+    assert np.array_equal(par2.gf16_muladd(inp, co, ctx=kctx), exp)
     # accumulate into existing contents
     base = rng.integers(0, 256, (r, s), dtype=np.uint8)
     out = base.copy()
-    par2.gf16_muladd(inp, co, out=out, accumulate=True, ctx=ctx)
+    par2.gf16_muladd(inp, co, out=out, accumulate=True, ctx=kctx)
     assert np.array_equal(out, exp ^ base)
 
 
-def test_gf16_muladd_device_strided(ctx, oracle):
+def test_gf16_muladd_device_strided(kctx, oracle):
     """Device rows with padding between them; bytes outside the slices are
     neither read as data nor written."""
     from parparpar_b200 import par2
@@ -63,14 +73,14 @@ def test_gf16_muladd_device_strided(ctx, oracle):
     exp = oracle.par2_muladd([big[i, :s] for i in range(n)], s, co)
     dout_np = rng.integers(0, 256, (r, stride), dtype=np.uint8)
     dout = _dev(dout_np)
-    par2.gf16_muladd(_dev(big)[:, :s], co, out=dout[:, :s], slice_bytes=s, ctx=ctx)
-    ctx.synchronize()
+    par2.gf16_muladd(_dev(big)[:, :s], co, out=dout[:, :s], slice_bytes=s, ctx=kctx)
+    kctx.synchronize()
     got = _host(dout)
     assert np.array_equal(got[:, :s], exp)
     assert np.array_equal(got[:, s:], dout_np[:, s:]), "wrote past the slice"
 
 
-def test_gf16_muladd_split_inputs(ctx, oracle):
+def test_gf16_muladd_split_inputs(kctx, oracle):
     """Many inputs and a small slice: the launcher splits the input range
     across blocks and combines with atomic XOR."""
     from parparpar_b200 import par2
@@ -79,10 +89,10 @@ def test_gf16_muladd_split_inputs(ctx, oracle):
     inp = rng.integers(0, 256, (n, s), dtype=np.uint8)
     co = rng.integers(0, 65536, (r, n)).astype(np.uint16)
     exp = oracle.par2_muladd(list(inp), s, co)
-    assert np.array_equal(par2.gf16_muladd(inp, co, ctx=ctx), exp)
+    assert np.array_equal(par2.gf16_muladd(inp, co, ctx=kctx), exp)
     out = _dev(np.zeros((r, s), dtype=np.uint8))
-    par2.gf16_muladd(_dev(inp), _dev(co), out=out, ctx=ctx)
-    ctx.synchronize()
+    par2.gf16_muladd(_dev(inp), _dev(co), out=out, ctx=kctx)
+    kctx.synchronize()
     assert np.array_equal(_host(out), exp)
 
 
@@ -107,7 +117,7 @@ def _ctrl_case(ctx, oracle, slice_size, last, n_in, n_out, seed, batch=0, areas=
     proc.deinit()
 
 
-def test_proc_test_ctrl_grid(ctx, oracle):
+def test_proc_test_ctrl_grid(kctx, oracle):
     """The grid of test/gf16/test-ctrl.cpp:281-306: slice sizes {2, 19998,
     20000}, last-slice sizes {1, 2, S-1, S}, 1/15/16 inputs x 1/15/16 outputs."""
     seed = 0x01020304
@@ -121,15 +131,15 @@ def test_proc_test_ctrl_grid(ctx, oracle):
                     if last != s and last != 1 and (n_in > 15 or n_out > 2):
                         continue
                     seed += 1
-                    _ctrl_case(ctx, oracle, s, last, n_in, n_out, seed)
+                    _ctrl_case(kctx, oracle, s, last, n_in, n_out, seed)
 
 
-def test_proc_batches_and_reuse(ctx, oracle):
+def test_proc_batches_and_reuse(kctx, oracle):
     from parparpar_b200 import par2
     # small batch to exercise several staging areas, flush, and a second pass
-    _ctrl_case(ctx, oracle, 4096, 4096, 50, 5, 77, batch=4, areas=3)
+    _ctrl_case(kctx, oracle, 4096, 4096, 50, 5, 77, batch=4, areas=3)
     rng = np.random.default_rng(78)
-    proc = par2.PAR2ProcCUDA(2048, 2, 3, ctx=ctx)
+    proc = par2.PAR2ProcCUDA(2048, 2, 3, ctx=kctx)
     proc.setRecoverySlices(3, [0, 1, 2])
     data = rng.integers(0, 256, (7, 2048), dtype=np.uint8)
     for rnd in range(2):
@@ -185,20 +195,20 @@ def test_par2_invert_vs_oracle(ctx, oracle):
         assert r2 == used and np.array_equal(m.factors, f)
 
 
-def test_par2_repair_roundtrip(ctx):
+def test_par2_repair_roundtrip(kctx):
     """create -> erase -> invert -> decode restores the erased slices."""
     from parparpar_b200 import par2
     rng = np.random.default_rng(31)
     n, s, r = 500, 8192, 12
     data = rng.integers(0, 256, (n, s), dtype=np.uint8)
     exps = list(range(r))
-    rec = par2.par2_create(data, np.arange(n), exps, ctx=ctx)
+    rec = par2.par2_create(data, np.arange(n), exps, ctx=kctx)
     lost = sorted(rng.choice(n, 10, replace=False).tolist())
     valid = np.ones(n, dtype=bool)
     valid[lost] = False
-    m = par2.Galois16RecMatrix(ctx=ctx)
+    m = par2.Galois16RecMatrix(ctx=kctx)
     used = list(exps)
     assert m.Compute(list(valid), int(valid.sum()), used)
     srcs = np.concatenate([data[valid], rec[[exps.index(e) for e in used]]], axis=0)
-    restored = par2.gf16_muladd(srcs, m.factors, ctx=ctx)
+    restored = par2.gf16_muladd(srcs, m.factors, ctx=kctx)
     assert np.array_equal(restored, data[lost])
