@@ -50,10 +50,12 @@ constexpr int kBBytes = kWords * 128;       // B tile: 512 rows x 128 B
 constexpr int kRawBytes = kStageIn * kWords * 2;
 constexpr int kThreads = 320;
 constexpr int kExp = 256;  // expander / epilogue threads (warps 2-9)
+constexpr int kLd = 4;                             // load ring depth (A tile + raw rows)
+constexpr int kBs = 2;                             // B tile ring depth
 constexpr int kOffA = 0;
-constexpr int kOffB = 2 * kABytes;                 // 32 KiB
-constexpr int kOffRaw = kOffB + 2 * kBBytes;       // 160 KiB
-constexpr int kOffBar = kOffRaw + 2 * kRawBytes;   // 176 KiB
+constexpr int kOffB = kLd * kABytes;               // 64 KiB
+constexpr int kOffRaw = kOffB + kBs * kBBytes;     // 192 KiB
+constexpr int kOffBar = kOffRaw + kLd * kRawBytes; // 224 KiB
 constexpr int kSmemBytes = kOffBar + 256 + 1024;   // + barriers + alignment slack
 constexpr uint64_t kWaitNs = 1000000000ull;        // bounded waits: 1 s
 
@@ -198,12 +200,23 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
   uint8_t* raw_p = smem + kOffRaw;
   uint8_t* b_p = smem + kOffB;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
-  // barriers: a_full[2], raw_full[2], b_full[2], stage_empty[2], raw_empty[2], d_full, done
   const uint32_t bar0 = smem_addr(bars);
+  // load ring: A_FULL, RAW_FULL, A_EMPTY, RAW_EMPTY  (kLd each)
+  // B ring:    B_FULL, B_EMPTY                       (kBs each)
+  enum {
+    A_FULL = 0,
+    RAW_FULL = A_FULL + kLd,
+    A_EMPTY = RAW_FULL + kLd,
+    RAW_EMPTY = A_EMPTY + kLd,
+    B_FULL = RAW_EMPTY + kLd,
+    B_EMPTY = B_FULL + kBs,
+    D_FULL = B_EMPTY + kBs,
+    DONE = D_FULL + 1,
+    NBARS = DONE + 1
+  };
   auto BAR = [&](int k) { return bar0 + 8u * (uint32_t)k; };
-  enum { A_FULL = 0, RAW_FULL = 2, B_FULL = 4, ST_EMPTY = 6, RAW_EMPTY = 8, D_FULL = 10, DONE = 11 };
-  volatile uint32_t* tmem_holder = reinterpret_cast<volatile uint32_t*>(smem + kOffBar + 128);
-  volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 136);
+  volatile uint32_t* tmem_holder = reinterpret_cast<volatile uint32_t*>(smem + kOffBar + 8 * NBARS);
+  volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 8 * NBARS + 8);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned g = blockIdx.x;  // output group
@@ -218,10 +231,10 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
   const uint32_t raw_copy = (uint32_t)((tile_bytes_valid + 15) & ~(size_t)15);
 
   if (threadIdx.x == 0) {
-    for (int k = 0; k < 10; k++) mbar_init(BAR(k), (k >= B_FULL && k < ST_EMPTY) || (k >= RAW_EMPTY && k < D_FULL)
-                                                          ? (uint32_t)kExp : 1u);
-    mbar_init(BAR(D_FULL), 1);
-    mbar_init(BAR(DONE), 1);
+    for (int k = 0; k < NBARS; k++) {
+      const bool by_expanders = (k >= RAW_EMPTY && k < RAW_EMPTY + kLd) || (k >= B_FULL && k < B_FULL + kBs);
+      mbar_init(BAR(k), by_expanders ? (uint32_t)kExp : 1u);
+    }
     *err = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -242,39 +255,38 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
     if (lane == 0) {
       unsigned issued = 0;
       for (unsigned k = 0; k < nst && !*err; k++) {
-        const unsigned s = k & 1, use = k >> 1;
-        if (k >= 2) {
-          if (!mbar_wait(BAR(ST_EMPTY + s), (use - 1) & 1) || !mbar_wait(BAR(RAW_EMPTY + s), (use - 1) & 1)) {
+        const unsigned sl = k % kLd, use = k / kLd;
+        if (k >= kLd) {
+          if (!mbar_wait(BAR(A_EMPTY + sl), (use - 1) & 1) || !mbar_wait(BAR(RAW_EMPTY + sl), (use - 1) & 1)) {
             *err = 1;
             break;
           }
         }
         const unsigned st = st_begin + k;
-        mbar_expect_tx(BAR(A_FULL + s), kABytes);
-        bulk_g2s(sA + s * kABytes, a_exp + ((size_t)g * n_stages_total + st) * kABytes, kABytes, BAR(A_FULL + s));
+        mbar_expect_tx(BAR(A_FULL + sl), kABytes);
+        bulk_g2s(sA + sl * kABytes, a_exp + ((size_t)g * n_stages_total + st) * kABytes, kABytes, BAR(A_FULL + sl));
         const unsigned i0 = st * kStageIn;
         const unsigned ni = min((unsigned)kStageIn, n_in - i0);
-        mbar_expect_tx(BAR(RAW_FULL + s), raw_copy * ni);
+        mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
         for (unsigned ii = 0; ii < ni; ii++)
-          bulk_g2s(sRaw + s * kRawBytes + ii * (kWords * 2), in + (size_t)(i0 + ii) * in_stride + 2 * w0, raw_copy,
-                   BAR(RAW_FULL + s));
+          bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 2), in + (size_t)(i0 + ii) * in_stride + 2 * w0, raw_copy,
+                   BAR(RAW_FULL + sl));
         issued = k + 1;
       }
-      // drain: the last stages' copies must land before the CTA exits
+      // drain: every issued copy lands before the CTA exits
       if (*err) {
-        for (unsigned k = issued >= 2 ? issued - 2 : 0; k < issued; k++) {
-          mbar_wait(BAR(A_FULL + (k & 1)), (k >> 1) & 1);
-          mbar_wait(BAR(RAW_FULL + (k & 1)), (k >> 1) & 1);
+        for (unsigned k = issued > (unsigned)kLd ? issued - kLd : 0; k < issued; k++) {
+          mbar_wait(BAR(A_FULL + k % kLd), (k / kLd) & 1);
+          mbar_wait(BAR(RAW_FULL + k % kLd), (k / kLd) & 1);
         }
       }
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      unsigned k = 0;
-      for (; k < nst; k++) {
-        const unsigned s = k & 1, use = k >> 1;
-        if (*err || !mbar_wait(BAR(A_FULL + s), use & 1) || !mbar_wait(BAR(B_FULL + s), use & 1)) {
+      for (unsigned k = 0; k < nst; k++) {
+        const unsigned sl = k % kLd, bs = k % kBs;
+        if (*err || !mbar_wait(BAR(A_FULL + sl), (k / kLd) & 1) || !mbar_wait(BAR(B_FULL + bs), (k / kBs) & 1)) {
           *err = 1;
           break;
         }
@@ -283,11 +295,12 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
         for (int kk = 0; kk < 4; kk++) {
 #pragma unroll
           for (int nn = 0; nn < 2; nn++) {
-            mma_i8(tmem + nn * 256, sw128_desc(sA + s * kABytes + 32 * kk),
-                   sw128_desc(sB + s * kBBytes + nn * (256 * 128) + 32 * kk), kIdesc, (k > 0 || kk > 0) ? 1u : 0u);
+            mma_i8(tmem + nn * 256, sw128_desc(sA + sl * kABytes + 32 * kk),
+                   sw128_desc(sB + bs * kBBytes + nn * (256 * 128) + 32 * kk), kIdesc, (k > 0 || kk > 0) ? 1u : 0u);
           }
         }
-        mma_commit(BAR(ST_EMPTY + s));
+        mma_commit(BAR(A_EMPTY + sl));
+        mma_commit(BAR(B_EMPTY + bs));
       }
       if (!*err) mma_commit(BAR(D_FULL));
       // all MMAs issued by this thread complete before TMEM is released
@@ -310,23 +323,24 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
     const uint32_t row0 = (n >> 3) * 1024 + (n & 7) * 128, r0 = n & 7;
     const uint32_t row1 = ((n + 1) >> 3) * 1024 + ((n + 1) & 7) * 128, r1 = (n + 1) & 7;
     for (unsigned k = 0; k < nst; k++) {
-      const unsigned s = k & 1, use = k >> 1;
-      if (*err || !mbar_wait(BAR(RAW_FULL + s), use & 1)) {
-        *err = 1;
-        break;
-      }
-      if (k >= 2 && !mbar_wait(BAR(ST_EMPTY + s), (use - 1) & 1)) {
+      const unsigned sl = k % kLd, bs = k % kBs;
+      if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
         *err = 1;
         break;
       }
       const unsigned i0 = (st_begin + k) * kStageIn;
       const unsigned ni = min((unsigned)kStageIn, n_in - i0);
-      const uint8_t* raw = raw_p + s * kRawBytes;
-      uint8_t* bt = b_p + s * kBBytes;
+      const uint8_t* raw = raw_p + sl * kRawBytes;
       uint32_t v[kStageIn];
 #pragma unroll
       for (int ii = 0; ii < kStageIn; ii++)
         v[ii] = (unsigned)ii < ni ? (*reinterpret_cast<const uint32_t*>(raw + ii * (kWords * 2) + 2 * n) & mask) : 0u;
+      mbar_arrive(BAR(RAW_EMPTY + sl));
+      if (k >= (unsigned)kBs && !mbar_wait(BAR(B_EMPTY + bs), (k / kBs - 1) & 1)) {
+        *err = 1;
+        break;
+      }
+      uint8_t* bt = b_p + bs * kBBytes;
       // row of word n: low halves of the 8 inputs; word n+1: high halves
       uint32_t p0[4], p1[4];
 #pragma unroll
@@ -342,8 +356,7 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
             make_uint4(p1[0] >> j, p1[1] >> j, p1[2] >> j, p1[3] >> j);
       }
       fence_async_smem();
-      mbar_arrive(BAR(RAW_EMPTY + s));
-      mbar_arrive(BAR(B_FULL + s));
+      mbar_arrive(BAR(B_FULL + bs));
     }
     // ------------------------------------------------------------ epilogue
     const bool have = nst > 0 && !*err && mbar_wait(BAR(D_FULL), 0);
