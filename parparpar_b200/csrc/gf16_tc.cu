@@ -320,8 +320,13 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
       if (n == last_word) mask &= 0xFFFF00FFu;
       else if (n + 1 == last_word) mask &= 0x00FFFFFFu;
     }
-    const uint32_t row0 = (n >> 3) * 1024 + (n & 7) * 128, r0 = n & 7;
-    const uint32_t row1 = ((n + 1) >> 3) * 1024 + ((n + 1) & 7) * 128, r1 = (n + 1) & 7;
+    // A 128-bit store is serviced in phases of 8 consecutive threads; threads
+    // with bit 2 set store the odd word of their pair first, so each phase
+    // covers all eight rows of a swizzle atom (conflict-free).
+    const unsigned sw = (e >> 2) & 1;
+    const unsigned mA = n + sw, mB = n + 1 - sw;
+    const uint32_t rowA = (mA >> 3) * 1024 + (mA & 7) * 128, rA = mA & 7;
+    const uint32_t rowB = (mB >> 3) * 1024 + (mB & 7) * 128, rB = mB & 7;
     for (unsigned k = 0; k < nst; k++) {
       const unsigned sl = k % kLd, bs = k % kBs;
       if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
@@ -342,18 +347,19 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
       }
       uint8_t* bt = b_p + bs * kBBytes;
       // row of word n: low halves of the 8 inputs; word n+1: high halves
-      uint32_t p0[4], p1[4];
+      uint32_t pA[4], pB[4];
+      const uint32_t selA = sw ? 0x7632u : 0x5410u, selB = sw ? 0x5410u : 0x7632u;
 #pragma unroll
       for (int q = 0; q < 4; q++) {
-        p0[q] = __byte_perm(v[2 * q], v[2 * q + 1], 0x5410);
-        p1[q] = __byte_perm(v[2 * q], v[2 * q + 1], 0x7632);
+        pA[q] = __byte_perm(v[2 * q], v[2 * q + 1], selA);
+        pB[q] = __byte_perm(v[2 * q], v[2 * q + 1], selB);
       }
 #pragma unroll
       for (int j = 0; j < 8; j++) {
-        *reinterpret_cast<uint4*>(bt + row0 + ((j ^ r0) << 4)) =
-            make_uint4(p0[0] >> j, p0[1] >> j, p0[2] >> j, p0[3] >> j);
-        *reinterpret_cast<uint4*>(bt + row1 + ((j ^ r1) << 4)) =
-            make_uint4(p1[0] >> j, p1[1] >> j, p1[2] >> j, p1[3] >> j);
+        *reinterpret_cast<uint4*>(bt + rowA + ((j ^ rA) << 4)) =
+            make_uint4(pA[0] >> j, pA[1] >> j, pA[2] >> j, pA[3] >> j);
+        *reinterpret_cast<uint4*>(bt + rowB + ((j ^ rB) << 4)) =
+            make_uint4(pB[0] >> j, pB[1] >> j, pB[2] >> j, pB[3] >> j);
       }
       fence_async_smem();
       mbar_arrive(BAR(B_FULL + bs));
