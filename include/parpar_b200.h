@@ -50,6 +50,7 @@ extern "C" {
 #define PP_ERR_NO_DEVICE (-7)
 #define PP_ERR_UNSUPPORTED (-8)
 #define PP_ERR_TIMEOUT (-9)       /* a bounded device-side wait gave up (kernel returned early) */
+#define PP_ERR_TOO_LARGE (-10)    /* size above a fixed maximum of an allocation-free entry point */
 
 /* reference PAR2ProcBackendAddResult (gf16/controller.h:38-43) */
 #define PP_PROC_ADD_OK 0
@@ -218,6 +219,24 @@ PP_API int pp_gf64_region_2d_muladd_arr(pp_ctx* ctx, uint64_t* const* outs, size
 /* out[i] = inverse(in[i]), inverse(0) = 0 (replaces gf64_inverse_batch,
  * gf64/gf64_invert.c:71-75). */
 PP_API int pp_gf64_inverse_batch(pp_ctx* ctx, uint64_t* out, const uint64_t* in, size_t n);
+
+/* Allocation-free solve.  No counterpart in the reference: an addition for
+ * callers that cannot allocate device memory where they need the repair solve
+ * (a device pool owned by another allocator with no headroom, latency-bound
+ * loops that cannot take cudaMalloc's device-wide synchronisation, services
+ * that must not fail for lack of memory after start-up).
+ * Same result and return codes as pp_gf64_solve_and_reconstruct, but: A and
+ * rhs must be device memory; work is enqueued on `cuda_stream` (NULL = the
+ * legacy default stream) and the call waits for it; nothing is allocated.
+ * Working storage is a fixed array inside the library (about 32 KiB, held on
+ * every GPU that loads the library until exit), so n is limited to
+ * PP_NOALLOC_SOLVE_MAX_N (larger n -> PP_ERR_TOO_LARGE), and calls that overlap
+ * on the GPU share that array and race.  The first call on a device looks up
+ * the array's device address (with that device current); make that first
+ * call before any stream capture. */
+#define PP_NOALLOC_SOLVE_MAX_N 4096
+PP_API int pp_gf64_solve_and_reconstruct_noalloc(uint64_t* A, uint64_t* rhs, size_t n, size_t block_size64,
+                                                 void* cuda_stream);
 
 /* Additive FFT over GF(2^64), novel-polynomial basis on the Cantor basis
  * (replaces gf64_addfft64_fwd_recursive_scratch / _inv_recursive_scratch,

@@ -24,6 +24,8 @@ PP_ERR_BUSY = -6
 PP_ERR_NO_DEVICE = -7
 PP_ERR_UNSUPPORTED = -8
 PP_ERR_TIMEOUT = -9
+PP_ERR_TOO_LARGE = -10
+PP_NOALLOC_SOLVE_MAX_N = 4096
 
 PP_GF16_KERNEL_AUTO = 0
 PP_GF16_KERNEL_LUT = 1
@@ -53,6 +55,7 @@ EXPORTS = [
     "pp_gf64_region_mul", "pp_gf64_region_mul_arr", "pp_gf64_region_muladd_arr",
     "pp_gf64_region_coupled_muladd_arr", "pp_gf64_region_fused_output_muladd_arr",
     "pp_gf64_region_2d_muladd_arr", "pp_gf64_inverse_batch", "pp_gf64_fft_fwd", "pp_gf64_fft_inv",
+    "pp_gf64_solve_and_reconstruct_noalloc",
 ]
 
 
@@ -131,6 +134,7 @@ _sig("pp_gf64_region_2d_muladd_arr", _I, _P, _P, _SZ, _P, _SZ, _P, _SZ, _SZ)
 _sig("pp_gf64_inverse_batch", _I, _P, _P, _P, _SZ)
 _sig("pp_gf64_fft_fwd", _I, _P, _P, _SZ, _SZ, _SZ)
 _sig("pp_gf64_fft_inv", _I, _P, _P, _SZ, _SZ, _SZ)
+_sig("pp_gf64_solve_and_reconstruct_noalloc", _I, _P, _P, _SZ, _SZ, _P)
 
 
 def status_string(s: int) -> str:

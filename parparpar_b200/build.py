@@ -24,6 +24,7 @@ SOURCES = [
     "gf64_kernels.cu",
     "gf64_fft.cu",
     "capi.cpp",
+    "noalloc.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

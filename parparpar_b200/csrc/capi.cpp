@@ -207,6 +207,8 @@ PP_API const char* pp_status_string(int s) {
     case PP_ERR_BUSY: return "staging area busy";
     case PP_ERR_NO_DEVICE: return "no CUDA device";
     case PP_ERR_UNSUPPORTED: return "unsupported";
+    case PP_ERR_TIMEOUT: return "device wait timed out";
+    case PP_ERR_TOO_LARGE: return "size above the entry point's fixed maximum";
     default: return "unknown status";
   }
 }
