@@ -198,6 +198,21 @@ PP_API int pp_gf64_compute_recovery_with_coeff(pp_ctx* ctx, const uint64_t* inpu
  * contents of A and rhs are unspecified. */
 PP_API int pp_gf64_solve_and_reconstruct(pp_ctx* ctx, uint64_t* A, uint64_t* rhs, size_t n, size_t block_size64);
 
+/* PAR3 repair in one call (the decode of lib/par3gen.js:3840-4010 on the
+ * device): with y_eq = first_recovery + eq for eq < n and x_k = first_input + k,
+ *   A[eq][col] = inv(x_{missing[col]} ^ y_eq)                 (0 -> 1)
+ *   rhs[eq]    = recovery[eq] (zero where recovery_present[eq] == 0)
+ *                ^ XOR_{k not missing} inv(x_k ^ y_eq) * inputs[k]
+ *   restored   = solution of A * restored = rhs  (Gauss-Jordan, as SolveAndReconstruct)
+ * inputs: num_inputs blocks of block_size64 words (rows of lost blocks are not
+ * read); missing: n distinct block indices; recovery: n blocks (block eq holds
+ * recovery block first_recovery + eq); recovery_present: n flags or NULL (all
+ * present); restored: n blocks, restored[col] = input block missing[col].
+ * Returns PP_ERR_SINGULAR where the reference's solve returns -1. */
+PP_API int pp_gf64_repair(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs, const uint64_t* missing, size_t n,
+                          const uint64_t* recovery, const uint8_t* recovery_present, size_t block_size64,
+                          uint64_t first_input, uint64_t first_recovery, uint64_t* restored);
+
 /* Region primitives (replace the gf64_region_* dispatch pointers,
  * gf64/gf64_global.h:23-37; semantics gf64/gf64_region_scalar.c:8-91). */
 PP_API int pp_gf64_region_mul(pp_ctx* ctx, uint64_t* out, const uint64_t* in, size_t len, uint64_t constant);

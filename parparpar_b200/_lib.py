@@ -55,7 +55,7 @@ EXPORTS = [
     "pp_gf64_region_mul", "pp_gf64_region_mul_arr", "pp_gf64_region_muladd_arr",
     "pp_gf64_region_coupled_muladd_arr", "pp_gf64_region_fused_output_muladd_arr",
     "pp_gf64_region_2d_muladd_arr", "pp_gf64_inverse_batch", "pp_gf64_fft_fwd", "pp_gf64_fft_inv",
-    "pp_gf64_solve_and_reconstruct_noalloc",
+    "pp_gf64_solve_and_reconstruct_noalloc", "pp_gf64_repair",
 ]
 
 
@@ -135,6 +135,7 @@ _sig("pp_gf64_inverse_batch", _I, _P, _P, _P, _SZ)
 _sig("pp_gf64_fft_fwd", _I, _P, _P, _SZ, _SZ, _SZ)
 _sig("pp_gf64_fft_inv", _I, _P, _P, _SZ, _SZ, _SZ)
 _sig("pp_gf64_solve_and_reconstruct_noalloc", _I, _P, _P, _SZ, _SZ, _P)
+_sig("pp_gf64_repair", _I, _P, _P, _SZ, _P, _SZ, _P, _P, _SZ, _U64, _U64, _P)
 
 
 def status_string(s: int) -> str:

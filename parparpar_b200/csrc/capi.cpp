@@ -1154,4 +1154,72 @@ PP_API int pp_gf64_fft_inv(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, 
   return gf64_fft_common(ctx, data, n, batch, ld, true);
 }
 
+PP_API int pp_gf64_repair(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs, const uint64_t* missing, size_t n,
+                          const uint64_t* recovery, const uint8_t* recovery_present, size_t B, uint64_t first_input,
+                          uint64_t first_recovery, uint64_t* restored) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (n == 0 || B == 0) return PP_OK;
+  if (!inputs || !missing || !recovery || !restored) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if (n > num_inputs) return set_err(ctx, PP_ERR_INVALID_ARG, "more lost blocks than inputs");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  // host bookkeeping: lost-block set and the per-input row pointers
+  std::vector<uint64_t> miss(n);
+  if (is_device_ptr(missing))
+    CUDA_TRY(ctx, cudaMemcpy(miss.data(), missing, n * 8, cudaMemcpyDeviceToHost));
+  else
+    memcpy(miss.data(), missing, n * 8);
+  std::vector<uint8_t> lost(num_inputs, 0);
+  for (size_t c = 0; c < n; c++) {
+    if (miss[c] >= num_inputs || lost[miss[c]]) return set_err(ctx, PP_ERR_INVALID_ARG, "bad missing index list");
+    lost[miss[c]] = 1;
+  }
+  const bool in_dev = is_device_ptr(inputs), out_dev = is_device_ptr(restored), rec_dev = is_device_ptr(recovery);
+  const uint64_t* din = inputs;
+  if (!in_dev) {
+    uint64_t* st = (uint64_t*)scratch(ctx, S_IN, num_inputs * B * 8);
+    if (!st) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging");
+    CUDA_TRY(ctx, cudaMemcpyAsync(st, inputs, num_inputs * B * 8, cudaMemcpyHostToDevice, ctx->stream));
+    din = st;
+  }
+  // rhs = recovery rows (absent rows zero), then the known-input sum
+  uint64_t* rhs = out_dev ? restored : (uint64_t*)scratch(ctx, S_OUT, n * B * 8);
+  uint64_t* zero = (uint64_t*)scratch(ctx, S_C, B * 8);
+  uint64_t* dA = (uint64_t*)scratch(ctx, S_D, n * n * 8 + n * 8);
+  uint64_t* dF = (uint64_t*)scratch(ctx, S_E, (n + 2) * 8 + 64);
+  if (!rhs || !zero || !dA || !dF) return set_err(ctx, PP_ERR_NO_MEMORY, "repair buffers");
+  uint64_t* dcols = dA + n * n;
+  CUDA_TRY(ctx, cudaMemsetAsync(zero, 0, B * 8, ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpyAsync(rhs, recovery, n * B * 8, rec_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                ctx->stream));
+  if (recovery_present) {
+    for (size_t eq = 0; eq < n; eq++)
+      if (!recovery_present[eq]) CUDA_TRY(ctx, cudaMemsetAsync(rhs + eq * B, 0, B * 8, ctx->stream));
+  }
+  int st;
+  uint64_t* M = cauchy_get(ctx, num_inputs, n, first_input, first_recovery, &st);
+  if (!M) return st;
+  std::vector<const uint64_t*> in_ptrs(num_inputs);
+  for (size_t k = 0; k < num_inputs; k++) in_ptrs[k] = lost[k] ? zero : din + k * B;
+  std::vector<uint64_t*> out_ptrs(n);
+  for (size_t eq = 0; eq < n; eq++) out_ptrs[eq] = rhs + eq * B;
+  const uint64_t* const* dpin = to_device(ctx, S_A, in_ptrs.data(), num_inputs, &st);
+  if (st) return st;
+  uint64_t* const* dpout = (uint64_t* const*)to_device(ctx, S_B, (const uint64_t* const*)out_ptrs.data(), n, &st);
+  if (st) return st;
+  CUDA_TRY(ctx, launch_gf64_2d_gather(dpout, n, dpin, num_inputs, M, num_inputs, B, ctx->sms, ctx->stream));
+  // the n x n system over the lost columns, then the solve
+  CUDA_TRY(ctx, cudaMemcpyAsync(dcols, miss.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(ctx, launch_gf64_cauchy_cols(dA, n, dcols, n, first_input, first_recovery, ctx->stream));
+  int* dS = (int*)(dF + n + 2);
+  CUDA_TRY(ctx, cudaMemsetAsync(dS, 0, sizeof(int), ctx->stream));
+  CUDA_TRY(ctx, launch_gf64_solve(dA, rhs, n, B, dF, dS, ctx->stream));
+  int hs = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&hs, dS, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(restored, rhs, n * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (hs != 0) return set_err(ctx, PP_ERR_SINGULAR, "repair matrix is singular");
+  return device_status(ctx);
+}
+
 }  // extern "C"

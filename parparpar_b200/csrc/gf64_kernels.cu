@@ -64,6 +64,29 @@ cudaError_t launch_gf64_cauchy(uint64_t* d_m, size_t n_in, size_t n_rec, uint64_
   return cudaGetLastError();
 }
 
+// A[r][c] = inv((fI + cols[c]) ^ (fR + r)), zero denominators mapped to 1:
+// the repair system of lib/par3gen.js:3864-3880 (rows = the first n recovery
+// equations, columns = the lost input blocks).
+__global__ void k_gf64_cauchy_cols(uint64_t* __restrict__ A, size_t n_rows, const uint64_t* __restrict__ cols,
+                                   size_t n_cols, uint64_t fI, uint64_t fR) {
+  const size_t total = n_rows * n_cols;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = t / n_cols, c = t % n_cols;
+    uint64_t d = (fI + cols[c]) ^ (fR + r);
+    A[t] = gf64_inv(d ? d : 1);
+  }
+}
+
+cudaError_t launch_gf64_cauchy_cols(uint64_t* d_A, size_t n_rows, const uint64_t* d_cols, size_t n_cols, uint64_t fI,
+                                    uint64_t fR, cudaStream_t s) {
+  const size_t total = n_rows * n_cols;
+  if (!total) return cudaSuccess;
+  size_t blocks = std::min<size_t>(ceil_div(total, 128), 148 * 64);
+  k_gf64_cauchy_cols<<<(unsigned)blocks, 128, 0, s>>>(d_A, n_rows, d_cols, n_cols, fI, fR);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // inverse of every element, inverse(0) = 0 (reference gf64/gf64_invert.c:29-75)
 __global__ void __launch_bounds__(128)
 k_gf64_inverse_batch(uint64_t* __restrict__ out, const uint64_t* __restrict__ in, size_t n) {

@@ -54,6 +54,8 @@ cudaError_t launch_gf16_build_rec_matrix(const uint16_t* d_logs, const uint32_t*
 // ------------------------------------------------------------ GF(2^64)
 cudaError_t launch_gf64_cauchy(uint64_t* d_m, size_t n_in, size_t n_rec, uint64_t first_in, uint64_t first_rec,
                                size_t ld, cudaStream_t s);
+cudaError_t launch_gf64_cauchy_cols(uint64_t* d_A, size_t n_rows, const uint64_t* d_cols, size_t n_cols, uint64_t fI,
+                                    uint64_t fR, cudaStream_t s);
 cudaError_t launch_gf64_inverse_batch(uint64_t* d_out, const uint64_t* d_in, size_t n, cudaStream_t s);
 
 // out[r][w] (^)= XOR_c coeff[r*ldc + c] * in[c][w]

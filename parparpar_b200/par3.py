@@ -189,6 +189,26 @@ def solve_and_reconstruct(A, rhs, n, blockSize):
     return rhs
 
 
+def repair(inputs, missing, recovery, block_size64, first_input, first_recovery, restored=None,
+           recovery_present=None, ctx=None):
+    """PAR3 repair on the device (lib/par3gen.js:3840-4010): solve for the
+    lost input blocks `missing` from the first len(missing) recovery blocks.
+    inputs: (N, B) words (lost rows ignored); recovery: (n, B); returns the
+    restored (n, B) blocks.  Raises PPError(PP_ERR_SINGULAR) where the
+    reference's solve returns -1."""
+    c = _ctx(ctx)
+    miss = np.ascontiguousarray(np.asarray(missing, dtype=np.uint64))
+    n = miss.size
+    num_inputs = inputs.shape[0]
+    if restored is None:
+        restored = np.zeros((n, block_size64), dtype=np.uint64)
+    pres = None if recovery_present is None else np.ascontiguousarray(np.asarray(recovery_present, dtype=np.uint8))
+    c.check(lib.pp_gf64_repair(c.h, ptr(inputs), num_inputs, ptr(miss), n, ptr(recovery),
+                               ptr(pres) if pres is not None else None, block_size64, _u64(first_input),
+                               _u64(first_recovery), ptr(restored)))
+    return restored
+
+
 # ------------------------------------------------------------- region table
 def gf64_region_mul(out, inp, length, constant, ctx=None):
     c = _ctx(ctx)

@@ -183,3 +183,39 @@ def test_par3_repair_roundtrip(ctx):
                                                        np.ascontiguousarray(M[:, known]), accumulate=True)
     assert par3.GF64Controller.SolveAndReconstruct(A, rhs, n, B) == 0
     assert np.array_equal(rhs, data[lost])
+
+
+def test_par3_repair_fused_vs_oracle(ctx, oracle):
+    """pp_gf64_repair (the decode of lib/par3gen.js:3840-4010 on the device):
+    restores the lost blocks; with an absent recovery block (its rhs row
+    zero-filled, as the reference does) it matches the oracle's solution of
+    the same system bit for bit."""
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(45)
+    N, R, B = 300, 12, 96
+    data = rng.integers(0, 2**64, (N, B), dtype=np.uint64)
+    rec = oracle.gf64_compute_recovery(data, R, 0, N)
+    lost = np.sort(rng.choice(N, 7, replace=False))
+    n = lost.size
+    damaged = data.copy()
+    damaged[lost] = rng.integers(0, 2**64, (n, B), dtype=np.uint64)  # lost rows must not be read
+    restored = par3.repair(damaged, lost, rec[:n].copy(), B, 0, N, ctx=ctx)
+    assert np.array_equal(restored, data[lost])
+    # device buffers
+    d_out = _dev(np.zeros((n, B), dtype=np.uint64))
+    par3.repair(_dev(damaged), lost, _dev(rec[:n]), B, 0, N, restored=d_out, ctx=ctx)
+    ctx.synchronize()
+    assert np.array_equal(_host(d_out), data[lost])
+    # recovery block 3 absent: rhs row 3 zero
+    present = np.ones(n, dtype=np.uint8)
+    present[3] = 0
+    got = par3.repair(damaged, lost, rec[:n].copy(), B, 0, N, recovery_present=present, ctx=ctx)
+    M = oracle.gf64_build_cauchy(N, n, 0, N)
+    known = np.setdiff1d(np.arange(N), lost)
+    rhs = rec[:n].copy()
+    rhs[3] = 0
+    oracle.gf64_matvec(np.ascontiguousarray(data[known]), np.ascontiguousarray(M[:, known]), out=rhs,
+                       accumulate=True)
+    A = np.ascontiguousarray(M[:, lost])
+    assert oracle.gf64_solve_and_reconstruct(A, rhs) == 0
+    assert np.array_equal(got, rhs)
