@@ -65,7 +65,7 @@ extern "C" {
 #define PP_GF64_KERNEL_BARYCENTRIC 2
 #define PP_GF64_KERNEL_FENGER 3
 
-/* GF(2^16) region kernel selection (pp_ctx_set_gf16_kernel) */
+/* Region kernel selection (pp_ctx_set_gf16_kernel / pp_ctx_set_gf64_kernel) */
 #define PP_GF16_KERNEL_AUTO 0
 #define PP_GF16_KERNEL_LUT 1      /* shared-memory 4-bit split tables */
 #define PP_GF16_KERNEL_TENSOR 2   /* tcgen05 u8 MMA over the GF(2) bit matrices */
@@ -90,6 +90,8 @@ PP_API uint64_t pp_launch_count(void);
 PP_API int pp_ctx_free_cache(pp_ctx* ctx);
 /* Choose the GF(2^16) region kernel used by this context (PP_GF16_KERNEL_*). */
 PP_API int pp_ctx_set_gf16_kernel(pp_ctx* ctx, int kernel);
+/* Choose the GF(2^64) region kernel used by this context (same constants). */
+PP_API int pp_ctx_set_gf64_kernel(pp_ctx* ctx, int kernel);
 
 /* ============================================================ PAR2 / GF16 */
 

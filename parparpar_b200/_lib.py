@@ -44,7 +44,7 @@ PP_GF64_KERNEL_FENGER = 3
 EXPORTS = [
     "pp_version", "pp_status_string", "pp_ctx_create", "pp_ctx_destroy", "pp_ctx_set_stream",
     "pp_ctx_get_stream", "pp_ctx_synchronize", "pp_ctx_last_error", "pp_launch_count", "pp_ctx_free_cache",
-    "pp_ctx_set_gf16_kernel",
+    "pp_ctx_set_gf16_kernel", "pp_ctx_set_gf64_kernel",
     "pp_par2_coeff", "pp_par2_input_log", "pp_par2_coeff_matrix", "pp_gf16_muladd", "pp_par2_create",
     "pp_par2_invert", "pp_par2_proc_create", "pp_par2_proc_destroy", "pp_par2_proc_set_current_slice_size",
     "pp_par2_proc_set_recovery_slices", "pp_par2_proc_can_add", "pp_par2_proc_wait_for_add",
@@ -100,6 +100,7 @@ _sig("pp_ctx_last_error", ctypes.c_char_p, _P)
 _sig("pp_launch_count", _U64)
 _sig("pp_ctx_free_cache", _I, _P)
 _sig("pp_ctx_set_gf16_kernel", _I, _P, _I)
+_sig("pp_ctx_set_gf64_kernel", _I, _P, _I)
 _sig("pp_par2_coeff", _U16, _U16, _U16)
 _sig("pp_par2_input_log", _U16, _U16)
 _sig("pp_par2_coeff_matrix", _I, _P, _P, _U, _P, _U, _P)
@@ -167,6 +168,10 @@ class Context:
     def set_gf16_kernel(self, kernel: int):
         """PP_GF16_KERNEL_AUTO / _LUT / _TENSOR"""
         self.check(lib.pp_ctx_set_gf16_kernel(self.h, kernel))
+
+    def set_gf64_kernel(self, kernel: int):
+        """PP_GF16_KERNEL_AUTO / _LUT / _TENSOR for the GF(2^64) region kernel"""
+        self.check(lib.pp_ctx_set_gf64_kernel(self.h, kernel))
 
     def free_cache(self):
         self.check(lib.pp_ctx_free_cache(self.h))

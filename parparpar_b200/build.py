@@ -22,6 +22,7 @@ SOURCES = [
     "gf16_kernels.cu",
     "gf16_tc.cu",
     "gf64_kernels.cu",
+    "gf64_tc.cu",
     "gf64_fft.cu",
     "capi.cpp",
     "noalloc.cu",

@@ -87,6 +87,7 @@ struct pp_ctx {
   size_t slot_n[S_NSLOTS] = {};
   std::list<CauchyEntry> cauchy;  // LRU, front = most recent
   int gf16_kernel = PP_GF16_KERNEL_AUTO;
+  int gf64_kernel = PP_GF16_KERNEL_AUTO;
   int* d_status = nullptr;  // set nonzero by a kernel whose bounded wait gave up
   std::mutex mu;
 };
@@ -246,6 +247,10 @@ PP_API int pp_ctx_create(int device, pp_ctx** out) {
     if (!strcmp(k, "lut")) ctx->gf16_kernel = PP_GF16_KERNEL_LUT;
     else if (!strcmp(k, "tensor")) ctx->gf16_kernel = PP_GF16_KERNEL_TENSOR;
   }
+  if (const char* k = getenv("PP_GF64_KERNEL")) {
+    if (!strcmp(k, "lut")) ctx->gf64_kernel = PP_GF16_KERNEL_LUT;
+    else if (!strcmp(k, "tensor")) ctx->gf64_kernel = PP_GF16_KERNEL_TENSOR;
+  }
   *out = ctx;
   return PP_OK;
 }
@@ -289,6 +294,12 @@ PP_API int pp_ctx_synchronize(pp_ctx* ctx) {
 PP_API int pp_ctx_set_gf16_kernel(pp_ctx* ctx, int kernel) {
   if (!ctx || kernel < PP_GF16_KERNEL_AUTO || kernel > PP_GF16_KERNEL_TENSOR) return PP_ERR_INVALID_ARG;
   ctx->gf16_kernel = kernel;
+  return PP_OK;
+}
+
+PP_API int pp_ctx_set_gf64_kernel(pp_ctx* ctx, int kernel) {
+  if (!ctx || kernel < PP_GF16_KERNEL_AUTO || kernel > PP_GF16_KERNEL_TENSOR) return PP_ERR_INVALID_ARG;
+  ctx->gf64_kernel = kernel;
   return PP_OK;
 }
 PP_API const char* pp_ctx_last_error(pp_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
@@ -867,6 +878,29 @@ PP_API int pp_gf64_build_cauchy(pp_ctx* ctx, uint64_t* coeff, size_t num_inputs,
   return PP_OK;
 }
 
+// GF(2^64) region dispatch.  The tensor-core kernel copies rows with 16-byte
+// bulk copies, so it needs 16-byte aligned rows and an even word count;
+// otherwise (or when the lookup kernel is selected) the lookup kernel runs.
+static bool aligned_rows64(const uint64_t* base, size_t stride) {
+  return ((uintptr_t)base % 16) == 0 && (stride % 2) == 0;
+}
+static cudaError_t gf64_region(pp_ctx* ctx, const uint64_t* din, const uint64_t* const* d_in_ptrs, size_t in_stride,
+                               size_t n_in, size_t words, const uint64_t* d_coeff, size_t ldc, size_t n_out,
+                               uint64_t* dout, uint64_t* const* d_out_ptrs, size_t out_stride, bool accumulate,
+                               bool rows_aligned) {
+  const bool tc_ok = rows_aligned && (words % 2) == 0 && n_in >= 2;
+  const bool tc = ctx->gf64_kernel == PP_GF16_KERNEL_TENSOR ? tc_ok
+                  : ctx->gf64_kernel == PP_GF16_KERNEL_LUT   ? false
+                                                             : tc_ok;
+  if (tc)
+    return launch_gf64_matvec_tc(din, d_in_ptrs, in_stride, n_in, words, d_coeff, ldc, n_out, dout, d_out_ptrs,
+                                 out_stride, accumulate, ctx->sms, ctx->d_status, ctx->stream);
+  if (d_in_ptrs || d_out_ptrs)
+    return launch_gf64_2d_gather(d_out_ptrs, n_out, d_in_ptrs, n_in, d_coeff, ldc, words, ctx->sms, ctx->stream);
+  return launch_gf64_matvec(din, in_stride, n_in, words, d_coeff, ldc, n_out, dout, out_stride, accumulate, ctx->sms,
+                            ctx->stream);
+}
+
 static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, uint64_t* recovery, size_t n_rec,
                             size_t B, const uint64_t* d_coeff, bool accumulate) {
   const bool in_dev = is_device_ptr(inputs);
@@ -885,10 +919,13 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
     if (accumulate)
       CUDA_TRY(ctx, cudaMemcpyAsync(dout, recovery, n_rec * B * 8, cudaMemcpyHostToDevice, ctx->stream));
   }
-  CUDA_TRY(ctx, launch_gf64_matvec(din, B, n_in, B, d_coeff, n_in, n_rec, dout, B, accumulate, ctx->sms,
-                                   ctx->stream));
+  CUDA_TRY(ctx, gf64_region(ctx, din, nullptr, B, n_in, B, d_coeff, n_in, n_rec, dout, nullptr, B, accumulate,
+                            aligned_rows64(din, B) && aligned_rows64(dout, B)));
   if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(recovery, dout, n_rec * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  if (!in_dev || !out_dev) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!in_dev || !out_dev) {
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return device_status(ctx);
+  }
   return PP_OK;
 }
 
@@ -1035,13 +1072,16 @@ static int region_2d(pp_ctx* ctx, uint64_t* const* outs, size_t K, const uint64_
   if (st) return st;
   uint64_t* const* dpout = (uint64_t* const*)to_device(ctx, S_B, (const uint64_t* const*)dout.data(), K, &st);
   if (st) return st;
-  CUDA_TRY(ctx, launch_gf64_2d_gather(dpout, K, dpin, G, dC, G, len, ctx->sms, ctx->stream));
+  bool al = (len % 2) == 0;
+  for (size_t g2 = 0; g2 < G && al; g2++) al = ((uintptr_t)din[g2] % 16) == 0;
+  for (size_t k = 0; k < K && al; k++) al = ((uintptr_t)dout[k] % 16) == 0;
+  CUDA_TRY(ctx, gf64_region(ctx, nullptr, dpin, 0, G, len, dC, G, K, nullptr, dpout, 0, true, al));
   if (!all_dev) {
     for (size_t k = 0; k < K; k++)
       CUDA_TRY(ctx, cudaMemcpyAsync(outs[k], sout + k * len, len * 8, cudaMemcpyDefault, ctx->stream));
   }
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  return PP_OK;
+  return device_status(ctx);
 }
 
 PP_API int pp_gf64_region_coupled_muladd_arr(pp_ctx* ctx, uint64_t* out, const uint64_t* const* in_blocks,
@@ -1207,7 +1247,8 @@ PP_API int pp_gf64_repair(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs
   if (st) return st;
   uint64_t* const* dpout = (uint64_t* const*)to_device(ctx, S_B, (const uint64_t* const*)out_ptrs.data(), n, &st);
   if (st) return st;
-  CUDA_TRY(ctx, launch_gf64_2d_gather(dpout, n, dpin, num_inputs, M, num_inputs, B, ctx->sms, ctx->stream));
+  bool al = (B % 2) == 0 && ((uintptr_t)din % 16) == 0 && ((uintptr_t)rhs % 16) == 0 && ((uintptr_t)zero % 16) == 0;
+  CUDA_TRY(ctx, gf64_region(ctx, nullptr, dpin, 0, num_inputs, B, M, num_inputs, n, nullptr, dpout, 0, true, al));
   // the n x n system over the lost columns, then the solve
   CUDA_TRY(ctx, cudaMemcpyAsync(dcols, miss.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(ctx, launch_gf64_cauchy_cols(dA, n, dcols, n, first_input, first_recovery, ctx->stream));

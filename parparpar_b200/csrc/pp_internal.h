@@ -64,6 +64,14 @@ cudaError_t launch_gf64_matvec(const uint64_t* d_in, size_t in_stride, size_t n_
                                const uint64_t* d_coeff, size_t ldc, size_t n_out, uint64_t* d_out,
                                size_t out_stride, bool accumulate, int sms, cudaStream_t s);
 
+// Tensor-core (tcgen05) variant of the matvec; optional device pointer tables
+// for the rows (NULL: strided).  Requires 16-byte aligned rows and an even
+// word count.  *d_status is set nonzero if a bounded device wait gave up.
+cudaError_t launch_gf64_matvec_tc(const uint64_t* d_in, const uint64_t* const* d_in_ptrs, size_t in_stride,
+                                  size_t n_in, size_t words, const uint64_t* d_coeff, size_t ldc, size_t n_out,
+                                  uint64_t* d_out, uint64_t* const* d_out_ptrs, size_t out_stride, bool accumulate,
+                                  int sms, int* d_status, cudaStream_t s);
+
 // Gather form used by the region entry points: pointer tables on the device.
 //   outs[k][w] ^= XOR_g in_blocks[g][w] * coeff[k*kstride + g]
 cudaError_t launch_gf64_2d_gather(uint64_t* const* d_outs, size_t K, const uint64_t* const* d_ins, size_t G,

@@ -8,6 +8,17 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=["lut", "tensor"])
+def kctx(ctx, request):
+    """The default context with the GF(2^64) region kernel forced to one
+    implementation (the tensor kernel applies where rows are 16-byte aligned
+    and the word count is even; other shapes use the lookup kernel)."""
+    import parparpar_b200._lib as L
+    ctx.set_gf64_kernel(L.PP_GF16_KERNEL_LUT if request.param == "lut" else L.PP_GF16_KERNEL_TENSOR)
+    yield ctx
+    ctx.set_gf64_kernel(L.PP_GF16_KERNEL_AUTO)
+
+
 def _dev(a):
     import torch
     return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
@@ -17,7 +28,7 @@ def _host(t):
     return t.cpu().numpy().view(np.uint64)
 
 
-def test_par3_golden_all_kernels(ctx, golden):
+def test_par3_golden_all_kernels(kctx, golden):
     from parparpar_b200 import par3
     g = golden("par3_golden.npz")
     inp = g["inputs"]
@@ -28,17 +39,17 @@ def test_par3_golden_all_kernels(ctx, golden):
         assert zlib.crc32(out.tobytes()) == 0x6A941C15, fn.__name__
 
 
-def test_gf64_ops_golden(ctx, golden):
+def test_gf64_ops_golden(kctx, golden):
     from parparpar_b200 import par3
     g = golden("gf64_ops.npz")
     a, b = g["a"], g["b"]
     out = np.zeros_like(a)
     for i in range(0, 64):
-        par3.gf64_region_mul(out[i:i + 1], a[i:i + 1], 1, int(b[i]), ctx)
+        par3.gf64_region_mul(out[i:i + 1], a[i:i + 1], 1, int(b[i]), kctx)
     assert np.array_equal(out[:64], g["prod"][:64])
     par3.gf64_region_mul_arr(out, a, b, a.size, 1)  # n_coeff=1: all by b[0]
     inv = np.zeros_like(a)
-    par3.gf64_inverse_batch(inv, a, a.size, ctx)
+    par3.gf64_inverse_batch(inv, a, a.size, kctx)
     assert np.array_equal(inv, g["inv"])
     assert np.array_equal(par3.GF64Controller.BuildCauchyMatrixAlloc(37, 9, 3, 40), g["cauchy"])
     assert np.array_equal(par3.GF64Controller.BuildCauchyMatrixAlloc(8, 4, 0, 2), g["cauchy_clash"])
@@ -76,8 +87,9 @@ def test_region_elementwise_vs_oracle(ctx, oracle):
 @pytest.mark.parametrize("n,r,b,fi,fr", [
     (1, 1, 1, 0, 1), (2, 7, 3, 0, 2), (5, 8, 128, 0, 5), (64, 9, 1000, 0, 64), (257, 33, 1025, 0, 257),
     (300, 8, 1024, 0, 300), (40, 17, 64, 5, 3), (1024, 1, 2048, 0, 1024), (3000, 8, 16, 0, 3000),
+    (3, 5, 514, 0, 3), (4001, 3, 1026, 7, 9000),
 ])
-def test_compute_recovery_vs_oracle(ctx, oracle, n, r, b, fi, fr):
+def test_compute_recovery_vs_oracle(kctx, oracle, n, r, b, fi, fr):
     from parparpar_b200 import par3
     rng = np.random.default_rng(n + r * 7 + b * 13)
     inp = rng.integers(0, 2**64, (n, b), dtype=np.uint64)
@@ -92,11 +104,11 @@ def test_compute_recovery_vs_oracle(ctx, oracle, n, r, b, fi, fr):
     # device-resident buffers
     dout = _dev(np.zeros((r, b), dtype=np.uint64))
     par3.GF64Controller.ComputeRecoveryBlocks(_dev(inp), n, dout, r, b, fi, fr)
-    ctx.synchronize()
+    kctx.synchronize()
     assert np.array_equal(_host(dout), exp)
 
 
-def test_with_coeff_and_build(ctx, oracle):
+def test_with_coeff_and_build(kctx, oracle):
     from parparpar_b200 import par3
     rng = np.random.default_rng(41)
     n, r, b = 70, 11, 300
@@ -110,11 +122,11 @@ def test_with_coeff_and_build(ctx, oracle):
     assert np.array_equal(m, oracle.gf64_build_cauchy(n, r, 2**40 + 3, 2**41 + 5))
     dm = _dev(np.zeros((r, n), dtype=np.uint64))
     par3.GF64Controller.BuildCauchyMatrix(dm, n, r, 7, 1000)
-    ctx.synchronize()
+    kctx.synchronize()
     assert np.array_equal(_host(dm), oracle.gf64_build_cauchy(n, r, 7, 1000))
 
 
-def test_pointer_table_region_ops(ctx, oracle):
+def test_pointer_table_region_ops(kctx, oracle):
     from parparpar_b200 import par3
     rng = np.random.default_rng(42)
     L, K, G = 777, 5, 9
@@ -165,7 +177,7 @@ def test_solve_vs_oracle(ctx, oracle):
             assert np.array_equal(A2, A1)
 
 
-def test_par3_repair_roundtrip(ctx):
+def test_par3_repair_roundtrip(kctx):
     """create -> erase -> (RHS via with_coeff) -> solve restores the blocks."""
     from parparpar_b200 import par3
     rng = np.random.default_rng(44)
@@ -185,7 +197,7 @@ def test_par3_repair_roundtrip(ctx):
     assert np.array_equal(rhs, data[lost])
 
 
-def test_par3_repair_fused_vs_oracle(ctx, oracle):
+def test_par3_repair_fused_vs_oracle(kctx, oracle):
     """pp_gf64_repair (the decode of lib/par3gen.js:3840-4010 on the device):
     restores the lost blocks; with an absent recovery block (its rhs row
     zero-filled, as the reference does) it matches the oracle's solution of
@@ -199,17 +211,17 @@ def test_par3_repair_fused_vs_oracle(ctx, oracle):
     n = lost.size
     damaged = data.copy()
     damaged[lost] = rng.integers(0, 2**64, (n, B), dtype=np.uint64)  # lost rows must not be read
-    restored = par3.repair(damaged, lost, rec[:n].copy(), B, 0, N, ctx=ctx)
+    restored = par3.repair(damaged, lost, rec[:n].copy(), B, 0, N, ctx=kctx)
     assert np.array_equal(restored, data[lost])
     # device buffers
     d_out = _dev(np.zeros((n, B), dtype=np.uint64))
-    par3.repair(_dev(damaged), lost, _dev(rec[:n]), B, 0, N, restored=d_out, ctx=ctx)
-    ctx.synchronize()
+    par3.repair(_dev(damaged), lost, _dev(rec[:n]), B, 0, N, restored=d_out, ctx=kctx)
+    kctx.synchronize()
     assert np.array_equal(_host(d_out), data[lost])
     # recovery block 3 absent: rhs row 3 zero
     present = np.ones(n, dtype=np.uint8)
     present[3] = 0
-    got = par3.repair(damaged, lost, rec[:n].copy(), B, 0, N, recovery_present=present, ctx=ctx)
+    got = par3.repair(damaged, lost, rec[:n].copy(), B, 0, N, recovery_present=present, ctx=kctx)
     M = oracle.gf64_build_cauchy(N, n, 0, N)
     known = np.setdiff1d(np.arange(N), lost)
     rhs = rec[:n].copy()
