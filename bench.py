@@ -208,6 +208,15 @@ def kernel_fn(job, ctx):
     return step_fn(job, ctx)
 
 
+def dominant_kernel(w, args):
+    """Name of the region kernel the library's dispatch picks for this workload
+    (AUTO: tensor cores for >= 8 GF(2^16) inputs, and for 16-byte aligned
+    GF(2^64) rows of an even word count)."""
+    if w["field"] == "gf16":
+        return "k_gf16_muladd_lut" if args.gf16_kernel == "lut" else "k_gf16_muladd_tc"
+    return "k_gf64_matvec_lut" if args.gf64_kernel == "lut" else "k_gf64_matvec_tc"
+
+
 def algo_bytes(job):
     if job["field"] == "gf64_repair":  # (N - n) known blocks + n recovery blocks read, n blocks written
         return (job["n"] + job["r"]) * job["s"]
@@ -326,6 +335,7 @@ def main():
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gf16-kernel", default="auto", choices=["auto", "lut", "tensor"])
+    ap.add_argument("--gf64-kernel", default="auto", choices=["auto", "lut", "tensor"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -353,6 +363,7 @@ def main():
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_gf16_kernel({"auto": 0, "lut": 1, "tensor": 2}[args.gf16_kernel])
+    ctx.set_gf64_kernel({"auto": 0, "lut": 1, "tensor": 2}[args.gf64_kernel])
     timer = Timer(stream)
     peak, peak_kind = load_peaks()
 
@@ -394,7 +405,13 @@ def main():
         h_in = torch.empty((w["n"], w["s"] // 8), dtype=torch.int64).pin_memory()
         h_in.copy_(job["d_in"])
         h_out = torch.empty((w["r"], w["s"] // 8), dtype=torch.int64).pin_memory()
-        e2e_f = lambda: par3.GF64Controller.ComputeRecoveryBlocks(h_in, w["n"], h_out, w["r"], w["s"] // 8, 0, w["n"])
+        if w["field"] == "gf64_repair":
+            h_rec = torch.empty_like(h_out).pin_memory()
+            h_rec.copy_(job["d_rec"])
+            e2e_f = lambda: par3.repair(h_in, job["lost"], h_rec, w["s"] // 8, 0, w["n"], restored=h_out, ctx=ctx)
+        else:
+            e2e_f = lambda: par3.GF64Controller.ComputeRecoveryBlocks(h_in, w["n"], h_out, w["r"], w["s"] // 8, 0,
+                                                                      w["n"])
     e2e_f()
     torch.cuda.synchronize()
     e2e_steps = max(2, min(args.steps, 5))
@@ -406,6 +423,7 @@ def main():
     del h_in, h_out
 
     input_bytes = w["n"] * w["s"]
+    h2d = input_bytes + (w["r"] * w["s"] if w["field"] == "gf64_repair" else 0)
     line = {
         "metric": f"{args.workload} input GB/s", "value": input_bytes * world / (ms * 1e-3) / 1e9, "unit": "GB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -416,10 +434,9 @@ def main():
                    "l2": "inputs (1 GiB) larger than L2; no flush needed"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                     else "fallback 6.65 TB/s", "kernel": "k_gf16_muladd_lut" if w["field"] == "gf16"
-                     else "k_gf64_matvec_lut", "kernel_ms": kms,
+                     else "fallback 6.65 TB/s", "kernel": dominant_kernel(w, args), "kernel_ms": kms,
                      "traffic": load_traffic(args.workload)},
-        "e2e": {"value": input_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": input_bytes,
+        "e2e": {"value": input_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": w["r"] * w["s"], "host_buffers": "pinned", "matches_device_result": bool(ok)},
         "gpu_launches": int(launches),
         "clocks": clocks,

@@ -399,7 +399,8 @@ cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigne
   const unsigned n_stages = (n_in + 7) / 8;
   const unsigned base = groups * wt;
   const unsigned target = (unsigned)(sms > 0 ? sms : 148);
-  unsigned splits = base >= target ? 1 : (unsigned)ceil_div(target, base);
+  // fill the SMs in one wave: floor, never more CTAs than SMs from splitting
+  unsigned splits = base >= target ? 1 : std::max(1u, target / base);
   // keep at least 8 stages per split so the pipeline fills
   unsigned max_splits = (unsigned)std::max<size_t>(1, n_stages / 8);
   if (splits > max_splits) splits = max_splits;

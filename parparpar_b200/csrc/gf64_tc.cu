@@ -21,11 +21,17 @@
 //
 //   warp 0      producer: cp.async.bulk of the 2 raw input rows of the tile
 //   warp 1      TMEM allocation + one thread issuing tcgen05.mma
-//   warps 2-9   per stage: each warp builds 32 rows of the A tile on the fly
-//               from one coefficient (64 products c*x^e, transposed with warp
-//               ballots into the rows Q_b); each thread writes the B rows of
-//               two words; then the epilogue (TMEM counts -> parity -> ballot
-//               -> 32-bit halves of the output words)
+//   warps 2-9   per stage: each thread builds one (row, input) half-chunk of
+//               the A tile from its coefficient with the closed form below
+//               and writes the B rows of two words; then the epilogue (TMEM
+//               counts -> parity -> ballot -> 32-bit halves of the output words)
+//
+// Closed form of the rows: with r = bitreverse(c) and x^64 = x^4+x^3+x+1,
+//   Q_b = (r >> (63-b)) ^ XOR_{s in {0,1,3,4}, d = b-s >= 0}
+//           [ (r << (d+1)) (d+1 < 64) ^ (r << (d+61)) (d <= 2) ^ (r << (d+62)) (d <= 1) ]
+// (the unreduced product c << e contributes r >> (63-b); each reduction term
+// s of x^64 contributes the bits of c >> (64-e) that land on bit b, and the
+// second fold of the top bits contributes the (d+61), (d+62) terms).
 //
 // Every mbarrier wait is bounded (about one second); on a timeout the CTA
 // records an error in *status, drains its copies and MMAs, frees TMEM and
@@ -167,19 +173,38 @@ k_gf64_matvec_tc(const uint64_t* __restrict__ in, const uint64_t* const* __restr
   } else {
     // ------------------------------------------------------------ operand builders
     const int e = threadIdx.x - 64;  // 0..255
-    const unsigned n = 2 * e;        // word pair n, n+1 of the tile
+    const unsigned n = 2 * e;        // B: word pair n, n+1 of the tile
     const unsigned sw = (e >> 2) & 1;  // store order: conflict-free 128-bit phases
     const unsigned mA = n + sw, mB = n + 1 - sw;
     const uint32_t rowA = (mA >> 3) * 1024 + (mA & 7) * 128, rA = mA & 7;
     const uint32_t rowB = (mB >> 3) * 1024 + (mB & 7) * 128, rB = mB & 7;
     const bool okA = mA < words_valid, okB = mB < words_valid;
-    // A-tile task of this warp: coefficient (oo, ii) and the half of the 64 bits
-    const int task = warp - 2;            // 0..7
-    const unsigned t_oo = task >> 2, t_ii = (task >> 1) & 1, t_half = task & 1;
-    const unsigned arow = 64 * t_oo + 32 * t_half + lane;  // A row written by this lane
-    const uint32_t arow_off = (arow >> 3) * 1024 + (arow & 7) * 128, ar7 = arow & 7;
+    // A: row m, input half ii (adjacent threads alternate ii so a 64-bit store
+    // phase of 16 threads covers 8 rows x 2 halves = all 32 banks)
+    const unsigned a_ii = e & 1, a_m = e >> 1, a_oo = a_m >> 6, a_b = a_m & 63;
+    const uint32_t arow_off = (a_m >> 3) * 1024 + (a_m & 7) * 128 + 8 * a_ii, ar7 = a_m & 7;
+    auto coef = [&](unsigned k) -> uint64_t {
+      const unsigned o = o0 + a_oo, i = (st_begin + k) * kStageIn + a_ii;
+      return (k < nst && o < n_out && i < n_in) ? coeff[(size_t)o * ldc + i] : 0ull;
+    };
+    uint64_t c_cur = coef(0);
     for (unsigned k = 0; k < nst; k++) {
       const unsigned sl = k % kLd, bs = k % kBs;
+      const uint64_t c_nxt = coef(k + 1);  // prefetch the next stage's coefficient
+      // row b of the multiplication matrix of c_cur (closed form, see header)
+      const uint64_t rv = __brevll(c_cur);
+      uint64_t qrow = rv >> (63 - a_b);
+#pragma unroll
+      for (int si = 0; si < 4; si++) {
+        const int sft = si == 0 ? 0 : si == 1 ? 1 : si == 2 ? 3 : 4;
+        const int d = (int)a_b - sft;
+        if (d >= 0) {
+          if (d + 1 < 64) qrow ^= rv << (d + 1);
+          if (d <= 2) qrow ^= rv << (d + 61);
+          if (d <= 1) qrow ^= rv << (d + 62);
+        }
+      }
+      const uint32_t qlo = (uint32_t)qrow, qhi = (uint32_t)(qrow >> 32);
       if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
         *err = 1;
         break;
@@ -204,26 +229,7 @@ k_gf64_matvec_tc(const uint64_t* __restrict__ in, const uint64_t* const* __restr
           if (okB) { xB.z = b.x; xB.w = b.y; }
         }
       }
-      // the coefficient of this warp's A task, and its 64 products c * x^e
-      uint64_t c = 0;
-      {
-        const unsigned o = o0 + t_oo, i = i0 + t_ii;
-        if (o < n_out && t_ii < ni) c = coeff[(size_t)o * ldc + i];
-      }
       mbar_arrive(BAR(RAW_EMPTY + sl));
-      const uint64_t P0 = lane ? gf64_reduce(c >> (64 - lane), c << lane) : c;           // c * x^lane
-      const uint64_t P1 = gf64_reduce(c >> (32 - lane), (c << (lane + 32)));            // c * x^(lane+32)
-      uint32_t qlo = 0, qhi = 0;
-#pragma unroll
-      for (int bb = 0; bb < 32; bb++) {
-        const int b = 32 * t_half + bb;
-        const uint32_t lo = __ballot_sync(0xFFFFFFFFu, (uint32_t)(P0 >> b) & 1u);
-        const uint32_t hi = __ballot_sync(0xFFFFFFFFu, (uint32_t)(P1 >> b) & 1u);
-        if (lane == bb) {
-          qlo = lo;
-          qhi = hi;
-        }
-      }
       if (k >= (unsigned)kBs && !mbar_wait(BAR(OP_EMPTY + bs), (k / kBs - 1) & 1)) {
         *err = 1;
         break;
@@ -232,12 +238,13 @@ k_gf64_matvec_tc(const uint64_t* __restrict__ in, const uint64_t* const* __restr
       uint8_t* bt = b_p + bs * kBBytes;
 #pragma unroll
       for (int j = 0; j < 8; j++) {
-        *reinterpret_cast<uint2*>(at + arow_off + ((j ^ ar7) << 4) + 8 * t_ii) = make_uint2(qlo >> j, qhi >> j);
+        *reinterpret_cast<uint2*>(at + arow_off + ((j ^ ar7) << 4)) = make_uint2(qlo >> j, qhi >> j);
         *reinterpret_cast<uint4*>(bt + rowA + ((j ^ rA) << 4)) = make_uint4(xA.x >> j, xA.y >> j, xA.z >> j, xA.w >> j);
         *reinterpret_cast<uint4*>(bt + rowB + ((j ^ rB) << 4)) = make_uint4(xB.x >> j, xB.y >> j, xB.z >> j, xB.w >> j);
       }
       fence_async_smem();
       mbar_arrive(BAR(OP_FULL + bs));
+      c_cur = c_nxt;
     }
     // ------------------------------------------------------------ epilogue
     const bool have = nst > 0 && !*err && mbar_wait(BAR(D_FULL), 0);
@@ -303,7 +310,8 @@ cudaError_t launch_gf64_matvec_tc(const uint64_t* d_in, const uint64_t* const* d
   const size_t n_stages = ceil_div(n_in, tc64::kStageIn);
   const size_t base = pairs * wt;
   const size_t target = (size_t)(sms > 0 ? sms : 148);
-  size_t splits = base >= target ? 1 : ceil_div(target, base);
+  // fill the SMs in one wave: floor, never more CTAs than SMs from splitting
+  size_t splits = base >= target ? 1 : std::max<size_t>(1, target / base);
   size_t max_splits = std::max<size_t>(1, n_stages / 16);
   if (splits > max_splits) splits = max_splits;
   size_t per = ceil_div(n_stages, splits);
