@@ -68,7 +68,7 @@ class PPError(RuntimeError):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m parparpar_b200.build` "
+            f"{LIB_PATH} is missing: build it with `python parparpar_b200/build.py` "
             "(the CUDA engine has no CPU fallback)")
     return ctypes.CDLL(LIB_PATH)
 

@@ -1,6 +1,6 @@
 """Build the sm_100a shared library libparpar_b200.so in-tree with nvcc.
 
-    python -m parparpar_b200.build        # or: python parparpar_b200/build.py
+    python parparpar_b200/build.py   (not -m: importing the package loads the library)
 
 Every CUDA translation unit is compiled with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo`` and linked into one

@@ -1210,9 +1210,13 @@ PP_API int pp_gf64_repair(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs
   else
     memcpy(miss.data(), missing, n * 8);
   std::vector<uint8_t> lost(num_inputs, 0);
+  // the system is a true Cauchy matrix (closed-form inverse) unless some lost
+  // column id fI + c equals a row id fR + j, whose entry the reference maps to 1
+  bool cauchy = true;
   for (size_t c = 0; c < n; c++) {
     if (miss[c] >= num_inputs || lost[miss[c]]) return set_err(ctx, PP_ERR_INVALID_ARG, "bad missing index list");
     lost[miss[c]] = 1;
+    if (first_input + miss[c] - first_recovery < n) cauchy = false;
   }
   const bool in_dev = is_device_ptr(inputs), out_dev = is_device_ptr(restored), rec_dev = is_device_ptr(recovery);
   const uint64_t* din = inputs;
@@ -1222,10 +1226,11 @@ PP_API int pp_gf64_repair(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs
     CUDA_TRY(ctx, cudaMemcpyAsync(st, inputs, num_inputs * B * 8, cudaMemcpyHostToDevice, ctx->stream));
     din = st;
   }
-  // rhs = recovery rows (absent rows zero), then the known-input sum
-  uint64_t* rhs = out_dev ? restored : (uint64_t*)scratch(ctx, S_OUT, n * B * 8);
+  // rhs = recovery rows (absent rows zero), then the known-input sum.  With
+  // the closed-form inverse the rhs is kept apart from the restored blocks.
+  uint64_t* rhs = (out_dev && !cauchy) ? restored : (uint64_t*)scratch(ctx, S_OUT, n * B * 8);
   uint64_t* zero = (uint64_t*)scratch(ctx, S_C, B * 8);
-  uint64_t* dA = (uint64_t*)scratch(ctx, S_D, n * n * 8 + n * 8);
+  uint64_t* dA = (uint64_t*)scratch(ctx, S_D, (cauchy ? 2 * n * n + 3 * n : n * n + n) * 8);
   uint64_t* dF = (uint64_t*)scratch(ctx, S_E, (n + 2) * 8 + 64);
   if (!rhs || !zero || !dA || !dF) return set_err(ctx, PP_ERR_NO_MEMORY, "repair buffers");
   uint64_t* dcols = dA + n * n;
@@ -1252,6 +1257,19 @@ PP_API int pp_gf64_repair(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs
   // the n x n system over the lost columns, then the solve
   CUDA_TRY(ctx, cudaMemcpyAsync(dcols, miss.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(ctx, launch_gf64_cauchy_cols(dA, n, dcols, n, first_input, first_recovery, ctx->stream));
+  if (cauchy) {
+    // restored = A^-1 * rhs: O(n^2) weights + one n x n region product
+    uint64_t* dW = dcols + n;
+    uint64_t* dAinv = dW + 2 * n;
+    uint64_t* dout = out_dev ? restored : (uint64_t*)scratch(ctx, S_COEF, n * B * 8);
+    if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "repair output");
+    CUDA_TRY(ctx, launch_gf64_cauchy_inverse(dA, dcols, n, first_input, first_recovery, dW, dAinv, ctx->stream));
+    const bool al2 = (B % 2) == 0 && ((uintptr_t)rhs % 16) == 0 && ((uintptr_t)dout % 16) == 0;
+    CUDA_TRY(ctx, gf64_region(ctx, rhs, nullptr, B, n, B, dAinv, n, n, dout, nullptr, B, false, al2));
+    if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(restored, dout, n * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return device_status(ctx);
+  }
   int* dS = (int*)(dF + n + 2);
   CUDA_TRY(ctx, cudaMemsetAsync(dS, 0, sizeof(int), ctx->stream));
   CUDA_TRY(ctx, launch_gf64_solve(dA, rhs, n, B, dF, dS, ctx->stream));

@@ -37,6 +37,7 @@
 // TMEM and returns.
 #include "pp_common.cuh"
 #include "pp_internal.h"
+#include "tc_batch.h"
 #include "tc_common.cuh"
 
 #include <algorithm>
@@ -117,11 +118,23 @@ k_gf16_tc_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigne
   }
 }
 
-// mode: 0 overwrite, 1 xor into existing, 2 atomic xor (inputs split across CTAs)
+// One CTA per work item of the job table (tc_batch.h): the item fixes the
+// job, the output group, the word tile and the stage range; mode 0 stores,
+// 1 XORs into the output, 2 XORs atomically (the job is split over CTAs).
 __global__ void __launch_bounds__(kThreads, 1)
-k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in, size_t slice_bytes,
-                 const uint8_t* __restrict__ a_exp, unsigned n_stages_total, unsigned n_out, uint8_t* __restrict__ out,
-                 size_t out_stride, unsigned stages_per_split, int mode, int* __restrict__ status) {
+k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ status) {
+  const TcSeg sg = tc_item(&batch, blockIdx.x);
+  const Gf16TcJob J = pinned_job(batch.job[sg.job]);
+  const uint8_t* __restrict__ in = J.in;
+  const size_t in_stride = J.in_stride;
+  const unsigned n_in = J.n_in;
+  const size_t slice_bytes = J.slice_bytes;
+  const uint8_t* __restrict__ a_exp = J.a_exp;
+  const unsigned n_stages_total = J.n_stages;
+  const unsigned n_out = J.n_out;
+  uint8_t* __restrict__ out = J.out;
+  const size_t out_stride = J.out_stride;
+  const int mode = sg.mode;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t base_s = smem_addr(smem_raw);
   const uint32_t pad = ((base_s + 1023) & ~1023u) - base_s;
@@ -149,11 +162,10 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
   volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 8 * NBARS + 8);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const unsigned g = blockIdx.x;  // output group
-  const size_t w0 = (size_t)blockIdx.y * kWords;
-  const unsigned st_begin = blockIdx.z * stages_per_split;
-  const unsigned st_end = min(n_stages_total, st_begin + stages_per_split);
-  const unsigned nst = st_end > st_begin ? st_end - st_begin : 0;
+  const unsigned g = (unsigned)(sg.tile % J.groups);  // output group
+  const size_t w0 = (size_t)(sg.tile / J.groups) * kWords;
+  const unsigned st_begin = sg.st0;
+  const unsigned nst = sg.st1 - sg.st0;
   const size_t total_words = (slice_bytes + 1) / 2;
   const unsigned words_valid = (unsigned)min((size_t)kWords, total_words - w0);
   // raw bytes copied per input row (16-byte multiple, inside the padded row)
@@ -360,6 +372,8 @@ k_gf16_muladd_tc(const uint8_t* __restrict__ in, size_t in_stride, unsigned n_in
   if (threadIdx.x == 0 && *err) atomicOr(status, 1);
 }
 
+static uint64_t tiles16(const Gf16TcJob& j) { return (uint64_t)j.groups * j.wt; }
+
 }  // namespace tc16
 
 size_t gf16_tc_coeff_bytes(unsigned n_in, unsigned n_out) {
@@ -377,15 +391,7 @@ cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned
   return cudaGetLastError();
 }
 
-cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigned n_in, size_t slice_bytes,
-                                  const uint8_t* d_aexp, unsigned n_out, uint8_t* d_out, size_t out_stride,
-                                  bool accumulate, int sms, int* d_status, cudaStream_t s) {
-  if (!n_out || !slice_bytes) return cudaSuccess;
-  if (!n_in) {
-    if (accumulate) return cudaSuccess;
-    note_launch();
-    return cudaMemset2DAsync(d_out, out_stride, 0, slice_bytes, n_out, s);
-  }
+cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -393,36 +399,57 @@ cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigne
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const unsigned groups = (n_out + 7) / 8;
-  const size_t words = (slice_bytes + 1) / 2;
-  const unsigned wt = (unsigned)ceil_div(words, tc16::kWords);
-  const unsigned n_stages = (n_in + 7) / 8;
-  const unsigned base = groups * wt;
-  const unsigned target = (unsigned)(sms > 0 ? sms : 148);
-  // fill the SMs in one wave: floor, never more CTAs than SMs from splitting
-  unsigned splits = base >= target ? 1 : std::max(1u, target / base);
-  // keep at least 8 stages per split so the pipeline fills
-  unsigned max_splits = (unsigned)std::max<size_t>(1, n_stages / 8);
-  if (splits > max_splits) splits = max_splits;
-  unsigned per = (unsigned)ceil_div(n_stages, splits);
-  splits = (unsigned)ceil_div(n_stages, per);
-  int mode;
-  if (splits == 1) {
-    mode = accumulate ? 1 : 0;
-  } else {
-    mode = 2;
-    if (!accumulate) {
-      cudaError_t e = cudaMemset2DAsync(d_out, out_stride, 0, slice_bytes, n_out, s);
+  uint32_t m = 0;
+  for (uint32_t j = 0; j < b.n_jobs; j++) {
+    Gf16TcJob& J = b.job[j];
+    if (!J.n_out || !J.slice_bytes) continue;
+    J.n_stages = (J.n_in + 7) / 8;
+    J.groups = (J.n_out + 7) / 8;
+    const size_t wt = ceil_div((J.slice_bytes + 1) / 2, tc16::kWords);
+    if (wt > 0xFFFFFFFFu) return cudaErrorInvalidValue;
+    J.wt = (uint32_t)wt;
+    if (!J.n_in) {
+      if (J.accumulate) continue;
+      cudaError_t e = cudaMemset2DAsync(J.out, J.out_stride, 0, J.slice_bytes, J.n_out, s);
       note_launch();
       if (e != cudaSuccess) return e;
+      continue;
     }
+    b.job[m++] = J;
   }
-  if (groups > 65535 || wt > 65535 || splits > 65535) return cudaErrorInvalidConfiguration;
-  dim3 grid(groups, wt, splits);
-  tc16::k_gf16_muladd_tc<<<grid, tc16::kThreads, tc16::kSmemBytes, s>>>(
-      d_in, in_stride, n_in, slice_bytes, d_aexp, n_stages, n_out, d_out, out_stride, per, mode, d_status);
+  b.n_jobs = m;
+  if (!m) return cudaGetLastError();
+  const uint64_t ctas = tc_batch_plan(b, tc16::tiles16, sms);
+  if (ctas > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+  for (uint32_t j = 0; j < m; j++) {
+    const Gf16TcJob& J = b.job[j];
+    if (J.splits == 1 || J.accumulate) continue;
+    cudaError_t e = cudaMemset2DAsync(J.out, J.out_stride, 0, J.slice_bytes, J.n_out, s);
+    note_launch();
+    if (e != cudaSuccess) return e;
+  }
+  tc16::k_gf16_muladd_tc<<<(unsigned)ctas, tc16::kThreads, tc16::kSmemBytes, s>>>(b, d_status);
   note_launch();
   return cudaGetLastError();
+}
+
+cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigned n_in, size_t slice_bytes,
+                                  const uint8_t* d_aexp, unsigned n_out, uint8_t* d_out, size_t out_stride,
+                                  bool accumulate, int sms, int* d_status, cudaStream_t s) {
+  if (!n_out || !slice_bytes) return cudaSuccess;
+  Gf16TcBatch b{};
+  b.n_jobs = 1;
+  Gf16TcJob& J = b.job[0];
+  J.in = d_in;
+  J.in_stride = in_stride;
+  J.a_exp = d_aexp;
+  J.out = d_out;
+  J.out_stride = out_stride;
+  J.slice_bytes = slice_bytes;
+  J.n_in = n_in;
+  J.n_out = n_out;
+  J.accumulate = accumulate ? 1 : 0;
+  return launch_gf16_tc_batch(b, sms, d_status, s);
 }
 
 }  // namespace pp

@@ -87,6 +87,78 @@ cudaError_t launch_gf64_cauchy_cols(uint64_t* d_A, size_t n_rows, const uint64_t
   return cudaGetLastError();
 }
 
+// Closed-form inverse of the repair system when it is a true Cauchy matrix
+// (rows x_j = fR + j, columns y_i = fI + cols[i], all x_j != y_i so that no
+// denominator was mapped to 1).  Over GF(2^m) (signs vanish):
+//   (A^-1)[i][j] = b_i * a_j / (x_j + y_i)
+//   a_j = prod_k (x_j + y_k) / prod_{k != j} (x_j + x_k)
+//   b_i = prod_k (x_k + y_i) / prod_{k != i} (y_i + y_k)
+// The solution of a nonsingular system is unique, so A^-1 * rhs equals the
+// Gauss-Jordan result of the reference's SolveAndReconstruct
+// (src/par3_engine.cc:980-1053) word for word.
+//
+// One warp per weight: lanes take every 32nd factor, then a shuffle tree
+// multiplies the 32 partial products.
+__device__ __forceinline__ uint64_t warp_gf64_prod(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = gf64_mul(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__global__ void __launch_bounds__(256) k_gf64_cauchy_inv_weights(const uint64_t* __restrict__ cols, size_t n,
+                                                                 uint64_t fI, uint64_t fR, uint64_t* __restrict__ wa,
+                                                                 uint64_t* __restrict__ wb) {
+  const unsigned lane = threadIdx.x & 31;
+  const size_t w = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= 2 * n) return;
+  uint64_t num = 1, den = 1;
+  if (w < n) {  // a_j, j = w
+    const uint64_t xj = fR + w;
+    for (size_t k = lane; k < n; k += 32) {
+      num = gf64_mul(num, xj ^ (fI + cols[k]));
+      if (k != w) den = gf64_mul(den, xj ^ (fR + k));
+    }
+  } else {  // b_i, i = w - n
+    const size_t i = w - n;
+    const uint64_t yi = fI + cols[i];
+    for (size_t k = lane; k < n; k += 32) {
+      num = gf64_mul(num, (fR + k) ^ yi);
+      if (k != i) den = gf64_mul(den, yi ^ (fI + cols[k]));
+    }
+  }
+  num = warp_gf64_prod(num);
+  den = warp_gf64_prod(den);
+  if (lane == 0) {
+    const uint64_t v = gf64_mul(num, gf64_inv(den));
+    if (w < n) wa[w] = v;
+    else wb[w - n] = v;
+  }
+}
+
+// Ainv[i][j] = wb[i] * wa[j] * A[j][i]  (A[j][i] = 1 / (x_j + y_i))
+__global__ void k_gf64_cauchy_inv_assemble(const uint64_t* __restrict__ A, const uint64_t* __restrict__ wa,
+                                           const uint64_t* __restrict__ wb, size_t n, uint64_t* __restrict__ Ainv) {
+  const size_t total = n * n;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = t / n, j = t % n;
+    Ainv[t] = gf64_mul(gf64_mul(wb[i], wa[j]), A[j * n + i]);
+  }
+}
+
+cudaError_t launch_gf64_cauchy_inverse(const uint64_t* d_A, const uint64_t* d_cols, size_t n, uint64_t fI,
+                                       uint64_t fR, uint64_t* d_w, uint64_t* d_Ainv, cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  const size_t warps = 2 * n;
+  k_gf64_cauchy_inv_weights<<<(unsigned)ceil_div(warps * 32, 256), 256, 0, s>>>(d_cols, n, fI, fR, d_w, d_w + n);
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t blocks = std::min<size_t>(ceil_div(n * n, 256), 148 * 32);
+  k_gf64_cauchy_inv_assemble<<<(unsigned)blocks, 256, 0, s>>>(d_A, d_w, d_w + n, n, d_Ainv);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // inverse of every element, inverse(0) = 0 (reference gf64/gf64_invert.c:29-75)
 __global__ void __launch_bounds__(128)
 k_gf64_inverse_batch(uint64_t* __restrict__ out, const uint64_t* __restrict__ in, size_t n) {

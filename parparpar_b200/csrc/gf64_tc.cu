@@ -40,6 +40,7 @@
 
 #include "pp_common.cuh"
 #include "pp_internal.h"
+#include "tc_batch.h"
 #include "tc_common.cuh"
 
 namespace pp {
@@ -62,22 +63,16 @@ constexpr int kOffBar = kOffRaw + kLd * kRawBytes;  // 192 KiB
 constexpr int kSmemBytes = kOffBar + 256 + 1024;
 constexpr uint32_t kIdesc = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
 
-// mode: 0 overwrite, 1 xor into existing, 2 atomic xor (inputs split across CTAs)
-// Rows: input i at in_ptrs ? in_ptrs[i] : in + i*in_stride (words); output r
-// at out_ptrs ? out_ptrs[r] : out + r*out_stride.
+// One CTA per work item of the job table (tc_batch.h): the item fixes the
+// job, the output pair, the word tile and the stage range; mode 0 stores,
+// 1 XORs into the output, 2 XORs atomically (the job is split over CTAs).
 __global__ void __launch_bounds__(kThreads, 1)
-k_gf64_matvec_tc(const uint64_t* __restrict__ in, const uint64_t* const* __restrict__ in_ptrs, size_t in_stride,
-                 unsigned n_in, size_t words, const uint64_t* __restrict__ coeff, size_t ldc, unsigned n_out,
-                 uint64_t* __restrict__ out, uint64_t* const* __restrict__ out_ptrs, size_t out_stride,
-                 unsigned stages_per_split, int mode, int* __restrict__ status) {
+k_gf64_matvec_tc(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ status) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t base_s = smem_addr(smem_raw);
   const uint32_t pad = ((base_s + 1023) & ~1023u) - base_s;
   uint8_t* smem = smem_raw + pad;
   const uint32_t sA = base_s + pad + kOffA, sB = base_s + pad + kOffB, sRaw = base_s + pad + kOffRaw;
-  uint8_t* a_p = smem + kOffA;
-  uint8_t* b_p = smem + kOffB;
-  const uint8_t* raw_p = smem + kOffRaw;
   const uint32_t bar0 = smem_addr(smem + kOffBar);
   enum {
     RAW_FULL = 0,
@@ -93,14 +88,6 @@ k_gf64_matvec_tc(const uint64_t* __restrict__ in, const uint64_t* const* __restr
   volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 8 * NBARS + 8);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const unsigned o0 = 2 * blockIdx.x;  // output pair
-  const size_t w0 = (size_t)blockIdx.y * kWords;
-  const unsigned n_stages_total = (n_in + kStageIn - 1) / kStageIn;
-  const unsigned st_begin = blockIdx.z * stages_per_split;
-  const unsigned st_end = min(n_stages_total, st_begin + stages_per_split);
-  const unsigned nst = st_end > st_begin ? st_end - st_begin : 0;
-  const unsigned words_valid = (unsigned)min((size_t)kWords, words - w0);
-  const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
 
   if (threadIdx.x == 0) {
     for (int k = 0; k < NBARS; k++) {
@@ -121,52 +108,63 @@ k_gf64_matvec_tc(const uint64_t* __restrict__ in, const uint64_t* const* __restr
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_holder;
+  const TcSeg sg = tc_item(&batch, blockIdx.x);
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
-      unsigned issued = 0;
-      for (unsigned k = 0; k < nst && !*err; k++) {
-        const unsigned sl = k % kLd, use = k / kLd;
-        if (k >= (unsigned)kLd && !mbar_wait(BAR(RAW_EMPTY + sl), (use - 1) & 1)) {
-          *err = 1;
-          break;
+      uint32_t g = 0;  // stages issued by this CTA
+      do {  // the CTA's one item
+        const Gf64TcJob J = pinned_job(batch.job[sg.job]);
+        const size_t w0 = (size_t)(sg.tile / J.pairs) * kWords;
+        const unsigned words_valid = (unsigned)min((size_t)kWords, J.words - w0);
+        const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
+        for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
+          const unsigned sl = g % kLd;
+          if (g >= (uint32_t)kLd && !mbar_wait(BAR(RAW_EMPTY + sl), (g / kLd - 1) & 1)) {
+            *err = 1;
+            break;
+          }
+          const unsigned i0 = st * kStageIn;
+          const unsigned ni = min((unsigned)kStageIn, J.n_in - i0);
+          mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
+          for (unsigned ii = 0; ii < ni; ii++) {
+            const uint64_t* row = J.in_ptrs ? J.in_ptrs[i0 + ii] : J.in + (size_t)(i0 + ii) * J.in_stride;
+            bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 8), row + w0, raw_copy, BAR(RAW_FULL + sl));
+          }
         }
-        const unsigned i0 = (st_begin + k) * kStageIn;
-        const unsigned ni = min((unsigned)kStageIn, n_in - i0);
-        mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
-        for (unsigned ii = 0; ii < ni; ii++) {
-          const uint64_t* row = in_ptrs ? in_ptrs[i0 + ii] : in + (size_t)(i0 + ii) * in_stride;
-          bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 8), row + w0, raw_copy, BAR(RAW_FULL + sl));
-        }
-        issued = k + 1;
-      }
-      if (*err) {
-        for (unsigned k = issued > (unsigned)kLd ? issued - kLd : 0; k < issued; k++)
+      } while (0);
+      if (*err) {  // every issued copy lands before the CTA exits
+        for (uint32_t k = g > (uint32_t)kLd ? g - kLd : 0; k < g; k++)
           mbar_wait(BAR(RAW_FULL + k % kLd), (k / kLd) & 1);
       }
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      for (unsigned k = 0; k < nst; k++) {
-        const unsigned bs = k % kBs;
-        if (*err || !mbar_wait(BAR(OP_FULL + bs), (k / kBs) & 1)) {
-          *err = 1;
-          break;
-        }
-        tc_fence_after();
-#pragma unroll
-        for (int kk = 0; kk < 4; kk++) {
-#pragma unroll
-          for (int nn = 0; nn < 2; nn++) {
-            mma_i8(tmem + nn * 256, sw128_desc(sA + bs * kABytes + 32 * kk),
-                   sw128_desc(sB + bs * kBBytes + nn * (256 * 128) + 32 * kk), kIdesc, (k > 0 || kk > 0) ? 1u : 0u);
+      uint32_t g = 0;
+      do {  // the CTA's one item
+        for (unsigned k = 0; k < sg.st1 - sg.st0; k++, g++) {
+          const unsigned bs = g % kBs;
+          if (*err || !mbar_wait(BAR(OP_FULL + bs), (g / kBs) & 1)) {
+            *err = 1;
+            break;
           }
+          tc_fence_after();
+#pragma unroll
+          for (int kk = 0; kk < 4; kk++) {
+#pragma unroll
+            for (int nn = 0; nn < 2; nn++) {
+              mma_i8(tmem + nn * 256, sw128_desc(sA + bs * kABytes + 32 * kk),
+                     sw128_desc(sB + bs * kBBytes + nn * (256 * 128) + 32 * kk), kIdesc,
+                     (k > 0 || kk > 0) ? 1u : 0u);
+            }
+          }
+          mma_commit(BAR(OP_EMPTY + bs));
         }
-        mma_commit(BAR(OP_EMPTY + bs));
-      }
-      if (!*err) mma_commit(BAR(D_FULL));
+        if (!*err) mma_commit(BAR(D_FULL));
+      } while (0);
+      // all MMAs issued by this thread complete before TMEM is released
       mma_commit(BAR(DONE));
       if (!mbar_wait(BAR(DONE), 0)) *err = 1;
     }
@@ -178,108 +176,117 @@ k_gf64_matvec_tc(const uint64_t* __restrict__ in, const uint64_t* const* __restr
     const unsigned mA = n + sw, mB = n + 1 - sw;
     const uint32_t rowA = (mA >> 3) * 1024 + (mA & 7) * 128, rA = mA & 7;
     const uint32_t rowB = (mB >> 3) * 1024 + (mB & 7) * 128, rB = mB & 7;
-    const bool okA = mA < words_valid, okB = mB < words_valid;
     // A: row m, input half ii (adjacent threads alternate ii so a 64-bit store
     // phase of 16 threads covers 8 rows x 2 halves = all 32 banks)
     const unsigned a_ii = e & 1, a_m = e >> 1, a_oo = a_m >> 6, a_b = a_m & 63;
     const uint32_t arow_off = (a_m >> 3) * 1024 + (a_m & 7) * 128 + 8 * a_ii, ar7 = a_m & 7;
-    auto coef = [&](unsigned k) -> uint64_t {
-      const unsigned o = o0 + a_oo, i = (st_begin + k) * kStageIn + a_ii;
-      return (k < nst && o < n_out && i < n_in) ? coeff[(size_t)o * ldc + i] : 0ull;
-    };
-    uint64_t c_cur = coef(0);
-    for (unsigned k = 0; k < nst; k++) {
-      const unsigned sl = k % kLd, bs = k % kBs;
-      const uint64_t c_nxt = coef(k + 1);  // prefetch the next stage's coefficient
-      // row b of the multiplication matrix of c_cur (closed form, see header)
-      const uint64_t rv = __brevll(c_cur);
-      uint64_t qrow = rv >> (63 - a_b);
+    // epilogue role: TMEM lane quarter q (rows 32q..32q+31), column half
+    const int q = warp & 3;
+    const int chalf = (warp - 2) >> 2;
+    uint32_t g = 0, nseg = 0;
+    do {  // the CTA's one item
+      const Gf64TcJob J = pinned_job(batch.job[sg.job]);
+      const unsigned o0 = 2 * (unsigned)(sg.tile % J.pairs);
+      const size_t w0 = (size_t)(sg.tile / J.pairs) * kWords;
+      const unsigned words_valid = (unsigned)min((size_t)kWords, J.words - w0);
+      const bool okA = mA < words_valid, okB = mB < words_valid;
+      const unsigned nst = sg.st1 - sg.st0;
+      auto coef = [&](unsigned k) -> uint64_t {
+        const unsigned o = o0 + a_oo, i = (sg.st0 + k) * kStageIn + a_ii;
+        return (k < nst && o < J.n_out && i < J.n_in) ? J.coeff[(size_t)o * J.ldc + i] : 0ull;
+      };
+      uint64_t c_cur = coef(0);
+      for (unsigned k = 0; k < nst; k++, g++) {
+        const unsigned sl = g % kLd, bs = g % kBs;
+        const uint64_t c_nxt = coef(k + 1);  // prefetch the next stage's coefficient
+        // row b of the multiplication matrix of c_cur (closed form, see header)
+        const uint64_t rv = __brevll(c_cur);
+        uint64_t qrow = rv >> (63 - a_b);
 #pragma unroll
-      for (int si = 0; si < 4; si++) {
-        const int sft = si == 0 ? 0 : si == 1 ? 1 : si == 2 ? 3 : 4;
-        const int d = (int)a_b - sft;
-        if (d >= 0) {
-          if (d + 1 < 64) qrow ^= rv << (d + 1);
-          if (d <= 2) qrow ^= rv << (d + 61);
-          if (d <= 1) qrow ^= rv << (d + 62);
+        for (int si = 0; si < 4; si++) {
+          const int sft = si == 0 ? 0 : si == 1 ? 1 : si == 2 ? 3 : 4;
+          const int d = (int)a_b - sft;
+          if (d >= 0) {
+            if (d + 1 < 64) qrow ^= rv << (d + 1);
+            if (d <= 2) qrow ^= rv << (d + 61);
+            if (d <= 1) qrow ^= rv << (d + 62);
+          }
         }
+        const uint32_t qlo = (uint32_t)qrow, qhi = (uint32_t)(qrow >> 32);
+        if (*err || !mbar_wait(BAR(RAW_FULL + sl), (g / kLd) & 1)) {
+          *err = 1;
+          break;
+        }
+        const unsigned i0 = (sg.st0 + k) * kStageIn;
+        const unsigned ni = min((unsigned)kStageIn, J.n_in - i0);
+        const uint32_t raw = sRaw + sl * kRawBytes + 8 * n;
+        // B rows of words mA and mB: (lo, hi) of input 0, then (lo, hi) of input 1
+        uint4 xA = make_uint4(0, 0, 0, 0), xB = make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int ii = 0; ii < kStageIn; ii++) {
+          if ((unsigned)ii >= ni) continue;
+          // v = word n (x, y) and word n+1 (z, w) of input ii
+          const uint4 v = lds128(raw + ii * (kWords * 8));
+          const uint2 a = sw ? make_uint2(v.z, v.w) : make_uint2(v.x, v.y);
+          const uint2 b = sw ? make_uint2(v.x, v.y) : make_uint2(v.z, v.w);
+          if (ii == 0) {
+            if (okA) { xA.x = a.x; xA.y = a.y; }
+            if (okB) { xB.x = b.x; xB.y = b.y; }
+          } else {
+            if (okA) { xA.z = a.x; xA.w = a.y; }
+            if (okB) { xB.z = b.x; xB.w = b.y; }
+          }
+        }
+        mbar_arrive(BAR(RAW_EMPTY + sl));
+        if (g >= (uint32_t)kBs && !mbar_wait(BAR(OP_EMPTY + bs), (g / kBs - 1) & 1)) {
+          *err = 1;
+          break;
+        }
+        const uint32_t at = sA + bs * kABytes, bt = sB + bs * kBBytes;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          sts64(at + arow_off + ((j ^ ar7) << 4), qlo >> j, qhi >> j);
+          sts128(bt + rowA + ((j ^ rA) << 4), xA.x >> j, xA.y >> j, xA.z >> j, xA.w >> j);
+          sts128(bt + rowB + ((j ^ rB) << 4), xB.x >> j, xB.y >> j, xB.z >> j, xB.w >> j);
+        }
+        fence_async_smem();
+        mbar_arrive(BAR(OP_FULL + bs));
+        c_cur = c_nxt;
       }
-      const uint32_t qlo = (uint32_t)qrow, qhi = (uint32_t)(qrow >> 32);
-      if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
+      // ---------------------------------------------------------- epilogue
+      if (*err || !mbar_wait(BAR(D_FULL), nseg & 1)) {
         *err = 1;
         break;
       }
-      const unsigned i0 = (st_begin + k) * kStageIn;
-      const unsigned ni = min((unsigned)kStageIn, n_in - i0);
-      const uint8_t* raw = raw_p + sl * kRawBytes;
-      // B rows of words mA and mB: (lo, hi) of input 0, then (lo, hi) of input 1
-      uint4 xA = make_uint4(0, 0, 0, 0), xB = make_uint4(0, 0, 0, 0);
-#pragma unroll
-      for (int ii = 0; ii < kStageIn; ii++) {
-        if ((unsigned)ii >= ni) continue;
-        // v = word n (x, y) and word n+1 (z, w) of input ii
-        const uint4 v = *reinterpret_cast<const uint4*>(raw + ii * (kWords * 8) + 8 * n);
-        const uint2 a = sw ? make_uint2(v.z, v.w) : make_uint2(v.x, v.y);
-        const uint2 b = sw ? make_uint2(v.x, v.y) : make_uint2(v.z, v.w);
-        if (ii == 0) {
-          if (okA) { xA.x = a.x; xA.y = a.y; }
-          if (okB) { xB.x = b.x; xB.y = b.y; }
-        } else {
-          if (okA) { xA.z = a.x; xA.w = a.y; }
-          if (okB) { xB.z = b.x; xB.w = b.y; }
-        }
-      }
-      mbar_arrive(BAR(RAW_EMPTY + sl));
-      if (k >= (unsigned)kBs && !mbar_wait(BAR(OP_EMPTY + bs), (k / kBs - 1) & 1)) {
-        *err = 1;
-        break;
-      }
-      uint8_t* at = a_p + bs * kABytes;
-      uint8_t* bt = b_p + bs * kBBytes;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        *reinterpret_cast<uint2*>(at + arow_off + ((j ^ ar7) << 4)) = make_uint2(qlo >> j, qhi >> j);
-        *reinterpret_cast<uint4*>(bt + rowA + ((j ^ rA) << 4)) = make_uint4(xA.x >> j, xA.y >> j, xA.z >> j, xA.w >> j);
-        *reinterpret_cast<uint4*>(bt + rowB + ((j ^ rB) << 4)) = make_uint4(xB.x >> j, xB.y >> j, xB.z >> j, xB.w >> j);
-      }
-      fence_async_smem();
-      mbar_arrive(BAR(OP_FULL + bs));
-      c_cur = c_nxt;
-    }
-    // ------------------------------------------------------------ epilogue
-    const bool have = nst > 0 && !*err && mbar_wait(BAR(D_FULL), 0);
-    if (nst > 0 && !have) *err = 1;
-    tc_fence_after();
-    const int q = warp & 3;             // TMEM lane quarter: rows 32q..32q+31
-    const int chalf = (warp - 2) >> 2;  // columns [256*chalf, 256*chalf + 256)
-    const unsigned o = o0 + (q >> 1);   // output of these rows
-    const unsigned half = q & 1;        // bits [32*half, 32*half + 32)
-    for (int cc = 8 * chalf; cc < 8 * chalf + 8; cc++) {
-      uint32_t r[32];
-      if (have) {
+      nseg++;
+      tc_fence_after();
+      const unsigned o = o0 + (q >> 1);  // output of these rows
+      const unsigned half = q & 1;       // bits [32*half, 32*half + 32)
+      uint64_t* orow = o < J.n_out ? (J.out_ptrs ? J.out_ptrs[o] : J.out + (size_t)o * J.out_stride) : nullptr;
+      for (int cc = 8 * chalf; cc < 8 * chalf + 8; cc++) {
+        uint32_t r[32];
         tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + 32 * cc, r);
-      } else {
+        uint32_t mine = 0;
 #pragma unroll
-        for (int jj = 0; jj < 32; jj++) r[jj] = 0;
+        for (int jj = 0; jj < 32; jj++) {
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, r[jj] & 1u);
+          if (lane == jj) mine = bal;
+        }
+        const unsigned widx = 32 * cc + lane;
+        if (!orow || widx >= words_valid) continue;
+        uint32_t* dst = reinterpret_cast<uint32_t*>(orow + w0 + widx) + half;
+        if (sg.mode == 2) {
+          if (mine) atomicXor(dst, mine);
+        } else if (sg.mode == 1) {
+          *dst ^= mine;
+        } else {
+          *dst = mine;
+        }
       }
-      uint32_t mine = 0;
-#pragma unroll
-      for (int jj = 0; jj < 32; jj++) {
-        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, r[jj] & 1u);
-        if (lane == jj) mine = bal;
-      }
-      const unsigned widx = 32 * cc + lane;
-      if (!have || o >= n_out || widx >= words_valid) continue;
-      uint64_t* orow = out_ptrs ? out_ptrs[o] : out + (size_t)o * out_stride;
-      uint32_t* dst = reinterpret_cast<uint32_t*>(orow + w0 + widx) + half;
-      if (mode == 2) {
-        if (mine) atomicXor(dst, mine);
-      } else if (mode == 1) {
-        *dst ^= mine;
-      } else {
-        *dst = mine;
-      }
-    }
+      // the TMEM reads above precede the arrive that releases the next
+      // segment's first MMA
+      tc_fence_before();
+    } while (0);
   }
 
   tc_fence_before();
@@ -291,13 +298,19 @@ k_gf64_matvec_tc(const uint64_t* __restrict__ in, const uint64_t* const* __restr
   if (threadIdx.x == 0 && *err) atomicOr(status, 1);
 }
 
+// zero rows given by a pointer table (outputs of a non-accumulating job whose
+// tiles are split across CTAs)
+__global__ void k_zero_rows(uint64_t* const* __restrict__ rows, unsigned n_rows, size_t words) {
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < (size_t)n_rows * words;
+       t += (size_t)gridDim.x * blockDim.x)
+    rows[t / words][t % words] = 0;
+}
+
+static uint64_t tiles64(const Gf64TcJob& j) { return (uint64_t)j.pairs * j.wt; }
+
 }  // namespace tc64
 
-cudaError_t launch_gf64_matvec_tc(const uint64_t* d_in, const uint64_t* const* d_in_ptrs, size_t in_stride,
-                                  size_t n_in, size_t words, const uint64_t* d_coeff, size_t ldc, size_t n_out,
-                                  uint64_t* d_out, uint64_t* const* d_out_ptrs, size_t out_stride, bool accumulate,
-                                  int sms, int* d_status, cudaStream_t s) {
-  if (!n_out || !words) return cudaSuccess;
+cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(tc64::k_gf64_matvec_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -305,36 +318,71 @@ cudaError_t launch_gf64_matvec_tc(const uint64_t* d_in, const uint64_t* const* d
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const size_t pairs = ceil_div(n_out, 2);
-  const size_t wt = ceil_div(words, tc64::kWords);
-  const size_t n_stages = ceil_div(n_in, tc64::kStageIn);
-  const size_t base = pairs * wt;
-  const size_t target = (size_t)(sms > 0 ? sms : 148);
-  // fill the SMs in one wave: floor, never more CTAs than SMs from splitting
-  size_t splits = base >= target ? 1 : std::max<size_t>(1, target / base);
-  size_t max_splits = std::max<size_t>(1, n_stages / 16);
-  if (splits > max_splits) splits = max_splits;
-  size_t per = ceil_div(n_stages, splits);
-  splits = ceil_div(n_stages, per);
-  int mode;
-  if (splits == 1) {
-    mode = accumulate ? 1 : 0;
-  } else {
-    mode = 2;
-    if (!accumulate) {
-      if (d_out_ptrs) return cudaErrorInvalidValue;
-      cudaError_t e = cudaMemset2DAsync(d_out, out_stride * 8, 0, words * 8, n_out, s);
+  // drop empty jobs (nothing to multiply) after zeroing their outputs
+  uint32_t m = 0;
+  for (uint32_t j = 0; j < b.n_jobs; j++) {
+    Gf64TcJob& J = b.job[j];
+    if (!J.n_out || !J.words) continue;
+    J.n_stages = (J.n_in + tc64::kStageIn - 1) / tc64::kStageIn;
+    J.pairs = (J.n_out + 1) / 2;
+    const size_t wt = ceil_div(J.words, tc64::kWords);
+    if (wt > 0xFFFFFFFFu) return cudaErrorInvalidValue;
+    J.wt = (uint32_t)wt;
+    if (!J.n_in) {
+      if (J.accumulate) continue;
+      if (J.out_ptrs) {
+        tc64::k_zero_rows<<<148, 256, 0, s>>>(const_cast<uint64_t* const*>(J.out_ptrs), J.n_out, J.words);
+      } else {
+        cudaError_t e = cudaMemset2DAsync(J.out, J.out_stride * 8, 0, J.words * 8, J.n_out, s);
+        if (e != cudaSuccess) return e;
+      }
       note_launch();
+      continue;
+    }
+    b.job[m++] = J;
+  }
+  b.n_jobs = m;
+  if (!m) return cudaGetLastError();
+  const uint64_t ctas = tc_batch_plan(b, tc64::tiles64, sms);
+  if (ctas > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+  for (uint32_t j = 0; j < m; j++) {
+    const Gf64TcJob& J = b.job[j];
+    if (J.splits == 1 || J.accumulate) continue;
+    if (J.out_ptrs) {
+      tc64::k_zero_rows<<<148, 256, 0, s>>>(const_cast<uint64_t* const*>(J.out_ptrs), J.n_out, J.words);
+    } else {
+      cudaError_t e = cudaMemset2DAsync(J.out, J.out_stride * 8, 0, J.words * 8, J.n_out, s);
       if (e != cudaSuccess) return e;
     }
+    note_launch();
   }
-  if (pairs > 0x7FFFFFFF || wt > 65535 || splits > 65535) return cudaErrorInvalidConfiguration;
-  dim3 grid((unsigned)pairs, (unsigned)wt, (unsigned)splits);
-  tc64::k_gf64_matvec_tc<<<grid, tc64::kThreads, tc64::kSmemBytes, s>>>(
-      d_in, d_in_ptrs, in_stride, (unsigned)n_in, words, d_coeff, ldc, (unsigned)n_out, d_out, d_out_ptrs,
-      out_stride, (unsigned)per, mode, d_status);
+  tc64::k_gf64_matvec_tc<<<(unsigned)ctas, tc64::kThreads, tc64::kSmemBytes, s>>>(b, d_status);
   note_launch();
   return cudaGetLastError();
+}
+
+cudaError_t launch_gf64_matvec_tc(const uint64_t* d_in, const uint64_t* const* d_in_ptrs, size_t in_stride,
+                                  size_t n_in, size_t words, const uint64_t* d_coeff, size_t ldc, size_t n_out,
+                                  uint64_t* d_out, uint64_t* const* d_out_ptrs, size_t out_stride, bool accumulate,
+                                  int sms, int* d_status, cudaStream_t s) {
+  if (!n_out || !words) return cudaSuccess;
+  if (n_in > 0xFFFFFFFFu || n_out > 0xFFFFFFFFu) return cudaErrorInvalidValue;
+  Gf64TcBatch b{};
+  b.n_jobs = 1;
+  Gf64TcJob& J = b.job[0];
+  J.in = d_in;
+  J.in_ptrs = d_in_ptrs;
+  J.in_stride = in_stride;
+  J.coeff = d_coeff;
+  J.ldc = ldc;
+  J.out = d_out;
+  J.out_ptrs = d_out_ptrs;
+  J.out_stride = out_stride;
+  J.words = words;
+  J.n_in = (uint32_t)n_in;
+  J.n_out = (uint32_t)n_out;
+  J.accumulate = accumulate ? 1 : 0;
+  return launch_gf64_tc_batch(b, sms, d_status, s);
 }
 
 }  // namespace pp

@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <string>
 
+#include "tc_batch.h"
+
 namespace pp {
 
 // Launch counter: every kernel launch issued by this library increments it
@@ -57,6 +59,11 @@ cudaError_t launch_gf64_cauchy(uint64_t* d_m, size_t n_in, size_t n_rec, uint64_
 cudaError_t launch_gf64_cauchy_cols(uint64_t* d_A, size_t n_rows, const uint64_t* d_cols, size_t n_cols, uint64_t fI,
                                     uint64_t fR, cudaStream_t s);
 cudaError_t launch_gf64_inverse_batch(uint64_t* d_out, const uint64_t* d_in, size_t n, cudaStream_t s);
+// inverse of the n x n Cauchy system built by launch_gf64_cauchy_cols (rows
+// fR + j, columns fI + cols[i], no zero denominator): d_w holds 2n words of
+// weights, d_Ainv receives A^-1 (n x n, row-major)
+cudaError_t launch_gf64_cauchy_inverse(const uint64_t* d_A, const uint64_t* d_cols, size_t n, uint64_t fI,
+                                       uint64_t fR, uint64_t* d_w, uint64_t* d_Ainv, cudaStream_t s);
 
 // out[r][w] (^)= XOR_c coeff[r*ldc + c] * in[c][w]
 // in rows in_stride words apart, out rows out_stride words apart.
@@ -67,6 +74,12 @@ cudaError_t launch_gf64_matvec(const uint64_t* d_in, size_t in_stride, size_t n_
 // Tensor-core (tcgen05) variant of the matvec; optional device pointer tables
 // for the rows (NULL: strided).  Requires 16-byte aligned rows and an even
 // word count.  *d_status is set nonzero if a bounded device wait gave up.
+// Tensor-core launches over a job table (tc_batch.h): one launch for all
+// jobs; the job fields the kernels derive (n_stages, groups / pairs,
+// wt) are filled in here and empty jobs are dropped, so the table is modified.
+cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStream_t s);
+cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s);
+
 cudaError_t launch_gf64_matvec_tc(const uint64_t* d_in, const uint64_t* const* d_in_ptrs, size_t in_stride,
                                   size_t n_in, size_t words, const uint64_t* d_coeff, size_t ldc, size_t n_out,
                                   uint64_t* d_out, uint64_t* const* d_out_ptrs, size_t out_stride, bool accumulate,

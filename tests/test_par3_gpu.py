@@ -231,3 +231,33 @@ def test_par3_repair_fused_vs_oracle(kctx, oracle):
     A = np.ascontiguousarray(M[:, lost])
     assert oracle.gf64_solve_and_reconstruct(A, rhs) == 0
     assert np.array_equal(got, rhs)
+
+
+@pytest.mark.parametrize("N,n,B,fI,fR", [
+    (2000, 150, 64, 0, 2000),     # closed-form Cauchy inverse, tensor-core n x n product
+    (50, 1, 8, 0, 50),            # one lost block
+    (64, 6, 16, 0, 10),           # lost ids meet row ids fR + j: entries mapped to 1, Gauss-Jordan
+    (64, 5, 16, 7, 2**64 - 3),    # row ids wrap around 2^64
+])
+def test_par3_repair_inverse_paths_vs_oracle(kctx, oracle, N, n, B, fI, fR):
+    """Both solve paths of pp_gf64_repair (closed-form Cauchy inverse when the
+    system is a true Cauchy matrix, Gauss-Jordan when a lost column id equals
+    a row id) give the oracle's Gauss-Jordan solution bit for bit."""
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(N + n)
+    data = rng.integers(0, 2**64, (N, B), dtype=np.uint64)
+    lost = np.sort(rng.choice(N, n, replace=False))
+    if fR == 10:
+        lost[0] = 12  # fI + 12 == fR + 2
+        lost = np.unique(lost)
+        n = lost.size
+    rec = rng.integers(0, 2**64, (n, B), dtype=np.uint64)  # any right-hand side
+    got = par3.repair(data, lost, rec.copy(), B, fI, fR, ctx=kctx)
+    M = oracle.gf64_build_cauchy(N, n, fI, fR)
+    known = np.setdiff1d(np.arange(N), lost)
+    rhs = rec.copy()
+    oracle.gf64_matvec(np.ascontiguousarray(data[known]), np.ascontiguousarray(M[:, known]), out=rhs,
+                       accumulate=True)
+    A = np.ascontiguousarray(M[:, lost])
+    assert oracle.gf64_solve_and_reconstruct(A, rhs) == 0
+    assert np.array_equal(got, rhs)
