@@ -296,6 +296,70 @@ def cpu_baseline_sample(name, budget_s=12.0, threads=0):
                 seconds_per_run=t, runs=len(times))
 
 
+def batched_repair_jobs(dev, seed=2024, count=16):
+    """16 PAR3 repair jobs of uneven sizes: input 64 MiB-1 GiB and block size
+    4-64 KiB, both log-uniform (seeded), 1 % of the blocks lost, recovery
+    rows fR = N onwards.  Inputs and recovery rows are seeded random device
+    data (the work does not depend on their values)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=f"cuda:{dev}")
+    g.manual_seed(seed)
+    jobs = []
+    for _ in range(count):
+        size = int(2 ** rng.uniform(26, 30))
+        sl = int(2 ** rng.uniform(12, 16)) // 16 * 16
+        N = size // sl
+        n = max(1, round(0.01 * N))
+        words = sl // 8
+        d_in = torch.randint(-2**63, 2**63 - 1, (N, words), dtype=torch.int64, device=f"cuda:{dev}", generator=g)
+        d_rec = torch.randint(-2**63, 2**63 - 1, (n, words), dtype=torch.int64, device=f"cuda:{dev}", generator=g)
+        lost = np.sort(rng.choice(N, n, replace=False)).astype(np.uint64)
+        jobs.append(dict(N=N, n=n, words=words, d_in=d_in, d_rec=d_rec, lost=lost))
+    return jobs
+
+
+def measure_batched_vs_plain(ctx, timer, steps, warmup, dev):
+    """The same 16 repair jobs run (a) one after another through the
+    single-job call par3.repair and (b) as one batch plan replayed from its
+    CUDA graph; both timed with CUDA events on the library's stream, outputs
+    compared bit for bit."""
+    import torch
+    from parparpar_b200 import batch as B
+    from parparpar_b200 import par3
+    jobs = batched_repair_jobs(dev)
+    in_bytes = sum(j["N"] * j["words"] * 8 for j in jobs)
+    plain_out = [torch.zeros((j["n"], j["words"]), dtype=torch.int64, device=f"cuda:{dev}") for j in jobs]
+    batch_out = [torch.zeros_like(o) for o in plain_out]
+
+    def plain():
+        for j, o in zip(jobs, plain_out):
+            par3.repair(j["d_in"], j["lost"], j["d_rec"], j["words"], 0, j["N"], restored=o, ctx=ctx)
+
+    for _ in range(max(1, warmup - 1)):
+        plain()
+    plain_ms = timer.run(plain, steps)
+    t0 = time.perf_counter()
+    b = B.Batch([B.par3_repair_job(j["d_in"], j["lost"], j["d_rec"], o) for j, o in zip(jobs, batch_out)],
+                tune=True, ctx=ctx)
+    ctx.synchronize()
+    create_s = time.perf_counter() - t0
+    for _ in range(warmup):
+        b.run()
+    batch_ms = timer.run(b.run, steps)
+    ctx.synchronize()
+    same = all(torch.equal(a, c) for a, c in zip(plain_out, batch_out))
+    launches = b.launches
+    b.close()
+    del jobs, plain_out, batch_out
+    torch.cuda.empty_cache()
+    return {"workload": "par3_repair_batch16_uneven_64MiB-1GiB_4-64KiB_1pct", "unit": "GB/s",
+            "input_bytes": in_bytes, "batched_value": in_bytes / (batch_ms * 1e-3) / 1e9, "batched_ms": batch_ms,
+            "plain_value": in_bytes / (plain_ms * 1e-3) / 1e9, "plain_ms": plain_ms,
+            "batched_over_plain": plain_ms / batch_ms, "batch_graph_launches": launches,
+            "batch_create_s": create_s, "outputs_identical": bool(same)}
+
+
 def run_reference(args, rank):
     """--impl reference: the reference's own CPU implementation on the host
     cores, on the same workload/metric (bounded sample per step)."""
@@ -333,6 +397,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=PRIMARY, choices=sorted(WORKLOADS))
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--batched-only", action="store_true", help="print only the batched-vs-plain comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gf16-kernel", default="auto", choices=["auto", "lut", "tensor"])
     ap.add_argument("--gf64-kernel", default="auto", choices=["auto", "lut", "tensor"])
@@ -366,6 +431,10 @@ def main():
     ctx.set_gf64_kernel({"auto": 0, "lut": 1, "tensor": 2}[args.gf64_kernel])
     timer = Timer(stream)
     peak, peak_kind = load_peaks()
+
+    if args.batched_only:
+        print(json.dumps(measure_batched_vs_plain(ctx, timer, args.steps, args.warmup, local)), flush=True)
+        return
 
     job = setup_job(args.workload, local, 1234 + rank, ctx)
     f = step_fn(job, ctx)
@@ -459,6 +528,12 @@ def main():
             except Exception as e:  # report, keep the primary line
                 sec.append({"workload": name, "error": str(e)[:200]})
         line["secondary"] = sec
+
+    if rank == 0 and world == 1 and not args.no_secondary:
+        try:
+            line["batched_vs_plain"] = measure_batched_vs_plain(ctx, timer, 3, 3, local)
+        except Exception as e:  # report, keep the primary line
+            line["batched_vs_plain"] = {"error": str(e)[:200]}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -265,6 +265,56 @@ PP_API int pp_gf64_solve_and_reconstruct_noalloc(uint64_t* A, uint64_t* rhs, siz
 PP_API int pp_gf64_fft_fwd(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld);
 PP_API int pp_gf64_fft_inv(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld);
 
+/* ------------------------------------------------------------ batches
+ * No counterpart in the reference (it runs one job at a time on its CPU
+ * threads).  A batch is a plan over device-resident jobs of mixed kinds and
+ * sizes: pp_batch_create builds every coefficient table the jobs need
+ * (PAR2 expanded coefficient bit matrices, PAR3 Cauchy matrices, the inverse
+ * of each repair system) and keeps them on the device, fuses the region
+ * products of all jobs into one tensor-core launch per field and phase, and
+ * captures the whole batch in a CUDA graph; pp_batch_run replays it on the
+ * context's stream (asynchronous; pp_ctx_synchronize reports the status).
+ * Results are bit-identical to running the jobs one by one through the
+ * single-job entry points.
+ *
+ * All job buffers are device memory and stay bound to the plan: inputs rows
+ * 16-byte aligned (base and stride), PAR3 outputs 8-byte aligned, PAR2
+ * outputs 4-byte aligned.  Creation runs the batch once (the outputs are
+ * written).  With PP_BATCH_TUNE it also times candidate work splits of each
+ * fused launch on the jobs' own buffers and keeps the fastest; the choice is
+ * remembered per shape for the process. */
+#define PP_JOB_PAR2_CREATE 1 /* outputs[e] = XOR_i c(input_ids[i], exponents[e]) * inputs[i] */
+#define PP_JOB_PAR3_CREATE 2 /* outputs[r] = XOR_c inv((fI+c)^(fR+r)) * inputs[c] */
+#define PP_JOB_PAR3_REPAIR 3 /* restored[k] = input block missing[k], from the first n recovery blocks */
+
+typedef struct pp_job {
+  int kind;
+  const void* inputs;        /* num_inputs rows (PAR3 repair: lost rows are not read) */
+  size_t input_stride;       /* bytes between input rows */
+  size_t num_inputs;
+  size_t slice_bytes;        /* PAR2: bytes per slice; PAR3: block bytes, a multiple of 8 */
+  const uint16_t* input_ids; /* PAR2: input slice numbers (host), NULL = 0..num_inputs-1 */
+  const uint16_t* exponents; /* PAR2: recovery exponents (host) */
+  size_t num_recovery;       /* PAR2 / PAR3 create: output rows; repair: ignored */
+  void* outputs;             /* PAR2 / PAR3 create: recovery rows; repair: restored rows */
+  size_t output_stride;      /* bytes between output rows */
+  uint64_t first_input;      /* PAR3 */
+  uint64_t first_recovery;   /* PAR3 */
+  const uint64_t* missing;   /* PAR3 repair: lost input indices (host), n of them */
+  size_t num_missing;
+  const void* recovery;      /* PAR3 repair: the first n recovery blocks (device) */
+  size_t recovery_stride;    /* bytes between recovery rows */
+  const uint8_t* recovery_present; /* PAR3 repair: NULL, or n flags (host); absent rows count as zero */
+} pp_job;
+
+typedef struct pp_batch pp_batch;
+#define PP_BATCH_TUNE 1
+PP_API int pp_batch_create(pp_ctx* ctx, const pp_job* jobs, size_t n_jobs, int flags, pp_batch** out);
+PP_API int pp_batch_run(pp_batch* batch);
+/* launches the batch's graph issues per run (kernels and memset/copy nodes) */
+PP_API int pp_batch_launches(const pp_batch* batch);
+PP_API void pp_batch_destroy(pp_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

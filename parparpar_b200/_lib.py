@@ -56,6 +56,7 @@ EXPORTS = [
     "pp_gf64_region_coupled_muladd_arr", "pp_gf64_region_fused_output_muladd_arr",
     "pp_gf64_region_2d_muladd_arr", "pp_gf64_inverse_batch", "pp_gf64_fft_fwd", "pp_gf64_fft_inv",
     "pp_gf64_solve_and_reconstruct_noalloc", "pp_gf64_repair",
+    "pp_batch_create", "pp_batch_run", "pp_batch_launches", "pp_batch_destroy",
 ]
 
 
@@ -137,6 +138,40 @@ _sig("pp_gf64_fft_fwd", _I, _P, _P, _SZ, _SZ, _SZ)
 _sig("pp_gf64_fft_inv", _I, _P, _P, _SZ, _SZ, _SZ)
 _sig("pp_gf64_solve_and_reconstruct_noalloc", _I, _P, _P, _SZ, _SZ, _P)
 _sig("pp_gf64_repair", _I, _P, _P, _SZ, _P, _SZ, _P, _P, _SZ, _U64, _U64, _P)
+
+PP_JOB_PAR2_CREATE = 1
+PP_JOB_PAR3_CREATE = 2
+PP_JOB_PAR3_REPAIR = 3
+PP_BATCH_TUNE = 1
+
+
+class PPJob(ctypes.Structure):
+    """struct pp_job (include/parpar_b200.h)"""
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("inputs", ctypes.c_void_p),
+        ("input_stride", ctypes.c_size_t),
+        ("num_inputs", ctypes.c_size_t),
+        ("slice_bytes", ctypes.c_size_t),
+        ("input_ids", ctypes.c_void_p),
+        ("exponents", ctypes.c_void_p),
+        ("num_recovery", ctypes.c_size_t),
+        ("outputs", ctypes.c_void_p),
+        ("output_stride", ctypes.c_size_t),
+        ("first_input", ctypes.c_uint64),
+        ("first_recovery", ctypes.c_uint64),
+        ("missing", ctypes.c_void_p),
+        ("num_missing", ctypes.c_size_t),
+        ("recovery", ctypes.c_void_p),
+        ("recovery_stride", ctypes.c_size_t),
+        ("recovery_present", ctypes.c_void_p),
+    ]
+
+
+_sig("pp_batch_create", _I, _P, ctypes.POINTER(PPJob), _SZ, _I, ctypes.POINTER(_P))
+_sig("pp_batch_run", _I, _P)
+_sig("pp_batch_launches", _I, _P)
+_sig("pp_batch_destroy", None, _P)
 
 
 def status_string(s: int) -> str:

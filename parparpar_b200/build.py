@@ -25,6 +25,7 @@ SOURCES = [
     "gf64_tc.cu",
     "gf64_fft.cu",
     "capi.cpp",
+    "batch.cpp",
     "noalloc.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

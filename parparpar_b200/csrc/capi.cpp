@@ -119,6 +119,16 @@ static int bind(pp_ctx* ctx) {
   return PP_OK;
 }
 
+// accessors for the other host translation units (batch.cpp, server.cpp)
+namespace pp {
+int ctx_device(const pp_ctx* c) { return c->device; }
+int ctx_sms(const pp_ctx* c) { return c->sms; }
+cudaStream_t ctx_stream(const pp_ctx* c) { return c->stream; }
+int* ctx_status_word(const pp_ctx* c) { return c->d_status; }
+std::mutex& ctx_mutex(pp_ctx* c) { return c->mu; }
+int ctx_fail(pp_ctx* c, int code, const char* msg) { return set_err(c, code, "%s", msg); }
+}  // namespace pp
+
 // Read and clear the device status word (after a synchronize).
 static int device_status(pp_ctx* ctx) {
   int h = 0;

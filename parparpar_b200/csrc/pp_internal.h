@@ -9,12 +9,24 @@
 
 #include "tc_batch.h"
 
+#include <mutex>
+
+struct pp_ctx;
+
 namespace pp {
 
 // Launch counter: every kernel launch issued by this library increments it
 // (reported by pp_ctx_launch_count so callers can account for native work).
 void note_launch(int n = 1);
 uint64_t launches();
+
+// context internals for the host translation units other than capi.cpp
+int ctx_device(const pp_ctx* c);
+int ctx_sms(const pp_ctx* c);
+cudaStream_t ctx_stream(const pp_ctx* c);
+int* ctx_status_word(const pp_ctx* c);
+std::mutex& ctx_mutex(pp_ctx* c);
+int ctx_fail(pp_ctx* c, int code, const char* msg);  // records the message, returns code
 
 // ------------------------------------------------------------ GF(2^16)
 // coeffs[o*N + i] = 2^(logs[i] * exps[o] mod 65535)   (device buffers)

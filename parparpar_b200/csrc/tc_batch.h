@@ -61,7 +61,8 @@ struct Gf64TcJob {
 template <class Job>
 struct TcBatch {
   uint32_t n_jobs;
-  uint32_t reserved;
+  uint32_t q_hint;                    // host: target stages per item, 0 = chosen by the estimate;
+                                      // tc_batch_plan leaves the value it used here
   uint64_t total;                     // items of all jobs
   uint64_t prefix[kTcMaxJobs + 1];    // items before job j
   Job job[kTcMaxJobs];
@@ -129,7 +130,7 @@ inline uint64_t tc_batch_plan(TcBatch<Job>& b, uint64_t tiles_of(const Job&), in
   std::vector<int64_t> load;
   uint64_t best = ~0ull;
   uint32_t best_q = smax;
-  for (uint32_t d = 1; d <= 256; d++) {
+  for (uint32_t d = 1; d <= 256 && !b.q_hint; d++) {
     const uint32_t q = (smax + d - 1) / d;  // target stages per item
     if (d > 1 && q == (smax + d - 2) / (d - 1)) continue;
     for (uint32_t j = 0; j < b.n_jobs; j++) tc_set_splits(b.job[j], (b.job[j].n_stages + q - 1) / q);
@@ -140,6 +141,8 @@ inline uint64_t tc_batch_plan(TcBatch<Job>& b, uint64_t tiles_of(const Job&), in
     }
     if (q <= 1) break;
   }
+  if (b.q_hint) best_q = b.q_hint;
+  b.q_hint = best_q;
   for (uint32_t j = 0; j < b.n_jobs; j++) tc_set_splits(b.job[j], (b.job[j].n_stages + best_q - 1) / best_q);
   b.total = 0;
   for (uint32_t j = 0; j < b.n_jobs; j++) {
