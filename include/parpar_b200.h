@@ -286,6 +286,8 @@ PP_API int pp_gf64_fft_inv(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, 
 #define PP_JOB_PAR2_CREATE 1 /* outputs[e] = XOR_i c(input_ids[i], exponents[e]) * inputs[i] */
 #define PP_JOB_PAR3_CREATE 2 /* outputs[r] = XOR_c inv((fI+c)^(fR+r)) * inputs[c] */
 #define PP_JOB_PAR3_REPAIR 3 /* restored[k] = input block missing[k], from the first n recovery blocks */
+#define PP_JOB_GF16_MULADD 4 /* outputs[o] = XOR_i coeffs[o][i] * inputs[i] (e.g. the PAR2 repair decode
+                              * with the factors of pp_par2_invert) */
 
 typedef struct pp_job {
   int kind;
@@ -305,6 +307,7 @@ typedef struct pp_job {
   const void* recovery;      /* PAR3 repair: the first n recovery blocks (device) */
   size_t recovery_stride;    /* bytes between recovery rows */
   const uint8_t* recovery_present; /* PAR3 repair: NULL, or n flags (host); absent rows count as zero */
+  const uint16_t* coeffs;    /* GF16 muladd: num_recovery x num_inputs coefficients, row-major (host) */
 } pp_job;
 
 typedef struct pp_batch pp_batch;
@@ -314,6 +317,39 @@ PP_API int pp_batch_run(pp_batch* batch);
 /* launches the batch's graph issues per run (kernels and memset/copy nodes) */
 PP_API int pp_batch_launches(const pp_batch* batch);
 PP_API void pp_batch_destroy(pp_batch* batch);
+
+/* ------------------------------------------------------------ serving loop
+ * No counterpart in the reference.  A server owns a context and a scheduler
+ * thread.  Submitted jobs (pp_job, host or device buffers; the small host
+ * arrays of the job are copied at submit, the data buffers must stay valid
+ * until the job completes) are admitted in arrival order while the device
+ * memory they need fits in hbm_budget_bytes (staging of host buffers, repair
+ * temporaries and the resident coefficient tables all count); admitted jobs
+ * are grouped into waves of at most max_jobs_per_wave and each wave runs as
+ * fused tensor-core launches on one of `lanes` streams, so a wave admitted
+ * while others are on the GPU overlaps with them (continuous batching).
+ * PAR3 Cauchy matrices and PAR2 coefficient tiles stay resident (LRU within
+ * the budget).  Every job's result is identical to running it alone.  Host
+ * buffers should be pinned for copies to overlap. */
+typedef struct pp_server pp_server;
+typedef struct pp_server_stats {
+  uint64_t submitted, completed, failed;
+  uint64_t waves;              /* fused waves launched */
+  uint64_t input_bytes;        /* input bytes of the completed jobs */
+  double elapsed_s;            /* first submit -> last completion */
+  double gbps;                 /* input_bytes / elapsed_s / 1e9 */
+  double p50_ms, p99_ms, max_ms; /* submit -> completion latency of completed jobs */
+  uint64_t hbm_peak_bytes;     /* most device memory held at once (jobs + tables) */
+  uint64_t tables_resident, table_bytes;
+} pp_server_stats;
+PP_API int pp_server_create(int device, size_t hbm_budget_bytes, int max_jobs_per_wave, int lanes, pp_server** out);
+PP_API int pp_server_submit(pp_server* srv, const pp_job* job, uint64_t* ticket);
+/* the job's status (PP_OK or its error), or PP_ERR_TIMEOUT if still running after timeout_ms (< 0: no limit) */
+PP_API int pp_server_wait(pp_server* srv, uint64_t ticket, int timeout_ms);
+PP_API int pp_server_get_stats(pp_server* srv, pp_server_stats* out);
+PP_API void pp_server_reset_stats(pp_server* srv);
+PP_API const char* pp_server_last_error(pp_server* srv);
+PP_API void pp_server_destroy(pp_server* srv); /* waits for every submitted job */
 
 #ifdef __cplusplus
 }

@@ -9,10 +9,10 @@ raises ImportError if that library has not been built; there is no CPU
 fallback.
 """
 from ._lib import (PP_ERR_BUSY, PP_ERR_CUDA, PP_ERR_INVALID_ARG, PP_ERR_NO_DEVICE, PP_ERR_NO_MEMORY,
-                   PP_ERR_NOT_INVERTIBLE, PP_ERR_SINGULAR, PP_OK, PP_PROC_ADD_FULL, PP_PROC_ADD_OK,
+                   PP_ERR_NOT_INVERTIBLE, PP_ERR_SINGULAR, PP_ERR_TIMEOUT, PP_ERR_TOO_LARGE, PP_OK, PP_PROC_ADD_FULL, PP_PROC_ADD_OK,
                    PP_PROC_ADD_OK_BUSY, Context, PPError, default_context, launch_count)
-from . import batch, par2, par3
+from . import batch, par2, par3, server
 
-__all__ = ["batch", "par2", "par3", "Context", "PPError", "default_context", "launch_count", "PP_OK",
+__all__ = ["batch", "par2", "par3", "server", "Context", "PPError", "default_context", "launch_count", "PP_OK",
            "PP_ERR_INVALID_ARG", "PP_ERR_CUDA", "PP_ERR_NO_MEMORY", "PP_ERR_SINGULAR", "PP_ERR_NOT_INVERTIBLE",
-           "PP_ERR_BUSY", "PP_ERR_NO_DEVICE", "PP_PROC_ADD_OK", "PP_PROC_ADD_OK_BUSY", "PP_PROC_ADD_FULL"]
+           "PP_ERR_BUSY", "PP_ERR_NO_DEVICE", "PP_ERR_TIMEOUT", "PP_ERR_TOO_LARGE", "PP_PROC_ADD_OK", "PP_PROC_ADD_OK_BUSY", "PP_PROC_ADD_FULL"]

@@ -57,6 +57,8 @@ EXPORTS = [
     "pp_gf64_region_2d_muladd_arr", "pp_gf64_inverse_batch", "pp_gf64_fft_fwd", "pp_gf64_fft_inv",
     "pp_gf64_solve_and_reconstruct_noalloc", "pp_gf64_repair",
     "pp_batch_create", "pp_batch_run", "pp_batch_launches", "pp_batch_destroy",
+    "pp_server_create", "pp_server_submit", "pp_server_wait", "pp_server_get_stats", "pp_server_reset_stats",
+    "pp_server_last_error", "pp_server_destroy",
 ]
 
 
@@ -142,6 +144,7 @@ _sig("pp_gf64_repair", _I, _P, _P, _SZ, _P, _SZ, _P, _P, _SZ, _U64, _U64, _P)
 PP_JOB_PAR2_CREATE = 1
 PP_JOB_PAR3_CREATE = 2
 PP_JOB_PAR3_REPAIR = 3
+PP_JOB_GF16_MULADD = 4
 PP_BATCH_TUNE = 1
 
 
@@ -165,6 +168,18 @@ class PPJob(ctypes.Structure):
         ("recovery", ctypes.c_void_p),
         ("recovery_stride", ctypes.c_size_t),
         ("recovery_present", ctypes.c_void_p),
+        ("coeffs", ctypes.c_void_p),
+    ]
+
+
+class PPServerStats(ctypes.Structure):
+    """struct pp_server_stats (include/parpar_b200.h)"""
+    _fields_ = [
+        ("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+        ("waves", ctypes.c_uint64), ("input_bytes", ctypes.c_uint64), ("elapsed_s", ctypes.c_double),
+        ("gbps", ctypes.c_double), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+        ("max_ms", ctypes.c_double), ("hbm_peak_bytes", ctypes.c_uint64), ("tables_resident", ctypes.c_uint64),
+        ("table_bytes", ctypes.c_uint64),
     ]
 
 
@@ -172,6 +187,13 @@ _sig("pp_batch_create", _I, _P, ctypes.POINTER(PPJob), _SZ, _I, ctypes.POINTER(_
 _sig("pp_batch_run", _I, _P)
 _sig("pp_batch_launches", _I, _P)
 _sig("pp_batch_destroy", None, _P)
+_sig("pp_server_create", _I, _I, _SZ, _I, _I, ctypes.POINTER(_P))
+_sig("pp_server_submit", _I, _P, ctypes.POINTER(PPJob), ctypes.POINTER(_U64))
+_sig("pp_server_wait", _I, _P, _U64, _I)
+_sig("pp_server_get_stats", _I, _P, ctypes.POINTER(PPServerStats))
+_sig("pp_server_reset_stats", None, _P)
+_sig("pp_server_last_error", ctypes.c_char_p, _P)
+_sig("pp_server_destroy", None, _P)
 
 
 def status_string(s: int) -> str:

@@ -14,8 +14,8 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (PP_BATCH_TUNE, PP_JOB_PAR2_CREATE, PP_JOB_PAR3_CREATE, PP_JOB_PAR3_REPAIR, PPJob,
-                   default_context, lib, ptr)
+from ._lib import (PP_BATCH_TUNE, PP_JOB_GF16_MULADD, PP_JOB_PAR2_CREATE, PP_JOB_PAR3_CREATE, PP_JOB_PAR3_REPAIR,
+                   PPJob, default_context, lib, ptr)
 
 
 def _ctx(ctx):
@@ -23,11 +23,22 @@ def _ctx(ctx):
 
 
 def _rows(t):
-    if not hasattr(t, "data_ptr") or not t.is_cuda:
-        raise TypeError("batch jobs take CUDA tensors")
-    if t.dim() != 2 or t.stride(1) != 1:
-        raise ValueError("rows must be a 2-D tensor with contiguous rows")
-    return t.shape[0], t.stride(0) * t.element_size()
+    """(rows, row stride in bytes) of a 2-D torch tensor or numpy array with
+    contiguous rows (batches need CUDA tensors; the server also takes host
+    buffers)."""
+    if hasattr(t, "data_ptr"):
+        if t.dim() != 2 or t.stride(1) != 1:
+            raise ValueError("rows must be a 2-D tensor with contiguous rows")
+        return t.shape[0], t.stride(0) * t.element_size()
+    if isinstance(t, np.ndarray):
+        if t.ndim != 2 or t.strides[1] != t.itemsize:
+            raise ValueError("rows must be a 2-D array with contiguous rows")
+        return t.shape[0], t.strides[0]
+    raise TypeError("job buffers are torch tensors or numpy arrays")
+
+
+def _width(t):
+    return t.shape[1] * (t.element_size() if hasattr(t, "element_size") else t.itemsize)
 
 
 def par2_create_job(inputs, exponents, outputs, input_ids=None, slice_bytes=None):
@@ -39,7 +50,7 @@ def par2_create_job(inputs, exponents, outputs, input_ids=None, slice_bytes=None
     if exps.size != r:
         raise ValueError("one exponent per output row")
     j = PPJob(kind=PP_JOB_PAR2_CREATE, inputs=ptr(inputs), input_stride=istride, num_inputs=n,
-              slice_bytes=slice_bytes if slice_bytes is not None else inputs.shape[1] * inputs.element_size(),
+              slice_bytes=slice_bytes if slice_bytes is not None else _width(inputs),
               input_ids=ptr(ids) if ids is not None else None, exponents=ptr(exps), num_recovery=r,
               outputs=ptr(outputs), output_stride=ostride)
     return j, (inputs, outputs, exps, ids)
@@ -51,7 +62,7 @@ def par3_create_job(inputs, outputs, first_input=0, first_recovery=None):
     r, ostride = _rows(outputs)
     fr = n if first_recovery is None else first_recovery
     j = PPJob(kind=PP_JOB_PAR3_CREATE, inputs=ptr(inputs), input_stride=istride, num_inputs=n,
-              slice_bytes=inputs.shape[1] * inputs.element_size(), num_recovery=r, outputs=ptr(outputs),
+              slice_bytes=_width(inputs), num_recovery=r, outputs=ptr(outputs),
               output_stride=ostride, first_input=first_input & (2**64 - 1), first_recovery=fr & (2**64 - 1))
     return j, (inputs, outputs)
 
@@ -68,11 +79,25 @@ def par3_repair_job(inputs, missing, recovery, restored, first_input=0, first_re
     pres = None if recovery_present is None else np.ascontiguousarray(np.asarray(recovery_present, dtype=np.uint8))
     fr = n_in if first_recovery is None else first_recovery
     j = PPJob(kind=PP_JOB_PAR3_REPAIR, inputs=ptr(inputs), input_stride=istride, num_inputs=n_in,
-              slice_bytes=inputs.shape[1] * inputs.element_size(), outputs=ptr(restored), output_stride=ostride,
+              slice_bytes=_width(inputs), outputs=ptr(restored), output_stride=ostride,
               first_input=first_input & (2**64 - 1), first_recovery=fr & (2**64 - 1), missing=ptr(miss),
               num_missing=miss.size, recovery=ptr(recovery), recovery_stride=rstride,
               recovery_present=ptr(pres) if pres is not None else None)
     return j, (inputs, recovery, restored, miss, pres)
+
+
+def gf16_muladd_job(inputs, coeffs, outputs, slice_bytes=None):
+    """outputs[o] = XOR_i coeffs[o, i] * inputs[i] over GF(2^16), e.g. the PAR2
+    repair decode with the factors of par2.Galois16RecMatrix."""
+    n, istride = _rows(inputs)
+    r, ostride = _rows(outputs)
+    co = np.ascontiguousarray(np.asarray(coeffs, dtype=np.uint16))
+    if co.shape != (r, n):
+        raise ValueError("coeffs must be (num_outputs, num_inputs)")
+    j = PPJob(kind=PP_JOB_GF16_MULADD, inputs=ptr(inputs), input_stride=istride, num_inputs=n,
+              slice_bytes=slice_bytes if slice_bytes is not None else _width(inputs), num_recovery=r,
+              outputs=ptr(outputs), output_stride=ostride, coeffs=ptr(co))
+    return j, (inputs, outputs, co)
 
 
 class Batch:

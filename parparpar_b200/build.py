@@ -26,6 +26,7 @@ SOURCES = [
     "gf64_fft.cu",
     "capi.cpp",
     "batch.cpp",
+    "server.cpp",
     "noalloc.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -210,29 +210,34 @@ PP_API int pp_batch_create(pp_ctx* ctx, const pp_job* jobs, size_t n_jobs, int f
   std::vector<Gf64TcJob> j64a, j64b;
   for (size_t k = 0; k < n_jobs; k++) {
     const pp_job& J = jobs[k];
-    if (J.kind == PP_JOB_PAR2_CREATE) {
+    if (J.kind == PP_JOB_PAR2_CREATE || J.kind == PP_JOB_GF16_MULADD) {
+      const bool custom = J.kind == PP_JOB_GF16_MULADD;
       const size_t n = J.num_inputs, r = J.num_recovery, sb = J.slice_bytes;
       if (!r || !sb) continue;
-      if (n > 32768 || r > 65535 || !J.exponents) BFAIL(PP_ERR_INVALID_ARG, "PAR2 job: bad counts or no exponents");
+      if (n > 32768 || r > 65535 || (custom ? !J.coeffs : !J.exponents))
+        BFAIL(PP_ERR_INVALID_ARG, "GF16 job: bad counts, or no exponents / coefficients");
       if (!J.inputs || !J.outputs || !aligned(J.inputs, 16) || J.input_stride % 16 ||
           J.input_stride < ((sb + 15) & ~(size_t)15) || !aligned(J.outputs, 4) || J.output_stride % 4 ||
           J.output_stride < sb)
-        BFAIL(PP_ERR_INVALID_ARG, "PAR2 job: inputs need 16-byte aligned rows of >= slice bytes rounded to 16, "
+        BFAIL(PP_ERR_INVALID_ARG, "GF16 job: inputs need 16-byte aligned rows of >= slice bytes rounded to 16, "
                                   "outputs 4-byte aligned rows");
       // coefficient matrix -> expanded tensor-core tiles, resident
-      std::vector<uint16_t> logs(n), exps(J.exponents, J.exponents + r);
-      for (size_t i = 0; i < n; i++) logs[i] = pp_par2_input_log(J.input_ids ? J.input_ids[i] : (uint16_t)i);
-      uint16_t* d_logs = (uint16_t*)b->alloc(n * 2);
-      uint16_t* d_exps = (uint16_t*)b->alloc(r * 2);
       uint16_t* d_coef = (uint16_t*)b->alloc(n * r * 2);
       uint8_t* d_aexp = (uint8_t*)b->alloc(gf16_tc_coeff_bytes((unsigned)n, (unsigned)r));
-      if (!d_logs || !d_exps || !d_coef || !d_aexp) BFAIL(PP_ERR_NO_MEMORY, "PAR2 coefficient tables");
-      if (n) {
+      if (!d_coef || !d_aexp) BFAIL(PP_ERR_NO_MEMORY, "GF16 coefficient tables");
+      if (n && custom) {
+        BTRY(cudaMemcpyAsync(d_coef, J.coeffs, n * r * 2, cudaMemcpyHostToDevice, s), "copy coefficients");
+      } else if (n) {
+        std::vector<uint16_t> logs(n), exps(J.exponents, J.exponents + r);
+        for (size_t i = 0; i < n; i++) logs[i] = pp_par2_input_log(J.input_ids ? J.input_ids[i] : (uint16_t)i);
+        uint16_t* d_logs = (uint16_t*)b->alloc(n * 2);
+        uint16_t* d_exps = (uint16_t*)b->alloc(r * 2);
+        if (!d_logs || !d_exps) BFAIL(PP_ERR_NO_MEMORY, "PAR2 coefficient tables");
         BTRY(cudaMemcpyAsync(d_logs, logs.data(), n * 2, cudaMemcpyHostToDevice, s), "copy input logs");
         BTRY(cudaMemcpyAsync(d_exps, exps.data(), r * 2, cudaMemcpyHostToDevice, s), "copy exponents");
         BTRY(launch_gf16_coeff_matrix(d_logs, (unsigned)n, d_exps, (unsigned)r, d_coef, s), "coefficients");
-        BTRY(launch_gf16_tc_expand(d_coef, n, (unsigned)n, (unsigned)r, d_aexp, s), "coefficient tiles");
       }
+      if (n) BTRY(launch_gf16_tc_expand(d_coef, n, (unsigned)n, (unsigned)r, d_aexp, s), "coefficient tiles");
       Gf16TcJob t{};
       t.in = (const uint8_t*)J.inputs;
       t.in_stride = J.input_stride;
