@@ -360,6 +360,145 @@ def measure_batched_vs_plain(ctx, timer, steps, warmup, dev):
             "batch_create_s": create_s, "outputs_identical": bool(same)}
 
 
+def serving_jobs(dev, seed=5, count=32):
+    """Mixed stream: PAR2 / PAR3 create and repair, input size log-uniform
+    1 MiB-1 GiB, slice size log-uniform 4 KiB-1 MiB, R uniform 4-512 for
+    creates, 1 % of the slices lost for repairs (at least one).  PAR2 slices
+    are raised so that N <= 32768 and rounded to even bytes, PAR3 blocks to
+    16 bytes.  Data is seeded random bytes in pinned host memory (the PAR2
+    repair decode coefficients and the recovery rows are random: the work
+    does not depend on their values)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=f"cuda:{dev}")
+    g.manual_seed(seed)
+
+    def pinned(shape, dtype):
+        t = torch.empty(shape, dtype=dtype).pin_memory()
+        lo, hi = (0, 256) if dtype == torch.uint8 else (-2**63, 2**63 - 1)
+        rows = max(1, (256 << 20) // max(1, t[0].numel() * t.element_size()))
+        for r0 in range(0, shape[0], rows):  # generate on the device in chunks
+            r1 = min(shape[0], r0 + rows)
+            t[r0:r1].copy_(torch.randint(lo, hi, (r1 - r0,) + tuple(shape[1:]), dtype=dtype,
+                                         device=f"cuda:{dev}", generator=g))
+        return t
+
+    jobs = []
+    for _ in range(count):
+        kind = str(rng.choice(["par2_create", "par2_repair", "par3_create", "par3_repair"]))
+        size = int(2 ** rng.uniform(20, 30))
+        sl = int(2 ** rng.uniform(12, 20))
+        R = int(rng.integers(4, 513))
+        if kind.startswith("par2"):
+            sl = max(sl, -(-size // 32768))
+            sl = (sl + 1) // 2 * 2
+            N = max(1, size // sl)
+            inp = pinned((N, sl), torch.uint8)
+            if kind == "par2_create":
+                jobs.append(dict(kind=kind, N=N, sl=sl, R=R, inp=inp, exps=np.arange(R, dtype=np.uint16)))
+            else:
+                m = max(1, round(0.01 * N))
+                co = rng.integers(1, 65536, (m, N), dtype=np.uint16)
+                jobs.append(dict(kind=kind, N=N, sl=sl, R=m, inp=inp, coeffs=co))
+        else:
+            sl = max(16, sl // 16 * 16)
+            N = max(1, size // sl)
+            inp = pinned((N, sl // 8), torch.int64)
+            if kind == "par3_create":
+                jobs.append(dict(kind=kind, N=N, sl=sl, R=R, inp=inp))
+            else:
+                n = max(1, round(0.01 * N))
+                lost = np.sort(rng.choice(N, n, replace=False)).astype(np.uint64)
+                jobs.append(dict(kind=kind, N=N, sl=sl, R=n, inp=inp, lost=lost, rec=pinned((n, sl // 8), torch.int64)))
+    return jobs
+
+
+def measure_serving(ctx, dev, count=32, seed=5, budget=120 * 10**9):
+    """The mixed job stream (a) run one job at a time through the single-job
+    calls with the same host buffers, wall clock, and (b) submitted to the
+    serving loop with Poisson arrivals at twice the plain service rate;
+    outputs compared bit for bit."""
+    import torch
+    from parparpar_b200 import batch as B
+    from parparpar_b200 import par2, par3
+    from parparpar_b200.server import Server
+    jobs = serving_jobs(dev, seed, count)
+    in_bytes = sum(j["N"] * j["sl"] for j in jobs)
+
+    def out_of(j):
+        w = j["sl"] if j["kind"].startswith("par2") else j["sl"] // 8
+        dt = torch.uint8 if j["kind"].startswith("par2") else torch.int64
+        return torch.zeros((j["R"], w), dtype=dt).pin_memory()
+
+    plain_out = [out_of(j) for j in jobs]
+
+    def run_plain(j, o):
+        k = j["kind"]
+        if k == "par2_create":
+            par2.par2_create(j["inp"], np.arange(j["N"]), j["exps"], out=o, ctx=ctx)
+        elif k == "par2_repair":
+            par2.gf16_muladd(j["inp"], j["coeffs"], out=o, ctx=ctx)
+        elif k == "par3_create":
+            par3.GF64Controller.ctx = ctx
+            par3.GF64Controller.ComputeRecoveryBlocks(j["inp"], j["N"], o, j["R"], j["sl"] // 8, 0, j["N"])
+        else:
+            par3.repair(j["inp"], j["lost"], j["rec"], j["sl"] // 8, 0, j["N"], restored=o, ctx=ctx)
+
+    run_plain(jobs[0], plain_out[0])  # warm-up (kernels, tables)
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    plain_lat = []
+    for j, o in zip(jobs, plain_out):
+        a = time.perf_counter()
+        run_plain(j, o)
+        ctx.synchronize()
+        plain_lat.append((time.perf_counter() - a) * 1e3)
+    plain_s = time.perf_counter() - t0
+
+    def job_of(j, o):
+        k = j["kind"]
+        if k == "par2_create":
+            return B.par2_create_job(j["inp"], j["exps"], o)
+        if k == "par2_repair":
+            return B.gf16_muladd_job(j["inp"], j["coeffs"], o)
+        if k == "par3_create":
+            return B.par3_create_job(j["inp"], o, 0, j["N"])
+        return B.par3_repair_job(j["inp"], j["lost"], j["rec"], o, 0, j["N"])
+
+    srv = Server(dev, hbm_budget_bytes=budget, lanes=2)
+    srv_out = [out_of(j) for j in jobs]
+    srv.wait(srv.submit(job_of(jobs[0], srv_out[0])))  # warm-up
+    srv.reset_stats()
+    rate = 2.0 * len(jobs) / plain_s  # arrivals per second: twice the plain service rate
+    arr = np.cumsum(np.random.default_rng(seed + 1).exponential(1.0 / rate, len(jobs)))
+    tickets = []
+    t0 = time.perf_counter()
+    for j, o, at in zip(jobs, srv_out, arr):
+        d = at - (time.perf_counter() - t0)
+        if d > 0:
+            time.sleep(d)
+        tickets.append(srv.submit(job_of(j, o)))
+    statuses = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    same = all(torch.equal(a, b) for a, b in zip(plain_out, srv_out)) and all(x == 0 for x in statuses)
+    pl = sorted(plain_lat)
+    kinds = {}
+    for j in jobs:
+        kinds[j["kind"]] = kinds.get(j["kind"], 0) + 1
+    del jobs, plain_out, srv_out
+    return {"workload": f"serving_{count}jobs_mixed_1MiB-1GiB_4KiB-1MiB_R4-512_1pct", "jobs": count,
+            "kinds": kinds, "input_bytes": in_bytes, "host_buffers": "pinned", "hbm_budget_bytes": budget,
+            "arrivals": f"Poisson, {rate:.1f}/s (twice the plain service rate)",
+            "served_gbps": st["gbps"], "served_p50_ms": st["p50_ms"], "served_p99_ms": st["p99_ms"],
+            "served_max_ms": st["max_ms"], "served_elapsed_s": st["elapsed_s"], "waves": st["waves"],
+            "hbm_peak_bytes": st["hbm_peak_bytes"], "tables_resident": st["tables_resident"],
+            "plain_gbps": in_bytes / plain_s / 1e9, "plain_elapsed_s": plain_s,
+            "plain_job_p50_ms": pl[len(pl) // 2], "plain_job_p99_ms": pl[min(len(pl) - 1, int(0.99 * len(pl)))],
+            "served_over_plain": (in_bytes / max(st["elapsed_s"], 1e-9)) / (in_bytes / plain_s),
+            "outputs_identical": bool(same)}
+
+
 def run_reference(args, rank):
     """--impl reference: the reference's own CPU implementation on the host
     cores, on the same workload/metric (bounded sample per step)."""
@@ -398,6 +537,7 @@ def main():
     ap.add_argument("--workload", default=PRIMARY, choices=sorted(WORKLOADS))
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--batched-only", action="store_true", help="print only the batched-vs-plain comparison")
+    ap.add_argument("--serving-only", action="store_true", help="print only the serving-loop comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gf16-kernel", default="auto", choices=["auto", "lut", "tensor"])
     ap.add_argument("--gf64-kernel", default="auto", choices=["auto", "lut", "tensor"])
@@ -434,6 +574,9 @@ def main():
 
     if args.batched_only:
         print(json.dumps(measure_batched_vs_plain(ctx, timer, args.steps, args.warmup, local)), flush=True)
+        return
+    if args.serving_only:
+        print(json.dumps(measure_serving(ctx, local)), flush=True)
         return
 
     job = setup_job(args.workload, local, 1234 + rank, ctx)
@@ -534,6 +677,10 @@ def main():
             line["batched_vs_plain"] = measure_batched_vs_plain(ctx, timer, 3, 3, local)
         except Exception as e:  # report, keep the primary line
             line["batched_vs_plain"] = {"error": str(e)[:200]}
+        try:
+            line["serving"] = measure_serving(ctx, local)
+        except Exception as e:
+            line["serving"] = {"error": str(e)[:200]}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
