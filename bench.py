@@ -51,16 +51,88 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def int8_peak_tops(dev):
+    """Dense int8 tensor throughput measured here: cuBLASLt int8 GEMM
+    (torch._int_mm, 8192^3, 2 ops per MAC), best of 10 after warm-up."""
+    import torch
+    try:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device=f"cuda:{dev}")
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device=f"cuda:{dev}")
+        for _ in range(3):
+            torch._int_mm(a, b)
+        best = 1e30
+        for _ in range(10):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2 * 8192**3 / (best * 1e-3) / 1e12
+    except Exception:
+        return None
+
+
+def bit_macs(w):
+    """GF(2) multiply-accumulates of a create: every (input word, output)
+    pair is a 16x16 (GF(2^16)) or 64x64 (GF(2^64)) bit-matrix product; the
+    tensor-core kernels run exactly these as int8 MACs."""
+    if w["field"] == "gf16":
+        return (w["n"] * w["s"] // 2) * w["r"] * 256
+    if w["field"] == "gf64":
+        return (w["n"] * w["s"] // 8) * w["r"] * 4096
+    n_known = w["n"] - w["r"]  # repair: the known-input sum dominates
+    return (n_known * w["s"] // 8) * w["r"] * 4096
+
+
+def roofline(w, args, hbm_achieved, hbm_peak, peak_kind, kms, int8_tops):
+    """Roofline of the dominant kernel.  The tensor-core kernels compute each
+    GF product as a dense GF(2) bit-matrix contraction in int8 MMAs, so their
+    binding unit is the int8 tensor pipe: achieved = 2 x bit-MACs / kernel
+    time against the dense int8 GEMM throughput measured in the same run
+    (cuBLASLt); the HBM view of the same launch (algorithmic bytes / time
+    against MEASURED_PEAKS.json) is given beside it."""
+    kern = dominant_kernel(w, args)
+    hbm = {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_achieved / hbm_peak,
+           "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+           else "fallback 6.65 TB/s"}
+    r = {"kernel": kern, "kernel_ms": kms, "traffic": load_traffic(f"{kern}.{args.workload}")}
+    if kern.endswith("_tc"):
+        tops = 2 * bit_macs(w) / (kms * 1e-3) / 1e12
+        if int8_tops:
+            peak, kind = int8_tops, "measured here: cuBLASLt dense int8 GEMM 8192^3 (torch._int_mm), best of 10"
+        else:
+            peak, kind = 2 * load_bf16_peak(), "2 x MEASURED_PEAKS.json bf16_tflops (int8 dense rate = 2x bf16)"
+        r.update({"bound": "tensor", "achieved": tops, "peak": peak, "unit": "TFLOP/s", "frac": tops / peak,
+                  "peak_kind": kind, "ops": "int8 tensor ops (2 per MAC), one MAC per GF(2) bit product",
+                  "hbm": hbm})
+    else:
+        r.update({"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                  "frac": hbm_achieved / hbm_peak, "peak_kind": hbm["peak_kind"]})
+    return r
+
+
+def load_bf16_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f).get("bf16_tflops", 1590.0))
+    except Exception:
+        return 1590.0
+
+
+# DRAM bytes (read + write) per launch of the dominant kernel, from the ncu
+# captures summarised in profiles/ (the file named after kernel and workload)
+TRAFFIC = {
+    "k_gf16_muladd_tc.par2_create_32768x32KiB_R64": 2465423872 + 10860288,
+    "k_gf16_muladd_tc.par2_create_1024x1MiB_R8": 1087907000 + 10907904,
+    "k_gf64_matvec_tc.par3_create_131072x8KiB_R8": 1083011000 + 3985664,
+}
+
+
 def load_traffic(name):
-    """dram bytes per launch from a committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        try:
-            with open(p) as f:
-                return json.load(f).get(name)
-        except Exception:
-            return None
-    return None
+    return TRAFFIC.get(name)
 
 
 class ClockSampler:
@@ -131,6 +203,7 @@ WORKLOADS = {
     "par2_create_1024x1MiB_R8": dict(field="gf16", n=1024, s=1 << 20, r=8),
     "par2_create_256x64KiB_R8": dict(field="gf16", n=256, s=64 * 1024, r=8),
     "par3_create_131072x8KiB_R8": dict(field="gf64", n=131072, s=8 * 1024, r=8),
+    "par3_create_131072x8KiB_R1024": dict(field="gf64", n=131072, s=8 * 1024, r=1024),
     # 1 % of 262,144 blocks lost, solved from the first 2,621 of R=4,096 recovery blocks
     "par3_repair_262144x4KiB_R4096_1pct": dict(field="gf64_repair", n=262144, s=4 * 1024, r=2621),
 }
@@ -599,6 +672,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
 
+    int8_tops = int8_peak_tops(local)
+
     # dominant kernel alone, for the roofline
     kf = kernel_fn(job, ctx)
     kf()
@@ -644,10 +719,7 @@ def main():
         "config": {"workload": args.workload, "num_inputs": w["n"], "slice_bytes": w["s"], "num_recovery": w["r"],
                    "exponents": f"0..{w['r'] - 1}", "parallelism": f"replicas x{world} (one job per GPU)",
                    "l2": "inputs (1 GiB) larger than L2; no flush needed"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                     else "fallback 6.65 TB/s", "kernel": dominant_kernel(w, args), "kernel_ms": kms,
-                     "traffic": load_traffic(args.workload)},
+        "roofline": roofline(w, args, achieved, peak, peak_kind, kms, int8_tops),
         "e2e": {"value": input_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": w["r"] * w["s"], "host_buffers": "pinned", "matches_device_result": bool(ok)},
         "gpu_launches": int(launches),
@@ -661,11 +733,13 @@ def main():
                 continue
             try:
                 j = setup_job(name, local, 77, ctx)
-                heavy = WORKLOADS[name]["field"] == "gf64_repair"
+                heavy = WORKLOADS[name]["field"] == "gf64_repair" or WORKLOADS[name]["r"] >= 1024
                 m = measure(j, ctx, timer, 2 if heavy else 5, 1 if heavy else 3, peak)
-                sec.append({"workload": name, "value": input_bytes_of(name) / (m["ms"] * 1e-3) / 1e9,
-                            "unit": "GB/s", "ms_per_step": m["ms"], "kernel_ms": m["kernel_ms"],
-                            "roofline_frac": m["frac"]})
+                ent = {"workload": name, "value": input_bytes_of(name) / (m["ms"] * 1e-3) / 1e9,
+                       "unit": "GB/s", "ms_per_step": m["ms"], "kernel_ms": m["kernel_ms"], "hbm_frac": m["frac"]}
+                if int8_tops and dominant_kernel(WORKLOADS[name], args).endswith("_tc"):
+                    ent["tensor_frac"] = 2 * bit_macs(WORKLOADS[name]) / (m["kernel_ms"] * 1e-3) / 1e12 / int8_tops
+                sec.append(ent)
                 del j
                 torch.cuda.empty_cache()
             except Exception as e:  # report, keep the primary line
