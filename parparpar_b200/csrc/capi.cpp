@@ -77,6 +77,18 @@ struct CauchyEntry {
   uint64_t* d;
 };
 
+// Resident PAR2 coefficient table: the coefficient matrix of (input slice
+// numbers, exponents) and, for the tensor-core kernel, its expanded bit-matrix
+// tiles; keyed by the two index lists.
+struct Par2Entry {
+  std::string key;
+  uint16_t* d_coef = nullptr;
+  uint8_t* d_aexp = nullptr;
+  size_t bytes = 0;
+};
+constexpr size_t kPar2CacheEntries = 4;
+constexpr size_t kPar2CacheBytes = (size_t)4 << 30;
+
 struct pp_ctx {
   int device = 0;
   int sms = 148;
@@ -86,6 +98,7 @@ struct pp_ctx {
   void* slot_p[S_NSLOTS] = {};
   size_t slot_n[S_NSLOTS] = {};
   std::list<CauchyEntry> cauchy;  // LRU, front = most recent
+  std::list<Par2Entry> par2;      // LRU, front = most recent
   int gf16_kernel = PP_GF16_KERNEL_AUTO;
   int gf64_kernel = PP_GF16_KERNEL_AUTO;
   int* d_status = nullptr;  // set nonzero by a kernel whose bounded wait gave up
@@ -277,6 +290,11 @@ PP_API int pp_ctx_free_cache(pp_ctx* ctx) {
   }
   for (auto& e : ctx->cauchy) cudaFree(e.d);
   ctx->cauchy.clear();
+  for (auto& e : ctx->par2) {
+    cudaFree(e.d_coef);
+    cudaFree(e.d_aexp);
+  }
+  ctx->par2.clear();
   return PP_OK;
 }
 
@@ -342,6 +360,64 @@ static int par2_coeff_matrix_dev(pp_ctx* ctx, const uint16_t* input_idx, unsigne
   return PP_OK;
 }
 
+static bool use_tensor(int sel, unsigned n_in, unsigned n_out);
+
+// The resident coefficient table of (input_idx, exps): built on first use
+// (coefficient matrix, plus the expanded tiles when the tensor-core kernel is
+// selected), then found by key; least recently used tables are dropped beyond
+// kPar2CacheEntries / kPar2CacheBytes.
+static int par2_table(pp_ctx* ctx, const uint16_t* input_idx, unsigned n_in, const uint16_t* exps, unsigned n_out,
+                      const Par2Entry** out) {
+  std::string key(2 * (size_t)(n_in + n_out) + 1, '\0');
+  if (is_device_ptr(input_idx)) {
+    CUDA_TRY(ctx, cudaMemcpy(&key[0], input_idx, n_in * 2, cudaMemcpyDeviceToHost));
+  } else {
+    memcpy(&key[0], input_idx, n_in * 2);
+  }
+  memcpy(&key[2 * (size_t)n_in], exps, n_out * 2);
+  const bool tc = use_tensor(ctx->gf16_kernel, n_in, n_out);
+  key.back() = tc ? 1 : 0;
+  for (auto it = ctx->par2.begin(); it != ctx->par2.end(); ++it) {
+    if (it->key == key) {
+      ctx->par2.splice(ctx->par2.begin(), ctx->par2, it);
+      *out = &ctx->par2.front();
+      return PP_OK;
+    }
+  }
+  Par2Entry e;
+  e.key = std::move(key);
+  const size_t cbytes = (size_t)n_in * n_out * 2, tbytes = tc ? gf16_tc_coeff_bytes(n_in, n_out) : 0;
+  e.bytes = cbytes + tbytes;
+  size_t total = e.bytes;
+  for (auto& x : ctx->par2) total += x.bytes;
+  while (!ctx->par2.empty() && (ctx->par2.size() >= kPar2CacheEntries || total > kPar2CacheBytes)) {
+    cudaStreamSynchronize(ctx->stream);
+    total -= ctx->par2.back().bytes;
+    cudaFree(ctx->par2.back().d_coef);
+    cudaFree(ctx->par2.back().d_aexp);
+    ctx->par2.pop_back();
+  }
+  if (cudaMalloc(&e.d_coef, cbytes) != cudaSuccess || (tbytes && cudaMalloc(&e.d_aexp, tbytes) != cudaSuccess)) {
+    cudaGetLastError();
+    cudaFree(e.d_coef);
+    return set_err(ctx, PP_ERR_NO_MEMORY, "PAR2 coefficient table (%zu bytes)", e.bytes);
+  }
+  int r = par2_coeff_matrix_dev(ctx, input_idx, n_in, exps, n_out, e.d_coef);
+  if (!r && tc) {
+    cudaError_t ce = launch_gf16_tc_expand(e.d_coef, n_in, n_in, n_out, e.d_aexp, ctx->stream);
+    if (ce != cudaSuccess) r = set_err(ctx, PP_ERR_CUDA, "tile expansion: %s", cudaGetErrorString(ce));
+  }
+  if (r) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(e.d_coef);
+    cudaFree(e.d_aexp);
+    return r;
+  }
+  ctx->par2.push_front(std::move(e));
+  *out = &ctx->par2.front();
+  return PP_OK;
+}
+
 PP_API int pp_par2_coeff_matrix(pp_ctx* ctx, const uint16_t* input_idx, unsigned num_inputs, const uint16_t* exps,
                                 unsigned num_outputs, uint16_t* coeffs) {
   if (!ctx) return PP_ERR_INVALID_ARG;
@@ -372,12 +448,17 @@ static bool use_tensor(int sel, unsigned n_in, unsigned n_out) {
   if (sel == PP_GF16_KERNEL_TENSOR) return true;
   return n_in >= 8 && n_out >= 1;
 }
+// aexp_ready: aexp already holds the expanded tiles of d_coeffs (a resident
+// table), so the expansion is skipped
 static cudaError_t gf16_region(int sel, const uint8_t* din, size_t dstride, unsigned n_in, size_t slice,
                                const uint16_t* d_coeffs, size_t ldc, unsigned n_out, uint8_t* dout, size_t ostride,
-                               bool accumulate, int sms, uint8_t* aexp, int* d_status, cudaStream_t s) {
+                               bool accumulate, int sms, uint8_t* aexp, int* d_status, cudaStream_t s,
+                               bool aexp_ready = false) {
   if (use_tensor(sel, n_in, n_out) && aexp) {
-    cudaError_t e = launch_gf16_tc_expand(d_coeffs, ldc, n_in, n_out, aexp, s);
-    if (e != cudaSuccess) return e;
+    if (!aexp_ready) {
+      cudaError_t e = launch_gf16_tc_expand(d_coeffs, ldc, n_in, n_out, aexp, s);
+      if (e != cudaSuccess) return e;
+    }
     return launch_gf16_muladd_tc(din, dstride, n_in, slice, aexp, n_out, dout, ostride, accumulate, sms, d_status, s);
   }
   return launch_gf16_muladd(din, dstride, n_in, slice, d_coeffs, ldc, n_out, dout, ostride, accumulate, sms, s);
@@ -386,7 +467,7 @@ static cudaError_t gf16_region(int sel, const uint8_t* din, size_t dstride, unsi
 // Region muladd with staging of host / unaligned buffers.
 static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, unsigned n_in, size_t slice,
                             const uint16_t* d_coeffs, size_t ldc, unsigned n_out, void* outputs, size_t out_stride,
-                            bool accumulate) {
+                            bool accumulate, uint8_t* aexp_ready = nullptr) {
   const bool in_dev = is_device_ptr(inputs);
   const bool out_dev = is_device_ptr(outputs);
   const size_t row = round16(slice);
@@ -411,13 +492,13 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
       CUDA_TRY(ctx, cudaMemcpy2DAsync(dout, row, outputs, out_stride, slice, n_out,
                                       out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
   }
-  uint8_t* aexp = nullptr;
-  if (use_tensor(ctx->gf16_kernel, n_in, n_out)) {
+  uint8_t* aexp = aexp_ready;
+  if (!aexp && use_tensor(ctx->gf16_kernel, n_in, n_out)) {
     aexp = (uint8_t*)scratch(ctx, S_AEXP, gf16_tc_coeff_bytes(n_in, n_out));
     if (!aexp) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficient tiles");
   }
   CUDA_TRY(ctx, gf16_region(ctx->gf16_kernel, din, dstride, n_in, slice, d_coeffs, ldc, n_out, dout, ostride,
-                            accumulate, ctx->sms, aexp, ctx->d_status, ctx->stream));
+                            accumulate, ctx->sms, aexp, ctx->d_status, ctx->stream, aexp_ready != nullptr));
   if (stage_out) {
     CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,
                                     out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
@@ -472,14 +553,13 @@ PP_API int pp_par2_create(pp_ctx* ctx, const void* inputs, size_t input_stride, 
   std::lock_guard<std::mutex> g(ctx->mu);
   if (int r = bind(ctx)) return r;
   if (output_stride < slice_bytes) output_stride = round16(slice_bytes);
-  uint16_t* dc = nullptr;
-  if (num_inputs) {
-    dc = (uint16_t*)scratch(ctx, S_COEF, (size_t)num_inputs * num_outputs * 2);
-    if (!dc) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficients");
-    if (int r = par2_coeff_matrix_dev(ctx, input_idx, num_inputs, exps, num_outputs, dc)) return r;
-  }
-  return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, dc, num_inputs, num_outputs, outputs,
-                          output_stride, false);
+  if (!num_inputs)
+    return gf16_muladd_impl(ctx, inputs, input_stride, 0, slice_bytes, nullptr, 0, num_outputs, outputs,
+                            output_stride, false);
+  const Par2Entry* t = nullptr;
+  if (int r = par2_table(ctx, input_idx, num_inputs, exps, num_outputs, &t)) return r;
+  return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, t->d_coef, num_inputs, num_outputs,
+                          outputs, output_stride, false, t->d_aexp);
 }
 
 PP_API int pp_par2_invert(pp_ctx* ctx, const uint8_t* valid, unsigned num_inputs, uint16_t* recovery,

@@ -212,3 +212,22 @@ def test_par2_repair_roundtrip(kctx):
     srcs = np.concatenate([data[valid], rec[[exps.index(e) for e in used]]], axis=0)
     restored = par2.gf16_muladd(srcs, m.factors, ctx=kctx)
     assert np.array_equal(restored, data[lost])
+
+
+def test_par2_create_resident_tables_across_calls(kctx, oracle):
+    """pp_par2_create keeps the coefficient table of (input numbers,
+    exponents) on the device between calls: repeated keys with new data,
+    more distinct keys than the cache holds (eviction), and the same key
+    again afterwards all give the oracle's result."""
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(77)
+    keys = []
+    for k in range(6):
+        n, r = int(rng.integers(9, 60)), int(rng.integers(1, 12))
+        keys.append((rng.choice(32768, n, replace=False).astype(np.uint16),
+                     rng.choice(65535, r, replace=False).astype(np.uint16)))
+    for ids, exps in keys + keys[:2] + keys[:1]:
+        data = rng.integers(0, 256, (ids.size, 640), dtype=np.uint8)
+        got = par2.par2_create(data, ids, exps, ctx=kctx)
+        co = oracle.par2_coeff_matrix(ids, list(exps))
+        assert np.array_equal(got, oracle.par2_muladd(list(data), 640, co))
