@@ -106,7 +106,8 @@ def roofline(w, args, hbm_achieved, hbm_peak, peak_kind, kms, int8_tops):
             peak, kind = 2 * load_bf16_peak(), "2 x MEASURED_PEAKS.json bf16_tflops (int8 dense rate = 2x bf16)"
         r.update({"bound": "tensor", "achieved": tops, "peak": peak, "unit": "TFLOP/s", "frac": tops / peak,
                   "peak_kind": kind, "ops": "int8 tensor ops (2 per MAC), one MAC per GF(2) bit product",
-                  "hbm": hbm})
+                  "nominal_peak": 4500.0, "frac_of_nominal": tops / 4500.0,
+                  "nominal_kind": "B200 dense int8 tensor rate (NVIDIA's 4.5 POP/s dense figure)", "hbm": hbm})
     else:
         r.update({"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
                   "frac": hbm_achieved / hbm_peak, "peak_kind": hbm["peak_kind"]})
@@ -273,11 +274,9 @@ def step_fn(job, ctx):
 
 
 def kernel_fn(job, ctx):
-    """The dominant kernel alone (coefficients already resident)."""
-    from parparpar_b200 import par2, par3
-    if job["field"] == "gf16":
-        return lambda: par2.gf16_muladd(job["d_in"], job["coeffs"], out=job["d_out"], ctx=ctx)
-    # the Cauchy matrix is cached on the device after the first call
+    """The dominant kernel alone: after the first call the coefficient table
+    (PAR2 tiles / PAR3 Cauchy matrix) is resident, so a step is the region
+    kernel (plus, when the job is split over CTAs, a memset of the outputs)."""
     return step_fn(job, ctx)
 
 

@@ -14,6 +14,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <functional>
 #include <list>
 #include <mutex>
 #include <string>
@@ -99,6 +101,7 @@ struct pp_ctx {
   size_t slot_n[S_NSLOTS] = {};
   std::list<CauchyEntry> cauchy;  // LRU, front = most recent
   std::list<Par2Entry> par2;      // LRU, front = most recent
+  std::deque<size_t> par2_seen;   // hashes of recent PAR2 keys without a table
   int gf16_kernel = PP_GF16_KERNEL_AUTO;
   int gf64_kernel = PP_GF16_KERNEL_AUTO;
   int* d_status = nullptr;  // set nonzero by a kernel whose bounded wait gave up
@@ -362,10 +365,10 @@ static int par2_coeff_matrix_dev(pp_ctx* ctx, const uint16_t* input_idx, unsigne
 
 static bool use_tensor(int sel, unsigned n_in, unsigned n_out);
 
-// The resident coefficient table of (input_idx, exps): built on first use
-// (coefficient matrix, plus the expanded tiles when the tensor-core kernel is
-// selected), then found by key; least recently used tables are dropped beyond
-// kPar2CacheEntries / kPar2CacheBytes.
+// The resident coefficient table of (input_idx, exps): built the second time
+// a key is used (coefficient matrix, plus the expanded tiles when the
+// tensor-core kernel is selected), then found by key; least recently used
+// tables are dropped beyond kPar2CacheEntries / kPar2CacheBytes.
 static int par2_table(pp_ctx* ctx, const uint16_t* input_idx, unsigned n_in, const uint16_t* exps, unsigned n_out,
                       const Par2Entry** out) {
   std::string key(2 * (size_t)(n_in + n_out) + 1, '\0');
@@ -383,6 +386,16 @@ static int par2_table(pp_ctx* ctx, const uint16_t* input_idx, unsigned n_in, con
       *out = &ctx->par2.front();
       return PP_OK;
     }
+  }
+  // a key seen for the first time gets no table (*out = nullptr: the caller
+  // uses the context's reusable scratch buffers); a table is built when the
+  // key comes back, so a stream of one-off jobs allocates nothing per call
+  const size_t h = std::hash<std::string>()(key);
+  if (std::find(ctx->par2_seen.begin(), ctx->par2_seen.end(), h) == ctx->par2_seen.end()) {
+    ctx->par2_seen.push_back(h);
+    if (ctx->par2_seen.size() > 64) ctx->par2_seen.pop_front();
+    *out = nullptr;
+    return PP_OK;
   }
   Par2Entry e;
   e.key = std::move(key);
@@ -558,8 +571,14 @@ PP_API int pp_par2_create(pp_ctx* ctx, const void* inputs, size_t input_stride, 
                             output_stride, false);
   const Par2Entry* t = nullptr;
   if (int r = par2_table(ctx, input_idx, num_inputs, exps, num_outputs, &t)) return r;
-  return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, t->d_coef, num_inputs, num_outputs,
-                          outputs, output_stride, false, t->d_aexp);
+  if (t)
+    return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, t->d_coef, num_inputs, num_outputs,
+                            outputs, output_stride, false, t->d_aexp);
+  uint16_t* dc = (uint16_t*)scratch(ctx, S_COEF, (size_t)num_inputs * num_outputs * 2);
+  if (!dc) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficients");
+  if (int r = par2_coeff_matrix_dev(ctx, input_idx, num_inputs, exps, num_outputs, dc)) return r;
+  return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, dc, num_inputs, num_outputs, outputs,
+                          output_stride, false);
 }
 
 PP_API int pp_par2_invert(pp_ctx* ctx, const uint8_t* valid, unsigned num_inputs, uint16_t* recovery,

@@ -83,6 +83,7 @@ k_gf64_matvec_tc(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
     DONE = D_FULL + 1,
     NBARS = DONE + 1
   };
+  static_assert(8 * NBARS + 16 <= 256, "barrier area");
   auto BAR = [&](int k) { return bar0 + 8u * (uint32_t)k; };
   volatile uint32_t* tmem_holder = reinterpret_cast<volatile uint32_t*>(smem + kOffBar + 8 * NBARS);
   volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 8 * NBARS + 8);

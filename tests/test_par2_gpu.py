@@ -226,7 +226,7 @@ def test_par2_create_resident_tables_across_calls(kctx, oracle):
         n, r = int(rng.integers(9, 60)), int(rng.integers(1, 12))
         keys.append((rng.choice(32768, n, replace=False).astype(np.uint16),
                      rng.choice(65535, r, replace=False).astype(np.uint16)))
-    for ids, exps in keys + keys[:2] + keys[:1]:
+    for ids, exps in keys + keys + keys[:2]:  # first sightings, tables (6 > 4: evictions), hits
         data = rng.integers(0, 256, (ids.size, 640), dtype=np.uint8)
         got = par2.par2_create(data, ids, exps, ctx=kctx)
         co = oracle.par2_coeff_matrix(ids, list(exps))
