@@ -644,8 +644,12 @@ struct pp_par2_proc {
   pp_ctx* ctx = nullptr;
   size_t alloc_size = 0, cur_size = 0, row = 0;
   unsigned batch = 12, n_areas = 2;
+  unsigned batch_alloc = 12;  // rows allocated per staging area
+  bool batch_fixed = false;   // the caller chose the batch size
   struct Area {
     uint8_t* d_in = nullptr;
+    uint8_t* h_in = nullptr;        // pinned host rows: host inputs are staged here
+    std::vector<uint8_t> host_row;  // row i of this batch sits in h_in (else already in d_in)
     uint16_t* d_coeff = nullptr;  // [n_out][batch]
     uint8_t* d_aexp = nullptr;    // tensor-core coefficient tiles
     std::vector<uint16_t> h_coeff;
@@ -664,16 +668,35 @@ struct pp_par2_proc {
   cudaEvent_t copied = nullptr;
 };
 
+// host slices of at least this many bytes are copied straight from the
+// caller's buffer (one DMA beats a host memcpy into the pinned rows)
+constexpr size_t kProcDirectBytes = 256 << 10;
+
 static int proc_alloc_inputs(pp_par2_proc* p) {
   for (auto& a : p->areas) {
     if (a.d_in) cudaFree(a.d_in);
+    if (a.h_in) cudaFreeHost(a.h_in);
     a.d_in = nullptr;
-    if (cudaMalloc(&a.d_in, p->row * p->batch) != cudaSuccess) {
+    a.h_in = nullptr;
+    // pinned rows only for slices small enough to be staged (larger ones are
+    // copied straight from the caller's buffer)
+    if (cudaMalloc(&a.d_in, p->row * p->batch_alloc) != cudaSuccess ||
+        (p->row < kProcDirectBytes && cudaMallocHost(&a.h_in, p->row * p->batch_alloc) != cudaSuccess)) {
       cudaGetLastError();
       return PP_ERR_NO_MEMORY;
     }
+    a.host_row.assign(p->batch_alloc, 0);
   }
   return PP_OK;
+}
+
+// Default batch: about 128 MiB of input per staging area (64-8192 slices),
+// so one tensor-core launch covers many stages; set_recovery_slices lowers it
+// so that an area's coefficient tiles stay within 256 MiB.
+static unsigned proc_batch_for(const pp_par2_proc* p, size_t n_out) {
+  size_t b = std::max<size_t>(64, std::min<size_t>(8192, (128u << 20) / p->row));
+  if (n_out) b = std::min(b, std::max<size_t>(64, ((size_t)256 << 20) / (n_out * 256)));
+  return (unsigned)std::min<size_t>(b, p->batch_alloc);
 }
 
 PP_API int pp_par2_proc_create(pp_ctx* ctx, size_t slice_size, unsigned staging_areas, unsigned input_batch,
@@ -686,13 +709,13 @@ PP_API int pp_par2_proc_create(pp_ctx* ctx, size_t slice_size, unsigned staging_
   p->alloc_size = p->cur_size = slice_size;
   p->row = round16(slice_size);
   p->n_areas = staging_areas ? staging_areas : 2;
-  // A GPU batch amortises launch latency; the default keeps a staging area
-  // at ~32 MiB of input or 64 slices, whichever is fewer (at least 12).
+  // A GPU batch amortises launch latency and the tensor-core pipeline fill
   if (input_batch) {
-    p->batch = input_batch;
+    p->batch = p->batch_alloc = input_batch;
+    p->batch_fixed = true;
   } else {
-    size_t b = (32u << 20) / p->row;
-    p->batch = (unsigned)std::max<size_t>(12, std::min<size_t>(64, b));
+    p->batch_alloc = std::max<unsigned>(64, std::min<size_t>(8192, (128u << 20) / p->row));
+    p->batch = proc_batch_for(p, 0);
   }
   p->areas.resize(p->n_areas);
   if (cudaStreamCreateWithFlags(&p->s_copy, cudaStreamNonBlocking) != cudaSuccess ||
@@ -724,6 +747,7 @@ PP_API void pp_par2_proc_destroy(pp_par2_proc* p) {
   if (p->s_copy) cudaStreamSynchronize(p->s_copy);
   for (auto& a : p->areas) {
     if (a.d_in) cudaFree(a.d_in);
+    if (a.h_in) cudaFreeHost(a.h_in);
     if (a.d_coeff) cudaFree(a.d_coeff);
     if (a.d_aexp) cudaFree(a.d_aexp);
     if (a.done) cudaEventDestroy(a.done);
@@ -753,6 +777,10 @@ PP_API int pp_par2_proc_set_current_slice_size(pp_par2_proc* p, size_t size) {
     cudaStreamSynchronize(p->s_comp);
     p->alloc_size = size;
     p->row = round16(size);
+    if (!p->batch_fixed) {  // larger rows: fewer of them (never more than the coefficient buffers hold)
+      p->batch_alloc = std::max<unsigned>(64, std::min<size_t>(8192, (128u << 20) / p->row));
+      p->batch = std::min(p->batch, proc_batch_for(p, p->exps.size()));
+    }
     if (proc_alloc_inputs(p) != PP_OK) return set_err(p->ctx, PP_ERR_NO_MEMORY, "staging realloc");
     if (p->d_out) {
       cudaFree(p->d_out);
@@ -784,6 +812,7 @@ PP_API int pp_par2_proc_set_recovery_slices(pp_par2_proc* p, unsigned num, const
   cudaStreamSynchronize(p->s_comp);
   p->exps.assign(num, 1);  // default 1 (custom-coefficient use), as gf16/controller_cpu.cpp:176
   if (exps) memcpy(p->exps.data(), exps, num * 2);
+  if (!p->batch_fixed) p->batch = proc_batch_for(p, num);
   for (auto& a : p->areas) {
     a.h_coeff.assign((size_t)num * p->batch, 0);
     if (a.d_coeff) cudaFree(a.d_coeff);
@@ -826,6 +855,18 @@ static int proc_submit(pp_par2_proc* p) {
   auto& a = p->areas[p->cur];
   if (!a.count) return PP_OK;
   const unsigned n_out = (unsigned)p->exps.size();
+  // host-staged rows: one copy per run of consecutive rows
+  for (unsigned i = 0; i < a.count;) {
+    if (!a.host_row[i]) {
+      i++;
+      continue;
+    }
+    unsigned j = i;
+    while (j < a.count && a.host_row[j]) a.host_row[j++] = 0;
+    CUDA_TRY(p->ctx, cudaMemcpyAsync(a.d_in + (size_t)i * p->row, a.h_in + (size_t)i * p->row,
+                                     (size_t)(j - i) * p->row, cudaMemcpyHostToDevice, p->s_copy));
+    i = j;
+  }
   // coefficient block [n_out][batch] (only the first `count` columns are used)
   CUDA_TRY(p->ctx, cudaMemcpyAsync(a.d_coeff, a.h_coeff.data(), (size_t)n_out * p->batch * 2,
                                    cudaMemcpyHostToDevice, p->s_copy));
@@ -855,11 +896,23 @@ static int proc_add(pp_par2_proc* p, const void* buf, size_t size, const uint16_
   const unsigned idx = a.count;
   for (unsigned o = 0; o < n_out; o++)
     a.h_coeff[(size_t)o * p->batch + idx] = coeffs ? coeffs[o] : gf16h().coeff(input_num, p->exps[o]);
-  uint8_t* dst = a.d_in + (size_t)idx * p->row;
-  if (size) CUDA_TRY(p->ctx, cudaMemcpyAsync(dst, buf, size, cudaMemcpyDefault, p->s_copy));
-  if (size < p->row) CUDA_TRY(p->ctx, cudaMemsetAsync(dst + size, 0, p->row - size, p->s_copy));
-  // the caller may reuse the buffer once the copy has consumed it
-  CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_copy));
+  if (size && (size >= kProcDirectBytes || !a.h_in || is_device_ptr(buf))) {
+    // device input, or a large host slice (one DMA beats a host memcpy into
+    // the pinned rows): copied into the area now, so that the caller may
+    // reuse the buffer on return
+    uint8_t* dst = a.d_in + (size_t)idx * p->row;
+    CUDA_TRY(p->ctx, cudaMemcpyAsync(dst, buf, size, cudaMemcpyDefault, p->s_copy));
+    if (size < p->row) CUDA_TRY(p->ctx, cudaMemsetAsync(dst + size, 0, p->row - size, p->s_copy));
+    CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_copy));
+    a.host_row[idx] = 0;
+  } else {
+    // host input: into the area's pinned rows; the whole batch goes to the
+    // device in one copy at submit
+    uint8_t* dst = a.h_in + (size_t)idx * p->row;
+    if (size) memcpy(dst, buf, size);
+    if (size < p->row) memset(dst + size, 0, p->row - size);
+    a.host_row[idx] = 1;
+  }
   a.count++;
   if (flush || a.count == p->batch) return proc_submit(p);
   return PP_OK;

@@ -167,6 +167,40 @@ def test_proc_batches_and_reuse(kctx, oracle):
     proc.deinit()
 
 
+def test_proc_mixed_host_device_inputs_reused_on_return(kctx, oracle):
+    """Host inputs are staged in pinned rows and copied per batch, device
+    inputs are copied at once; mixed in one batch, each buffer overwritten as
+    soon as addInput returns (the caller may reuse it), the outputs are the
+    oracle's."""
+    import torch
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(79)
+    n, sb, exps = 37, 3000, [0, 5, 9, 11]
+    data = rng.integers(0, 256, (n, sb), dtype=np.uint8)
+    proc = par2.PAR2ProcCUDA(sb, ctx=kctx)
+    assert proc.setRecoverySlices(len(exps), exps)
+    host_buf = np.zeros(sb, dtype=np.uint8)
+    dev_buf = torch.zeros(sb, dtype=torch.uint8, device="cuda")
+    for i in range(n):
+        proc.waitForAdd()
+        if i % 3 == 1:
+            dev_buf.copy_(torch.from_numpy(data[i]))
+            torch.cuda.synchronize()
+            proc.addInput(dev_buf, sb, i)
+            dev_buf.fill_(0xAB)
+        else:
+            host_buf[:] = data[i]
+            proc.addInput(host_buf, sb, i)
+            host_buf[:] = 0xCD
+    proc.endInput()
+    exp = oracle.par2_muladd(list(data), sb, oracle.par2_coeff_matrix(range(n), exps))
+    for o in range(len(exps)):
+        buf = np.zeros(sb, dtype=np.uint8)
+        assert proc.getOutput(o, buf)
+        assert np.array_equal(buf, exp[o]), o
+    proc.deinit()
+
+
 def test_par2_invert_golden(ctx, golden):
     from parparpar_b200 import par2
     g = golden("par2_invert.npz")
