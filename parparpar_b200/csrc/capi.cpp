@@ -105,6 +105,8 @@ struct pp_ctx {
   int gf16_kernel = PP_GF16_KERNEL_AUTO;
   int gf64_kernel = PP_GF16_KERNEL_AUTO;
   int* d_status = nullptr;  // set nonzero by a kernel whose bounded wait gave up
+  cudaStream_t copy = nullptr;     // host-to-device copies overlapped with the region kernels
+  cudaEvent_t copy_ev = nullptr, start_ev = nullptr;
   std::mutex mu;
 };
 
@@ -305,6 +307,9 @@ PP_API void pp_ctx_destroy(pp_ctx* ctx) {
   if (!ctx) return;
   pp_ctx_free_cache(ctx);
   if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->copy) cudaStreamDestroy(ctx->copy);
+  if (ctx->copy_ev) cudaEventDestroy(ctx->copy_ev);
+  if (ctx->start_ev) cudaEventDestroy(ctx->start_ev);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
 }
@@ -478,12 +483,72 @@ static cudaError_t gf16_region(int sel, const uint8_t* din, size_t dstride, unsi
 }
 
 // Region muladd with staging of host / unaligned buffers.
+// Host inputs of a large tensor-core job are copied in chunks of
+// kCopyChunk slices on the context's copy stream; the region kernel of chunk
+// c (accumulating from the second chunk on) waits only for that chunk, so the
+// copies overlap the products and the job takes about as long as its copies.
+constexpr unsigned kCopyChunk = 4096;
+constexpr size_t kGf16TileBytes = 128 * 128;  // one expanded tile (8 outputs x 8 inputs)
+
+static int ensure_copy_stream(pp_ctx* ctx) {
+  if (ctx->copy) return PP_OK;
+  if (cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->copy_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->start_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, PP_ERR_CUDA, "copy stream");
+  }
+  return PP_OK;
+}
+
 static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, unsigned n_in, size_t slice,
                             const uint16_t* d_coeffs, size_t ldc, unsigned n_out, void* outputs, size_t out_stride,
                             bool accumulate, uint8_t* aexp_ready = nullptr) {
   const bool in_dev = is_device_ptr(inputs);
   const bool out_dev = is_device_ptr(outputs);
   const size_t row = round16(slice);
+  if (!in_dev && n_in >= 2 * kCopyChunk && use_tensor(ctx->gf16_kernel, n_in, n_out)) {
+    // ---- chunked: copies of chunk c+1 overlap the products of chunk c
+    if (int r = ensure_copy_stream(ctx)) return r;
+    uint8_t* din = (uint8_t*)scratch(ctx, S_IN, row * n_in);
+    if (!din) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", row * n_in);
+    uint8_t* dout = (uint8_t*)outputs;
+    size_t ostride = out_stride;
+    const bool stage_out = !out_dev || !aligned16(outputs, out_stride);
+    if (stage_out) {
+      dout = (uint8_t*)scratch(ctx, S_OUT, row * n_out);
+      if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "output staging (%zu bytes)", row * n_out);
+      ostride = row;
+      if (accumulate)
+        CUDA_TRY(ctx, cudaMemcpy2DAsync(dout, row, outputs, out_stride, slice, n_out,
+                                        out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    }
+    uint8_t* aexp = aexp_ready;
+    if (!aexp) {
+      aexp = (uint8_t*)scratch(ctx, S_AEXP, gf16_tc_coeff_bytes(n_in, n_out));
+      if (!aexp) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficient tiles");
+      CUDA_TRY(ctx, launch_gf16_tc_expand(d_coeffs, ldc, n_in, n_out, aexp, ctx->stream));
+    }
+    const unsigned stages = (n_in + 7) / 8;
+    // the staging rows are free once earlier work on the context's stream is done
+    CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
+    for (unsigned c0 = 0; c0 < n_in; c0 += kCopyChunk) {
+      const unsigned nc = std::min(kCopyChunk, n_in - c0);
+      CUDA_TRY(ctx, cudaMemcpy2DAsync(din + (size_t)c0 * row, row, (const uint8_t*)inputs + (size_t)c0 * in_stride,
+                                      in_stride, slice, nc, cudaMemcpyHostToDevice, ctx->copy));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
+      CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev, 0));
+      CUDA_TRY(ctx, launch_gf16_muladd_tc(din + (size_t)c0 * row, row, nc, slice, aexp + (size_t)(c0 / 8) * kGf16TileBytes,
+                                          n_out, dout, ostride, accumulate || c0 > 0, ctx->sms, ctx->d_status,
+                                          ctx->stream, stages));
+    }
+    if (stage_out)
+      CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,
+                                      out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return device_status(ctx);
+  }
   const uint8_t* din = (const uint8_t*)inputs;
   size_t dstride = in_stride;
   if (n_in && (!in_dev || !aligned16(inputs, in_stride))) {

@@ -130,7 +130,7 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
   const unsigned n_in = J.n_in;
   const size_t slice_bytes = J.slice_bytes;
   const uint8_t* __restrict__ a_exp = J.a_exp;
-  const unsigned n_stages_total = J.n_stages;
+  const unsigned n_stages_total = J.a_stride;  // tile-buffer stride (the launcher defaults it to n_stages)
   const unsigned n_out = J.n_out;
   uint8_t* __restrict__ out = J.out;
   const size_t out_stride = J.out_stride;
@@ -405,6 +405,7 @@ cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStr
     Gf16TcJob& J = b.job[j];
     if (!J.n_out || !J.slice_bytes) continue;
     J.n_stages = (J.n_in + 7) / 8;
+    if (!J.a_stride) J.a_stride = J.n_stages;
     J.groups = (J.n_out + 7) / 8;
     const size_t wt = ceil_div((J.slice_bytes + 1) / 2, tc16::kWords);
     if (wt > 0xFFFFFFFFu) return cudaErrorInvalidValue;
@@ -436,7 +437,7 @@ cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStr
 
 cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigned n_in, size_t slice_bytes,
                                   const uint8_t* d_aexp, unsigned n_out, uint8_t* d_out, size_t out_stride,
-                                  bool accumulate, int sms, int* d_status, cudaStream_t s) {
+                                  bool accumulate, int sms, int* d_status, cudaStream_t s, unsigned a_stride) {
   if (!n_out || !slice_bytes) return cudaSuccess;
   Gf16TcBatch b{};
   b.n_jobs = 1;
@@ -450,6 +451,7 @@ cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigne
   J.n_in = n_in;
   J.n_out = n_out;
   J.accumulate = accumulate ? 1 : 0;
+  J.a_stride = a_stride;
   return launch_gf16_tc_batch(b, sms, d_status, s);
 }
 

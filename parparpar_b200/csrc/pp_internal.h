@@ -52,7 +52,8 @@ cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned
                                   uint8_t* d_aexp, cudaStream_t s);
 cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigned n_in, size_t slice_bytes,
                                   const uint8_t* d_aexp, unsigned n_out, uint8_t* d_out, size_t out_stride,
-                                  bool accumulate, int sms, int* d_status, cudaStream_t s);
+                                  bool accumulate, int sms, int* d_status, cudaStream_t s,
+                                  unsigned a_stride = 0);  // 0: the tiles of exactly these n_in inputs
 
 // PAR2 inversion (Gauss-Jordan without pivoting, identity columns in place).
 // d_mat: m rows x ncols (row stride ld elements).  Runs all m pivot steps;

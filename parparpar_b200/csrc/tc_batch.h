@@ -38,6 +38,10 @@ struct Gf16TcJob {
   uint32_t wt;            // word tiles: ceil(words / 512)
   uint32_t accumulate;
   uint32_t splits, per;   // stage range cut into `splits` parts of `per` stages
+  uint32_t a_stride;      // stages per output group in a_exp (0: n_stages); a job over a
+                          // column range of a larger coefficient matrix points a_exp at its
+                          // first stage and keeps the whole matrix's stride
+  uint32_t reserved;
 };
 
 struct Gf64TcJob {

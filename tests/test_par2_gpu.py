@@ -265,3 +265,23 @@ def test_par2_create_resident_tables_across_calls(kctx, oracle):
         got = par2.par2_create(data, ids, exps, ctx=kctx)
         co = oracle.par2_coeff_matrix(ids, list(exps))
         assert np.array_equal(got, oracle.par2_muladd(list(data), 640, co))
+
+
+def test_par2_create_host_inputs_in_overlapped_chunks(kctx, oracle):
+    """Host inputs of >= 8192 slices go to the device in chunks of 4096 whose
+    copies overlap the products of the previous chunk (each chunk's kernel
+    accumulates); 10,003 slices make a ragged last chunk.  Checked against the
+    oracle for create (first call: scratch tiles; second: resident table) and
+    for an accumulating region product."""
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(80)
+    n, sb, exps = 10003, 66, [0, 1, 7, 300, 65000]
+    data = rng.integers(0, 256, (n, sb), dtype=np.uint8)
+    co = oracle.par2_coeff_matrix(np.arange(n), exps)
+    want = oracle.par2_muladd(list(data), sb, co)
+    for _ in range(2):
+        assert np.array_equal(par2.par2_create(data, np.arange(n), exps, ctx=kctx), want)
+    base = rng.integers(0, 256, (len(exps), sb), dtype=np.uint8)
+    out = base.copy()
+    par2.gf16_muladd(data, co, out=out, accumulate=True, ctx=kctx)
+    assert np.array_equal(out, base ^ want)
