@@ -1133,6 +1133,34 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
   const bool in_dev = is_device_ptr(inputs);
   const bool out_dev = is_device_ptr(recovery);
   const uint64_t* din = inputs;
+  const size_t chunk = std::max<size_t>(1024, (64u << 20) / (B * 8));  // input blocks per ~64 MiB copy
+  if (!in_dev && n_in >= 2 * chunk) {
+    // ---- chunked: the copy of chunk c+1 overlaps the product of chunk c
+    // (each chunk's product accumulates into the outputs after the first)
+    if (int r = ensure_copy_stream(ctx)) return r;
+    uint64_t* s = (uint64_t*)scratch(ctx, S_IN, n_in * B * 8);
+    if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", n_in * B * 8);
+    uint64_t* dout = recovery;
+    if (!out_dev) {
+      dout = (uint64_t*)scratch(ctx, S_OUT, n_rec * B * 8);
+      if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "output staging");
+      if (accumulate)
+        CUDA_TRY(ctx, cudaMemcpyAsync(dout, recovery, n_rec * B * 8, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
+    for (size_t c0 = 0; c0 < n_in; c0 += chunk) {
+      const size_t nc = std::min(chunk, n_in - c0);
+      CUDA_TRY(ctx, cudaMemcpyAsync(s + c0 * B, inputs + c0 * B, nc * B * 8, cudaMemcpyHostToDevice, ctx->copy));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
+      CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev, 0));
+      CUDA_TRY(ctx, gf64_region(ctx, s + c0 * B, nullptr, B, nc, B, d_coeff + c0, n_in, n_rec, dout, nullptr, B,
+                                accumulate || c0 > 0, aligned_rows64(s, B) && aligned_rows64(dout, B)));
+    }
+    if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(recovery, dout, n_rec * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return device_status(ctx);
+  }
   if (!in_dev) {
     uint64_t* s = (uint64_t*)scratch(ctx, S_IN, n_in * B * 8);
     if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", n_in * B * 8);

@@ -261,3 +261,22 @@ def test_par3_repair_inverse_paths_vs_oracle(kctx, oracle, N, n, B, fI, fR):
     A = np.ascontiguousarray(M[:, lost])
     assert oracle.gf64_solve_and_reconstruct(A, rhs) == 0
     assert np.array_equal(got, rhs)
+
+
+def test_compute_recovery_host_inputs_in_overlapped_chunks(kctx, oracle):
+    """Host inputs of >= two 64 MiB chunks are copied chunk by chunk on a copy
+    stream while the previous chunk's product runs (products accumulate from
+    the second chunk on); 16,385 blocks of 8 KiB leave a one-block last chunk.
+    Sampled word ranges of every block against the oracle, plus accumulate."""
+    from parparpar_b200 import par3
+    rng = np.random.default_rng(81)
+    N, B, R, fI, fR = 16385, 1024, 3, 5, 20000
+    data = rng.integers(0, 2**64, (N, B), dtype=np.uint64)
+    out = np.zeros((R, B), dtype=np.uint64)
+    par3.GF64Controller.ComputeRecoveryBlocks(data, N, out, R, B, fI, fR)
+    for w in (0, 1000):
+        want = oracle.gf64_compute_recovery(np.ascontiguousarray(data[:, w:w + 2]), R, fI, fR)
+        assert np.array_equal(out[:, w:w + 2], want), w
+    acc = out.copy()
+    par3.GF64Controller.ComputeRecoveryBlocks(data, N, acc, R, B, fI, fR, accumulate=True)
+    assert not acc.any()  # x ^ x
