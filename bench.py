@@ -207,6 +207,8 @@ WORKLOADS = {
     "par3_create_131072x8KiB_R1024": dict(field="gf64", n=131072, s=8 * 1024, r=1024),
     # 1 % of 262,144 blocks lost, solved from the first 2,621 of R=4,096 recovery blocks
     "par3_repair_262144x4KiB_R4096_1pct": dict(field="gf64_repair", n=262144, s=4 * 1024, r=2621),
+    # forward additive FFT of the same 1 GiB: 1,024 word columns of 131,072 coefficients
+    "par3_fft_fwd_131072x8KiB": dict(field="fft", n=131072, s=8 * 1024, r=0),
 }
 PRIMARY = "par2_create_32768x32KiB_R64"
 
@@ -266,6 +268,8 @@ def step_fn(job, ctx):
     if job["field"] == "gf16":
         return lambda: par2.par2_create(job["d_in"], job["idx"], job["exps"], out=job["d_out"], ctx=ctx)
     par3.GF64Controller.ctx = ctx
+    if job["field"] == "fft":  # in place; each step transforms the previous result
+        return lambda: par3.gf64_addfft64_fwd(job["d_in"], job["n"], job["words"], job["words"], ctx=ctx)
     if job["field"] == "gf64_repair":
         return lambda: par3.repair(job["d_in"], job["lost"], job["d_rec"], job["words"], 0, job["n"],
                                    restored=job["d_out"], ctx=ctx)
@@ -286,10 +290,14 @@ def dominant_kernel(w, args):
     GF(2^64) rows of an even word count)."""
     if w["field"] == "gf16":
         return "k_gf16_muladd_lut" if args.gf16_kernel == "lut" else "k_gf16_muladd_tc"
+    if w["field"] == "fft":
+        return "k_fft_*"
     return "k_gf64_matvec_lut" if args.gf64_kernel == "lut" else "k_gf64_matvec_tc"
 
 
 def algo_bytes(job):
+    if job["field"] == "fft":  # the data read and written once
+        return 2 * job["n"] * job["s"]
     if job["field"] == "gf64_repair":  # (N - n) known blocks + n recovery blocks read, n blocks written
         return (job["n"] + job["r"]) * job["s"]
     return (job["n"] + job["r"]) * job["s"]

@@ -1432,9 +1432,7 @@ static int gf64_fft_common(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, 
     if (!d) return set_err(ctx, PP_ERR_NO_MEMORY, "fft staging");
     CUDA_TRY(ctx, cudaMemcpy2DAsync(d, dld * 8, data, ld * 8, batch * 8, n, cudaMemcpyHostToDevice, ctx->stream));
   }
-  uint64_t* tmp = (uint64_t*)scratch(ctx, S_OUT, n * dld * 8);
-  if (!tmp) return set_err(ctx, PP_ERR_NO_MEMORY, "fft scratch");
-  CUDA_TRY(ctx, launch_gf64_fft(d, tmp, n, batch, dld, inverse, ctx->stream));
+  CUDA_TRY(ctx, launch_gf64_fft(d, n, batch, dld, inverse, ctx->stream));
   if (!dev) {
     CUDA_TRY(ctx, cudaMemcpy2DAsync(data, ld * 8, d, dld * 8, batch * 8, n, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
