@@ -265,6 +265,45 @@ PP_API int pp_gf64_solve_and_reconstruct_noalloc(uint64_t* A, uint64_t* rhs, siz
 PP_API int pp_gf64_fft_fwd(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld);
 PP_API int pp_gf64_fft_inv(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, size_t ld);
 
+/* ------------------------------------------------------------ block hashes
+ * Buffers may be host or device memory; device inputs are hashed where they
+ * lie (slices already resident for a region pass are not re-read from the
+ * host).  Host outputs are written before the call returns. */
+
+/* PAR2 input-slice checksums, the 20-byte IFSC entries: for each block i,
+ * MD5 (16 bytes) then CRC32 (4 bytes, little-endian) of the block's first
+ * lengths[i] bytes followed by slice_size - lengths[i] zero bytes.  Replaces
+ * HasherInput::getBlock(md5crc, zeroPad) (hasher/hasher_input_base.h:104-117)
+ * as the PAR2 hasher binding drives it per slice (src/gf.cc:928-957 with
+ * zeroPad 0, :1034-1036 for the zero-padded last slice of a file).  Block i
+ * starts at blocks + i * block_stride; lengths NULL means every block is
+ * slice_size bytes; lengths[i] > slice_size is an error.  block_stride must
+ * cover the longest block.  The whole-file MD5 that HasherInput::end also
+ * returns is a serial hash of the file stream and stays with the caller. */
+PP_API int pp_par2_block_hashes(pp_ctx* ctx, const void* blocks, size_t block_stride, size_t num_blocks,
+                                size_t slice_size, const uint64_t* lengths, uint8_t* md5crc);
+
+/* PAR3 data-block checksums (lib/par3gen.js:1001-1017, _inlineHashBlock):
+ * hashes[16*i..] = BLAKE3(after_checksum[0..24) || u64le(first_index + i) ||
+ * block_i)[0..16), block_i = block_size bytes at blocks + i * block_stride.
+ * after_checksum is the data packet's 24 header bytes after its checksum
+ * field (total length, input-set id, type; lib/par3gen.js:1237), host memory. */
+PP_API int pp_par3_block_hashes(pp_ctx* ctx, const void* blocks, size_t block_stride, size_t num_blocks,
+                                size_t block_size, uint64_t first_index, const uint8_t* after_checksum,
+                                uint8_t* hashes);
+
+/* PAR3 recovery packets (replaces assemble_recovery_packets,
+ * src/gf64_addon.cc:2784-2936): packets receives num_recovery packets of
+ * 64 + block_size bytes -- magic "PAR3\0PKT", the 16-byte BLAKE3 checksum of
+ * packet bytes [24, 64 + block_size), u64le total length, the 8-byte
+ * input-set id (host memory), type "PAR REC\0", u64le(first_recovery_index +
+ * i), u64le(1), then recovery block i (recovery + i * block_size).
+ * num_recovery or block_size 0, or num_recovery * block_size above 1 TiB,
+ * is PP_ERR_INVALID_ARG (the reference's RangeErrors). */
+PP_API int pp_par3_assemble_recovery_packets(pp_ctx* ctx, const void* recovery, size_t num_recovery,
+                                             size_t block_size, const uint8_t* input_set_id,
+                                             uint64_t first_recovery_index, uint8_t* packets);
+
 /* ------------------------------------------------------------ batches
  * No counterpart in the reference (it runs one job at a time on its CPU
  * threads).  A batch is a plan over device-resident jobs of mixed kinds and

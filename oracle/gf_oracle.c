@@ -444,3 +444,140 @@ void or_gf64_fft_inv(uint64_t* a, size_t n) {
 	}
 	icvt(a, (int)n, 0, L);
 }
+
+/* ------------------------------------------------------------- BLAKE3 */
+/* BLAKE3 in its default hash mode, written from the published
+ * specification's recursive definition: the message is cut into 1024-byte
+ * chunks, each a chain of 64-byte block compressions keyed by the IV; a
+ * message of more than one chunk is split so that the left subtree holds the
+ * largest power-of-two number of chunks that leaves the right subtree
+ * non-empty, and each parent compresses its children's chaining values.  The
+ * reference hashes PAR3 blocks with the npm `blake3` package
+ * (lib/par3gen.js:1001-1017) and packet checksums with its port of BLAKE3
+ * v1.8.7 (hasher/hasher_blake3.c, called at src/gf64_addon.cc:2925-2932). */
+static const uint32_t B3_IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
+                                  0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
+static const uint8_t B3_PERM[16] = {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8};
+enum { B3_CHUNK_START = 1, B3_CHUNK_END = 2, B3_PARENT = 4, B3_ROOT = 8 };
+
+static uint32_t b3_rotr(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+
+static void b3_g(uint32_t* v, int a, int b, int c, int d, uint32_t x, uint32_t y) {
+	v[a] = v[a] + v[b] + x;
+	v[d] = b3_rotr(v[d] ^ v[a], 16);
+	v[c] = v[c] + v[d];
+	v[b] = b3_rotr(v[b] ^ v[c], 12);
+	v[a] = v[a] + v[b] + y;
+	v[d] = b3_rotr(v[d] ^ v[a], 8);
+	v[c] = v[c] + v[d];
+	v[b] = b3_rotr(v[b] ^ v[c], 7);
+}
+
+static void b3_compress(const uint32_t cv[8], const uint32_t block[16], uint64_t counter, uint32_t len,
+                        uint32_t flags, uint32_t out[8]) {
+	uint32_t v[16], m[16], t[16];
+	for (int i = 0; i < 8; i++) v[i] = cv[i];
+	for (int i = 0; i < 4; i++) v[8 + i] = B3_IV[i];
+	v[12] = (uint32_t)counter;
+	v[13] = (uint32_t)(counter >> 32);
+	v[14] = len;
+	v[15] = flags;
+	memcpy(m, block, sizeof m);
+	for (int r = 0; r < 7; r++) {
+		b3_g(v, 0, 4, 8, 12, m[0], m[1]);
+		b3_g(v, 1, 5, 9, 13, m[2], m[3]);
+		b3_g(v, 2, 6, 10, 14, m[4], m[5]);
+		b3_g(v, 3, 7, 11, 15, m[6], m[7]);
+		b3_g(v, 0, 5, 10, 15, m[8], m[9]);
+		b3_g(v, 1, 6, 11, 12, m[10], m[11]);
+		b3_g(v, 2, 7, 8, 13, m[12], m[13]);
+		b3_g(v, 3, 4, 9, 14, m[14], m[15]);
+		for (int i = 0; i < 16; i++) t[i] = m[B3_PERM[i]];
+		memcpy(m, t, sizeof m);
+	}
+	for (int i = 0; i < 8; i++) out[i] = v[i] ^ v[i + 8];
+}
+
+static void b3_block_words(const uint8_t* p, size_t n, uint32_t m[16]) {
+	uint8_t buf[64] = {0};
+	memcpy(buf, p, n);
+	for (int i = 0; i < 16; i++)
+		m[i] = (uint32_t)buf[4 * i] | (uint32_t)buf[4 * i + 1] << 8 | (uint32_t)buf[4 * i + 2] << 16 |
+		       (uint32_t)buf[4 * i + 3] << 24;
+}
+
+/* chaining value of chunk `counter` (n <= 1024 bytes); `extra` = ROOT for a
+ * one-chunk message */
+static void b3_chunk(const uint8_t* p, size_t n, uint64_t counter, uint32_t extra, uint32_t out[8]) {
+	uint32_t cv[8], m[16];
+	memcpy(cv, B3_IV, sizeof cv);
+	size_t nb = n ? (n + 63) / 64 : 1;
+	for (size_t b = 0; b < nb; b++) {
+		size_t len = n - 64 * b < 64 ? n - 64 * b : 64;
+		uint32_t flags = (b == 0 ? B3_CHUNK_START : 0) | (b == nb - 1 ? B3_CHUNK_END | extra : 0);
+		b3_block_words(p + 64 * b, len, m);
+		b3_compress(cv, m, counter, (uint32_t)len, flags, cv);
+	}
+	memcpy(out, cv, sizeof cv);
+}
+
+static void b3_node(const uint8_t* p, size_t n, uint64_t counter, uint32_t extra, uint32_t out[8]) {
+	if (n <= 1024) {
+		b3_chunk(p, n, counter, extra, out);
+		return;
+	}
+	size_t chunks = (n + 1023) / 1024, left = 1;
+	while (2 * left < chunks) left *= 2;
+	uint32_t m[16];
+	b3_node(p, left * 1024, counter, 0, m);
+	b3_node(p + left * 1024, n - left * 1024, counter + left, 0, m + 8);
+	b3_compress(B3_IV, m, 0, 64, B3_PARENT | extra, out);
+}
+
+void or_blake3(const uint8_t* in, size_t len, uint8_t* out, size_t out_len) {
+	uint32_t h[8];
+	b3_node(in, len, 0, B3_ROOT, h);
+	for (size_t i = 0; i < out_len && i < 32; i++) out[i] = (uint8_t)(h[i / 4] >> (8 * (i % 4)));
+}
+
+static void put_le64(uint8_t* p, uint64_t v) {
+	for (int b = 0; b < 8; b++) p[b] = (uint8_t)(v >> (8 * b));
+}
+
+/* lib/par3gen.js:1001-1017 (_inlineHashBlock): the data-packet checksum of
+ * block `first_index + i`, the packet's 24 post-checksum header bytes
+ * followed by the body (u64le block index, block data). */
+void or_par3_block_hashes(const uint8_t* blocks, size_t stride, size_t n, size_t block_size,
+                          uint64_t first_index, const uint8_t* after_checksum, uint8_t* out16) {
+	uint8_t* msg = (uint8_t*)malloc(32 + block_size);
+	memcpy(msg, after_checksum, 24);
+	for (size_t i = 0; i < n; i++) {
+		put_le64(msg + 24, first_index + i);
+		memcpy(msg + 32, blocks + i * stride, block_size);
+		or_blake3(msg, 32 + block_size, out16 + 16 * i, 16);
+	}
+	free(msg);
+}
+
+/* src/gf64_addon.cc:2884-2934 (AssembleRecoveryPackets_NAPI): per packet the
+ * magic "PAR3\0PKT", the 16-byte checksum, u64le total length, the 8-byte
+ * input-set id, the type "PAR REC\0", then the body u64le(first_index + i),
+ * u64le(1) and the block; checksum = BLAKE3(packet[24 .. 64 + block_size))[0:16]. */
+void or_par3_recovery_packets(const uint8_t* recovery, size_t n, size_t block_size,
+                              const uint8_t* input_set_id, uint64_t first_index, uint8_t* packets) {
+	static const uint8_t magic[8] = {'P', 'A', 'R', '3', 0, 'P', 'K', 'T'};
+	static const uint8_t type[8] = {'P', 'A', 'R', ' ', 'R', 'E', 'C', 0};
+	size_t pkt = 64 + block_size;
+	for (size_t i = 0; i < n; i++) {
+		uint8_t* p = packets + i * pkt;
+		memcpy(p, magic, 8);
+		memset(p + 8, 0, 16);
+		put_le64(p + 24, pkt);
+		memcpy(p + 32, input_set_id, 8);
+		memcpy(p + 40, type, 8);
+		put_le64(p + 48, first_index + i);
+		put_le64(p + 56, 1);
+		memcpy(p + 64, recovery + i * block_size, block_size);
+		or_blake3(p + 24, 40 + block_size, p + 8, 16);
+	}
+}

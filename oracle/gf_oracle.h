@@ -58,6 +58,17 @@ uint64_t or_gf64_cantor(int i);
 void or_gf64_fft_fwd(uint64_t* a, size_t n);
 void or_gf64_fft_inv(uint64_t* a, size_t n);
 
+/* ---------------- block hashes ---------------------------------------- */
+/* BLAKE3, default hash mode; out_len <= 32 */
+void or_blake3(const uint8_t* in, size_t len, uint8_t* out, size_t out_len);
+/* PAR3 data-block hashes (lib/par3gen.js:1001-1017):
+ * out[16*i..] = BLAKE3(after_checksum[24] || u64le(first_index+i) || block_i)[0:16] */
+void or_par3_block_hashes(const uint8_t* blocks, size_t stride, size_t n, size_t block_size,
+                          uint64_t first_index, const uint8_t* after_checksum, uint8_t* out16);
+/* PAR3 recovery packets (src/gf64_addon.cc:2884-2934): n packets of 64 + block_size bytes */
+void or_par3_recovery_packets(const uint8_t* recovery, size_t n, size_t block_size,
+                              const uint8_t* input_set_id, uint64_t first_index, uint8_t* packets);
+
 #ifdef __cplusplus
 }
 #endif

@@ -155,6 +155,64 @@ class Oracle:
         return out
 
 
+    # ---- block hashes -----------------------------------------------------
+    def blake3(self, data, out_len: int = 32) -> bytes:
+        a = np.frombuffer(bytes(data), dtype=np.uint8)
+        out = np.zeros(out_len, dtype=np.uint8)
+        self.L.or_blake3(_ptr(a) if a.size else None, _SZ(a.size), _ptr(out), _SZ(out_len))
+        return out.tobytes()
+
+    def par3_block_hashes(self, blocks: np.ndarray, first_index: int, after_checksum: bytes) -> np.ndarray:
+        """blocks: (n, block_size) uint8 -> (n, 16) (lib/par3gen.js:1001-1017)."""
+        blocks = np.ascontiguousarray(blocks, dtype=np.uint8)
+        n, bs = blocks.shape
+        ac = np.frombuffer(bytes(after_checksum), dtype=np.uint8).copy()
+        out = np.zeros((n, 16), dtype=np.uint8)
+        self.L.or_par3_block_hashes(_ptr(blocks), _SZ(bs), _SZ(n), _SZ(bs), _U64(first_index), _ptr(ac), _ptr(out))
+        return out
+
+    def par3_recovery_packets(self, recovery: np.ndarray, input_set_id: bytes, first_index: int) -> np.ndarray:
+        """recovery: (n, block_size) uint8 -> n * (64 + block_size) bytes
+        (src/gf64_addon.cc:2884-2934)."""
+        recovery = np.ascontiguousarray(recovery, dtype=np.uint8)
+        n, bs = recovery.shape
+        sid = np.frombuffer(bytes(input_set_id), dtype=np.uint8).copy()
+        out = np.zeros(n * (64 + bs), dtype=np.uint8)
+        self.L.or_par3_recovery_packets(_ptr(recovery), _SZ(n), _SZ(bs), _ptr(sid), _U64(first_index), _ptr(out))
+        return out
+
+
+def par2_block_hashes(blocks: np.ndarray, slice_size: int, lengths=None) -> np.ndarray:
+    """PAR2 IFSC entries, HasherInput::getBlock(md5crc, zeroPad)
+    (hasher/hasher_input_base.h:104-117): MD5 of the block's data followed by
+    zeroPad zero bytes, then CRC32 of the same bytes, little-endian.  MD5 is
+    RFC 1321 and CRC32 the reflected 0xEDB88320 CRC with ~0 init and final
+    xor, here from Python's hashlib and zlib."""
+    import hashlib
+    import zlib
+
+    blocks = np.asarray(blocks, dtype=np.uint8)
+    n = blocks.shape[0]
+    out = np.zeros((n, 20), dtype=np.uint8)
+    for i in range(n):
+        ln = slice_size if lengths is None else int(lengths[i])
+        msg = blocks[i, :ln].tobytes() + bytes(slice_size - ln)
+        out[i, :16] = np.frombuffer(hashlib.md5(msg).digest(), dtype=np.uint8)
+        out[i, 16:] = np.frombuffer((zlib.crc32(msg) & 0xFFFFFFFF).to_bytes(4, "little"), dtype=np.uint8)
+    return out
+
+
+def pattern_bytes(n: int, seed: int) -> np.ndarray:
+    """Deterministic pseudo-random bytes (a multiplicative hash of the index),
+    independent of any RNG implementation; fixtures store only outputs."""
+    with np.errstate(over="ignore"):
+        x = np.arange(n, dtype=np.uint64) + np.uint64(seed)
+        x = x * np.uint64(0x9E3779B97F4A7C15)
+        x ^= x >> np.uint64(29)
+        x = x * np.uint64(0xBF58476D1CE4E5B9)
+    return (x >> np.uint64(56)).astype(np.uint8)
+
+
 class Reference:
     """The reference's own implementation, built from its sources (oracle/_ref)."""
 
@@ -248,3 +306,20 @@ class Reference:
         a = np.ascontiguousarray(a, dtype=np.uint64).copy()
         self.L.ref_gf64_fft_inv(_ptr(a), _SZ(a.size))
         return a
+
+    # ---- block hashes -----------------------------------------------------
+    def par2_hash_file(self, data: np.ndarray, slice_size: int):
+        """One file through the reference hasher: (IFSC entries (n, 20), file MD5)."""
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        n = (data.size + slice_size - 1) // slice_size
+        ifsc = np.zeros((max(n, 1), 20), dtype=np.uint8)
+        md5 = np.zeros(16, dtype=np.uint8)
+        self.L.ref_par2_hash_file(_ptr(data) if data.size else None, _SZ(data.size), _SZ(slice_size), _ptr(ifsc),
+                                  _ptr(md5))
+        return ifsc[:n], md5.tobytes()
+
+    def blake3(self, data, out_len: int = 32) -> bytes:
+        a = np.frombuffer(bytes(data), dtype=np.uint8)
+        out = np.zeros(out_len, dtype=np.uint8)
+        self.L.ref_blake3(_ptr(a) if a.size else None, _SZ(a.size), _ptr(out), _SZ(out_len))
+        return out.tobytes()

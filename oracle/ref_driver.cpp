@@ -16,6 +16,10 @@
 //   region ops   : gf64_region_* dispatch table (gf64/gf64_global.h:23-37)
 //   FFT          : gf64_addfft64_{fwd,inv}_recursive_scratch
 //                  (gf64/gf64_additive_fft_hqc2026.c:1656,1680)
+//   block hashes : HasherInput_Scalar update / getBlock / end
+//                  (hasher/hasher_input_base.h:44-128), driven like the PAR2
+//                  hasher binding (src/gf.cc:928-1037); blake3_hash
+//                  (hasher/hasher_blake3.h:50)
 
 #include "controller.h"
 #include "controller_cpu.h"
@@ -24,7 +28,9 @@
 #include "par3_engine.h"
 extern "C" {
 #include "gf64_additive_fft.h"
+#include "hasher_blake3.h"
 }
+#include "hasher_input_impl.h"
 #include <cstdint>
 #include <cstring>
 #include <future>
@@ -208,5 +214,28 @@ void ref_gf64_poly_mul(uint64_t* out, const uint64_t* a, size_t la, const uint64
 	std::vector<gf64_t> scratch(gf64_addfft64_poly_mul_recursive_scratch_words(n) + 1);
 	gf64_addfft64_poly_mul_recursive_scratch(out, a, la, b, lb, outLen, scratch.data(), scratch.size());
 }
+
+// One PAR2 input file through the reference hasher, as the binding feeds it:
+// every full slice gets getBlock(md5crc, 0); a trailing partial slice gets
+// getBlock(md5crc, slice - tail) (zero padding); then end() gives the file MD5.
+// ifsc receives ceil(len / slice) 20-byte entries.
+void ref_par2_hash_file(const uint8_t* data, size_t len, size_t slice, uint8_t* ifsc, uint8_t* file_md5) {
+	IHasherInput* h = HasherInput_Scalar::create();
+	size_t pos = 0;
+	while (len - pos >= slice) {
+		h->update(data + pos, slice);
+		h->getBlock(ifsc, 0);
+		ifsc += 20;
+		pos += slice;
+	}
+	if (pos < len) {
+		h->update(data + pos, len - pos);
+		h->getBlock(ifsc, slice - (len - pos));
+	}
+	h->end(file_md5);
+	h->destroy();
+}
+
+void ref_blake3(const uint8_t* in, size_t len, uint8_t* out, size_t out_len) { blake3_hash(in, len, out, out_len); }
 
 }  // extern "C"

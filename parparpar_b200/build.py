@@ -28,6 +28,7 @@ SOURCES = [
     "batch.cpp",
     "server.cpp",
     "noalloc.cu",
+    "hash_kernels.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1534,4 +1534,182 @@ PP_API int pp_gf64_repair(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs
   return device_status(ctx);
 }
 
+// ------------------------------------------------------------ block hashes
+// A strided list of n rows as device rows: device rows are used in place when
+// they meet the alignment asked for; otherwise they are copied into scratch
+// slot `s` with a 16-byte rounded stride.  `width` bytes are read from each of
+// the first n - 1 rows and `last` from the last one.
+static const uint8_t* rows_on_device(pp_ctx* ctx, Slot s, const void* rows, size_t stride, size_t n, size_t width,
+                                     size_t last, bool need16, size_t* dstride, int* st) {
+  *st = PP_OK;
+  const bool dev = is_device_ptr(rows);
+  if (dev && (!need16 || aligned16(rows, n > 1 ? stride : 0))) {
+    *dstride = stride;
+    return (const uint8_t*)rows;
+  }
+  const size_t ds = round16(std::max(width, last));
+  uint8_t* d = (uint8_t*)scratch(ctx, s, ds * n);
+  if (!d) {
+    *st = set_err(ctx, PP_ERR_NO_MEMORY, "device allocation of %zu bytes failed", ds * n);
+    return nullptr;
+  }
+  const cudaMemcpyKind k = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  cudaError_t e = cudaSuccess;
+  if (n > 1 && width) e = cudaMemcpy2DAsync(d, ds, rows, stride, width, n - 1, k, ctx->stream);
+  if (e == cudaSuccess && last)
+    e = cudaMemcpyAsync(d + ds * (n - 1), (const uint8_t*)rows + stride * (n - 1), last, k, ctx->stream);
+  if (e != cudaSuccess) {
+    *st = set_err(ctx, PP_ERR_CUDA, "row staging: %s", cudaGetErrorString(e));
+    return nullptr;
+  }
+  *dstride = ds;
+  return d;
+}
+
+// Read a small argument that may live on either side.
+static int host_bytes(pp_ctx* ctx, const void* p, size_t n, void* out) {
+  if (is_device_ptr(p)) {
+    CUDA_TRY(ctx, cudaMemcpy(out, p, n, cudaMemcpyDeviceToHost));
+  } else {
+    memcpy(out, p, n);
+  }
+  return PP_OK;
+}
+
+static inline uint32_t le32(const uint8_t* p) {
+  return (uint32_t)p[0] | (uint32_t)p[1] << 8 | (uint32_t)p[2] << 16 | (uint32_t)p[3] << 24;
+}
+
+PP_API int pp_par2_block_hashes(pp_ctx* ctx, const void* blocks, size_t block_stride, size_t num_blocks,
+                                size_t slice_size, const uint64_t* lengths, uint8_t* md5crc) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_blocks == 0) return PP_OK;
+  if (!blocks || !md5crc) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const size_t n = num_blocks;
+  size_t width = slice_size, last = slice_size;
+  const uint64_t* dlen = nullptr;
+  int st = PP_OK;
+  if (lengths) {
+    std::vector<uint64_t> hl(n);
+    if (int r = host_bytes(ctx, lengths, n * 8, hl.data())) return r;
+    uint64_t mx = 0;
+    for (size_t i = 0; i < n; i++) {
+      if (hl[i] > slice_size)
+        return set_err(ctx, PP_ERR_INVALID_ARG, "block %zu: length %llu exceeds the slice size %zu", i,
+                       (unsigned long long)hl[i], slice_size);
+      mx = std::max<uint64_t>(mx, hl[i]);
+    }
+    width = (size_t)mx;
+    last = (size_t)hl[n - 1];
+    dlen = to_device(ctx, S_A, lengths, n, &st);
+    if (st) return st;
+  }
+  if (n > 1 && block_stride < width) return set_err(ctx, PP_ERR_INVALID_ARG, "block_stride is shorter than a block");
+  size_t dstride = 0;
+  const uint8_t* drows = rows_on_device(ctx, S_IN, blocks, block_stride, n, width, last, true, &dstride, &st);
+  if (!drows) return st;
+  const bool out_dev = is_device_ptr(md5crc) && ((uintptr_t)md5crc % 4) == 0;
+  uint8_t* dout = out_dev ? md5crc : (uint8_t*)scratch(ctx, S_OUT, 20 * n);
+  if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "hash output");
+  CUDA_TRY(ctx, launch_par2_block_hash(drows, dstride, n, slice_size, dlen, dout, ctx->stream));
+  if (!out_dev)
+    CUDA_TRY(ctx, cudaMemcpyAsync(md5crc, dout, 20 * n, cudaMemcpyDefault, ctx->stream));
+  if (!out_dev || drows != blocks || lengths) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+PP_API int pp_par3_block_hashes(pp_ctx* ctx, const void* blocks, size_t block_stride, size_t num_blocks,
+                                size_t block_size, uint64_t first_index, const uint8_t* after_checksum,
+                                uint8_t* hashes) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_blocks == 0) return PP_OK;
+  if (!blocks || !after_checksum || !hashes) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if (num_blocks > 1 && block_stride < block_size)
+    return set_err(ctx, PP_ERR_INVALID_ARG, "block_stride is shorter than a block");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const size_t n = num_blocks;
+  uint8_t after[24];
+  if (int r = host_bytes(ctx, after_checksum, 24, after)) return r;
+  int st = PP_OK;
+  size_t dstride = 0;
+  const uint8_t* drows =
+      rows_on_device(ctx, S_IN, blocks, block_stride, n, block_size, block_size, false, &dstride, &st);
+  if (!drows) return st;
+  const bool out_dev = is_device_ptr(hashes);
+  uint8_t* dout = out_dev ? hashes : (uint8_t*)scratch(ctx, S_OUT, 16 * n);
+  const size_t sw = blake3_scratch_words(n, 32 + (uint64_t)block_size);
+  uint32_t* dcv = sw ? (uint32_t*)scratch(ctx, S_B, sw * 4) : nullptr;
+  if (!dout || (sw && !dcv)) return set_err(ctx, PP_ERR_NO_MEMORY, "hash buffers");
+  B3Job J;
+  J.data = drows;
+  J.stride = dstride;
+  J.D = block_size;
+  J.P = 32;
+  for (int k = 0; k < 6; k++) J.pre[k] = le32(after + 4 * k);
+  J.first_index = first_index;
+  J.n = n;
+  J.hash_out = dout;
+  J.hash_stride = 16;
+  CUDA_TRY(ctx, launch_blake3_blocks(J, dcv, ctx->stream));
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(hashes, dout, 16 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!out_dev || drows != blocks) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+PP_API int pp_par3_assemble_recovery_packets(pp_ctx* ctx, const void* recovery, size_t num_recovery,
+                                             size_t block_size, const uint8_t* input_set_id,
+                                             uint64_t first_recovery_index, uint8_t* packets) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_recovery == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "numRecovery must be a positive integer");
+  if (block_size == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "blockSize must be a positive integer");
+  if (num_recovery > ((size_t)1 << 40) / block_size)
+    return set_err(ctx, PP_ERR_INVALID_ARG, "numRecovery * blockSize exceeds 1 TiB cap");
+  if (!recovery || !input_set_id || !packets) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const size_t n = num_recovery, pkt = 64 + block_size;
+  uint8_t sid[8];
+  if (int r = host_bytes(ctx, input_set_id, 8, sid)) return r;
+  int st = PP_OK;
+  size_t dstride = 0;
+  const uint8_t* drows = rows_on_device(ctx, S_IN, recovery, block_size, n, block_size, block_size, false,
+                                        &dstride, &st);
+  if (!drows) return st;
+  const bool out_dev = is_device_ptr(packets);
+  uint8_t* dpk = out_dev ? packets : (uint8_t*)scratch(ctx, S_OUT, n * pkt);
+  const size_t sw = blake3_scratch_words(n, 40 + (uint64_t)block_size);
+  uint32_t* dcv = sw ? (uint32_t*)scratch(ctx, S_B, sw * 4) : nullptr;
+  if (!dpk || (sw && !dcv)) return set_err(ctx, PP_ERR_NO_MEMORY, "packet buffers");
+  uint64_t sid64 = 0;
+  for (int b = 0; b < 8; b++) sid64 |= (uint64_t)sid[b] << (8 * b);
+  CUDA_TRY(ctx, launch_par3_packet_headers(dpk, n, block_size, sid64, first_recovery_index, ctx->stream));
+  // checksum input: header bytes [24, 48) = total length, set id, "PAR REC\0";
+  // then the body u64le(index), u64le(1), block
+  B3Job J;
+  J.data = drows;
+  J.stride = dstride;
+  J.D = block_size;
+  J.P = 40;
+  J.pre[0] = (uint32_t)pkt;
+  J.pre[1] = (uint32_t)((uint64_t)pkt >> 32);
+  J.pre[2] = le32(sid);
+  J.pre[3] = le32(sid + 4);
+  J.pre[4] = 0x20524150u;  // "PAR "
+  J.pre[5] = 0x00434552u;  // "REC\0"
+  J.first_index = first_recovery_index;
+  J.extra = 1;
+  J.n = n;
+  J.copy_to = dpk + 64;
+  J.copy_stride = pkt;
+  J.hash_out = dpk + 8;
+  J.hash_stride = pkt;
+  CUDA_TRY(ctx, launch_blake3_blocks(J, dcv, ctx->stream));
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(packets, dpk, n * pkt, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!out_dev || drows != recovery) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
 }  // extern "C"

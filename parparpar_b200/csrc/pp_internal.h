@@ -120,4 +120,38 @@ cudaError_t launch_gf64_solve(uint64_t* d_A, uint64_t* d_rhs, size_t n, size_t B
 // b at data[c*ld + b]).
 cudaError_t launch_gf64_fft(uint64_t* d_data, size_t n, size_t batch, size_t ld, bool inverse, cudaStream_t s);
 
+// ------------------------------------------------------------ block hashes
+// PAR2 input-slice checksums: out[20*i..] = MD5 || CRC32le of the first
+// min(lengths[i], slice) bytes of row i followed by zeros up to slice bytes
+// (lengths NULL: every row is slice bytes).  Rows 16-byte aligned.
+cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
+                                   const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s);
+
+// BLAKE3 over n messages "prefix || data_i": the prefix is P bytes (32 or 40)
+// made of pre[0..6) (24 bytes), u64le(first_index + i) and, when P == 40,
+// u64le(extra).  The 16-byte truncated digest of message i goes to
+// hash_out + i * hash_stride; with copy_to set, the data bytes are also
+// written to copy_to + i * copy_stride.  C is derived by the launcher.
+struct B3Job {
+  const uint8_t* data = nullptr;
+  size_t stride = 0;
+  uint64_t D = 0;
+  uint32_t P = 32;
+  uint32_t pre[6] = {};
+  uint64_t first_index = 0;
+  uint64_t extra = 0;
+  uint64_t n = 0;
+  uint64_t C = 0;
+  uint8_t* copy_to = nullptr;
+  size_t copy_stride = 0;
+  uint8_t* hash_out = nullptr;
+  size_t hash_stride = 16;
+};
+size_t blake3_scratch_words(size_t n, uint64_t message_bytes);  // chunk chaining values (2 levels)
+cudaError_t launch_blake3_blocks(const B3Job& job, uint32_t* d_scratch, cudaStream_t s);
+// headers of n PAR3 recovery packets (64 + block_size bytes each), all but
+// the checksum field
+cudaError_t launch_par3_packet_headers(uint8_t* d_pkts, size_t n, size_t block_size, uint64_t set_id_le,
+                                       uint64_t first, cudaStream_t s);
+
 }  // namespace pp

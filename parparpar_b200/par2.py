@@ -12,6 +12,9 @@ finds the same names, argument meaning and error behaviour:
 * ``gf16_muladd`` / ``par2_create`` / ``coeff_matrix`` — one-call forms.
 * ``gfmat_coeff`` / ``gfmat_input_log`` — scalar coefficient helpers
                           (reference gf16/gfmat_coeff.c:80-101).
+* ``block_hashes`` / ``HasherInput`` — input-slice MD5 + CRC32 (IFSC
+                          entries) on the device; ``HasherInput`` mirrors the
+                          reference's hasher binding (src/gf.cc:869-1060).
 
 Buffers are numpy arrays (host) or torch tensors (host or CUDA).
 """
@@ -220,3 +223,106 @@ class PAR2ProcCUDA:
 
 __all__ = ["PAR2ProcCUDA", "Galois16RecMatrix", "gf16_muladd", "par2_create", "coeff_matrix", "gfmat_coeff",
            "gfmat_input_log", "PPError"]
+
+
+# ------------------------------------------------------------ block hashes
+def block_hashes(blocks, slice_size=None, lengths=None, out=None, ctx=None):
+    """IFSC entries of input slices on the device: row i of the (n, 20) result
+    is MD5 || CRC32 (little-endian) of ``blocks[i, :lengths[i]]`` followed by
+    zeros up to ``slice_size`` bytes -- HasherInput::getBlock(md5crc, zeroPad)
+    (hasher/hasher_input_base.h:104-117).
+
+    blocks: 2-D uint8 numpy array or torch tensor (host or CUDA), one slice per
+    row; slice_size defaults to the row length; lengths (n,) or None (full
+    rows).  out: an (n, 20) uint8 buffer (host or CUDA) or None (numpy)."""
+    c = _ctx(ctx)
+    n, row_bytes, stride = _rows(blocks)
+    slice_size = row_bytes if slice_size is None else int(slice_size)
+    if out is None:
+        out = np.empty((n, 20), dtype=np.uint8)
+    lens = None
+    if lengths is not None:
+        lens = lengths if hasattr(lengths, "data_ptr") else np.ascontiguousarray(np.asarray(lengths, dtype=np.uint64))
+    c.check(lib.pp_par2_block_hashes(c.h, ptr(blocks), stride, n, slice_size, ptr(lens), ptr(out)))
+    return out
+
+
+class HasherInput:
+    """The reference's PAR2 input hasher object (src/gf.cc:869-1060:
+    ``new HasherInput(sliceSize, ifscBuf)``, ``update(buf)``, ``end(md5Buf)``,
+    ``reset()``): a file's bytes are fed in order; every completed slice gets
+    its 20-byte IFSC entry written into ``ifsc`` (in order, while room
+    remains), the zero-padded last partial slice at ``end``, which also writes
+    the whole-file MD5 into ``md5`` (16 bytes).
+
+    Slice hashes run on the device in batches of ``batch`` slices; the file
+    MD5 is one serial hash of the stream and is computed on the host as the
+    bytes go by."""
+
+    def __init__(self, slice_size: int, ifsc, batch: int = 1024, ctx=None):
+        if slice_size <= 0:
+            raise ValueError("Requires a size and buffer")
+        self.slice = int(slice_size)
+        self.ifsc = np.frombuffer(memoryview(ifsc).cast("B"), dtype=np.uint8) if not isinstance(ifsc, np.ndarray) \
+            else ifsc.reshape(-1).view(np.uint8)
+        # staging rows: at most `batch` slices and about 256 MiB
+        self.batch = max(1, min(int(batch), (256 << 20) // self.slice))
+        self.ctx = _ctx(ctx)
+        self.reset()
+
+    def reset(self):
+        import hashlib
+
+        self._md5 = hashlib.md5()
+        self._rows = np.zeros((self.batch, self.slice), dtype=np.uint8)
+        self._n = 0        # slices buffered in _rows (the last may be partial)
+        self._pos = 0      # bytes in the current (partial) slice
+        self._done = 0     # IFSC entries written
+        self._ended = False
+
+    def _flush(self, lengths=None):
+        n = self._n
+        if n == 0:
+            return
+        room = self.ifsc.size // 20 - self._done
+        n_out = min(n, max(room, 0))
+        if n_out:
+            h = block_hashes(self._rows[:n_out], self.slice, lengths[:n_out] if lengths is not None else None,
+                             ctx=self.ctx)
+            self.ifsc[20 * self._done: 20 * (self._done + n_out)] = h.reshape(-1)
+            self._done += n_out
+        self._n = 0
+
+    def update(self, data):
+        if self._ended:
+            raise RuntimeError("Process already ended")
+        buf = np.frombuffer(memoryview(data).cast("B"), dtype=np.uint8)
+        self._md5.update(buf)
+        i = 0
+        while i < buf.size:
+            take = min(self.slice - self._pos, buf.size - i)
+            self._rows[self._n, self._pos: self._pos + take] = buf[i: i + take]
+            self._pos += take
+            i += take
+            if self._pos == self.slice:
+                self._n += 1
+                self._pos = 0
+                if self._n == self.batch:
+                    self._flush()
+
+    def end(self, md5_out):
+        if self._ended:
+            raise RuntimeError("Process already ended")
+        lengths = None
+        if self._pos:
+            self._rows[self._n, self._pos:] = 0
+            lengths = np.full(self._n + 1, self.slice, dtype=np.uint64)
+            lengths[-1] = self._pos
+            self._n += 1
+        self._flush(lengths)
+        out = np.frombuffer(memoryview(md5_out).cast("B"), dtype=np.uint8) if not isinstance(md5_out, np.ndarray) \
+            else md5_out.reshape(-1).view(np.uint8)
+        if out.size < 16:
+            raise ValueError("Buffer must be at least 16 bytes long")
+        out[:16] = np.frombuffer(self._md5.digest(), dtype=np.uint8)
+        self._ended = True

@@ -10,6 +10,9 @@ Mirrors the reference's PAR3 operator surface:
   ``TypeError`` / ``ValueError``).
 * ``gf64_region_*`` / ``gf64_inverse_batch`` — the region dispatch table
   (gf64/gf64_global.h:23-37).
+* ``block_hashes`` / ``assemble_recovery_packets`` — BLAKE3 block checksums
+  (lib/par3gen.js:1001-1017) and recovery packets (src/gf64_addon.cc:2784-2936)
+  on the device.
 
 Buffers: numpy uint64 arrays (host) or torch int64/uint64 tensors (host or
 CUDA).  numThreads arguments are accepted for interface parity; the device
@@ -313,3 +316,65 @@ class Gf64Encoder:
 
     def two_d_muladd_arr(self, outs, K, in_blocks, G, coeff2d, K_stride, length):
         gf64_region_2d_muladd_arr(outs, K, in_blocks, G, coeff2d, K_stride, length, self.ctx)
+
+
+# ------------------------------------------------------------ block hashes
+def _nbytes(buf):
+    return buf.numel() * buf.element_size() if hasattr(buf, "numel") else buf.nbytes
+
+
+def block_hashes(blocks, block_size, first_index, after_checksum, num_blocks=None, block_stride=None, out=None,
+                 ctx=None):
+    """PAR3 data-block checksums (lib/par3gen.js:1001-1017, _inlineHashBlock):
+    row i of the (n, 16) result is BLAKE3(after_checksum || u64le(first_index
+    + i) || block_i)[:16].  blocks: a buffer of num_blocks blocks block_stride
+    bytes apart (default: contiguous); after_checksum: 24 bytes."""
+    c = _ctx(ctx)
+    block_size = int(block_size)
+    block_stride = block_size if block_stride is None else int(block_stride)
+    if num_blocks is None:
+        num_blocks = _nbytes(blocks) // block_stride if block_stride else 0
+    ac = np.frombuffer(bytes(after_checksum), dtype=np.uint8)
+    if ac.size != 24:
+        raise ValueError("after_checksum must be 24 bytes")
+    if out is None:
+        out = np.empty((num_blocks, 16), dtype=np.uint8)
+    c.check(lib.pp_par3_block_hashes(c.h, ptr(blocks), block_stride, num_blocks, block_size, _u64(first_index),
+                                     ptr(ac), ptr(out)))
+    return out
+
+
+def assemble_recovery_packets(recoveryBlocksBuf, inputSetIdBuf, firstRecoveryIndex, numRecovery, blockSize,
+                              out=None, ctx=None):
+    """gf64_addon assemble_recovery_packets (src/gf64_addon.cc:2784-2936):
+    numRecovery PAR3 RECOVERY packets of 64 + blockSize bytes, concatenated,
+    with their BLAKE3 checksums.  Same argument checks (TypeError / RangeError
+    become TypeError / ValueError).  Returns a numpy uint8 array unless an
+    output buffer (host or CUDA) is given."""
+    if recoveryBlocksBuf is None or not (hasattr(recoveryBlocksBuf, "data_ptr") or
+                                         hasattr(recoveryBlocksBuf, "ctypes")):
+        raise TypeError("recoveryBlocksBuf must be a Buffer")
+    sid = np.frombuffer(bytes(inputSetIdBuf), dtype=np.uint8) if isinstance(inputSetIdBuf, (bytes, bytearray)) \
+        else np.asarray(inputSetIdBuf, dtype=np.uint8).reshape(-1)
+    if sid.size != 8:
+        raise TypeError("inputSetIdBuf must be a 8-byte Buffer")
+    if isinstance(firstRecoveryIndex, bool) or not isinstance(firstRecoveryIndex, (int, np.integer)):
+        raise TypeError("firstRecoveryIndex must be a BigInt or Number")
+    numRecovery = int(numRecovery)
+    blockSize = int(blockSize)
+    if numRecovery <= 0:
+        raise ValueError("numRecovery must be a positive integer")
+    if blockSize <= 0:
+        raise ValueError("blockSize must be a positive integer")
+    if numRecovery > (1 << 40) // blockSize:
+        raise ValueError("numRecovery * blockSize exceeds 1 TiB cap")
+    if _nbytes(recoveryBlocksBuf) != numRecovery * blockSize:
+        raise ValueError("recoveryBlocksBuf length must equal numRecovery * blockSize")
+    if out is None:
+        out = np.empty(numRecovery * (64 + blockSize), dtype=np.uint8)
+    elif _nbytes(out) < numRecovery * (64 + blockSize):
+        raise ValueError("output buffer too small")
+    c = _ctx(ctx)
+    c.check(lib.pp_par3_assemble_recovery_packets(c.h, ptr(recoveryBlocksBuf), numRecovery, blockSize, ptr(sid),
+                                                  _u64(firstRecoveryIndex), ptr(out)))
+    return out

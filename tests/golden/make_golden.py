@@ -18,6 +18,13 @@ Fixtures:
                    test/gf16/test-inv.cpp:100-140 (incl. the PAR2 flaw).
   gf64_ops.npz     gf64 mul/inverse pairs, a Cauchy matrix, a matvec, a solve.
   gf64_fft.npz     additive FFT forward/inverse (recursive, Cantor basis).
+  hashes.npz       block hashes from the reference's hasher: PAR2 IFSC entries
+                   and file MD5s (HasherInput_Scalar driven like src/gf.cc:928-1037),
+                   BLAKE3 digests (hasher/hasher_blake3.c), the PAR3 data-block
+                   checksum layout of lib/par3gen.js:1001-1017 and recovery
+                   packets laid out as src/gf64_addon.cc:2884-2934, checksummed
+                   with the reference's BLAKE3.  Inputs are oracle.pattern_bytes
+                   streams, regenerated by the tests from (length, seed).
 """
 from __future__ import annotations
 
@@ -29,7 +36,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
-from oracle import Reference  # noqa: E402
+from oracle import Reference, pattern_bytes  # noqa: E402
 
 
 def par3_golden(R: Reference):
@@ -154,8 +161,62 @@ def gf64_fft(R: Reference):
     np.savez_compressed(os.path.join(HERE, "gf64_fft.npz"), **d)
 
 
+def hashes(R: Reference):
+    d = {}
+    # BLAKE3 over lengths around the 64-byte block and 1 KiB chunk boundaries
+    b3_lens = [0, 1, 63, 64, 65, 1023, 1024, 1025, 2048, 2049, 3072, 3073, 4096, 4097, 5121, 8192, 8193, 8224,
+               16384, 31744, 102400]
+    d["b3_lens"] = np.asarray(b3_lens, dtype=np.int64)
+    d["b3_digests"] = np.stack([np.frombuffer(R.blake3(pattern_bytes(n, 1000 + n)), dtype=np.uint8)
+                                for n in b3_lens])
+    # PAR2: whole files through the reference hasher (slice, file length, seed)
+    par2 = [(4, 10, 1), (64, 64 * 7, 2), (100, 1000, 3), (1024, 5000, 4), (4096, 4096 * 3 + 17, 5),
+            (32768, 32768 * 4, 6), (65536, 65536 + 1, 7), (1028, 1027, 8)]
+    d["par2_cases"] = np.asarray(par2, dtype=np.int64)
+    for k, (sl, ln, seed) in enumerate(par2):
+        ifsc, md5 = R.par2_hash_file(pattern_bytes(ln, seed), sl)
+        d[f"par2_ifsc{k}"] = ifsc
+        d[f"par2_md5_{k}"] = np.frombuffer(md5, dtype=np.uint8)
+    # PAR3 data-block checksums: (n, block_size, first_index, seed)
+    par3 = [(5, 8, 0, 11), (3, 992, 5, 12), (4, 1000, 2**40 + 3, 13), (3, 4096, 7, 14), (2, 8192, 1, 15),
+            (2, 65536, 123456789, 16)]
+    d["par3_cases"] = np.asarray(par3, dtype=np.uint64)
+    after = pattern_bytes(24, 99)
+    d["par3_after"] = after
+    for k, (n, bs, first, seed) in enumerate(par3):
+        blocks = pattern_bytes(int(n) * int(bs), int(seed)).reshape(int(n), int(bs))
+        hs = []
+        for i in range(int(n)):
+            msg = after.tobytes() + int(first + i).to_bytes(8, "little") + blocks[i].tobytes()
+            hs.append(np.frombuffer(R.blake3(msg, 16), dtype=np.uint8))
+        d[f"par3_hash{k}"] = np.stack(hs)
+    # PAR3 recovery packets: (n, block_size, first_index, seed)
+    pk = [(3, 1000, 5, 21), (2, 4096, 2**33, 22), (1, 8, 0, 23)]
+    d["pkt_cases"] = np.asarray(pk, dtype=np.uint64)
+    sid = pattern_bytes(8, 77)
+    d["pkt_set_id"] = sid
+    for k, (n, bs, first, seed) in enumerate(pk):
+        n, bs = int(n), int(bs)
+        rec = pattern_bytes(n * bs, int(seed)).reshape(n, bs)
+        out = bytearray()
+        for i in range(n):
+            p = bytearray(64 + bs)
+            p[0:8] = b"PAR3\x00PKT"
+            p[24:32] = (64 + bs).to_bytes(8, "little")
+            p[32:40] = sid.tobytes()
+            p[40:48] = b"PAR REC\x00"
+            p[48:56] = int(first + i).to_bytes(8, "little")
+            p[56:64] = (1).to_bytes(8, "little")
+            p[64:] = rec[i].tobytes()
+            p[8:24] = R.blake3(bytes(p[24:]), 16)
+            out += p
+        d[f"pkt{k}"] = np.frombuffer(bytes(out), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "hashes.npz"), **d)
+
+
 def main():
     R = Reference()
+    hashes(R)
     par3_golden(R)
     par2_create(R)
     par2_invert(R)

@@ -80,3 +80,24 @@ def test_null_context_is_rejected():
     import parparpar_b200._lib as L
     assert L.lib.pp_gf64_compute_recovery(None, None, 1, None, 1, 1, 0, 1, 0, 0) == L.PP_ERR_INVALID_ARG
     assert L.lib.pp_par2_create(None, None, 0, 0, 0, None, None, 0, None, 0) == L.PP_ERR_INVALID_ARG
+
+
+def test_assemble_recovery_packets_argument_errors():
+    """The N-API argument checks of assemble_recovery_packets
+    (src/gf64_addon.cc:2813-2884) run before any device work."""
+    from parparpar_b200 import par3
+    rec = np.zeros(64, dtype=np.uint8)
+    with pytest.raises(TypeError):
+        par3.assemble_recovery_packets(None, b"12345678", 0, 1, 64)
+    with pytest.raises(TypeError):
+        par3.assemble_recovery_packets(rec, b"1234567", 0, 1, 64)
+    with pytest.raises(TypeError):
+        par3.assemble_recovery_packets(rec, b"12345678", 1.5, 1, 64)
+    with pytest.raises(ValueError):
+        par3.assemble_recovery_packets(rec, b"12345678", 0, 0, 64)
+    with pytest.raises(ValueError):
+        par3.assemble_recovery_packets(rec, b"12345678", 0, 1, 0)
+    with pytest.raises(ValueError):
+        par3.assemble_recovery_packets(rec, b"12345678", 0, 2, 64)
+    with pytest.raises(ValueError):
+        par3.assemble_recovery_packets(rec, b"12345678", 0, 1 << 21, 1 << 20)

@@ -1,0 +1,200 @@
+"""Device block hashes against the oracle (and, through the oracle's pins,
+the reference's hasher):
+
+* PAR2 IFSC entries -- MD5 + CRC32 of zero-padded slices
+  (HasherInput::getBlock, hasher/hasher_input_base.h:104-117);
+* PAR3 data-block BLAKE3 checksums (lib/par3gen.js:1001-1017);
+* PAR3 recovery packets (src/gf64_addon.cc:2784-2936).
+
+Bit-exact comparisons throughout: every byte of every digest.
+"""
+import numpy as np
+import pytest
+
+from oracle import par2_block_hashes as par2_oracle
+from oracle import pattern_bytes
+
+gpu = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+# ------------------------------------------------------------------- PAR2
+@gpu
+@pytest.mark.parametrize("slice_size", [4, 8, 60, 64, 100, 1000, 1028, 4096, 32768, 65540])
+def test_par2_block_hashes_full_rows(ctx, rng, slice_size):
+    from parparpar_b200 import par2
+    n = 37
+    blocks = rng.integers(0, 256, (n, slice_size), dtype=np.uint8)
+    got = par2.block_hashes(blocks, ctx=ctx)
+    assert (got == par2_oracle(blocks, slice_size)).all()
+
+
+@gpu
+def test_par2_block_hashes_ragged_lengths_and_zero_pad(ctx, rng):
+    from parparpar_b200 import par2
+    sl = 4096
+    lens = np.array([0, 1, 3, 4, 63, 64, 65, 127, 128, 1000, 4095, 4096, 2048, 17], dtype=np.uint64)
+    blocks = rng.integers(0, 256, (lens.size, sl), dtype=np.uint8)  # bytes past each length are NOT zero
+    got = par2.block_hashes(blocks, sl, lengths=lens, ctx=ctx)
+    assert (got == par2_oracle(blocks, sl, lens)).all()
+
+
+@gpu
+def test_par2_block_hashes_device_rows_in_place_and_misaligned(ctx, rng):
+    torch = _torch()
+    from parparpar_b200 import par2
+    sl, n = 3000, 65
+    host = rng.integers(0, 256, (n, sl + 40), dtype=np.uint8)
+    dev = torch.from_numpy(host).cuda()
+    want = par2_oracle(host[:, :sl], sl)
+    # 16-aligned rows used in place, outputs on the device
+    d_al = torch.zeros((n, 3008), dtype=torch.uint8, device="cuda")
+    d_al[:, :sl] = dev[:, :sl]
+    out = torch.zeros((n, 20), dtype=torch.uint8, device="cuda")
+    par2.block_hashes(d_al[:, :sl], sl, out=out, ctx=ctx)
+    assert (out.cpu().numpy() == want).all()
+    # a misaligned view (offset 3 bytes, stride 3040) is staged
+    view = dev[:, 3:3 + sl]
+    want2 = par2_oracle(host[:, 3:3 + sl], sl)
+    assert (par2.block_hashes(view, sl, ctx=ctx) == want2).all()
+
+
+@gpu
+def test_par2_block_hashes_length_above_slice_is_an_error(ctx):
+    from parparpar_b200 import PPError, par2
+    blocks = np.zeros((2, 64), dtype=np.uint8)
+    with pytest.raises(PPError):
+        par2.block_hashes(blocks, 64, lengths=[64, 65], ctx=ctx)
+
+
+@gpu
+def test_hasher_input_matches_reference_stream(ctx, golden):
+    """HasherInput fed in odd pieces reproduces the reference hasher's IFSC
+    entries and file MD5 (fixture from the reference build)."""
+    from parparpar_b200 import par2
+    g = golden("hashes.npz")
+    for k, (sl, ln, seed) in enumerate(g["par2_cases"]):
+        sl, ln = int(sl), int(ln)
+        data = pattern_bytes(ln, int(seed)).tobytes()
+        n = (ln + sl - 1) // sl
+        ifsc = bytearray(20 * n)
+        h = par2.HasherInput(sl, ifsc, batch=3, ctx=ctx)
+        pos, step = 0, 1
+        while pos < ln:
+            h.update(data[pos:pos + step])
+            pos += step
+            step = step * 3 + 1
+        md5 = bytearray(16)
+        h.end(md5)
+        assert bytes(ifsc) == g[f"par2_ifsc{k}"].tobytes(), (sl, ln)
+        assert bytes(md5) == g[f"par2_md5_{k}"].tobytes()
+
+
+# ------------------------------------------------------------------- PAR3
+@gpu
+@pytest.mark.parametrize("block_size", [8, 24, 992, 1000, 1024, 2016, 2048, 4096, 8192, 24 * 1024 + 8])
+def test_par3_block_hashes(ctx, oracle, rng, block_size):
+    from parparpar_b200 import par3
+    n = 23
+    blocks = rng.integers(0, 256, (n, block_size), dtype=np.uint8)
+    after = rng.integers(0, 256, 24, dtype=np.uint8).tobytes()
+    first = (1 << 40) + 12345
+    got = par3.block_hashes(blocks, block_size, first, after, num_blocks=n, ctx=ctx)
+    assert (got == oracle.par3_block_hashes(blocks, first, after)).all()
+
+
+@gpu
+def test_par3_block_hashes_golden(ctx, golden):
+    from parparpar_b200 import par3
+    g = golden("hashes.npz")
+    after = g["par3_after"].tobytes()
+    for k, (n, bs, first, seed) in enumerate(g["par3_cases"]):
+        blocks = pattern_bytes(int(n) * int(bs), int(seed))
+        got = par3.block_hashes(blocks, int(bs), int(first), after, ctx=ctx)
+        assert (got == g[f"par3_hash{k}"]).all(), (n, bs)
+
+
+@gpu
+def test_par3_block_hashes_unaligned_layouts_on_device(ctx, oracle, rng):
+    torch = _torch()
+    from parparpar_b200 import par3
+    # odd block size and stride (byte-granular path); device rows and outputs
+    bs, stride, n = 1001, 1013, 19
+    host = rng.integers(0, 256, n * stride + 16, dtype=np.uint8)
+    dev = torch.from_numpy(host).cuda()
+    rows = np.stack([host[5 + i * stride: 5 + i * stride + bs] for i in range(n)])
+    after = rng.integers(0, 256, 24, dtype=np.uint8).tobytes()
+    out = torch.zeros((n, 16), dtype=torch.uint8, device="cuda")
+    par3.block_hashes(dev[5:], bs, 9, after, num_blocks=n, block_stride=stride, out=out, ctx=ctx)
+    assert (out.cpu().numpy() == oracle.par3_block_hashes(rows, 9, after)).all()
+
+
+@gpu
+@pytest.mark.parametrize("block_size", [8, 984, 1000, 4096, 8192, 65536 + 8])
+def test_par3_recovery_packets(ctx, oracle, rng, block_size):
+    from parparpar_b200 import par3
+    n = 7
+    rec = rng.integers(0, 256, (n, block_size), dtype=np.uint8)
+    sid = rng.integers(0, 256, 8, dtype=np.uint8).tobytes()
+    first = 2**35 + 3
+    got = par3.assemble_recovery_packets(rec.reshape(-1), sid, first, n, block_size, ctx=ctx)
+    assert (got == oracle.par3_recovery_packets(rec, sid, first)).all()
+
+
+@gpu
+def test_par3_recovery_packets_golden_device_buffers(ctx, golden):
+    torch = _torch()
+    from parparpar_b200 import par3
+    g = golden("hashes.npz")
+    sid = g["pkt_set_id"].tobytes()
+    for k, (n, bs, first, seed) in enumerate(g["pkt_cases"]):
+        n, bs = int(n), int(bs)
+        rec = torch.from_numpy(pattern_bytes(n * bs, int(seed))).cuda()
+        out = torch.zeros(n * (64 + bs), dtype=torch.uint8, device="cuda")
+        par3.assemble_recovery_packets(rec, sid, int(first), n, bs, out=out, ctx=ctx)
+        assert (out.cpu().numpy() == g[f"pkt{k}"]).all(), (n, bs)
+
+
+# ------------------------------------------------------------- full size
+@gpu
+def test_par2_block_hashes_full_size_sampled(ctx):
+    """1 GiB of slices (32768 x 32 KiB) resident on the device; every digest
+    of a sample of rows against the oracle, and the digests of all rows
+    distinct (a checksum-of-checksums property at full size)."""
+    torch = _torch()
+    from parparpar_b200 import par2
+    n, sl = 32768, 32768
+    g = torch.Generator(device="cuda").manual_seed(5)
+    d = torch.randint(0, 256, (n, sl), dtype=torch.uint8, device="cuda", generator=g)
+    out = torch.zeros((n, 20), dtype=torch.uint8, device="cuda")
+    par2.block_hashes(d, sl, out=out, ctx=ctx)
+    got = out.cpu().numpy()
+    idx = np.linspace(0, n - 1, 256).astype(np.int64)
+    rows = d[torch.from_numpy(idx).cuda()].cpu().numpy()
+    assert (got[idx] == par2_oracle(rows, sl)).all()
+    assert len({r.tobytes() for r in got}) == n
+    del d
+
+
+@gpu
+def test_par3_block_hashes_full_size_sampled(ctx, oracle):
+    """131072 x 8 KiB blocks resident on the device (1 GiB)."""
+    torch = _torch()
+    from parparpar_b200 import par3
+    n, bs = 131072, 8192
+    g = torch.Generator(device="cuda").manual_seed(6)
+    d = torch.randint(0, 256, (n, bs), dtype=torch.uint8, device="cuda", generator=g)
+    after = bytes(range(24))
+    out = torch.zeros((n, 16), dtype=torch.uint8, device="cuda")
+    par3.block_hashes(d, bs, 1000, after, num_blocks=n, out=out, ctx=ctx)
+    got = out.cpu().numpy()
+    idx = np.linspace(0, n - 1, 512).astype(np.int64)
+    rows = d[torch.from_numpy(idx).cuda()].cpu().numpy()
+    want = np.stack([oracle.par3_block_hashes(rows[j:j + 1], 1000 + int(i), after)[0] for j, i in enumerate(idx)])
+    assert (got[idx] == want).all()
+    assert len({r.tobytes() for r in got}) == n
+    del d

@@ -141,3 +141,72 @@ def test_oracle_vs_reference_fft(oracle, reference):
         x = rng.integers(0, 2**64, n, dtype=np.uint64)
         assert np.array_equal(oracle.gf64_fft(x), reference.gf64_fft_fwd(x)), n
         assert np.array_equal(oracle.gf64_fft(x, True), reference.gf64_fft_inv(x)), n
+
+
+# ---------------------------------------------------------------- block hashes
+def test_blake3_published_empty_digest(oracle):
+    # the BLAKE3 specification's digest of the empty input
+    assert oracle.blake3(b"").hex() == "af1349b9f5f9a1a6a0404dea36dcc9499bcb25c9adc112b7cc9a93cae41f3262"
+
+
+def test_blake3_golden(oracle, golden):
+    from oracle import pattern_bytes
+    g = golden("hashes.npz")
+    for n, dig in zip(g["b3_lens"], g["b3_digests"]):
+        assert oracle.blake3(pattern_bytes(int(n), 1000 + int(n))) == dig.tobytes(), int(n)
+
+
+def test_par2_block_hash_golden(golden):
+    import hashlib
+
+    from oracle import par2_block_hashes, pattern_bytes
+    g = golden("hashes.npz")
+    for k, (sl, ln, seed) in enumerate(g["par2_cases"]):
+        sl, ln = int(sl), int(ln)
+        data = pattern_bytes(ln, int(seed))
+        n = (ln + sl - 1) // sl
+        rows = np.zeros((n, sl), dtype=np.uint8)
+        lens = []
+        for i in range(n):
+            c = data[i * sl:(i + 1) * sl]
+            rows[i, :c.size] = c
+            lens.append(c.size)
+        assert (par2_block_hashes(rows, sl, lens) == g[f"par2_ifsc{k}"]).all(), (sl, ln)
+        assert hashlib.md5(data.tobytes()).digest() == g[f"par2_md5_{k}"].tobytes()
+
+
+def test_par3_block_hash_golden(oracle, golden):
+    from oracle import pattern_bytes
+    g = golden("hashes.npz")
+    after = g["par3_after"].tobytes()
+    for k, (n, bs, first, seed) in enumerate(g["par3_cases"]):
+        blocks = pattern_bytes(int(n) * int(bs), int(seed)).reshape(int(n), int(bs))
+        assert (oracle.par3_block_hashes(blocks, int(first), after) == g[f"par3_hash{k}"]).all(), (n, bs)
+
+
+def test_par3_recovery_packets_golden(oracle, golden):
+    from oracle import pattern_bytes
+    g = golden("hashes.npz")
+    sid = g["pkt_set_id"].tobytes()
+    for k, (n, bs, first, seed) in enumerate(g["pkt_cases"]):
+        rec = pattern_bytes(int(n) * int(bs), int(seed)).reshape(int(n), int(bs))
+        assert (oracle.par3_recovery_packets(rec, sid, int(first)) == g[f"pkt{k}"]).all(), (n, bs)
+
+
+def test_hash_oracle_vs_reference(oracle, reference, rng):
+    from oracle import par2_block_hashes
+    for n in list(rng.integers(0, 9000, 40)) + [1024 * 33 + 7]:
+        d = rng.integers(0, 256, int(n), dtype=np.uint8)
+        assert oracle.blake3(d.tobytes()) == reference.blake3(d.tobytes())
+    for sl in (4, 12, 64, 1000, 4096):
+        ln = int(rng.integers(0, 5 * sl))
+        d = rng.integers(0, 256, ln, dtype=np.uint8)
+        ifsc, _ = reference.par2_hash_file(d, sl)
+        n = ifsc.shape[0]
+        rows = np.zeros((n, sl), dtype=np.uint8)
+        lens = []
+        for i in range(n):
+            c = d[i * sl:(i + 1) * sl]
+            rows[i, :c.size] = c
+            lens.append(c.size)
+        assert (par2_block_hashes(rows, sl, lens) == ifsc).all()
