@@ -209,7 +209,14 @@ WORKLOADS = {
     "par3_repair_262144x4KiB_R4096_1pct": dict(field="gf64_repair", n=262144, s=4 * 1024, r=2621),
     # forward additive FFT of the same 1 GiB: 1,024 word columns of 131,072 coefficients
     "par3_fft_fwd_131072x8KiB": dict(field="fft", n=131072, s=8 * 1024, r=0),
+    # block hashes over 1 GiB of resident slices / blocks
+    "par2_hash_32768x32KiB": dict(field="hash2", n=32768, s=32 * 1024, r=0),
+    "par3_hash_131072x8KiB": dict(field="hash3", n=131072, s=8 * 1024, r=0),
+    "par3_packets_131072x8KiB": dict(field="pkt3", n=131072, s=8 * 1024, r=0),
 }
+HASH_FIELDS = ("hash2", "hash3", "pkt3")
+PAR3_AFTER = bytes(range(24))      # a data packet's post-checksum header bytes (synthetic)
+PAR3_SET_ID = b"\x5a" * 8           # input-set id (synthetic)
 PRIMARY = "par2_create_32768x32KiB_R64"
 
 
@@ -241,7 +248,12 @@ def setup_job(name, dev, seed, ctx):
     g = torch.Generator(device=f"cuda:{dev}")
     g.manual_seed(seed)
     job = dict(w)
-    if w["field"] == "gf16":
+    if w["field"] in HASH_FIELDS:
+        d_in = torch.randint(0, 256, (w["n"], w["s"]), dtype=torch.uint8, device=f"cuda:{dev}", generator=g)
+        out_bytes = {"hash2": 20, "hash3": 16, "pkt3": 64 + w["s"]}[w["field"]]
+        d_out = torch.zeros((w["n"], out_bytes), dtype=torch.uint8, device=f"cuda:{dev}")
+        job.update(d_in=d_in, d_out=d_out)
+    elif w["field"] == "gf16":
         d_in = torch.randint(0, 256, (w["n"], w["s"]), dtype=torch.uint8, device=f"cuda:{dev}", generator=g)
         d_out = torch.zeros((w["r"], w["s"]), dtype=torch.uint8, device=f"cuda:{dev}")
         idx = np.arange(w["n"], dtype=np.uint16)
@@ -267,6 +279,8 @@ def step_fn(job, ctx):
     from parparpar_b200 import par2, par3
     if job["field"] == "gf16":
         return lambda: par2.par2_create(job["d_in"], job["idx"], job["exps"], out=job["d_out"], ctx=ctx)
+    if job["field"] in HASH_FIELDS:
+        return hash_fn(job, job["d_in"], job["d_out"], ctx)
     par3.GF64Controller.ctx = ctx
     if job["field"] == "fft":  # in place; each step transforms the previous result
         return lambda: par3.gf64_addfft64_fwd(job["d_in"], job["n"], job["words"], job["words"], ctx=ctx)
@@ -275,6 +289,23 @@ def step_fn(job, ctx):
                                    restored=job["d_out"], ctx=ctx)
     return lambda: par3.GF64Controller.ComputeRecoveryBlocks(job["d_in"], job["n"], job["d_out"], job["r"],
                                                              job["words"], 0, job["n"])
+
+
+def dtype_of(w):
+    """Arithmetic type of the path: GF(2^16) symbols, GF(2^64) words, or the
+    32-bit words of MD5 / CRC32 / BLAKE3."""
+    return {"gf16": "u16"}.get(w["field"], "u32" if w["field"] in HASH_FIELDS else "u64")
+
+
+def hash_fn(job, src, dst, ctx):
+    from parparpar_b200 import par2, par3
+    n, s = job["n"], job["s"]
+    if job["field"] == "hash2":
+        return lambda: par2.block_hashes(src, s, out=dst, ctx=ctx)
+    if job["field"] == "hash3":
+        return lambda: par3.block_hashes(src, s, 0, PAR3_AFTER, num_blocks=n, out=dst, ctx=ctx)
+    return lambda: par3.assemble_recovery_packets(src.reshape(-1), PAR3_SET_ID, n, n, s, out=dst.reshape(-1),
+                                                  ctx=ctx)
 
 
 def kernel_fn(job, ctx):
@@ -292,12 +323,22 @@ def dominant_kernel(w, args):
         return "k_gf16_muladd_lut" if args.gf16_kernel == "lut" else "k_gf16_muladd_tc"
     if w["field"] == "fft":
         return "k_fft_*"
+    if w["field"] == "hash2":
+        return "k_par2_block_hash"
+    if w["field"] in ("hash3", "pkt3"):
+        return "k_b3_chunks"
     return "k_gf64_matvec_lut" if args.gf64_kernel == "lut" else "k_gf64_matvec_tc"
 
 
 def algo_bytes(job):
     if job["field"] == "fft":  # the data read and written once
         return 2 * job["n"] * job["s"]
+    if job["field"] == "hash2":  # slices read, 20-byte entries written
+        return job["n"] * (job["s"] + 20)
+    if job["field"] == "hash3":
+        return job["n"] * (job["s"] + 16)
+    if job["field"] == "pkt3":  # blocks read, packets written
+        return job["n"] * (2 * job["s"] + 64)
     if job["field"] == "gf64_repair":  # (N - n) known blocks + n recovery blocks read, n blocks written
         return (job["n"] + job["r"]) * job["s"]
     return (job["n"] + job["r"]) * job["s"]
@@ -332,7 +373,33 @@ def cpu_baseline_sample(name, budget_s=12.0, threads=0):
     w = WORKLOADS[name]
     rng = np.random.default_rng(99)
     cores = os.cpu_count() or 1
-    if orc.Reference.available():
+    if w["field"] in HASH_FIELDS:
+        # one thread: the reference hashes each file / packet batch on one thread
+        sub_n = {"hash2": 256, "hash3": 1024, "pkt3": 1024}[w["field"]]
+        inp = rng.integers(0, 256, (sub_n, w["s"]), dtype=np.uint8)
+        nbytes = inp.nbytes
+        if orc.Reference.available():
+            R, kind = orc.Reference(), "reference"
+        else:
+            orc.build()
+            R, kind = orc.Oracle(), "port"
+        if w["field"] == "hash2":
+            if kind == "reference":
+                run = lambda: R.par2_hash_file(inp.reshape(-1), w["s"])
+                what = "HasherInput_Scalar (block MD5+CRC32 and the file MD5 lane)"
+            else:
+                run = lambda: orc.par2_block_hashes(inp, w["s"])
+                what = "hashlib MD5 + zlib CRC32"
+        elif w["field"] == "hash3":
+            run = lambda: R.par3_block_hashes(inp, 0, bytes(range(24)))
+            what = "BLAKE3 per block (hasher/hasher_blake3.c)" if kind == "reference" else "oracle BLAKE3"
+        else:
+            run = lambda: R.par3_recovery_packets(inp, b"\x5a" * 8, 0)
+            what = ("assemble_recovery_packets loop around the reference BLAKE3" if kind == "reference"
+                    else "oracle packet assembly")
+        sample = f"{sub_n} x {w['s']} B of the workload's {w['n']} blocks; {what}; 1 thread"
+        cores = 1
+    elif orc.Reference.available():
         R = orc.Reference()
         kind = "reference"
         if w["field"] == "gf16":
@@ -598,7 +665,7 @@ def run_reference(args, rank):
     line = {
         "impl": "reference", "metric": f"{name} input GB/s", "value": val, "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": spr * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u16" if w["field"] == "gf16" else "u64",
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(w),
         "data": "synthetic (seeded uniform random bytes)",
         "config": {"workload": name, "num_inputs": w["n"], "slice_bytes": w["s"], "num_recovery": w["r"]},
         "cpu_baseline": {"value": val, "unit": "GB/s", "cores": times[0]["cores"], "kind": times[0]["kind"],
@@ -690,7 +757,12 @@ def main():
     # end to end through the public API with pinned host buffers
     w = WORKLOADS[args.workload]
     from parparpar_b200 import par2, par3
-    if w["field"] == "gf16":
+    if w["field"] in HASH_FIELDS:
+        h_in = torch.empty((w["n"], w["s"]), dtype=torch.uint8).pin_memory()
+        h_in.copy_(job["d_in"])
+        h_out = torch.empty(tuple(job["d_out"].shape), dtype=torch.uint8).pin_memory()
+        e2e_f = hash_fn(job, h_in, h_out, ctx)
+    elif w["field"] == "gf16":
         h_in = torch.empty((w["n"], w["s"]), dtype=torch.uint8).pin_memory()
         h_in.copy_(job["d_in"])
         h_out = torch.empty((w["r"], w["s"]), dtype=torch.uint8).pin_memory()
@@ -718,17 +790,18 @@ def main():
 
     input_bytes = w["n"] * w["s"]
     h2d = input_bytes + (w["r"] * w["s"] if w["field"] == "gf64_repair" else 0)
+    d2h = job["d_out"].numel() * job["d_out"].element_size()
     line = {
         "metric": f"{args.workload} input GB/s", "value": input_bytes * world / (ms * 1e-3) / 1e9, "unit": "GB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u16" if w["field"] == "gf16" else "u64",
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(w),
         "data": "synthetic (seeded uniform random bytes, generated on the device)",
         "config": {"workload": args.workload, "num_inputs": w["n"], "slice_bytes": w["s"], "num_recovery": w["r"],
                    "exponents": f"0..{w['r'] - 1}", "parallelism": f"replicas x{world} (one job per GPU)",
                    "l2": "inputs (1 GiB) larger than L2; no flush needed"},
         "roofline": roofline(w, args, achieved, peak, peak_kind, kms, int8_tops),
         "e2e": {"value": input_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": w["r"] * w["s"], "host_buffers": "pinned", "matches_device_result": bool(ok)},
+                "d2h_bytes_per_step": d2h, "host_buffers": "pinned", "matches_device_result": bool(ok)},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }

@@ -323,3 +323,20 @@ class Reference:
         out = np.zeros(out_len, dtype=np.uint8)
         self.L.ref_blake3(_ptr(a) if a.size else None, _SZ(a.size), _ptr(out), _SZ(out_len))
         return out.tobytes()
+
+    def par3_block_hashes(self, blocks: np.ndarray, first_index: int, after_checksum: bytes) -> np.ndarray:
+        blocks = np.ascontiguousarray(blocks, dtype=np.uint8)
+        n, bs = blocks.shape
+        ac = np.frombuffer(bytes(after_checksum), dtype=np.uint8).copy()
+        out = np.zeros((n, 16), dtype=np.uint8)
+        self.L.ref_par3_block_hashes(_ptr(blocks), _SZ(n), _SZ(bs), _U64(first_index), _ptr(ac), _ptr(out))
+        return out
+
+    def par3_recovery_packets(self, recovery: np.ndarray, input_set_id: bytes, first_index: int) -> np.ndarray:
+        recovery = np.ascontiguousarray(recovery, dtype=np.uint8)
+        n, bs = recovery.shape
+        sid = np.frombuffer(bytes(input_set_id), dtype=np.uint8).copy()
+        out = np.zeros(n * (64 + bs), dtype=np.uint8)
+        self.L.ref_par3_assemble_recovery_packets(_ptr(recovery), _SZ(n), _SZ(bs), _ptr(sid), _U64(first_index),
+                                                  _ptr(out))
+        return out

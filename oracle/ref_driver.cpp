@@ -238,4 +238,50 @@ void ref_par2_hash_file(const uint8_t* data, size_t len, size_t slice, uint8_t* 
 
 void ref_blake3(const uint8_t* in, size_t len, uint8_t* out, size_t out_len) { blake3_hash(in, len, out, out_len); }
 
+// PAR3 data-block checksums as lib/par3gen.js:1001-1017 computes them
+// (createHash().update(afterChecksum).update(u64le index).update(block)),
+// here with the reference's own BLAKE3.
+void ref_par3_block_hashes(const uint8_t* blocks, size_t n, size_t bs, uint64_t first, const uint8_t* after,
+                           uint8_t* out16) {
+	for (size_t i = 0; i < n; i++) {
+		uint8_t idx[8];
+		for (int b = 0; b < 8; b++) idx[b] = (uint8_t)((first + i) >> (8 * b));
+		blake3_hasher h;
+		blake3_hasher_init(&h);
+		blake3_hasher_update(&h, after, 24);
+		blake3_hasher_update(&h, idx, 8);
+		blake3_hasher_update(&h, blocks + i * bs, bs);
+		blake3_hasher_finalize(&h, out16 + 16 * i, 16);
+	}
+}
+
+// The body of AssembleRecoveryPackets_NAPI (src/gf64_addon.cc:2884-2934; the
+// N-API wrapper needs node headers, so its loop is driven directly): header
+// fields, block copy, BLAKE3 of packet[24 .. 64 + bs) with the reference's
+// hasher, truncated to 16 bytes at packet[8].
+void ref_par3_assemble_recovery_packets(const uint8_t* rec, size_t n, size_t bs, const uint8_t* sid,
+                                        uint64_t first, uint8_t* out) {
+	static const uint8_t magic[8] = {'P', 'A', 'R', '3', 0, 'P', 'K', 'T'};
+	static const uint8_t type[8] = {'P', 'A', 'R', ' ', 'R', 'E', 'C', 0};
+	const size_t pkt_size = 64 + bs;
+	for (size_t i = 0; i < n; i++) {
+		uint8_t* pkt = out + i * pkt_size;
+		memcpy(pkt, magic, 8);
+		memset(pkt + 8, 0, 16);
+		for (int b = 0; b < 8; b++) pkt[24 + b] = (uint8_t)((uint64_t)pkt_size >> (8 * b));
+		memcpy(pkt + 32, sid, 8);
+		memcpy(pkt + 40, type, 8);
+		for (int b = 0; b < 8; b++) pkt[48 + b] = (uint8_t)((first + i) >> (8 * b));
+		for (int b = 0; b < 8; b++) pkt[56 + b] = (uint8_t)(b == 0);
+		memcpy(pkt + 64, rec + i * bs, bs);
+		blake3_hasher h;
+		blake3_hasher_init(&h);
+		blake3_hasher_update(&h, pkt + 24, 24);
+		blake3_hasher_update(&h, pkt + 48, 16 + bs);
+		uint8_t full[32];
+		blake3_hasher_finalize(&h, full, 32);
+		memcpy(pkt + 8, full, 16);
+	}
+}
+
 }  // extern "C"

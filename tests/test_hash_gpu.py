@@ -56,6 +56,7 @@ def test_par2_block_hashes_device_rows_in_place_and_misaligned(ctx, rng):
     d_al[:, :sl] = dev[:, :sl]
     out = torch.zeros((n, 20), dtype=torch.uint8, device="cuda")
     par2.block_hashes(d_al[:, :sl], sl, out=out, ctx=ctx)
+    ctx.synchronize()  # device buffers only: the call is asynchronous
     assert (out.cpu().numpy() == want).all()
     # a misaligned view (offset 3 bytes, stride 3040) is staged
     view = dev[:, 3:3 + sl]
@@ -130,6 +131,7 @@ def test_par3_block_hashes_unaligned_layouts_on_device(ctx, oracle, rng):
     after = rng.integers(0, 256, 24, dtype=np.uint8).tobytes()
     out = torch.zeros((n, 16), dtype=torch.uint8, device="cuda")
     par3.block_hashes(dev[5:], bs, 9, after, num_blocks=n, block_stride=stride, out=out, ctx=ctx)
+    ctx.synchronize()
     assert (out.cpu().numpy() == oracle.par3_block_hashes(rows, 9, after)).all()
 
 
@@ -156,6 +158,7 @@ def test_par3_recovery_packets_golden_device_buffers(ctx, golden):
         rec = torch.from_numpy(pattern_bytes(n * bs, int(seed))).cuda()
         out = torch.zeros(n * (64 + bs), dtype=torch.uint8, device="cuda")
         par3.assemble_recovery_packets(rec, sid, int(first), n, bs, out=out, ctx=ctx)
+        ctx.synchronize()
         assert (out.cpu().numpy() == g[f"pkt{k}"]).all(), (n, bs)
 
 
@@ -172,6 +175,7 @@ def test_par2_block_hashes_full_size_sampled(ctx):
     d = torch.randint(0, 256, (n, sl), dtype=torch.uint8, device="cuda", generator=g)
     out = torch.zeros((n, 20), dtype=torch.uint8, device="cuda")
     par2.block_hashes(d, sl, out=out, ctx=ctx)
+    ctx.synchronize()
     got = out.cpu().numpy()
     idx = np.linspace(0, n - 1, 256).astype(np.int64)
     rows = d[torch.from_numpy(idx).cuda()].cpu().numpy()
@@ -191,6 +195,7 @@ def test_par3_block_hashes_full_size_sampled(ctx, oracle):
     after = bytes(range(24))
     out = torch.zeros((n, 16), dtype=torch.uint8, device="cuda")
     par3.block_hashes(d, bs, 1000, after, num_blocks=n, out=out, ctx=ctx)
+    ctx.synchronize()
     got = out.cpu().numpy()
     idx = np.linspace(0, n - 1, 512).astype(np.int64)
     rows = d[torch.from_numpy(idx).cuda()].cpu().numpy()

@@ -210,3 +210,13 @@ def test_hash_oracle_vs_reference(oracle, reference, rng):
             rows[i, :c.size] = c
             lens.append(c.size)
         assert (par2_block_hashes(rows, sl, lens) == ifsc).all()
+
+
+def test_par3_hash_oracle_vs_reference(oracle, reference, rng):
+    from oracle import pattern_bytes
+    for n, bs in [(3, 8), (2, 1000), (2, 4096), (1, 65536 + 8)]:
+        b = pattern_bytes(n * bs, bs).reshape(n, bs)
+        after = rng.integers(0, 256, 24, dtype=np.uint8).tobytes()
+        assert (oracle.par3_block_hashes(b, 2**40, after) == reference.par3_block_hashes(b, 2**40, after)).all()
+        assert (oracle.par3_recovery_packets(b, b"idid-idi", 77) ==
+                reference.par3_recovery_packets(b, b"idid-idi", 77)).all()
