@@ -283,6 +283,16 @@ PP_API int pp_gf64_fft_inv(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, 
 PP_API int pp_par2_block_hashes(pp_ctx* ctx, const void* blocks, size_t block_stride, size_t num_blocks,
                                 size_t slice_size, const uint64_t* lengths, uint8_t* md5crc);
 
+/* pp_par2_create that also returns the inputs' IFSC entries (as
+ * pp_par2_block_hashes with every input a full slice_bytes row, the caller
+ * having zero-padded a file's last slice as pp_par2_create requires) computed
+ * in the same pass over the inputs: each staged chunk of input rows is hashed
+ * on the device beside the region kernels, so host inputs cross PCIe once for
+ * both.  md5crc: num_inputs x 20 bytes, host or device. */
+PP_API int pp_par2_create_hashed(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
+                                 size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps,
+                                 unsigned num_outputs, void* outputs, size_t output_stride, uint8_t* md5crc);
+
 /* PAR3 data-block checksums (lib/par3gen.js:1001-1017, _inlineHashBlock):
  * hashes[16*i..] = BLAKE3(after_checksum[0..24) || u64le(first_index + i) ||
  * block_i)[0..16), block_i = block_size bytes at blocks + i * block_stride.
@@ -303,6 +313,21 @@ PP_API int pp_par3_block_hashes(pp_ctx* ctx, const void* blocks, size_t block_st
 PP_API int pp_par3_assemble_recovery_packets(pp_ctx* ctx, const void* recovery, size_t num_recovery,
                                              size_t block_size, const uint8_t* input_set_id,
                                              uint64_t first_recovery_index, uint8_t* packets);
+
+/* One PAR3 create pass over the input blocks: the num_recovery recovery
+ * blocks first_recovery.. (as pp_gf64_compute_recovery) come back as
+ * assembled RECOVERY packets (as pp_par3_assemble_recovery_packets,
+ * num_recovery x (64 + 8 * block_size64) bytes), and, when data_hashes is not
+ * NULL, every input block's data-packet checksum (as pp_par3_block_hashes
+ * with first_index = first_input; num_inputs x 16 bytes) is computed from the
+ * same staged input rows.  This is the reference's create flow of
+ * _processRecoveryBatch + _finalizeRecoveryBlocks + assemble_recovery_packets
+ * (lib/par3gen.js:1686-1712,1750-1898) plus the data-packet hashing of its
+ * read loop (lib/par3gen.js:2790-2830), with the input crossing PCIe once. */
+PP_API int pp_par3_create_packets(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs, size_t block_size64,
+                                  uint64_t first_input, size_t num_recovery, uint64_t first_recovery,
+                                  const uint8_t* data_after_checksum, uint8_t* data_hashes,
+                                  const uint8_t* input_set_id, uint8_t* packets);
 
 /* ------------------------------------------------------------ batches
  * No counterpart in the reference (it runs one job at a time on its CPU

@@ -71,7 +71,7 @@ const Gf16Host& gf16h() {
 }  // namespace
 
 // -------------------------------------------------------------------- ctx
-enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_AEXP, S_NSLOTS };
+enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_AEXP, S_HASH, S_HCV, S_PKT, S_NSLOTS };
 
 struct CauchyEntry {
   size_t n_in, n_rec;
@@ -107,6 +107,8 @@ struct pp_ctx {
   int* d_status = nullptr;  // set nonzero by a kernel whose bounded wait gave up
   cudaStream_t copy = nullptr;     // host-to-device copies overlapped with the region kernels
   cudaEvent_t copy_ev = nullptr, start_ev = nullptr;
+  cudaStream_t hash = nullptr;     // block hashes of staged inputs, beside the region kernels
+  cudaEvent_t hash_ev = nullptr, staged_ev = nullptr;
   std::mutex mu;
 };
 
@@ -310,6 +312,9 @@ PP_API void pp_ctx_destroy(pp_ctx* ctx) {
   if (ctx->copy) cudaStreamDestroy(ctx->copy);
   if (ctx->copy_ev) cudaEventDestroy(ctx->copy_ev);
   if (ctx->start_ev) cudaEventDestroy(ctx->start_ev);
+  if (ctx->hash) cudaStreamDestroy(ctx->hash);
+  if (ctx->hash_ev) cudaEventDestroy(ctx->hash_ev);
+  if (ctx->staged_ev) cudaEventDestroy(ctx->staged_ev);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
 }
@@ -501,12 +506,49 @@ static int ensure_copy_stream(pp_ctx* ctx) {
   return PP_OK;
 }
 
+static int ensure_hash_stream(pp_ctx* ctx) {
+  if (ctx->hash) return PP_OK;
+  if (cudaStreamCreateWithFlags(&ctx->hash, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->hash_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->staged_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, PP_ERR_CUDA, "hash stream");
+  }
+  return PP_OK;
+}
+
+// Where the IFSC entries of a hashed region pass go on the device.
+static uint8_t* hash_buffer(pp_ctx* ctx, uint8_t* hashes, unsigned n_in) {
+  if (!hashes) return nullptr;
+  if (is_device_ptr(hashes) && ((uintptr_t)hashes % 4) == 0) return hashes;
+  return (uint8_t*)scratch(ctx, S_HASH, (size_t)20 * n_in);
+}
+
+// hashes: optional IFSC entries (MD5 || CRC32 of each input row's slice
+// bytes), computed on the hash stream from the device rows as they are staged,
+// concurrently with the region kernels; host or device memory, n_in x 20.
 static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, unsigned n_in, size_t slice,
                             const uint16_t* d_coeffs, size_t ldc, unsigned n_out, void* outputs, size_t out_stride,
-                            bool accumulate, uint8_t* aexp_ready = nullptr) {
+                            bool accumulate, uint8_t* aexp_ready = nullptr, uint8_t* hashes = nullptr) {
   const bool in_dev = is_device_ptr(inputs);
   const bool out_dev = is_device_ptr(outputs);
   const size_t row = round16(slice);
+  if (hashes && n_in == 0) hashes = nullptr;
+  uint8_t* dh = hash_buffer(ctx, hashes, n_in);
+  if (hashes) {
+    if (!dh) return set_err(ctx, PP_ERR_NO_MEMORY, "hash output");
+    if (int r = ensure_hash_stream(ctx)) return r;
+  }
+  // after the region work: the hash stream's work joins the context's stream,
+  // and host hash outputs are copied back
+  auto join_hashes = [&]() -> int {
+    if (!hashes) return PP_OK;
+    CUDA_TRY(ctx, cudaEventRecord(ctx->hash_ev, ctx->hash));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->hash_ev, 0));
+    if (dh != hashes)
+      CUDA_TRY(ctx, cudaMemcpyAsync(hashes, dh, (size_t)20 * n_in, cudaMemcpyDefault, ctx->stream));
+    return PP_OK;
+  };
   if (!in_dev && n_in >= 2 * kCopyChunk && use_tensor(ctx->gf16_kernel, n_in, n_out)) {
     // ---- chunked: copies of chunk c+1 overlap the products of chunk c
     if (int r = ensure_copy_stream(ctx)) return r;
@@ -533,12 +575,18 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
     // the staging rows are free once earlier work on the context's stream is done
     CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
     CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
+    if (hashes) CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->start_ev, 0));
     for (unsigned c0 = 0; c0 < n_in; c0 += kCopyChunk) {
       const unsigned nc = std::min(kCopyChunk, n_in - c0);
       CUDA_TRY(ctx, cudaMemcpy2DAsync(din + (size_t)c0 * row, row, (const uint8_t*)inputs + (size_t)c0 * in_stride,
                                       in_stride, slice, nc, cudaMemcpyHostToDevice, ctx->copy));
       CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
       CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev, 0));
+      if (hashes) {
+        CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->copy_ev, 0));
+        CUDA_TRY(ctx, launch_par2_block_hash(din + (size_t)c0 * row, row, nc, slice, nullptr, dh + (size_t)20 * c0,
+                                             ctx->hash));
+      }
       CUDA_TRY(ctx, launch_gf16_muladd_tc(din + (size_t)c0 * row, row, nc, slice, aexp + (size_t)(c0 / 8) * kGf16TileBytes,
                                           n_out, dout, ostride, accumulate || c0 > 0, ctx->sms, ctx->d_status,
                                           ctx->stream, stages));
@@ -546,6 +594,7 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
     if (stage_out)
       CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,
                                       out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    if (int r = join_hashes()) return r;
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return device_status(ctx);
   }
@@ -558,6 +607,11 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
                                     in_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     din = s;
     dstride = row;
+  }
+  if (hashes) {  // hash the staged rows beside the region kernel
+    CUDA_TRY(ctx, cudaEventRecord(ctx->staged_ev, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->staged_ev, 0));
+    CUDA_TRY(ctx, launch_par2_block_hash(din, dstride, n_in, slice, nullptr, dh, ctx->hash));
   }
   uint8_t* dout = (uint8_t*)outputs;
   size_t ostride = out_stride;
@@ -581,7 +635,8 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
     CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,
                                     out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
   }
-  if (!in_dev || !out_dev) {
+  if (int r = join_hashes()) return r;
+  if (!in_dev || !out_dev || (hashes && dh != hashes)) {
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return device_status(ctx);
   }
@@ -619,9 +674,9 @@ PP_API int pp_gf16_muladd(pp_ctx* ctx, const void* inputs, size_t input_stride, 
                           output_stride, accumulate != 0);
 }
 
-PP_API int pp_par2_create(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
-                          size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps, unsigned num_outputs,
-                          void* outputs, size_t output_stride) {
+static int par2_create_impl(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
+                            size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps, unsigned num_outputs,
+                            void* outputs, size_t output_stride, uint8_t* hashes) {
   if (!ctx) return PP_ERR_INVALID_ARG;
   if (!outputs || (num_inputs && (!inputs || !input_idx)) || (num_outputs && !exps))
     return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
@@ -638,12 +693,29 @@ PP_API int pp_par2_create(pp_ctx* ctx, const void* inputs, size_t input_stride, 
   if (int r = par2_table(ctx, input_idx, num_inputs, exps, num_outputs, &t)) return r;
   if (t)
     return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, t->d_coef, num_inputs, num_outputs,
-                            outputs, output_stride, false, t->d_aexp);
+                            outputs, output_stride, false, t->d_aexp, hashes);
   uint16_t* dc = (uint16_t*)scratch(ctx, S_COEF, (size_t)num_inputs * num_outputs * 2);
   if (!dc) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficients");
   if (int r = par2_coeff_matrix_dev(ctx, input_idx, num_inputs, exps, num_outputs, dc)) return r;
   return gf16_muladd_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, dc, num_inputs, num_outputs, outputs,
-                          output_stride, false);
+                          output_stride, false, nullptr, hashes);
+}
+
+PP_API int pp_par2_create(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
+                          size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps, unsigned num_outputs,
+                          void* outputs, size_t output_stride) {
+  return par2_create_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, input_idx, exps, num_outputs, outputs,
+                          output_stride, nullptr);
+}
+
+PP_API int pp_par2_create_hashed(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
+                                 size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps,
+                                 unsigned num_outputs, void* outputs, size_t output_stride, uint8_t* md5crc) {
+  if (ctx && num_inputs && !md5crc) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if (ctx && num_inputs && (!num_outputs || !slice_bytes))  // nothing to create: the hashes alone
+    return pp_par2_block_hashes(ctx, inputs, input_stride, num_inputs, slice_bytes, nullptr, md5crc);
+  return par2_create_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, input_idx, exps, num_outputs, outputs,
+                          output_stride, md5crc);
 }
 
 PP_API int pp_par2_invert(pp_ctx* ctx, const uint8_t* valid, unsigned num_inputs, uint16_t* recovery,
@@ -1128,11 +1200,35 @@ static cudaError_t gf64_region(pp_ctx* ctx, const uint64_t* din, const uint64_t*
                             ctx->stream);
 }
 
+// hj: optional BLAKE3 block-hash job over the input blocks (prefix fields and
+// hash_out for block 0 set; data, n and the offsets are filled per staged
+// chunk), run on the hash stream beside the products; hcv = its chaining-value
+// scratch, sized for the whole input.  The hash work is joined into the
+// context's stream before return.
 static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, uint64_t* recovery, size_t n_rec,
-                            size_t B, const uint64_t* d_coeff, bool accumulate) {
+                            size_t B, const uint64_t* d_coeff, bool accumulate, const B3Job* hj = nullptr,
+                            uint32_t* hcv = nullptr) {
   const bool in_dev = is_device_ptr(inputs);
   const bool out_dev = is_device_ptr(recovery);
   const uint64_t* din = inputs;
+  if (hj)
+    if (int r = ensure_hash_stream(ctx)) return r;
+  auto hash_rows = [&](const uint64_t* rows, size_t first, size_t count) -> cudaError_t {
+    B3Job J = *hj;
+    J.data = (const uint8_t*)rows;
+    J.stride = B * 8;
+    J.D = B * 8;
+    J.n = count;
+    J.first_index = hj->first_index + first;
+    J.hash_out = hj->hash_out + first * hj->hash_stride;
+    return launch_blake3_blocks(J, hcv, ctx->hash);
+  };
+  auto join_hash = [&]() -> int {
+    if (!hj) return PP_OK;
+    CUDA_TRY(ctx, cudaEventRecord(ctx->hash_ev, ctx->hash));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->hash_ev, 0));
+    return PP_OK;
+  };
   const size_t chunk = std::max<size_t>(1024, (64u << 20) / (B * 8));  // input blocks per ~64 MiB copy
   if (!in_dev && n_in >= 2 * chunk) {
     // ---- chunked: the copy of chunk c+1 overlaps the product of chunk c
@@ -1154,10 +1250,15 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
       CUDA_TRY(ctx, cudaMemcpyAsync(s + c0 * B, inputs + c0 * B, nc * B * 8, cudaMemcpyHostToDevice, ctx->copy));
       CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
       CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev, 0));
+      if (hj) {
+        CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->copy_ev, 0));
+        CUDA_TRY(ctx, hash_rows(s + c0 * B, c0, nc));
+      }
       CUDA_TRY(ctx, gf64_region(ctx, s + c0 * B, nullptr, B, nc, B, d_coeff + c0, n_in, n_rec, dout, nullptr, B,
                                 accumulate || c0 > 0, aligned_rows64(s, B) && aligned_rows64(dout, B)));
     }
     if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(recovery, dout, n_rec * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (int r = join_hash()) return r;
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return device_status(ctx);
   }
@@ -1166,6 +1267,11 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
     if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", n_in * B * 8);
     CUDA_TRY(ctx, cudaMemcpyAsync(s, inputs, n_in * B * 8, cudaMemcpyHostToDevice, ctx->stream));
     din = s;
+  }
+  if (hj) {  // hash the device rows beside the product
+    CUDA_TRY(ctx, cudaEventRecord(ctx->staged_ev, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->staged_ev, 0));
+    CUDA_TRY(ctx, hash_rows(din, 0, n_in));
   }
   uint64_t* dout = recovery;
   if (!out_dev) {
@@ -1177,6 +1283,7 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
   CUDA_TRY(ctx, gf64_region(ctx, din, nullptr, B, n_in, B, d_coeff, n_in, n_rec, dout, nullptr, B, accumulate,
                             aligned_rows64(din, B) && aligned_rows64(dout, B)));
   if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(recovery, dout, n_rec * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (int r = join_hash()) return r;
   if (!in_dev || !out_dev) {
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return device_status(ctx);
@@ -1659,33 +1766,18 @@ PP_API int pp_par3_block_hashes(pp_ctx* ctx, const void* blocks, size_t block_st
   return PP_OK;
 }
 
-PP_API int pp_par3_assemble_recovery_packets(pp_ctx* ctx, const void* recovery, size_t num_recovery,
-                                             size_t block_size, const uint8_t* input_set_id,
-                                             uint64_t first_recovery_index, uint8_t* packets) {
-  if (!ctx) return PP_ERR_INVALID_ARG;
-  if (num_recovery == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "numRecovery must be a positive integer");
-  if (block_size == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "blockSize must be a positive integer");
-  if (num_recovery > ((size_t)1 << 40) / block_size)
-    return set_err(ctx, PP_ERR_INVALID_ARG, "numRecovery * blockSize exceeds 1 TiB cap");
-  if (!recovery || !input_set_id || !packets) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
-  std::lock_guard<std::mutex> g(ctx->mu);
-  if (int r = bind(ctx)) return r;
-  const size_t n = num_recovery, pkt = 64 + block_size;
-  uint8_t sid[8];
-  if (int r = host_bytes(ctx, input_set_id, 8, sid)) return r;
-  int st = PP_OK;
-  size_t dstride = 0;
-  const uint8_t* drows = rows_on_device(ctx, S_IN, recovery, block_size, n, block_size, block_size, false,
-                                        &dstride, &st);
-  if (!drows) return st;
-  const bool out_dev = is_device_ptr(packets);
-  uint8_t* dpk = out_dev ? packets : (uint8_t*)scratch(ctx, S_OUT, n * pkt);
+// Headers + BLAKE3 of n recovery packets built from device recovery rows
+// (dstride bytes apart) into device packets dpk; enqueued on the context's
+// stream.
+static int assemble_packets(pp_ctx* ctx, const uint8_t* drows, size_t dstride, size_t n, size_t block_size,
+                            const uint8_t sid[8], uint64_t first, uint8_t* dpk) {
+  const size_t pkt = 64 + block_size;
   const size_t sw = blake3_scratch_words(n, 40 + (uint64_t)block_size);
   uint32_t* dcv = sw ? (uint32_t*)scratch(ctx, S_B, sw * 4) : nullptr;
-  if (!dpk || (sw && !dcv)) return set_err(ctx, PP_ERR_NO_MEMORY, "packet buffers");
+  if (sw && !dcv) return set_err(ctx, PP_ERR_NO_MEMORY, "packet hash scratch");
   uint64_t sid64 = 0;
   for (int b = 0; b < 8; b++) sid64 |= (uint64_t)sid[b] << (8 * b);
-  CUDA_TRY(ctx, launch_par3_packet_headers(dpk, n, block_size, sid64, first_recovery_index, ctx->stream));
+  CUDA_TRY(ctx, launch_par3_packet_headers(dpk, n, block_size, sid64, first, ctx->stream));
   // checksum input: header bytes [24, 48) = total length, set id, "PAR REC\0";
   // then the body u64le(index), u64le(1), block
   B3Job J;
@@ -1699,7 +1791,7 @@ PP_API int pp_par3_assemble_recovery_packets(pp_ctx* ctx, const void* recovery, 
   J.pre[3] = le32(sid + 4);
   J.pre[4] = 0x20524150u;  // "PAR "
   J.pre[5] = 0x00434552u;  // "REC\0"
-  J.first_index = first_recovery_index;
+  J.first_index = first;
   J.extra = 1;
   J.n = n;
   J.copy_to = dpk + 64;
@@ -1707,8 +1799,93 @@ PP_API int pp_par3_assemble_recovery_packets(pp_ctx* ctx, const void* recovery, 
   J.hash_out = dpk + 8;
   J.hash_stride = pkt;
   CUDA_TRY(ctx, launch_blake3_blocks(J, dcv, ctx->stream));
+  return PP_OK;
+}
+
+static int check_packet_args(pp_ctx* ctx, size_t num_recovery, size_t block_size) {
+  if (num_recovery == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "numRecovery must be a positive integer");
+  if (block_size == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "blockSize must be a positive integer");
+  if (num_recovery > ((size_t)1 << 40) / block_size)
+    return set_err(ctx, PP_ERR_INVALID_ARG, "numRecovery * blockSize exceeds 1 TiB cap");
+  return PP_OK;
+}
+
+PP_API int pp_par3_assemble_recovery_packets(pp_ctx* ctx, const void* recovery, size_t num_recovery,
+                                             size_t block_size, const uint8_t* input_set_id,
+                                             uint64_t first_recovery_index, uint8_t* packets) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (int r = check_packet_args(ctx, num_recovery, block_size)) return r;
+  if (!recovery || !input_set_id || !packets) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const size_t n = num_recovery, pkt = 64 + block_size;
+  uint8_t sid[8];
+  if (int r = host_bytes(ctx, input_set_id, 8, sid)) return r;
+  int st = PP_OK;
+  size_t dstride = 0;
+  const uint8_t* drows = rows_on_device(ctx, S_IN, recovery, block_size, n, block_size, block_size, false,
+                                        &dstride, &st);
+  if (!drows) return st;
+  const bool out_dev = is_device_ptr(packets);
+  uint8_t* dpk = out_dev ? packets : (uint8_t*)scratch(ctx, S_OUT, n * pkt);
+  if (!dpk) return set_err(ctx, PP_ERR_NO_MEMORY, "packet buffer");
+  if (int r = assemble_packets(ctx, drows, dstride, n, block_size, sid, first_recovery_index, dpk)) return r;
   if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(packets, dpk, n * pkt, cudaMemcpyDeviceToHost, ctx->stream));
   if (!out_dev || drows != recovery) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
+PP_API int pp_par3_create_packets(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs, size_t block_size64,
+                                  uint64_t first_input, size_t num_recovery, uint64_t first_recovery,
+                                  const uint8_t* data_after_checksum, uint8_t* data_hashes,
+                                  const uint8_t* input_set_id, uint8_t* packets) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_inputs == 0 || block_size64 == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "no input blocks");
+  const size_t bs = block_size64 * 8;
+  if (int r = check_packet_args(ctx, num_recovery, bs)) return r;
+  if (!inputs || !input_set_id || !packets || (data_hashes && !data_after_checksum))
+    return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  uint8_t sid[8];
+  if (int r = host_bytes(ctx, input_set_id, 8, sid)) return r;
+  int st;
+  uint64_t* M = cauchy_get(ctx, num_inputs, num_recovery, first_input, first_recovery, &st);
+  if (!M) return st;
+  uint64_t* drec = (uint64_t*)scratch(ctx, S_PKT, num_recovery * bs);
+  if (!drec) return set_err(ctx, PP_ERR_NO_MEMORY, "recovery blocks (%zu bytes)", num_recovery * bs);
+  // data-block hashes of the inputs, in the same pass
+  B3Job hj;
+  uint32_t* hcv = nullptr;
+  uint8_t* dh = nullptr;
+  if (data_hashes) {
+    uint8_t after[24];
+    if (int r = host_bytes(ctx, data_after_checksum, 24, after)) return r;
+    dh = is_device_ptr(data_hashes) ? data_hashes : (uint8_t*)scratch(ctx, S_HASH, 16 * num_inputs);
+    const size_t sw = blake3_scratch_words(num_inputs, 32 + (uint64_t)bs);
+    hcv = sw ? (uint32_t*)scratch(ctx, S_HCV, sw * 4) : nullptr;
+    if (!dh || (sw && !hcv)) return set_err(ctx, PP_ERR_NO_MEMORY, "hash buffers");
+    hj.P = 32;
+    for (int k = 0; k < 6; k++) hj.pre[k] = le32(after + 4 * k);
+    hj.first_index = first_input;
+    hj.hash_out = dh;
+    hj.hash_stride = 16;
+  }
+  if (int r = gf64_matvec_impl(ctx, inputs, num_inputs, drec, num_recovery, block_size64, M, false,
+                               data_hashes ? &hj : nullptr, hcv))
+    return r;
+  const bool out_dev = is_device_ptr(packets);
+  const size_t pkt = 64 + bs;
+  uint8_t* dpk = out_dev ? packets : (uint8_t*)scratch(ctx, S_OUT, num_recovery * pkt);
+  if (!dpk) return set_err(ctx, PP_ERR_NO_MEMORY, "packet buffer");
+  if (int r = assemble_packets(ctx, (const uint8_t*)drec, bs, num_recovery, bs, sid, first_recovery, dpk)) return r;
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(packets, dpk, num_recovery * pkt, cudaMemcpyDeviceToHost, ctx->stream));
+  if (data_hashes && dh != data_hashes)
+    CUDA_TRY(ctx, cudaMemcpyAsync(data_hashes, dh, 16 * num_inputs, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!out_dev || (data_hashes && dh != data_hashes) || !is_device_ptr(inputs)) {
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return device_status(ctx);
+  }
   return PP_OK;
 }
 

@@ -94,8 +94,12 @@ def gf16_muladd(inputs, coeffs, out=None, slice_bytes=None, accumulate=False, ct
     return out
 
 
-def par2_create(inputs, input_idx, exps, out=None, slice_bytes=None, ctx=None):
-    """PAR2 recovery slices: out[o] = XOR_i gfmat_coeff(input_idx[i], exps[o]) * inputs[i]."""
+def par2_create(inputs, input_idx, exps, out=None, slice_bytes=None, hashes=None, ctx=None):
+    """PAR2 recovery slices: out[o] = XOR_i gfmat_coeff(input_idx[i], exps[o]) * inputs[i].
+
+    hashes: optional (n, 20) uint8 buffer (host or CUDA) that receives the
+    inputs' IFSC entries (MD5 || CRC32 of each input row), computed on the
+    device in the same pass over the inputs."""
     c = _ctx(ctx)
     n, s, istride = _rows(inputs)
     if slice_bytes is None:
@@ -107,6 +111,10 @@ def par2_create(inputs, input_idx, exps, out=None, slice_bytes=None, ctx=None):
     if out is None:
         out = np.zeros((ex.size, slice_bytes), dtype=np.uint8)
     ro, so, ostride = _rows(out)
+    if hashes is not None:
+        c.check(lib.pp_par2_create_hashed(c.h, ptr(inputs), istride, n, slice_bytes, ptr(idx), ptr(ex), ex.size,
+                                          ptr(out), ostride, ptr(hashes)))
+        return out
     c.check(lib.pp_par2_create(c.h, ptr(inputs), istride, n, slice_bytes, ptr(idx), ptr(ex), ex.size, ptr(out),
                                ostride))
     return out

@@ -378,3 +378,29 @@ def assemble_recovery_packets(recoveryBlocksBuf, inputSetIdBuf, firstRecoveryInd
     c.check(lib.pp_par3_assemble_recovery_packets(c.h, ptr(recoveryBlocksBuf), numRecovery, blockSize, ptr(sid),
                                                   _u64(firstRecoveryIndex), ptr(out)))
     return out
+
+
+def create_packets(inputs, num_inputs, block_size64, first_input, num_recovery, first_recovery, input_set_id,
+                   data_after_checksum=None, data_hashes=None, packets=None, ctx=None):
+    """One create pass: the recovery packets of recovery blocks
+    first_recovery.. and (when data_after_checksum is given) the input blocks'
+    data-packet checksums, both from one staging of the inputs.  Returns
+    (packets, data_hashes) -- numpy arrays unless buffers are given."""
+    c = _ctx(ctx)
+    sid = np.frombuffer(bytes(input_set_id), dtype=np.uint8)
+    if sid.size != 8:
+        raise TypeError("inputSetIdBuf must be a 8-byte Buffer")
+    bs = int(block_size64) * 8
+    if packets is None:
+        packets = np.empty(int(num_recovery) * (64 + bs), dtype=np.uint8)
+    ac = None
+    if data_after_checksum is not None:
+        ac = np.frombuffer(bytes(data_after_checksum), dtype=np.uint8)
+        if ac.size != 24:
+            raise ValueError("data_after_checksum must be 24 bytes")
+        if data_hashes is None:
+            data_hashes = np.empty((int(num_inputs), 16), dtype=np.uint8)
+    c.check(lib.pp_par3_create_packets(c.h, ptr(inputs), num_inputs, block_size64, _u64(first_input), num_recovery,
+                                       _u64(first_recovery), ptr(ac), ptr(data_hashes) if ac is not None else 0,
+                                       ptr(sid), ptr(packets)))
+    return packets, data_hashes

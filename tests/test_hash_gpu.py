@@ -203,3 +203,82 @@ def test_par3_block_hashes_full_size_sampled(ctx, oracle):
     assert (got[idx] == want).all()
     assert len({r.tobytes() for r in got}) == n
     del d
+
+
+# ------------------------------------------------------------- fused pass
+@gpu
+@pytest.mark.parametrize("n", [5, 300, 10003])
+def test_par2_create_hashed_host_inputs(ctx, oracle, rng, n):
+    """Recovery slices and the inputs' IFSC entries from one pass over host
+    inputs (10003 slices takes the chunked copy path)."""
+    from parparpar_b200 import par2
+    sl = 1024
+    data = rng.integers(0, 256, (n, sl), dtype=np.uint8)
+    exps = [0, 1, 7, 300]
+    hashes = np.zeros((n, 20), dtype=np.uint8)
+    out = par2.par2_create(data, np.arange(n), exps, hashes=hashes, ctx=ctx)
+    assert (hashes == par2_oracle(data, sl)).all()
+    # the recovery slices are those of the plain create (itself pinned to the oracle elsewhere)
+    assert (out == par2.par2_create(data, np.arange(n), exps, ctx=ctx)).all()
+    if n <= 300:
+        co = oracle.par2_coeff_matrix(np.arange(n), exps)
+        assert (out == oracle.par2_muladd(list(data), sl, co)).all()
+
+
+@gpu
+def test_par2_create_hashed_device_inputs(ctx, rng):
+    torch = _torch()
+    from parparpar_b200 import par2
+    n, sl = 77, 4096
+    data = rng.integers(0, 256, (n, sl), dtype=np.uint8)
+    d_in = torch.from_numpy(data).cuda()
+    d_out = torch.zeros((3, sl), dtype=torch.uint8, device="cuda")
+    d_h = torch.zeros((n, 20), dtype=torch.uint8, device="cuda")
+    par2.par2_create(d_in, np.arange(n), [1, 2, 3], out=d_out, hashes=d_h, ctx=ctx)
+    ctx.synchronize()
+    assert (d_h.cpu().numpy() == par2_oracle(data, sl)).all()
+    ref = par2.par2_create(data, np.arange(n), [1, 2, 3], ctx=ctx)
+    assert (d_out.cpu().numpy() == ref).all()
+
+
+@gpu
+@pytest.mark.parametrize("n_in,words", [(40, 128), (20000, 512)])
+def test_par3_create_packets_matches_separate_steps(ctx, oracle, rng, n_in, words):
+    """Fused create: packets == assemble(compute_recovery(inputs)) and data
+    hashes == block hashes of the inputs; 20000 x 4 KiB host inputs take the
+    chunked copy path."""
+    from parparpar_b200 import par3
+    R, fI, fR = 6, 3, n_in + 3
+    x = rng.integers(0, 2**64, (n_in, words), dtype=np.uint64)
+    after = rng.integers(0, 256, 24, dtype=np.uint8).tobytes()
+    sid = b"setid-01"
+    pk, dh = par3.create_packets(x, n_in, words, fI, R, fR, sid, data_after_checksum=after, ctx=ctx)
+    rec = np.zeros((R, words), dtype=np.uint64)
+    par3.GF64Controller.ComputeRecoveryBlocks(x, n_in, rec, R, words, fI, fR)
+    want_pk = oracle.par3_recovery_packets(rec.view(np.uint8).reshape(R, words * 8), sid, fR)
+    assert (pk == want_pk).all()
+    rows = np.linspace(0, n_in - 1, min(n_in, 200)).astype(np.int64)
+    blocks = x.view(np.uint8).reshape(n_in, words * 8)
+    want_h = np.stack([oracle.par3_block_hashes(blocks[i:i + 1], fI + int(i), after)[0] for i in rows])
+    assert (dh[rows] == want_h).all()
+    if n_in <= 64:
+        assert (rec == oracle.gf64_compute_recovery(x, R, fI, fR)).all()
+
+
+@gpu
+def test_par3_create_packets_device_buffers(ctx, oracle, rng):
+    torch = _torch()
+    from parparpar_b200 import par3
+    n_in, words, R = 300, 256, 4
+    x = rng.integers(0, 2**64, (n_in, words), dtype=np.uint64)
+    d_x = torch.from_numpy(x.view(np.int64)).cuda()
+    d_pk = torch.zeros(R * (64 + words * 8), dtype=torch.uint8, device="cuda")
+    d_h = torch.zeros((n_in, 16), dtype=torch.uint8, device="cuda")
+    after = bytes(range(100, 124))
+    par3.create_packets(d_x, n_in, words, 0, R, n_in, b"ABCDEFGH", data_after_checksum=after, data_hashes=d_h,
+                        packets=d_pk, ctx=ctx)
+    ctx.synchronize()
+    rec = oracle.gf64_compute_recovery(x, R, 0, n_in)
+    assert (d_pk.cpu().numpy() == oracle.par3_recovery_packets(rec.view(np.uint8).reshape(R, -1), b"ABCDEFGH",
+                                                               n_in)).all()
+    assert (d_h.cpu().numpy() == oracle.par3_block_hashes(x.view(np.uint8).reshape(n_in, -1), 0, after)).all()
