@@ -293,6 +293,20 @@ PP_API int pp_par2_create_hashed(pp_ctx* ctx, const void* inputs, size_t input_s
                                  size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps,
                                  unsigned num_outputs, void* outputs, size_t output_stride, uint8_t* md5crc);
 
+/* PAR2 memory checksums: the checksum block the reference's PAR2 staging
+ * appends to every slice (gf16/gf16_cksum_base.h:40-55 with the block step of
+ * gf16/gf16_checksum_generic.h gf16_multi_mul2: C = 2*C ^ block), here with
+ * 16-byte blocks of 8 little-endian GF(2^16) lanes: row i's first
+ * slice_bytes bytes, zero-extended to a multiple of 16, as blocks B_0..B_nb-1
+ * give out16[16*i..] = sum_j 2^(nb-1-j) * B_j lane-wise.  The function is
+ * linear, so the PAR2 processor stages each input row with its checksum
+ * block, multiplies it along with the data and reports, per output, whether
+ * the carried block still equals the checksum of the output data
+ * (pp_par2_proc_get_output's valid, as finish_packed_cksum,
+ * gf16/controller_cpu.cpp:423-443). */
+PP_API int pp_par2_memory_checksums(pp_ctx* ctx, const void* rows, size_t row_stride, size_t num_rows,
+                                    size_t slice_bytes, uint8_t* out16);
+
 /* PAR3 data-block checksums (lib/par3gen.js:1001-1017, _inlineHashBlock):
  * hashes[16*i..] = BLAKE3(after_checksum[0..24) || u64le(first_index + i) ||
  * block_i)[0..16), block_i = block_size bytes at blocks + i * block_stride.

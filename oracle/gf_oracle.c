@@ -581,3 +581,25 @@ void or_par3_recovery_packets(const uint8_t* recovery, size_t n, size_t block_si
 		or_blake3(p + 24, 40 + block_size, p + 8, 16);
 	}
 }
+
+/* ------------------------------------------------- PAR2 memory checksum */
+/* The staging checksum of the reference's PAR2 processors: each block is
+ * folded in as ck = ck * 2 ^ block, lane-wise over GF(2^16) (gf16_multi_mul2,
+ * gf16/gf16_checksum_generic.h; the copy loop of gf16/gf16_cksum_base.h:20-55).
+ * The reference's block width is its SIMD width; this restatement and the
+ * device both use 16 bytes. */
+void or_par2_mem_cksum(const uint8_t* data, size_t len, uint8_t* out) {
+	uint16_t c[8] = {0};
+	for (size_t o = 0; o < len; o += 16) {
+		for (int l = 0; l < 8; l++) {
+			uint16_t w = 0;
+			for (int b = 0; b < 2; b++)
+				if (o + 2 * l + b < len) w |= (uint16_t)(data[o + 2 * l + b] << (8 * b));
+			c[l] = (uint16_t)(or_gf16_mul(c[l], 2) ^ w);
+		}
+	}
+	for (int l = 0; l < 8; l++) {
+		out[2 * l] = (uint8_t)c[l];
+		out[2 * l + 1] = (uint8_t)(c[l] >> 8);
+	}
+}

@@ -58,6 +58,12 @@ uint64_t or_gf64_cantor(int i);
 void or_gf64_fft_fwd(uint64_t* a, size_t n);
 void or_gf64_fft_inv(uint64_t* a, size_t n);
 
+/* ---------------- PAR2 memory checksum --------------------------------- */
+/* gf16/gf16_cksum_base.h:40-55 with gf16_multi_mul2 (gf16_checksum_generic.h):
+ * C = 2*C ^ B_j over 16-byte blocks (8 LE GF(2^16) lanes) of the first len
+ * bytes zero-extended to a multiple of 16; out: 16 bytes */
+void or_par2_mem_cksum(const uint8_t* data, size_t len, uint8_t* out);
+
 /* ---------------- block hashes ---------------------------------------- */
 /* BLAKE3, default hash mode; out_len <= 32 */
 void or_blake3(const uint8_t* in, size_t len, uint8_t* out, size_t out_len);

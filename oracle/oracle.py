@@ -182,6 +182,14 @@ class Oracle:
         return out
 
 
+    def par2_memory_checksums(self, rows: np.ndarray, slice_size: int) -> np.ndarray:
+        rows = np.ascontiguousarray(rows, dtype=np.uint8)
+        out = np.zeros((rows.shape[0], 16), dtype=np.uint8)
+        for r in range(rows.shape[0]):
+            self.L.or_par2_mem_cksum(_ptr(rows[r]), _SZ(slice_size), _ptr(out[r]))
+        return out
+
+
 def par2_block_hashes(blocks: np.ndarray, slice_size: int, lengths=None) -> np.ndarray:
     """PAR2 IFSC entries, HasherInput::getBlock(md5crc, zeroPad)
     (hasher/hasher_input_base.h:104-117): MD5 of the block's data followed by

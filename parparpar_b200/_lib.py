@@ -60,7 +60,7 @@ EXPORTS = [
     "pp_server_create", "pp_server_submit", "pp_server_wait", "pp_server_get_stats", "pp_server_reset_stats",
     "pp_server_last_error", "pp_server_destroy",
     "pp_par2_block_hashes", "pp_par3_block_hashes", "pp_par3_assemble_recovery_packets",
-    "pp_par2_create_hashed", "pp_par3_create_packets",
+    "pp_par2_create_hashed", "pp_par3_create_packets", "pp_par2_memory_checksums",
 ]
 
 
@@ -143,6 +143,7 @@ _sig("pp_gf64_fft_inv", _I, _P, _P, _SZ, _SZ, _SZ)
 _sig("pp_gf64_solve_and_reconstruct_noalloc", _I, _P, _P, _SZ, _SZ, _P)
 _sig("pp_gf64_repair", _I, _P, _P, _SZ, _P, _SZ, _P, _P, _SZ, _U64, _U64, _P)
 _sig("pp_par2_block_hashes", _I, _P, _P, _SZ, _SZ, _SZ, _P, _P)
+_sig("pp_par2_memory_checksums", _I, _P, _P, _SZ, _SZ, _SZ, _P)
 _sig("pp_par2_create_hashed", _I, _P, _P, _SZ, _U, _SZ, _P, _P, _U, _P, _SZ, _P)
 _sig("pp_par3_block_hashes", _I, _P, _P, _SZ, _SZ, _SZ, _U64, _P, _P)
 _sig("pp_par3_assemble_recovery_packets", _I, _P, _P, _SZ, _SZ, _P, _U64, _P)

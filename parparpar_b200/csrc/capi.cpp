@@ -800,6 +800,9 @@ struct pp_par2_proc {
   uint8_t* d_out = nullptr;
   size_t d_out_n = 0;
   bool has_output = false;
+  int* d_valid = nullptr;         // per-output memory-checksum result
+  std::vector<int> valid;         // its host copy, once checked
+  bool checked = false;
   unsigned batches_started = 0;
   cudaStream_t s_copy = nullptr, s_comp = nullptr;
   cudaEvent_t copied = nullptr;
@@ -808,6 +811,13 @@ struct pp_par2_proc {
 // host slices of at least this many bytes are copied straight from the
 // caller's buffer (one DMA beats a host memcpy into the pinned rows)
 constexpr size_t kProcDirectBytes = 256 << 10;
+
+// Staged rows and output rows: the slice rounded up to 16 bytes, then the
+// 16-byte memory checksum block (the reference's packed staging appends one
+// checksum block per slice, gf16/gf16_global.h:214-218), which the region
+// kernels carry like data.
+static size_t proc_row(size_t slice) { return round16(slice) + 16; }
+static size_t proc_ck_off(const pp_par2_proc* p) { return round16(p->cur_size); }
 
 static int proc_alloc_inputs(pp_par2_proc* p) {
   for (auto& a : p->areas) {
@@ -844,7 +854,7 @@ PP_API int pp_par2_proc_create(pp_ctx* ctx, size_t slice_size, unsigned staging_
   auto* p = new pp_par2_proc();
   p->ctx = ctx;
   p->alloc_size = p->cur_size = slice_size;
-  p->row = round16(slice_size);
+  p->row = proc_row(slice_size);
   p->n_areas = staging_areas ? staging_areas : 2;
   // A GPU batch amortises launch latency and the tensor-core pipeline fill
   if (input_batch) {
@@ -890,6 +900,7 @@ PP_API void pp_par2_proc_destroy(pp_par2_proc* p) {
     if (a.done) cudaEventDestroy(a.done);
   }
   if (p->d_out) cudaFree(p->d_out);
+  if (p->d_valid) cudaFree(p->d_valid);
   if (p->copied) cudaEventDestroy(p->copied);
   if (p->s_copy) cudaStreamDestroy(p->s_copy);
   if (p->s_comp) cudaStreamDestroy(p->s_comp);
@@ -913,7 +924,7 @@ PP_API int pp_par2_proc_set_current_slice_size(pp_par2_proc* p, size_t size) {
   if (size > p->alloc_size) {
     cudaStreamSynchronize(p->s_comp);
     p->alloc_size = size;
-    p->row = round16(size);
+    p->row = proc_row(size);
     if (!p->batch_fixed) {  // larger rows: fewer of them (never more than the coefficient buffers hold)
       p->batch_alloc = std::max<unsigned>(64, std::min<size_t>(8192, (128u << 20) / p->row));
       p->batch = std::min(p->batch, proc_batch_for(p, p->exps.size()));
@@ -931,6 +942,12 @@ PP_API int pp_par2_proc_set_current_slice_size(pp_par2_proc* p, size_t size) {
 
 static int proc_ensure_out(pp_par2_proc* p) {
   size_t need = p->row * std::max<size_t>(1, p->exps.size());
+  if (p->d_valid) cudaFree(p->d_valid);
+  p->d_valid = nullptr;
+  if (cudaMalloc(&p->d_valid, sizeof(int) * std::max<size_t>(1, p->exps.size())) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(p->ctx, PP_ERR_NO_MEMORY, "checksum flags");
+  }
   if (p->d_out_n >= need) return PP_OK;
   if (p->d_out) cudaFree(p->d_out);
   p->d_out = nullptr;
@@ -1009,9 +1026,14 @@ static int proc_submit(pp_par2_proc* p) {
                                    cudaMemcpyHostToDevice, p->s_copy));
   CUDA_TRY(p->ctx, cudaEventRecord(p->copied, p->s_copy));
   CUDA_TRY(p->ctx, cudaStreamWaitEvent(p->s_comp, p->copied, 0));
-  CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_in, p->row, a.count, p->cur_size, a.d_coeff, p->batch,
+  // attach each row's memory checksum, then multiply-accumulate data and
+  // checksum blocks together
+  const size_t ck = proc_ck_off(p);
+  CUDA_TRY(p->ctx, launch_par2_cksum(a.d_in, p->row, a.count, ck, a.d_in + ck, p->row, nullptr, p->s_comp));
+  CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_in, p->row, a.count, ck + 16, a.d_coeff, p->batch,
                                n_out, p->d_out, p->row, p->has_output, p->ctx->sms, a.d_aexp, p->ctx->d_status,
                                p->s_comp));
+  p->checked = false;
   CUDA_TRY(p->ctx, cudaEventRecord(a.done, p->s_comp));
   a.active = true;
   a.count = 0;
@@ -1088,14 +1110,24 @@ PP_API int pp_par2_proc_get_output(pp_par2_proc* p, unsigned index, void* output
   bind(p->ctx);
   if (valid) *valid = 0;
   CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_comp));
+  const unsigned n_out = (unsigned)p->exps.size();
   if (!p->has_output) {
     // no input was added: the recovery data is all zero
     CUDA_TRY(p->ctx, cudaMemsetAsync(p->d_out + (size_t)index * p->row, 0, p->cur_size, p->s_copy));
+  } else if (!p->checked) {
+    // verify every output's carried checksum against its data once
+    // (finish_packed_cksum, gf16/controller_cpu.cpp:423-443)
+    const size_t ck = proc_ck_off(p);
+    CUDA_TRY(p->ctx, launch_par2_cksum(p->d_out, p->row, n_out, ck, p->d_out + ck, p->row, p->d_valid, p->s_copy));
+    p->valid.assign(n_out, 0);
+    CUDA_TRY(p->ctx, cudaMemcpyAsync(p->valid.data(), p->d_valid, sizeof(int) * n_out, cudaMemcpyDeviceToHost,
+                                     p->s_copy));
+    p->checked = true;
   }
   CUDA_TRY(p->ctx, cudaMemcpyAsync(output, p->d_out + (size_t)index * p->row, p->cur_size, cudaMemcpyDefault,
                                    p->s_copy));
   CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_copy));
-  if (valid) *valid = 1;
+  if (valid) *valid = p->has_output ? p->valid[index] : 1;
   return PP_OK;
 }
 
@@ -1886,6 +1918,28 @@ PP_API int pp_par3_create_packets(pp_ctx* ctx, const uint64_t* inputs, size_t nu
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return device_status(ctx);
   }
+  return PP_OK;
+}
+
+PP_API int pp_par2_memory_checksums(pp_ctx* ctx, const void* rows, size_t row_stride, size_t num_rows,
+                                    size_t slice_bytes, uint8_t* out16) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_rows == 0) return PP_OK;
+  if (!rows || !out16) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if (num_rows > 1 && row_stride < slice_bytes) return set_err(ctx, PP_ERR_INVALID_ARG, "row_stride < slice_bytes");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  int st = PP_OK;
+  size_t dstride = 0;
+  const uint8_t* drows =
+      rows_on_device(ctx, S_IN, rows, row_stride, num_rows, slice_bytes, slice_bytes, true, &dstride, &st);
+  if (!drows) return st;
+  const bool out_dev = is_device_ptr(out16) && ((uintptr_t)out16 % 4) == 0;
+  uint8_t* dout = out_dev ? out16 : (uint8_t*)scratch(ctx, S_OUT, 16 * num_rows);
+  if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "checksum output");
+  CUDA_TRY(ctx, launch_par2_cksum(drows, dstride, num_rows, slice_bytes, dout, 16, nullptr, ctx->stream));
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(out16, dout, 16 * num_rows, cudaMemcpyDefault, ctx->stream));
+  if (!out_dev || drows != rows) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return PP_OK;
 }
 

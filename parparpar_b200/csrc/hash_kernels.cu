@@ -406,6 +406,117 @@ __global__ void k_par3_packet_headers(uint8_t* __restrict__ pkts, size_t n, uint
   }
 }
 
+// ---------------------------------------------------- PAR2 memory checksum
+// The staging checksum of the reference's PAR2 processors
+// (gf16/gf16_checksum_generic.h gf16_multi_mul2, gf16/gf16_cksum_base.h:40-55):
+// a row is read as nb 16-byte blocks B_j of 8 little-endian GF(2^16) lanes
+// and C = 2*C ^ B_j over the blocks, i.e. C = sum_j 2^(nb-1-j) * B_j lane-wise.
+// It is linear, so the region product of the inputs' checksums is the
+// checksum of the product: carried through the multiply-accumulate as one
+// more block per row, it checks the outputs.
+__device__ __forceinline__ uint32_t gf16x2_dbl(uint32_t v) {
+  return ((v << 1) & 0xFFFEFFFEu) ^ (((v >> 15) & 0x00010001u) * 0x100Bu);
+}
+
+__device__ __forceinline__ uint32_t gf16x2_mul(uint32_t v, uint32_t g) {
+  uint32_t r = 0;
+  for (int b = 15; b >= 0; b--) {
+    r = gf16x2_dbl(r);
+    if ((g >> b) & 1u) r ^= v;
+  }
+  return r;
+}
+
+struct CksumArgs {
+  const uint8_t* rows;
+  size_t stride;
+  size_t n;
+  uint64_t len;     // bytes of data per row (later bytes read as zero)
+  uint64_t nb;      // 16-byte blocks per row: ceil(len / 16)
+  uint64_t k;       // blocks per lane: ceil(nb / 32)
+  uint32_t g[5];    // 2^(k * 2^L), the weight of the right-hand group at tree level L
+  uint8_t* out;     // make: checksum of row i at out + i * out_stride
+  size_t out_stride;
+  int* valid;       // check: valid[i] = (checksum == the 16 bytes at out + i * out_stride)
+};
+
+// One warp per row.  The blocks are dealt to the lanes end-aligned, k per
+// lane (lane t ends at block nb - (31 - t) k; blocks before 0 are zeros, which
+// Horner from zero ignores), so every right-hand group at tree level L is
+// 2^L k blocks long and the combine weights are uniform.
+__global__ void __launch_bounds__(256) k_par2_cksum(const CksumArgs A) {
+  const size_t r = (size_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (r >= A.n) return;
+  const unsigned lane = threadIdx.x & 31;
+  const uint8_t* row = A.rows + r * A.stride;
+  const int64_t s1 = (int64_t)A.nb - (int64_t)(31 - lane) * (int64_t)A.k;
+  int64_t j = s1 - (int64_t)A.k;
+  if (j < 0) j = 0;
+  uint32_t c[4] = {0, 0, 0, 0};
+  for (; j < s1; j++) {
+    uint32_t w[4];
+    const uint64_t o = 16 * (uint64_t)j;
+    if (o + 16 <= A.len) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + o));
+      w[0] = v.x;
+      w[1] = v.y;
+      w[2] = v.z;
+      w[3] = v.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        uint32_t x = 0;
+        for (int b = 0; b < 4; b++)
+          if (o + 4 * q + b < A.len) x |= (uint32_t)row[o + 4 * q + b] << (8 * b);
+        w[q] = x;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) c[q] = gf16x2_dbl(c[q]) ^ w[q];
+  }
+#pragma unroll
+  for (int L = 0; L < 5; L++) {
+    const unsigned d = 1u << L;
+    uint32_t left[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) left[q] = __shfl_up_sync(0xFFFFFFFFu, c[q], d);
+    if ((lane & (2 * d - 1)) == 2 * d - 1) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) c[q] ^= gf16x2_mul(left[q], A.g[L]);
+    }
+  }
+  if (lane == 31) {
+    uint32_t* o = reinterpret_cast<uint32_t*>(A.out + r * A.out_stride);
+    if (A.valid) {
+      A.valid[r] = (o[0] == c[0] && o[1] == c[1] && o[2] == c[2] && o[3] == c[3]) ? 1 : 0;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; q++) o[q] = c[q];
+    }
+  }
+}
+
+// host: 2^e in GF(2^16)
+uint32_t gf16_pow2(uint64_t e) {
+  e %= 65535;
+  uint32_t r = 1, b = 2;
+  auto mul = [](uint32_t a, uint32_t x) {
+    uint32_t p = 0;
+    for (int i = 15; i >= 0; i--) {
+      p <<= 1;
+      if (p & 0x10000u) p ^= 0x1100Bu;
+      if ((x >> i) & 1u) p ^= a;
+    }
+    return p;
+  };
+  while (e) {
+    if (e & 1) r = mul(r, b);
+    b = mul(b, b);
+    e >>= 1;
+  }
+  return r;
+}
+
 }  // namespace
 
 cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
@@ -465,6 +576,25 @@ cudaError_t launch_par3_packet_headers(uint8_t* d_pkts, size_t n, size_t block_s
   const uint64_t t = (uint64_t)n * 6;
   k_par3_packet_headers<<<(unsigned)((t + 255) / 256), 256, 0, s>>>(d_pkts, n, 64 + (uint64_t)block_size,
                                                                     set_id_le, first);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_par2_cksum(const uint8_t* d_rows, size_t stride, size_t n, uint64_t len, uint8_t* d_out,
+                              size_t out_stride, int* d_valid, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  CksumArgs A;
+  A.rows = d_rows;
+  A.stride = stride;
+  A.n = n;
+  A.len = len;
+  A.nb = (len + 15) / 16;
+  A.k = (A.nb + 31) / 32;
+  for (int L = 0; L < 5; L++) A.g[L] = gf16_pow2(A.k << L);
+  A.out = d_out;
+  A.out_stride = out_stride;
+  A.valid = d_valid;
+  k_par2_cksum<<<(unsigned)((n + 7) / 8), 256, 0, s>>>(A);
   note_launch();
   return cudaGetLastError();
 }

@@ -154,4 +154,11 @@ cudaError_t launch_blake3_blocks(const B3Job& job, uint32_t* d_scratch, cudaStre
 cudaError_t launch_par3_packet_headers(uint8_t* d_pkts, size_t n, size_t block_size, uint64_t set_id_le,
                                        uint64_t first, cudaStream_t s);
 
+// PAR2 memory checksum of each row's first len bytes (16-byte blocks, see
+// hash_kernels.cu).  d_valid NULL: write the 16-byte checksum of row i to
+// d_out + i * out_stride; else set d_valid[i] to whether it equals the 16
+// bytes stored there.  Rows 16-byte aligned; d_out 4-byte aligned.
+cudaError_t launch_par2_cksum(const uint8_t* d_rows, size_t stride, size_t n, uint64_t len, uint8_t* d_out,
+                              size_t out_stride, int* d_valid, cudaStream_t s);
+
 }  // namespace pp

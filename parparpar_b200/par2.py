@@ -230,7 +230,7 @@ class PAR2ProcCUDA:
 
 
 __all__ = ["PAR2ProcCUDA", "Galois16RecMatrix", "gf16_muladd", "par2_create", "coeff_matrix", "gfmat_coeff",
-           "gfmat_input_log", "PPError"]
+           "gfmat_input_log", "PPError", "block_hashes", "HasherInput", "memory_checksums"]
 
 
 # ------------------------------------------------------------ block hashes
@@ -334,3 +334,17 @@ class HasherInput:
             raise ValueError("Buffer must be at least 16 bytes long")
         out[:16] = np.frombuffer(self._md5.digest(), dtype=np.uint8)
         self._ended = True
+
+
+def memory_checksums(rows, slice_size=None, out=None, ctx=None):
+    """PAR2 memory checksum blocks (16 bytes per row) of the staged-slice
+    checksum the processor carries through the region pass
+    (gf16/gf16_cksum_base.h:40-55): C = sum_j 2^(nb-1-j) * B_j over the row's
+    16-byte blocks, lane-wise in GF(2^16)."""
+    c = _ctx(ctx)
+    n, row_bytes, stride = _rows(rows)
+    slice_size = row_bytes if slice_size is None else int(slice_size)
+    if out is None:
+        out = np.empty((n, 16), dtype=np.uint8)
+    c.check(lib.pp_par2_memory_checksums(c.h, ptr(rows), stride, n, slice_size, ptr(out)))
+    return out

@@ -282,3 +282,35 @@ def test_par3_create_packets_device_buffers(ctx, oracle, rng):
     assert (d_pk.cpu().numpy() == oracle.par3_recovery_packets(rec.view(np.uint8).reshape(R, -1), b"ABCDEFGH",
                                                                n_in)).all()
     assert (d_h.cpu().numpy() == oracle.par3_block_hashes(x.view(np.uint8).reshape(n_in, -1), 0, after)).all()
+
+
+# ---------------------------------------------------- PAR2 memory checksum
+@gpu
+@pytest.mark.parametrize("sl", [2, 16, 30, 512, 4100, 32768, 100000])
+def test_par2_memory_checksums(ctx, oracle, rng, sl):
+    from parparpar_b200 import par2
+    rows = rng.integers(0, 256, (45, sl + 7), dtype=np.uint8)
+    got = par2.memory_checksums(rows, sl, ctx=ctx)
+    assert (got == oracle.par2_memory_checksums(rows[:, :sl], sl)).all()
+
+
+@gpu
+@pytest.mark.parametrize("sl,shrink", [(4096, 4096), (4096, 1002), (1 << 20, (1 << 20) - 6)])
+def test_proc_outputs_pass_the_memory_checksum(ctx, oracle, rng, sl, shrink):
+    """Every processor output reports valid: the checksum blocks attached at
+    staging, multiplied with the data, equal the checksums of the outputs."""
+    from parparpar_b200 import par2
+    n, exps = 20, [0, 3, 9]
+    data = rng.integers(0, 256, (n, shrink), dtype=np.uint8)
+    proc = par2.PAR2ProcCUDA(sl, ctx=ctx)
+    proc.setCurrentSliceSize(shrink)
+    proc.setRecoverySlices(len(exps), exps)
+    for i in range(n):
+        proc.addInput(data[i], shrink, i, flush=(i == 7))
+    proc.endInput()
+    want = oracle.par2_muladd(list(data), shrink, oracle.par2_coeff_matrix(np.arange(n), exps))
+    for o in range(len(exps)):
+        buf = np.zeros(shrink, dtype=np.uint8)
+        assert proc.getOutput(o, buf) is True
+        assert (buf == want[o]).all()
+    proc.deinit()

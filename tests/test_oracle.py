@@ -220,3 +220,28 @@ def test_par3_hash_oracle_vs_reference(oracle, reference, rng):
         assert (oracle.par3_block_hashes(b, 2**40, after) == reference.par3_block_hashes(b, 2**40, after)).all()
         assert (oracle.par3_recovery_packets(b, b"idid-idi", 77) ==
                 reference.par3_recovery_packets(b, b"idid-idi", 77)).all()
+
+
+# ------------------------------------------------------- PAR2 memory checksum
+def test_memory_checksum_is_carried_by_the_region_product(oracle, rng):
+    """The staging checksum is GF(2^16)-linear: the region product of the
+    inputs' checksum blocks equals the checksum of the product (what lets the
+    processor carry it as one more block per row)."""
+    n, sl = 9, 100
+    data = rng.integers(0, 256, (n, sl), dtype=np.uint8)
+    ck = oracle.par2_memory_checksums(data, sl)
+    co = oracle.par2_coeff_matrix(np.arange(n), [0, 1, 5, 65534])
+    prod = oracle.par2_muladd(list(data), sl, co)
+    carried = oracle.par2_muladd(list(ck), 16, co)
+    assert (oracle.par2_memory_checksums(prod, sl) == carried).all()
+
+
+def test_memory_checksum_detects_single_bit_errors(oracle, rng):
+    sl = 72
+    row = rng.integers(0, 256, (1, sl), dtype=np.uint8)
+    base = oracle.par2_memory_checksums(row, sl)
+    for byte in range(sl):
+        for bit in range(8):
+            bad = row.copy()
+            bad[0, byte] ^= 1 << bit
+            assert (oracle.par2_memory_checksums(bad, sl) != base).any(), (byte, bit)
