@@ -51,6 +51,7 @@ extern "C" {
 #define PP_ERR_UNSUPPORTED (-8)
 #define PP_ERR_TIMEOUT (-9)       /* a bounded device-side wait gave up (kernel returned early) */
 #define PP_ERR_TOO_LARGE (-10)    /* size above a fixed maximum of an allocation-free entry point */
+#define PP_ERR_IO (-11)           /* a file could not be opened or read (streaming create) */
 
 /* reference PAR2ProcBackendAddResult (gf16/controller.h:38-43) */
 #define PP_PROC_ADD_OK 0
@@ -342,6 +343,33 @@ PP_API int pp_par3_create_packets(pp_ctx* ctx, const uint64_t* inputs, size_t nu
                                   uint64_t first_input, size_t num_recovery, uint64_t first_recovery,
                                   const uint8_t* data_after_checksum, uint8_t* data_hashes,
                                   const uint8_t* input_set_id, uint8_t* packets);
+
+/* Streaming PAR3 create from a file (replaces par3_create_streaming,
+ * src/gf64_create_streaming.cc:93-245): the file at source_path is cut into
+ * ceil(size / block_size) input blocks, the last zero-padded; recovery
+ * receives the num_recovery recovery blocks first_recovery.. of inputs
+ * first_input.. (num_recovery x block_size bytes, host or device), as
+ * ComputeRecoveryBlocksFull.  The file is read in chunks by parallel preads
+ * into pinned buffers; each chunk is copied to the device and multiplied into
+ * the recovery while the next chunk is read, so reading, copying and the
+ * products overlap and the input is never held whole in memory.  With
+ * data_hashes not NULL, every input block's data-packet checksum (as
+ * pp_par3_block_hashes with first_index = first_input and
+ * data_after_checksum) is computed from the same staged chunks
+ * (ceil(size / block_size) x 16 bytes).  block_size must be a positive
+ * multiple of 8 and num_recovery positive (PP_ERR_INVALID_ARG, the
+ * reference's RangeErrors); a file that cannot be opened or read, or is
+ * empty, gives PP_ERR_IO with the reference's message. */
+typedef struct pp_stream_stats {
+  uint64_t bytes_read;  /* file bytes read */
+  uint64_t num_inputs;  /* input blocks */
+  double seconds;       /* wall time of the call */
+  double read_seconds;  /* time spent waiting for file reads */
+} pp_stream_stats;
+PP_API int pp_par3_create_streaming(pp_ctx* ctx, const char* source_path, size_t block_size, size_t num_recovery,
+                                    uint64_t first_input, uint64_t first_recovery, uint8_t* recovery,
+                                    const uint8_t* data_after_checksum, uint8_t* data_hashes,
+                                    pp_stream_stats* stats);
 
 /* ------------------------------------------------------------ batches
  * No counterpart in the reference (it runs one job at a time on its CPU

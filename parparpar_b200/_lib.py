@@ -25,6 +25,7 @@ PP_ERR_NO_DEVICE = -7
 PP_ERR_UNSUPPORTED = -8
 PP_ERR_TIMEOUT = -9
 PP_ERR_TOO_LARGE = -10
+PP_ERR_IO = -11
 PP_NOALLOC_SOLVE_MAX_N = 4096
 
 PP_GF16_KERNEL_AUTO = 0
@@ -60,7 +61,7 @@ EXPORTS = [
     "pp_server_create", "pp_server_submit", "pp_server_wait", "pp_server_get_stats", "pp_server_reset_stats",
     "pp_server_last_error", "pp_server_destroy",
     "pp_par2_block_hashes", "pp_par3_block_hashes", "pp_par3_assemble_recovery_packets",
-    "pp_par2_create_hashed", "pp_par3_create_packets", "pp_par2_memory_checksums",
+    "pp_par2_create_hashed", "pp_par3_create_packets", "pp_par2_memory_checksums", "pp_par3_create_streaming",
 ]
 
 
@@ -144,6 +145,15 @@ _sig("pp_gf64_solve_and_reconstruct_noalloc", _I, _P, _P, _SZ, _SZ, _P)
 _sig("pp_gf64_repair", _I, _P, _P, _SZ, _P, _SZ, _P, _P, _SZ, _U64, _U64, _P)
 _sig("pp_par2_block_hashes", _I, _P, _P, _SZ, _SZ, _SZ, _P, _P)
 _sig("pp_par2_memory_checksums", _I, _P, _P, _SZ, _SZ, _SZ, _P)
+
+
+class PPStreamStats(ctypes.Structure):
+    _fields_ = [("bytes_read", ctypes.c_uint64), ("num_inputs", ctypes.c_uint64), ("seconds", ctypes.c_double),
+                ("read_seconds", ctypes.c_double)]
+
+
+_sig("pp_par3_create_streaming", _I, _P, ctypes.c_char_p, _SZ, _SZ, _U64, _U64, _P, _P, _P,
+     ctypes.POINTER(PPStreamStats))
 _sig("pp_par2_create_hashed", _I, _P, _P, _SZ, _U, _SZ, _P, _P, _U, _P, _SZ, _P)
 _sig("pp_par3_block_hashes", _I, _P, _P, _SZ, _SZ, _SZ, _U64, _P, _P)
 _sig("pp_par3_assemble_recovery_packets", _I, _P, _P, _SZ, _SZ, _P, _U64, _P)

@@ -7,9 +7,14 @@
 #include "../../include/parpar_b200.h"
 
 #include <cuda_runtime.h>
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
+#include <cerrno>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -19,6 +24,7 @@
 #include <list>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pp_internal.h"
@@ -71,7 +77,7 @@ const Gf16Host& gf16h() {
 }  // namespace
 
 // -------------------------------------------------------------------- ctx
-enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_AEXP, S_HASH, S_HCV, S_PKT, S_NSLOTS };
+enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_AEXP, S_HASH, S_HCV, S_PKT, S_STREAM, S_NSLOTS };
 
 struct CauchyEntry {
   size_t n_in, n_rec;
@@ -109,6 +115,8 @@ struct pp_ctx {
   cudaEvent_t copy_ev = nullptr, start_ev = nullptr;
   cudaStream_t hash = nullptr;     // block hashes of staged inputs, beside the region kernels
   cudaEvent_t hash_ev = nullptr, staged_ev = nullptr;
+  uint8_t* pinned = nullptr;       // streaming reads: two pinned chunk buffers
+  size_t pinned_n = 0;
   std::mutex mu;
 };
 
@@ -240,6 +248,7 @@ PP_API const char* pp_status_string(int s) {
     case PP_ERR_UNSUPPORTED: return "unsupported";
     case PP_ERR_TIMEOUT: return "device wait timed out";
     case PP_ERR_TOO_LARGE: return "size above the entry point's fixed maximum";
+    case PP_ERR_IO: return "file open or read failed";
     default: return "unknown status";
   }
 }
@@ -312,6 +321,7 @@ PP_API void pp_ctx_destroy(pp_ctx* ctx) {
   if (ctx->copy) cudaStreamDestroy(ctx->copy);
   if (ctx->copy_ev) cudaEventDestroy(ctx->copy_ev);
   if (ctx->start_ev) cudaEventDestroy(ctx->start_ev);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->hash) cudaStreamDestroy(ctx->hash);
   if (ctx->hash_ev) cudaEventDestroy(ctx->hash_ev);
   if (ctx->staged_ev) cudaEventDestroy(ctx->staged_ev);
@@ -1941,6 +1951,187 @@ PP_API int pp_par2_memory_checksums(pp_ctx* ctx, const void* rows, size_t row_st
   if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(out16, dout, 16 * num_rows, cudaMemcpyDefault, ctx->stream));
   if (!out_dev || drows != rows) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return PP_OK;
+}
+
+// ------------------------------------------------------------ streaming create
+namespace {
+// pread `n` bytes at `off` with `threads` parallel readers; returns 0, an
+// errno, or -1 for a file that ended early
+int pread_all(int fd, uint8_t* dst, size_t n, uint64_t off, unsigned threads) {
+  std::atomic<int> err{0};
+  auto work = [&](size_t a, size_t b) {
+    size_t pos = a;
+    while (pos < b && !err.load(std::memory_order_relaxed)) {
+      ssize_t r = ::pread(fd, dst + pos, b - pos, (off_t)(off + pos));
+      if (r < 0) {
+        if (errno == EINTR) continue;
+        err = errno;
+        return;
+      }
+      if (r == 0) {
+        err = -1;
+        return;
+      }
+      pos += (size_t)r;
+    }
+  };
+  const size_t per = std::max<size_t>((size_t)4 << 20, (n + threads - 1) / threads);
+  std::vector<std::thread> ts;
+  for (size_t a = per; a < n; a += per) ts.emplace_back(work, a, std::min(n, a + per));
+  work(0, std::min(n, per));
+  for (auto& t : ts) t.join();
+  return err.load();
+}
+}  // namespace
+
+PP_API int pp_par3_create_streaming(pp_ctx* ctx, const char* source_path, size_t block_size, size_t num_recovery,
+                                    uint64_t first_input, uint64_t first_recovery, uint8_t* recovery,
+                                    const uint8_t* data_after_checksum, uint8_t* data_hashes,
+                                    pp_stream_stats* stats) {
+  using clk = std::chrono::steady_clock;
+  const auto t_start = clk::now();
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_recovery == 0) return set_err(ctx, PP_ERR_INVALID_ARG, "recoverySlices must be a positive integer");
+  if (block_size == 0 || block_size % 8)
+    return set_err(ctx, PP_ERR_INVALID_ARG, "blockSize must be positive and a multiple of 8");
+  if (!source_path || !recovery || (data_hashes && !data_after_checksum))
+    return set_err(ctx, PP_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const int fd = ::open(source_path, O_RDONLY);
+  if (fd < 0) {
+    const int e = errno;
+    return set_err(ctx, PP_ERR_IO, "open failed for sourcePath: errno=%d (%s)", e, strerror(e));
+  }
+  struct FdGuard {
+    int fd;
+    ~FdGuard() { ::close(fd); }
+  } guard{fd};
+  struct stat st;
+  if (::fstat(fd, &st) != 0) {
+    const int e = errno;
+    return set_err(ctx, PP_ERR_IO, "fstat failed: errno=%d (%s)", e, strerror(e));
+  }
+  if (st.st_size <= 0) return set_err(ctx, PP_ERR_IO, "sourcePath is empty");
+  const uint64_t total = (uint64_t)st.st_size;
+  const size_t bs = block_size, B = bs / 8;
+  const size_t N = (size_t)((total + bs - 1) / bs);
+  const size_t R = num_recovery;
+  int rc;
+  uint64_t* M = cauchy_get(ctx, N, R, first_input, first_recovery, &rc);
+  if (!M) return rc;
+  // chunks of about 64 MiB of whole blocks; two pinned and two device buffers
+  const size_t chunk = std::max<size_t>(1, ((size_t)64 << 20) / bs);
+  const size_t cbytes = chunk * bs;
+  if (ctx->pinned_n < 2 * cbytes) {
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_n = 0;
+    if (cudaMallocHost(&ctx->pinned, 2 * cbytes) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(ctx, PP_ERR_NO_MEMORY, "pinned read buffers (%zu bytes)", 2 * cbytes);
+    }
+    ctx->pinned_n = 2 * cbytes;
+  }
+  uint8_t* dbuf = (uint8_t*)scratch(ctx, S_STREAM, 2 * cbytes);
+  const bool out_dev = is_device_ptr(recovery);
+  uint64_t* drec = out_dev ? (uint64_t*)recovery : (uint64_t*)scratch(ctx, S_OUT, R * bs);
+  if (!dbuf || !drec) return set_err(ctx, PP_ERR_NO_MEMORY, "streaming device buffers");
+  if (int r = ensure_copy_stream(ctx)) return r;
+  B3Job hj;
+  uint32_t* hcv = nullptr;
+  uint8_t* dh = nullptr;
+  if (data_hashes) {
+    if (int r = ensure_hash_stream(ctx)) return r;
+    uint8_t after[24];
+    if (int r = host_bytes(ctx, data_after_checksum, 24, after)) return r;
+    dh = is_device_ptr(data_hashes) ? data_hashes : (uint8_t*)scratch(ctx, S_HASH, 16 * N);
+    const size_t sw = blake3_scratch_words(chunk, 32 + (uint64_t)bs);
+    hcv = sw ? (uint32_t*)scratch(ctx, S_HCV, sw * 4) : nullptr;
+    if (!dh || (sw && !hcv)) return set_err(ctx, PP_ERR_NO_MEMORY, "hash buffers");
+    hj.P = 32;
+    for (int k = 0; k < 6; k++) hj.pre[k] = le32(after + 4 * k);
+    hj.stride = bs;
+    hj.D = bs;
+    hj.hash_stride = 16;
+  }
+  // per device buffer: the copy into it waits for the work that last read it
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int i = 0; i < 4; i++)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } eg{ev};
+  for (int i = 0; i < 4; i++)
+    if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(ctx, PP_ERR_CUDA, "streaming events");
+    }
+  cudaEvent_t* freed = ev;       // [2]: the product (and hash) of the buffer's last chunk is done
+  cudaEvent_t* copied = ev + 2;  // [2]: the buffer's copy to the device is done
+  const unsigned readers = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  double read_s = 0;
+  auto read_chunk = [&](size_t c, uint8_t* dst) -> int {
+    const uint64_t off = (uint64_t)c * cbytes;
+    const size_t want = (size_t)std::min<uint64_t>(cbytes, total - off);
+    const size_t nblk = std::min(chunk, N - c * chunk);
+    const auto t0 = clk::now();
+    const int e = pread_all(fd, dst, want, off, readers);
+    read_s += std::chrono::duration<double>(clk::now() - t0).count();
+    if (e == -1) return set_err(ctx, PP_ERR_IO, "unexpected EOF while reading sourcePath");
+    if (e) return set_err(ctx, PP_ERR_IO, "read failed: errno=%d (%s)", e, strerror(e));
+    if (want < nblk * bs) memset(dst + want, 0, nblk * bs - want);  // zero-pad the last block
+    return PP_OK;
+  };
+  const size_t nchunks = (N + chunk - 1) / chunk;
+  CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));  // scratch is free once earlier work is done
+  CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
+  if (int r = read_chunk(0, ctx->pinned)) return r;
+  for (size_t c = 0; c < nchunks; c++) {
+    const int slot = (int)(c & 1);
+    const size_t c0 = c * chunk, nc = std::min(chunk, N - c0);
+    uint8_t* h = ctx->pinned + slot * cbytes;
+    uint8_t* d = dbuf + slot * cbytes;
+    if (c >= 2) CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, freed[slot], 0));
+    CUDA_TRY(ctx, cudaMemcpyAsync(d, h, nc * bs, cudaMemcpyHostToDevice, ctx->copy));
+    CUDA_TRY(ctx, cudaEventRecord(copied[slot], ctx->copy));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, copied[slot], 0));
+    CUDA_TRY(ctx, gf64_region(ctx, (const uint64_t*)d, nullptr, B, nc, B, M + c0, N, R, drec, nullptr, B, c > 0,
+                              aligned_rows64((const uint64_t*)d, B) && aligned_rows64(drec, B)));
+    if (data_hashes) {
+      CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, copied[slot], 0));
+      B3Job J = hj;
+      J.data = d;
+      J.n = nc;
+      J.first_index = first_input + c0;
+      J.hash_out = dh + 16 * c0;
+      CUDA_TRY(ctx, launch_blake3_blocks(J, hcv, ctx->hash));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->hash_ev, ctx->hash));
+      CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->hash_ev, 0));
+    }
+    CUDA_TRY(ctx, cudaEventRecord(freed[slot], ctx->stream));
+    if (c + 1 < nchunks) {
+      // the other pinned buffer is free once its copy (chunk c - 1) is done
+      if (c >= 1) CUDA_TRY(ctx, cudaEventSynchronize(copied[slot ^ 1]));
+      if (int r = read_chunk(c + 1, ctx->pinned + (slot ^ 1) * cbytes)) {
+        cudaStreamSynchronize(ctx->stream);
+        return r;
+      }
+    }
+  }
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(recovery, drec, R * bs, cudaMemcpyDeviceToHost, ctx->stream));
+  if (data_hashes && dh != data_hashes)
+    CUDA_TRY(ctx, cudaMemcpyAsync(data_hashes, dh, 16 * N, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (stats) {
+    stats->bytes_read = total;
+    stats->num_inputs = N;
+    stats->seconds = std::chrono::duration<double>(clk::now() - t_start).count();
+    stats->read_seconds = read_s;
+  }
+  return device_status(ctx);
 }
 
 }  // extern "C"

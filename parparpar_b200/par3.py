@@ -404,3 +404,63 @@ def create_packets(inputs, num_inputs, block_size64, first_input, num_recovery, 
                                        _u64(first_recovery), ptr(ac), ptr(data_hashes) if ac is not None else 0,
                                        ptr(sid), ptr(packets)))
     return packets, data_hashes
+
+
+def par3_create_streaming(sourcePath, options, callback=None, recovery=None, data_hashes=None,
+                          data_after_checksum=None, ctx=None):
+    """gf64_addon par3_create_streaming(sourcePath, options, callback)
+    (src/gf64_create_streaming.cc:93-506): PAR3 recovery blocks of a whole
+    file, read in pipelined chunks and multiplied on the device.
+
+    options: recoverySlices (required, > 0), blockSize (required, positive
+    multiple of 8), firstInput, firstRecovery (default 0), numThreads and
+    useMmap (accepted for parity; the reader uses parallel preads into pinned
+    memory).  Result: {recoveryBytes, throughputMBps, durationMs,
+    recoveryBuffer}; with callback, callback(err, result) is called instead of
+    returning / raising (the reference's async completion).  Optional
+    data_hashes (+ data_after_checksum) receive the input blocks' data-packet
+    checksums from the same pass."""
+    if not isinstance(options, dict):
+        raise TypeError("options must be an object")
+    if "recoverySlices" not in options:
+        raise TypeError("options.recoverySlices is required")
+    if "blockSize" not in options:
+        raise TypeError("options.blockSize is required")
+    R, bs = options["recoverySlices"], options["blockSize"]
+    if isinstance(bs, bool) or not isinstance(bs, (int, np.integer)):
+        raise TypeError("blockSize must be an integer")
+    if isinstance(R, bool) or not isinstance(R, (int, np.integer)) or R <= 0:
+        raise ValueError("recoverySlices must be a positive integer")
+    if bs <= 0 or bs % 8:
+        raise ValueError("blockSize must be positive and a multiple of 8")
+    fI = options.get("firstInput") or 0
+    fR = options.get("firstRecovery") or 0
+    for v, name in ((fI, "firstInput"), (fR, "firstRecovery")):
+        if isinstance(v, bool) or not isinstance(v, (int, np.integer)):
+            raise TypeError(f"{name} must be a Number or BigInt")
+    c = _ctx(ctx)
+    if recovery is None:
+        recovery = np.zeros(int(R) * int(bs), dtype=np.uint8)
+    ac = None
+    if data_hashes is not None:
+        ac = np.frombuffer(bytes(data_after_checksum), dtype=np.uint8)
+        if ac.size != 24:
+            raise ValueError("data_after_checksum must be 24 bytes")
+    st = _lib.PPStreamStats()
+    status = lib.pp_par3_create_streaming(c.h, str(sourcePath).encode(), int(bs), int(R), _u64(fI), _u64(fR),
+                                          ptr(recovery), ptr(ac), ptr(data_hashes), ctypes.byref(st))
+    if status != PP_OK:
+        err = PPError(status, lib.pp_ctx_last_error(c.h).decode())
+        if callback is not None:
+            callback(err, None)
+            return None
+        raise err
+    rbytes = int(R) * int(bs)
+    ms = st.seconds * 1e3
+    result = {"recoveryBytes": rbytes, "throughputMBps": (rbytes / 1048576.0) / st.seconds if st.seconds else 0.0,
+              "durationMs": ms, "recoveryBuffer": recovery, "bytesRead": int(st.bytes_read),
+              "numInputs": int(st.num_inputs), "readMs": st.read_seconds * 1e3}
+    if callback is not None:
+        callback(None, result)
+        return None
+    return result

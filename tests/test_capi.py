@@ -101,3 +101,21 @@ def test_assemble_recovery_packets_argument_errors():
         par3.assemble_recovery_packets(rec, b"12345678", 0, 2, 64)
     with pytest.raises(ValueError):
         par3.assemble_recovery_packets(rec, b"12345678", 0, 1 << 21, 1 << 20)
+
+
+def test_create_streaming_argument_errors():
+    """par3_create_streaming's option checks (src/gf64_create_streaming.cc:
+    365-430) run before any device work."""
+    from parparpar_b200 import par3
+    with pytest.raises(TypeError):
+        par3.par3_create_streaming("x", None)
+    with pytest.raises(TypeError):
+        par3.par3_create_streaming("x", {"blockSize": 64})
+    with pytest.raises(TypeError):
+        par3.par3_create_streaming("x", {"recoverySlices": 1})
+    with pytest.raises(ValueError):
+        par3.par3_create_streaming("x", {"recoverySlices": 0, "blockSize": 64})
+    with pytest.raises(ValueError):
+        par3.par3_create_streaming("x", {"recoverySlices": 1, "blockSize": 60})
+    with pytest.raises(TypeError):
+        par3.par3_create_streaming("x", {"recoverySlices": 1, "blockSize": 64, "firstInput": 1.5})

@@ -314,3 +314,55 @@ def test_proc_outputs_pass_the_memory_checksum(ctx, oracle, rng, sl, shrink):
         assert proc.getOutput(o, buf) is True
         assert (buf == want[o]).all()
     proc.deinit()
+
+
+# ------------------------------------------------------- streaming create
+def _file(tmp_path, name, data):
+    p = tmp_path / name
+    p.write_bytes(bytes(data))
+    return str(p)
+
+
+@gpu
+@pytest.mark.parametrize("size,bs", [(1, 8), (8 * 1000 + 3, 64), (200 * 1024 * 1024 + 13, 8192)])
+def test_par3_create_streaming_matches_in_memory_create(ctx, oracle, rng, tmp_path, size, bs):
+    """Recovery from a file, read in pipelined chunks (the 200 MiB case spans
+    four 64 MiB chunks), equals the create over the zero-padded blocks; the
+    data-block hashes come from the same pass."""
+    from parparpar_b200 import par3
+    data = rng.integers(0, 256, size, dtype=np.uint8)
+    path = _file(tmp_path, "src.bin", data)
+    n = (size + bs - 1) // bs
+    blocks = np.zeros(n * bs, dtype=np.uint8)
+    blocks[:size] = data
+    R, fI, fR = 5, 2, n + 9
+    after = bytes(range(7, 31))
+    hashes = np.zeros((n, 16), dtype=np.uint8)
+    res = par3.par3_create_streaming(path, {"recoverySlices": R, "blockSize": bs, "firstInput": fI,
+                                            "firstRecovery": fR}, data_hashes=hashes, data_after_checksum=after,
+                                     ctx=ctx)
+    assert res["recoveryBytes"] == R * bs and res["numInputs"] == n and res["bytesRead"] == size
+    x = blocks.view(np.uint64).reshape(n, bs // 8)
+    want = np.zeros((R, bs // 8), dtype=np.uint64)
+    par3.GF64Controller.ComputeRecoveryBlocks(x, n, want, R, bs // 8, fI, fR)
+    assert (res["recoveryBuffer"].view(np.uint64).reshape(R, -1) == want).all()
+    if n <= 2000:
+        assert (want == oracle.gf64_compute_recovery(x, R, fI, fR)).all()
+    rows = np.linspace(0, n - 1, min(n, 100)).astype(np.int64)
+    b8 = blocks.reshape(n, bs)
+    want_h = np.stack([oracle.par3_block_hashes(b8[i:i + 1], fI + int(i), after)[0] for i in rows])
+    assert (hashes[rows] == want_h).all()
+
+
+@gpu
+def test_par3_create_streaming_errors(ctx, tmp_path):
+    import parparpar_b200 as pp
+    from parparpar_b200 import par3
+    with pytest.raises(pp.PPError) as e:
+        par3.par3_create_streaming(str(tmp_path / "missing.bin"), {"recoverySlices": 2, "blockSize": 64}, ctx=ctx)
+    assert e.value.status == pp.PP_ERR_IO and "open failed for sourcePath" in str(e.value)
+    empty = _file(tmp_path, "empty.bin", b"")
+    got = []
+    par3.par3_create_streaming(empty, {"recoverySlices": 2, "blockSize": 64}, callback=lambda err, r: got.append((err, r)),
+                               ctx=ctx)
+    assert got[0][1] is None and got[0][0].status == pp.PP_ERR_IO and "sourcePath is empty" in str(got[0][0])
