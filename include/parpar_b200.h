@@ -308,6 +308,17 @@ PP_API int pp_par2_create_hashed(pp_ctx* ctx, const void* inputs, size_t input_s
 PP_API int pp_par2_memory_checksums(pp_ctx* ctx, const void* rows, size_t row_stride, size_t num_rows,
                                     size_t slice_bytes, uint8_t* out16);
 
+/* PAR2 recovery-slice packet headers (getRecoveryHeader with the packet MD5
+ * of _pullRecData / _getRecoveryPacketMD5, lib/par2.js:240-330,517-530):
+ * headers receives num_slices x 68 bytes -- "PAR2\0PKT", u64le(68 +
+ * slice_bytes), the MD5 of packet bytes [32, 68 + slice_bytes) (set id,
+ * "PAR 2.0\0RecvSlic", u32le(exps[i]), slice i), the 16-byte set id, the type
+ * and u32le(exps[i]); the packet is this header followed by the slice.
+ * slice_bytes a multiple of 4 (PAR2). set_id is host or device memory. */
+PP_API int pp_par2_recovery_packet_headers(pp_ctx* ctx, const void* slices, size_t slice_stride, size_t num_slices,
+                                           size_t slice_bytes, const uint8_t* set_id, const uint16_t* exps,
+                                           uint8_t* headers);
+
 /* PAR3 data-block checksums (lib/par3gen.js:1001-1017, _inlineHashBlock):
  * hashes[16*i..] = BLAKE3(after_checksum[0..24) || u64le(first_index + i) ||
  * block_i)[0..16), block_i = block_size bytes at blocks + i * block_stride.

@@ -210,6 +210,22 @@ def par2_block_hashes(blocks: np.ndarray, slice_size: int, lengths=None) -> np.n
     return out
 
 
+def par2_recovery_packet_headers(slices: np.ndarray, exps, set_id: bytes, slice_size: int) -> np.ndarray:
+    """lib/par2.js:240-330 (packet MD5 over set id, type, u32le exponent and
+    the slice) and :517-530 (getRecoveryHeader: magic, u64le length, MD5, set
+    id, type, exponent); MD5 from hashlib."""
+    import hashlib
+
+    n = slices.shape[0]
+    out = np.zeros((n, 68), dtype=np.uint8)
+    for i in range(n):
+        body = bytes(set_id) + b"PAR 2.0\x00RecvSlic" + int(exps[i]).to_bytes(4, "little")
+        md5 = hashlib.md5(body + slices[i, :slice_size].tobytes()).digest()
+        hdr = b"PAR2\x00PKT" + (68 + slice_size).to_bytes(8, "little") + md5 + body
+        out[i] = np.frombuffer(hdr, dtype=np.uint8)
+    return out
+
+
 def pattern_bytes(n: int, seed: int) -> np.ndarray:
     """Deterministic pseudo-random bytes (a multiplicative hash of the index),
     independent of any RNG implementation; fixtures store only outputs."""

@@ -2134,4 +2134,37 @@ PP_API int pp_par3_create_streaming(pp_ctx* ctx, const char* source_path, size_t
   return device_status(ctx);
 }
 
+PP_API int pp_par2_recovery_packet_headers(pp_ctx* ctx, const void* slices, size_t slice_stride, size_t num_slices,
+                                           size_t slice_bytes, const uint8_t* set_id, const uint16_t* exps,
+                                           uint8_t* headers) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (num_slices == 0) return PP_OK;
+  if (!slices || !set_id || !exps || !headers) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  if (slice_bytes % 4) return set_err(ctx, PP_ERR_INVALID_ARG, "PAR2 slice size must be a multiple of 4");
+  if (num_slices > 1 && slice_stride < slice_bytes)
+    return set_err(ctx, PP_ERR_INVALID_ARG, "slice_stride < slice_bytes");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  uint8_t sid[16];
+  if (int r = host_bytes(ctx, set_id, 16, sid)) return r;
+  uint32_t pre[8];
+  for (int k = 0; k < 4; k++) pre[k] = le32(sid + 4 * k);
+  static const uint8_t type[16] = {'P', 'A', 'R', ' ', '2', '.', '0', 0, 'R', 'e', 'c', 'v', 'S', 'l', 'i', 'c'};
+  for (int k = 0; k < 4; k++) pre[4 + k] = le32(type + 4 * k);
+  int st = PP_OK;
+  size_t dstride = 0;
+  const uint8_t* drows =
+      rows_on_device(ctx, S_IN, slices, slice_stride, num_slices, slice_bytes, slice_bytes, true, &dstride, &st);
+  if (!drows) return st;
+  const uint16_t* dex = to_device(ctx, S_A, exps, num_slices, &st);
+  if (st) return st;
+  const bool out_dev = is_device_ptr(headers) && ((uintptr_t)headers % 4) == 0;
+  uint8_t* dout = out_dev ? headers : (uint8_t*)scratch(ctx, S_OUT, 68 * num_slices);
+  if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "header output");
+  CUDA_TRY(ctx, launch_par2_packet_headers(drows, dstride, num_slices, slice_bytes, pre, dex, dout, ctx->stream));
+  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(headers, dout, 68 * num_slices, cudaMemcpyDefault, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
 }  // extern "C"

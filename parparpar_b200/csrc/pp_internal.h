@@ -161,4 +161,11 @@ cudaError_t launch_par3_packet_headers(uint8_t* d_pkts, size_t n, size_t block_s
 cudaError_t launch_par2_cksum(const uint8_t* d_rows, size_t stride, size_t n, uint64_t len, uint8_t* d_out,
                               size_t out_stride, int* d_valid, cudaStream_t s);
 
+// PAR2 recovery packet headers (68 bytes each, MD5 included) of n slices of
+// `slice` bytes (a multiple of 4; rows 4-byte aligned); pre = set id and
+// type words; d_out 4-byte aligned.
+cudaError_t launch_par2_packet_headers(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
+                                       const uint32_t pre[8], const uint16_t* d_exps, uint8_t* d_out,
+                                       cudaStream_t s);
+
 }  // namespace pp

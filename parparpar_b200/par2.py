@@ -230,7 +230,8 @@ class PAR2ProcCUDA:
 
 
 __all__ = ["PAR2ProcCUDA", "Galois16RecMatrix", "gf16_muladd", "par2_create", "coeff_matrix", "gfmat_coeff",
-           "gfmat_input_log", "PPError", "block_hashes", "HasherInput", "memory_checksums"]
+           "gfmat_input_log", "PPError", "block_hashes", "HasherInput", "memory_checksums",
+           "recovery_packet_headers"]
 
 
 # ------------------------------------------------------------ block hashes
@@ -347,4 +348,24 @@ def memory_checksums(rows, slice_size=None, out=None, ctx=None):
     if out is None:
         out = np.empty((n, 16), dtype=np.uint8)
     c.check(lib.pp_par2_memory_checksums(c.h, ptr(rows), stride, n, slice_size, ptr(out)))
+    return out
+
+
+def recovery_packet_headers(slices, exps, set_id, slice_size=None, out=None, ctx=None):
+    """68-byte PAR2 recovery packet headers with their MD5s (getRecoveryHeader
+    and the packet MD5 of lib/par2.js:240-330,517-530): row i describes
+    recovery slice ``slices[i]`` with exponent ``exps[i]``."""
+    c = _ctx(ctx)
+    n, row_bytes, stride = _rows(slices)
+    slice_size = row_bytes if slice_size is None else int(slice_size)
+    ex = np.ascontiguousarray(np.asarray(exps, dtype=np.uint16))
+    if ex.size != n:
+        raise ValueError("one exponent per slice")
+    sid = np.frombuffer(bytes(set_id), dtype=np.uint8)
+    if sid.size != 16:
+        raise ValueError("set_id must be 16 bytes")
+    if out is None:
+        out = np.empty((n, 68), dtype=np.uint8)
+    c.check(lib.pp_par2_recovery_packet_headers(c.h, ptr(slices), stride, n, slice_size, ptr(sid), ptr(ex),
+                                                ptr(out)))
     return out

@@ -366,3 +366,16 @@ def test_par3_create_streaming_errors(ctx, tmp_path):
     par3.par3_create_streaming(empty, {"recoverySlices": 2, "blockSize": 64}, callback=lambda err, r: got.append((err, r)),
                                ctx=ctx)
     assert got[0][1] is None and got[0][0].status == pp.PP_ERR_IO and "sourcePath is empty" in str(got[0][0])
+
+
+@gpu
+@pytest.mark.parametrize("sl", [4, 28, 32, 60, 1000, 32768, 1 << 20])
+def test_par2_recovery_packet_headers(ctx, rng, sl):
+    from oracle import par2_recovery_packet_headers as want_hdr
+    from parparpar_b200 import par2
+    n = 9
+    slices = rng.integers(0, 256, (n, sl), dtype=np.uint8)
+    exps = [0, 1, 2, 100, 65534, 7, 8, 9, 31000]
+    sid = rng.integers(0, 256, 16, dtype=np.uint8).tobytes()
+    got = par2.recovery_packet_headers(slices, exps, sid, ctx=ctx)
+    assert (got == want_hdr(slices, exps, sid, sl)).all()
