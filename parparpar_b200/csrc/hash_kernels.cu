@@ -4,8 +4,9 @@
 //    followed by zero padding up to the slice size -- the 20-byte IFSC entry
 //    that HasherInput::getBlock(md5crc, zeroPad) produces
 //    (hasher/hasher_input_base.h:104-117).  MD5 is a serial chain within a
-//    message, so one thread owns one slice's MD5 and a partner thread in
-//    another warp its CRC32, fed from the same load of each block.
+//    message, so one thread owns one slice and runs MD5 and CRC32 side by side
+//    on the same 64-byte block (one load of each byte, two independent
+//    dependency chains for the scheduler to interleave).
 //  * BLAKE3 of "prefix || block" messages: the PAR3 data-packet checksum of
 //    lib/par3gen.js:1001-1017 (prefix = the packet's 24 post-checksum header
 //    bytes + u64le block index) and the recovery packets of
@@ -114,134 +115,92 @@ __device__ __forceinline__ uint32_t masked_word(const uint8_t* row, uint64_t o, 
   return v;
 }
 
-constexpr int kHashSlices = 128;      // slices per CTA
-constexpr int kStageWords = 20;       // 64-byte block + 16 bytes of padding per slice: conflict-free 16-byte accesses
-constexpr int kStageSlots = 3;
-constexpr int kHashSmem = (kCrcWords + kStageSlots * kHashSlices * kStageWords) * 4;
-
-// Asynchronous copy of message block b of a row into its staging slot:
-// four 16-byte pieces, each zero-filled at and past len (a piece wholly past
-// len reads nothing).
-__device__ __forceinline__ void stage_block(uint32_t* slot, const uint8_t* row, uint64_t b, uint64_t len) {
-  const uint32_t dst = (uint32_t)__cvta_generic_to_shared(slot);
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const uint64_t o = 64 * b + 16 * q;
-    const uint32_t nbytes = o >= len ? 0u : (len - o >= 16 ? 16u : (uint32_t)(len - o));
-    const uint8_t* src = nbytes ? row + o : row;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst + 16 * q), "l"(src), "r"(nbytes)
-                 : "memory");
-  }
-}
-
-// 256 threads per CTA for 128 slices.  Threads 0-127 run MD5, one slice each:
-// they stream the slice's 64-byte message blocks into shared memory with
-// asynchronous copies (two blocks ahead, three staging slots) and compress
-// them.  Threads 128-255 run CRC32 on the same slices from the staged copies
-// (slice-by-4 tables in shared memory).  One named barrier per block makes a
-// staged block visible to both and frees the slot read in the previous step,
-// so the table lookups of CRC32 never stall the in-order issue of the MD5
-// chain and each byte is read from memory once.  Rows 16-byte aligned (data
-// and stride); the message is L bytes: the row's first len bytes, then zeros.
-__global__ void __launch_bounds__(256, 2) k_par2_block_hash(const uint8_t* __restrict__ data, size_t stride,
-                                                            size_t n, uint64_t L,
-                                                            const uint64_t* __restrict__ lengths,
-                                                            uint8_t* __restrict__ out) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  uint32_t* crc_tab = smem;
-  uint32_t* stage = smem + kCrcWords;
-  const bool md5_role = threadIdx.x < kHashSlices;
-  const unsigned t = threadIdx.x % kHashSlices;
-  const size_t i = (size_t)blockIdx.x * kHashSlices + t;
-  const bool live = i < n;
-  const uint8_t* row = data + (live ? i : 0) * stride;
-  const uint64_t len = !live ? 0 : lengths ? (lengths[i] < L ? lengths[i] : L) : L;
-  const uint64_t nblk = L / 64;  // whole message blocks; then one final block of L % 64 bytes (b = nblk)
-  const uint32_t tail = (uint32_t)(L % 64);
-  auto slot_of = [&](uint64_t b) { return stage + ((uint32_t)(b % kStageSlots) * kHashSlices + t) * kStageWords; };
-  if (md5_role) {  // prologue: blocks 0 and 1 in flight
-    stage_block(slot_of(0), row, 0, len);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    if (nblk >= 1) stage_block(slot_of(1), row, 1, len);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  }
+// One thread per slice.  Rows are 16-byte aligned (data and stride).  The
+// message is L bytes: the row's first len bytes, then zeros.
+__global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restrict__ data, size_t stride,
+                                                         size_t n, uint64_t L,
+                                                         const uint64_t* __restrict__ lengths,
+                                                         uint8_t* __restrict__ out) {
+  extern __shared__ uint32_t crc_tab[];
   crc_tables_init(crc_tab);
   __syncthreads();
-  if (md5_role) {
-    uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
-    uint32_t m[16];
-    for (uint64_t b = 0; b <= nblk; b++) {
-      asm volatile("cp.async.wait_group 1;" ::: "memory");  // block b has landed
-      asm volatile("bar.sync 1, 256;" ::: "memory");
-      if (b + 2 <= nblk) stage_block(slot_of(b + 2), row, b + 2, len);  // the slot read in step b - 1
-      asm volatile("cp.async.commit_group;" ::: "memory");
-      const uint4* sl = reinterpret_cast<const uint4*>(slot_of(b));
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t* tk = crc_tab + (threadIdx.x % kCrcCopies);
+  const uint8_t* row = data + i * stride;
+  const uint64_t len = lengths ? (lengths[i] < L ? lengths[i] : L) : L;
+  uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
+  uint32_t crc = 0xFFFFFFFFu;
+  uint32_t m[16];
+
+  // blocks wholly inside the data: 16-byte loads, one block prefetched
+  const uint64_t nfull = len / 64;
+  uint4 nx[4];
+  if (nfull) {
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const uint4 v = sl[q];
-        m[4 * q] = v.x;
-        m[4 * q + 1] = v.y;
-        m[4 * q + 2] = v.z;
-        m[4 * q + 3] = v.w;
-      }
-      if (b < nblk) md5_block(st, m);
-    }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // MD5 padding after the final L % 64 bytes (staged bytes past L are zero)
-#pragma unroll
-    for (int w = 0; w < 16; w++) {
-      const uint32_t lo = 4u * w;
-      if (lo < tail && tail < lo + 4) m[w] &= (1u << (8 * (tail - lo))) - 1u;
-      if (lo <= tail && tail < lo + 4) m[w] |= 0x80u << (8 * (tail - lo));
-    }
-    if (tail >= 56) {
-      md5_block(st, m);
-#pragma unroll
-      for (int w = 0; w < 16; w++) m[w] = 0;
-    }
-    m[14] = (uint32_t)(L << 3);
-    m[15] = (uint32_t)(L >> 29);
-    md5_block(st, m);
-    if (live) {
-      uint32_t* o = reinterpret_cast<uint32_t*>(out + 20 * i);
-      o[0] = st[0];
-      o[1] = st[1];
-      o[2] = st[2];
-      o[3] = st[3];
-    }
-  } else {
-    const uint32_t* tk = crc_tab + (t % kCrcCopies);
-    uint32_t crc = 0xFFFFFFFFu;
-    for (uint64_t b = 0; b <= nblk; b++) {
-      asm volatile("bar.sync 1, 256;" ::: "memory");
-      const uint4* sl = reinterpret_cast<const uint4*>(slot_of(b));
-      uint32_t m[16];
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const uint4 v = sl[q];
-        m[4 * q] = v.x;
-        m[4 * q + 1] = v.y;
-        m[4 * q + 2] = v.z;
-        m[4 * q + 3] = v.w;
-      }
-      if (b < nblk) {
-#pragma unroll
-        for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
-      } else {
-#pragma unroll
-        for (uint32_t w = 0; w < 16; w++) {
-          if (4 * w + 4 <= tail) {
-            crc = crc_word(crc, m[w], tk);
-          } else if (4 * w < tail) {
-#pragma unroll
-            for (uint32_t j = 0; j < 3; j++)
-              if (4 * w + j < tail) crc = crc_byte(crc, (m[w] >> (8 * j)) & 255u, tk);
-          }
-        }
-      }
-    }
-    if (live) reinterpret_cast<uint32_t*>(out + 20 * i)[4] = crc ^ 0xFFFFFFFFu;
+    for (int q = 0; q < 4; q++) nx[q] = __ldg(reinterpret_cast<const uint4*>(row) + q);
   }
+  for (uint64_t b = 0; b < nfull; b++) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      m[4 * q] = nx[q].x;
+      m[4 * q + 1] = nx[q].y;
+      m[4 * q + 2] = nx[q].z;
+      m[4 * q + 3] = nx[q].w;
+    }
+    if (b + 1 < nfull) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) nx[q] = __ldg(reinterpret_cast<const uint4*>(row + 64 * (b + 1)) + q);
+    }
+#pragma unroll
+    for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
+    md5_block(st, m);
+  }
+  // the rest of the L / 64 whole message blocks: data tail, then zero padding
+  const uint64_t nblk = L / 64;
+  for (uint64_t b = nfull; b < nblk; b++) {
+#pragma unroll
+    for (int w = 0; w < 16; w++) m[w] = masked_word(row, 64 * b + 4 * w, len);
+#pragma unroll
+    for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
+    md5_block(st, m);
+  }
+  // final partial block (L % 64 bytes) with the MD5 padding
+  const uint32_t tail = (uint32_t)(L % 64);
+  const uint64_t t0 = 64 * nblk;
+#pragma unroll
+  for (int w = 0; w < 16; w++) m[w] = (4u * w < tail) ? masked_word(row, t0 + 4 * w, len) : 0u;
+#pragma unroll
+  for (uint32_t w = 0; w < 16; w++) {
+    if (4 * w + 4 <= tail) {
+      crc = crc_word(crc, m[w], tk);
+    } else if (4 * w < tail) {
+#pragma unroll
+      for (uint32_t j = 0; j < 3; j++)
+        if (4 * w + j < tail) crc = crc_byte(crc, (m[w] >> (8 * j)) & 255u, tk);
+    }
+  }
+  // clear the bytes at and past `tail` in the last partial word, then 0x80
+#pragma unroll
+  for (int w = 0; w < 16; w++) {
+    const uint32_t lo = 4u * w;
+    if (lo < tail && tail < lo + 4) m[w] &= (1u << (8 * (tail - lo))) - 1u;
+    if (lo <= tail && tail < lo + 4) m[w] |= 0x80u << (8 * (tail - lo));
+  }
+  if (tail >= 56) {
+    md5_block(st, m);
+#pragma unroll
+    for (int w = 0; w < 16; w++) m[w] = 0;
+  }
+  m[14] = (uint32_t)(L << 3);
+  m[15] = (uint32_t)(L >> 29);
+  md5_block(st, m);
+  uint32_t* o = reinterpret_cast<uint32_t*>(out + 20 * i);
+  o[0] = st[0];
+  o[1] = st[1];
+  o[2] = st[2];
+  o[3] = st[3];
+  o[4] = crc ^ 0xFFFFFFFFu;
 }
 
 // PAR2 recovery-slice packet headers (lib/par2.js:517-530 getRecoveryHeader;
@@ -281,15 +240,27 @@ __global__ void __launch_bounds__(64) k_par2_packet_headers(const Par2PktArgs A)
   uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
   uint32_t m[16];
   const uint64_t nblk = T / 64;
+  // blocks after the first are whole data words (message byte 64b + 4w is
+  // data byte 64b + 4w - 36); the next block is loaded while this one is
+  // compressed
+  uint32_t nx[16];
+  if (nblk > 1) {
+    const uint32_t* p = reinterpret_cast<const uint32_t*>(row + 64 - 36);
+#pragma unroll
+    for (int w = 0; w < 16; w++) nx[w] = __ldg(p + w);
+  }
   for (uint64_t b = 0; b < nblk; b++) {
     if (b == 0) {
 #pragma unroll
       for (int w = 0; w < 16; w++) m[w] = pkt_word(A, row, ex, w);
     } else {
-      // whole data words: message byte 64b + 4w is data byte 64b + 4w - 36
-      const uint32_t* p = reinterpret_cast<const uint32_t*>(row + 64 * b - 36);
 #pragma unroll
-      for (int w = 0; w < 16; w++) m[w] = __ldg(p + w);
+      for (int w = 0; w < 16; w++) m[w] = nx[w];
+      if (b + 1 < nblk) {
+        const uint32_t* p = reinterpret_cast<const uint32_t*>(row + 64 * (b + 1) - 36);
+#pragma unroll
+        for (int w = 0; w < 16; w++) nx[w] = __ldg(p + w);
+      }
     }
     md5_block(st, m);
   }
@@ -639,10 +610,12 @@ uint32_t gf16_pow2(uint64_t e) {
 cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
                                    const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_par2_block_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, kHashSmem);
+  const int smem = kCrcWords * 4;
+  cudaError_t e = cudaFuncSetAttribute(k_par2_block_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  k_par2_block_hash<<<(unsigned)((n + kHashSlices - 1) / kHashSlices), 2 * kHashSlices, kHashSmem, s>>>(
-      d_data, stride, n, slice, d_lengths, d_out);
+  const unsigned threads = 128;
+  k_par2_block_hash<<<(unsigned)((n + threads - 1) / threads), threads, smem, s>>>(d_data, stride, n, slice,
+                                                                                   d_lengths, d_out);
   note_launch();
   return cudaGetLastError();
 }
