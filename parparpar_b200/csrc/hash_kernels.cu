@@ -38,6 +38,18 @@ __constant__ uint32_t c_md5k[64] = {
 
 __device__ __forceinline__ uint32_t rotl(uint32_t x, int s) { return __funnelshift_l(x, x, s); }
 
+// BLAKE3 is bound by the integer ALU pipe (its XORs, rotations and adds all
+// issue there) while the FMA pipe idles.  madd is a + b issued as an integer
+// multiply-add with a multiplier the compiler cannot see (`one`, a kernel
+// argument equal to 1), so it executes on the FMA pipe and leaves the ALU pipe
+// to the logic and rotate instructions.  (MD5's adds stay on the ALU: its
+// serial chain is latency-bound and the multiply-add is slower there.)
+__device__ __forceinline__ uint32_t madd(uint32_t a, uint32_t b, uint32_t one) {
+  uint32_t r;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(one), "r"(b));
+  return r;
+}
+
 __device__ __forceinline__ int md5_shift(int i) {
   const int r = i >> 4, k = i & 3;
   if (r == 0) return k == 0 ? 7 : k == 1 ? 12 : k == 2 ? 17 : 22;
@@ -66,9 +78,10 @@ __device__ __forceinline__ void md5_block(uint32_t st[4], const uint32_t m[16]) 
       g = (7 * i) & 15;
     }
     const uint32_t t = d;
+    const uint32_t x = a + c_md5k[i] + m[g];  // off the dependency chain
     d = c;
     c = b;
-    b = b + rotl(a + f + c_md5k[i] + m[g], md5_shift(i));
+    b = b + rotl(x + f, md5_shift(i));
     a = t;
   }
   st[0] += a;
@@ -298,20 +311,22 @@ constexpr uint32_t kB3ChunkStart = 1, kB3ChunkEnd = 2, kB3Parent = 4, kB3Root = 
 
 __device__ __forceinline__ uint32_t rotr(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
 
-__device__ __forceinline__ void b3_g(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t x, uint32_t y) {
-  a = a + b + x;
+// the additions on the FMA pipe (madd), the XORs and rotations on the ALU pipe
+__device__ __forceinline__ void b3_g(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t x, uint32_t y,
+                                     uint32_t one) {
+  a = madd(madd(a, x, one), b, one);
   d = __byte_perm(d ^ a, 0, 0x1032);  // rotr 16
-  c = c + d;
+  c = madd(c, d, one);
   b = rotr(b ^ c, 12);
-  a = a + b + y;
+  a = madd(madd(a, y, one), b, one);
   d = __byte_perm(d ^ a, 0, 0x0321);  // rotr 8
-  c = c + d;
+  c = madd(c, d, one);
   b = rotr(b ^ c, 7);
 }
 
 // cv <- first half of compress(cv, m, counter, len, flags)
 __device__ __forceinline__ void b3_compress(uint32_t cv[8], const uint32_t m_in[16], uint64_t counter,
-                                            uint32_t len, uint32_t flags) {
+                                            uint32_t len, uint32_t flags, uint32_t one) {
   uint32_t v[16], m[16];
 #pragma unroll
   for (int i = 0; i < 8; i++) v[i] = cv[i];
@@ -326,14 +341,14 @@ __device__ __forceinline__ void b3_compress(uint32_t cv[8], const uint32_t m_in[
   const int perm[16] = {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8};
 #pragma unroll
   for (int r = 0; r < 7; r++) {
-    b3_g(v[0], v[4], v[8], v[12], m[0], m[1]);
-    b3_g(v[1], v[5], v[9], v[13], m[2], m[3]);
-    b3_g(v[2], v[6], v[10], v[14], m[4], m[5]);
-    b3_g(v[3], v[7], v[11], v[15], m[6], m[7]);
-    b3_g(v[0], v[5], v[10], v[15], m[8], m[9]);
-    b3_g(v[1], v[6], v[11], v[12], m[10], m[11]);
-    b3_g(v[2], v[7], v[8], v[13], m[12], m[13]);
-    b3_g(v[3], v[4], v[9], v[14], m[14], m[15]);
+    b3_g(v[0], v[4], v[8], v[12], m[0], m[1], one);
+    b3_g(v[1], v[5], v[9], v[13], m[2], m[3], one);
+    b3_g(v[2], v[6], v[10], v[14], m[4], m[5], one);
+    b3_g(v[3], v[7], v[11], v[15], m[6], m[7], one);
+    b3_g(v[0], v[5], v[10], v[15], m[8], m[9], one);
+    b3_g(v[1], v[6], v[11], v[12], m[10], m[11], one);
+    b3_g(v[2], v[7], v[8], v[13], m[12], m[13], one);
+    b3_g(v[3], v[4], v[9], v[14], m[14], m[15], one);
     if (r < 6) {
       uint32_t t[16];
 #pragma unroll
@@ -420,7 +435,7 @@ __global__ void __launch_bounds__(128) k_b3_chunks(const B3Job J, uint32_t* __re
     const uint32_t blen = (uint32_t)((T - m0) < 64 ? (T - m0) : 64);
     uint32_t flags = (b == 0 ? kB3ChunkStart : 0u);
     if (b == nb - 1) flags |= kB3ChunkEnd | (J.C == 1 ? kB3Root : 0u);
-    b3_compress(cv, m, c, blen, flags);
+    b3_compress(cv, m, c, blen, flags, J.one);
   }
   if (J.C == 1) {
     store_digest16(J.hash_out + i * J.hash_stride, cv, kAligned);
@@ -459,7 +474,7 @@ __global__ void __launch_bounds__(128) k_b3_merge(const B3Job J, const uint32_t*
 #pragma unroll
   for (int k = 0; k < 8; k++) cv[k] = c_b3iv[k];
   const bool root = (m == 2);
-  b3_compress(cv, blk, 0, 64, kB3Parent | (root ? kB3Root : 0u));
+  b3_compress(cv, blk, 0, 64, kB3Parent | (root ? kB3Root : 0u), J.one);
   if (root) {
     store_digest16(J.hash_out + i * J.hash_stride, cv, kAligned);
   } else {
@@ -629,6 +644,7 @@ cudaError_t launch_blake3_blocks(const B3Job& job, uint32_t* d_scratch, cudaStre
   if (job.n == 0) return cudaSuccess;
   B3Job J = job;
   J.C = (J.P + J.D + 1023) / 1024;
+  J.one = 1;
   const bool al = ((uintptr_t)J.data % 8) == 0 && J.stride % 8 == 0 && J.D % 8 == 0 && J.P % 8 == 0 &&
                   ((uintptr_t)J.copy_to % 8) == 0 && J.copy_stride % 8 == 0 &&
                   ((uintptr_t)J.hash_out % 8) == 0 && J.hash_stride % 8 == 0;

@@ -146,6 +146,7 @@ struct B3Job {
   size_t copy_stride = 0;
   uint8_t* hash_out = nullptr;
   size_t hash_stride = 16;
+  uint32_t one = 1;  // set by the launcher
 };
 size_t blake3_scratch_words(size_t n, uint64_t message_bytes);  // chunk chaining values (2 levels)
 cudaError_t launch_blake3_blocks(const B3Job& job, uint32_t* d_scratch, cudaStream_t s);
