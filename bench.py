@@ -646,6 +646,28 @@ def measure_serving(ctx, dev, count=32, seed=5, budget=120 * 10**9):
             "outputs_identical": bool(same)}
 
 
+def profile_hashes(ctx, dev):
+    """The small ncu case of the hash kernels: 256 MiB of seeded device data
+    (larger than L2) hashed once each way -- PAR2 MD5 + CRC32 of 8,192 x
+    32 KiB slices, PAR3 BLAKE3 of 32,768 x 8 KiB blocks, PAR2 memory checksums
+    of the 8,192 slices."""
+    import torch
+    from parparpar_b200 import par2, par3
+    g = torch.Generator(device=f"cuda:{dev}")
+    g.manual_seed(1)
+    d = torch.randint(0, 256, (8192, 32768), dtype=torch.uint8, device=f"cuda:{dev}", generator=g)
+    o = torch.zeros((8192, 20), dtype=torch.uint8, device=f"cuda:{dev}")
+    par2.block_hashes(d, 32768, out=o, ctx=ctx)
+    ctx.synchronize()
+    o2 = torch.zeros((32768, 16), dtype=torch.uint8, device=f"cuda:{dev}")
+    par3.block_hashes(d.view(32768, 8192), 8192, 0, PAR3_AFTER, num_blocks=32768, out=o2, ctx=ctx)
+    ctx.synchronize()
+    o3 = torch.zeros((8192, 16), dtype=torch.uint8, device=f"cuda:{dev}")
+    par2.memory_checksums(d, 32768, out=o3, ctx=ctx)
+    ctx.synchronize()
+    print(json.dumps({"profile_hashes": "ok"}), flush=True)
+
+
 def run_reference(args, rank):
     """--impl reference: the reference's own CPU implementation on the host
     cores, on the same workload/metric (bounded sample per step)."""
@@ -686,6 +708,8 @@ def main():
     ap.add_argument("--batched-only", action="store_true", help="print only the batched-vs-plain comparison")
     ap.add_argument("--serving-only", action="store_true", help="print only the serving-loop comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-hashes", action="store_true",
+                    help="one launch of each block-hash kernel on 256 MiB (a small case for ncu), then exit")
     ap.add_argument("--gf16-kernel", default="auto", choices=["auto", "lut", "tensor"])
     ap.add_argument("--gf64-kernel", default="auto", choices=["auto", "lut", "tensor"])
     args = ap.parse_args()
@@ -719,6 +743,9 @@ def main():
     timer = Timer(stream)
     peak, peak_kind = load_peaks()
 
+    if args.profile_hashes:
+        profile_hashes(ctx, local)
+        return
     if args.batched_only:
         print(json.dumps(measure_batched_vs_plain(ctx, timer, args.steps, args.warmup, local)), flush=True)
         return
