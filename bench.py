@@ -646,6 +646,66 @@ def measure_serving(ctx, dev, count=32, seed=5, budget=120 * 10**9):
             "outputs_identical": bool(same)}
 
 
+def measure_fused(ctx, dev):
+    """End to end with pinned host inputs (1 GiB): each create with and
+    without the hashes of its inputs computed in the same pass, and the PAR3
+    streaming create from a 1 GiB file (page cache warm).  Median of 3."""
+    import tempfile
+
+    import torch
+    from parparpar_b200 import par2, par3
+
+    def med(f, reps=3):
+        f()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            f()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts)
+
+    out = {"unit": "GB/s", "host_buffers": "pinned"}
+    g = torch.Generator(device=f"cuda:{dev}")
+    g.manual_seed(3)
+    n, sl, r = 32768, 32768, 64
+    h_in = torch.empty((n, sl), dtype=torch.uint8).pin_memory()
+    h_in.copy_(torch.randint(0, 256, (n, sl), dtype=torch.uint8, device=f"cuda:{dev}", generator=g))
+    h_out = torch.empty((r, sl), dtype=torch.uint8).pin_memory()
+    h_hash = torch.empty((n, 20), dtype=torch.uint8).pin_memory()
+    idx, exps = np.arange(n), list(range(r))
+    t_plain = med(lambda: par2.par2_create(h_in, idx, exps, out=h_out, ctx=ctx))
+    t_hash = med(lambda: par2.par2_create(h_in, idx, exps, out=h_out, hashes=h_hash, ctx=ctx))
+    out["par2_create_32768x32KiB_R64"] = {"plain": n * sl / t_plain / 1e9, "with_ifsc_hashes": n * sl / t_hash / 1e9}
+    # the PAR3 inputs reuse the same pinned bytes as 131,072 x 8 KiB blocks
+    nb, words, R = 131072, 1024, 8
+    x = h_in.view(torch.int64).view(nb, words)
+    rec = torch.empty((R, words), dtype=torch.int64).pin_memory()
+    pk = torch.empty(R * (64 + 8 * words), dtype=torch.uint8).pin_memory()
+    dh = torch.empty((nb, 16), dtype=torch.uint8).pin_memory()
+    par3.GF64Controller.ctx = ctx
+    t_plain = med(lambda: par3.GF64Controller.ComputeRecoveryBlocks(x, nb, rec, R, words, 0, nb))
+    t_pk = med(lambda: par3.create_packets(x, nb, words, 0, R, nb, b"\x5a" * 8, data_after_checksum=PAR3_AFTER,
+                                           data_hashes=dh, packets=pk, ctx=ctx))
+    out["par3_create_131072x8KiB_R8"] = {"plain": nb * 8 * words / t_plain / 1e9,
+                                         "with_block_hashes_and_packets": nb * 8 * words / t_pk / 1e9}
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "src.bin")
+        with open(path, "wb") as f:
+            f.write(h_in.numpy().tobytes())
+        opts = {"recoverySlices": R, "blockSize": 8 * words, "firstInput": 0, "firstRecovery": nb}
+        t_st = med(lambda: par3.par3_create_streaming(path, opts, ctx=ctx))
+        t_sth = med(lambda: par3.par3_create_streaming(path, opts, data_hashes=dh.numpy(),
+                                                       data_after_checksum=PAR3_AFTER, ctx=ctx))
+        res = par3.par3_create_streaming(path, opts, ctx=ctx)
+        same = bool(np.array_equal(res["recoveryBuffer"].view(np.int64).reshape(R, words), rec.numpy()))
+    out["par3_create_streaming_1GiB_8KiB_R8"] = {"from_file": nb * 8 * words / t_st / 1e9,
+                                                 "with_block_hashes": nb * 8 * words / t_sth / 1e9,
+                                                 "read_share": res["readMs"] / res["durationMs"],
+                                                 "matches_in_memory_create": same}
+    del h_in, h_out, h_hash, rec, pk, dh
+    return out
+
+
 def profile_hashes(ctx, dev):
     """The small ncu case of the hash kernels: 256 MiB of seeded device data
     (larger than L2) hashed once each way -- PAR2 MD5 + CRC32 of 8,192 x
@@ -707,6 +767,8 @@ def main():
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--batched-only", action="store_true", help="print only the batched-vs-plain comparison")
     ap.add_argument("--serving-only", action="store_true", help="print only the serving-loop comparison")
+    ap.add_argument("--fused-only", action="store_true", help="print only the fused-pass (hashes, packets, "
+                    "streaming) end-to-end comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-hashes", action="store_true",
                     help="one launch of each block-hash kernel on 256 MiB (a small case for ncu), then exit")
@@ -751,6 +813,9 @@ def main():
         return
     if args.serving_only:
         print(json.dumps(measure_serving(ctx, local)), flush=True)
+        return
+    if args.fused_only:
+        print(json.dumps(measure_fused(ctx, local)), flush=True)
         return
 
     job = setup_job(args.workload, local, 1234 + rank, ctx)
@@ -862,6 +927,10 @@ def main():
             line["serving"] = measure_serving(ctx, local)
         except Exception as e:
             line["serving"] = {"error": str(e)[:200]}
+        try:
+            line["fused"] = measure_fused(ctx, local)
+        except Exception as e:
+            line["fused"] = {"error": str(e)[:200]}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -2071,7 +2071,7 @@ PP_API int pp_par3_create_streaming(pp_ctx* ctx, const char* source_path, size_t
     }
   cudaEvent_t* freed = ev;       // [2]: the product (and hash) of the buffer's last chunk is done
   cudaEvent_t* copied = ev + 2;  // [2]: the buffer's copy to the device is done
-  const unsigned readers = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const unsigned readers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
   double read_s = 0;
   auto read_chunk = [&](size_t c, uint8_t* dst) -> int {
     const uint64_t off = (uint64_t)c * cbytes;
