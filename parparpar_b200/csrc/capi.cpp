@@ -795,6 +795,7 @@ struct pp_par2_proc {
   bool batch_fixed = false;   // the caller chose the batch size
   struct Area {
     uint8_t* d_in = nullptr;
+    uint8_t* d_ck = nullptr;        // memory checksum block of each staged row (16 B rows)
     uint8_t* h_in = nullptr;        // pinned host rows: host inputs are staged here
     std::vector<uint8_t> host_row;  // row i of this batch sits in h_in (else already in d_in)
     uint16_t* d_coeff = nullptr;  // [n_out][batch]
@@ -810,6 +811,7 @@ struct pp_par2_proc {
   uint8_t* d_out = nullptr;
   size_t d_out_n = 0;
   bool has_output = false;
+  uint8_t* d_out_ck = nullptr;    // the outputs' carried checksum blocks (16 B rows)
   int* d_valid = nullptr;         // per-output memory-checksum result
   std::vector<int> valid;         // its host copy, once checked
   bool checked = false;
@@ -822,22 +824,24 @@ struct pp_par2_proc {
 // caller's buffer (one DMA beats a host memcpy into the pinned rows)
 constexpr size_t kProcDirectBytes = 256 << 10;
 
-// Staged rows and output rows: the slice rounded up to 16 bytes, then the
-// 16-byte memory checksum block (the reference's packed staging appends one
-// checksum block per slice, gf16/gf16_global.h:214-218), which the region
-// kernels carry like data.
-static size_t proc_row(size_t slice) { return round16(slice) + 16; }
-static size_t proc_ck_off(const pp_par2_proc* p) { return round16(p->cur_size); }
+// Staged rows and output rows: the slice rounded up to 16 bytes.  The memory
+// checksum block of each row (the reference's packed staging appends one per
+// slice, gf16/gf16_global.h:214-218) lives in a separate array of 16-byte
+// rows that the same coefficients multiply in a second, small launch.
+static size_t proc_row(size_t slice) { return round16(slice); }
 
 static int proc_alloc_inputs(pp_par2_proc* p) {
   for (auto& a : p->areas) {
     if (a.d_in) cudaFree(a.d_in);
+    if (a.d_ck) cudaFree(a.d_ck);
     if (a.h_in) cudaFreeHost(a.h_in);
     a.d_in = nullptr;
+    a.d_ck = nullptr;
     a.h_in = nullptr;
     // pinned rows only for slices small enough to be staged (larger ones are
     // copied straight from the caller's buffer)
     if (cudaMalloc(&a.d_in, p->row * p->batch_alloc) != cudaSuccess ||
+        cudaMalloc(&a.d_ck, (size_t)16 * p->batch_alloc) != cudaSuccess ||
         (p->row < kProcDirectBytes && cudaMallocHost(&a.h_in, p->row * p->batch_alloc) != cudaSuccess)) {
       cudaGetLastError();
       return PP_ERR_NO_MEMORY;
@@ -904,12 +908,14 @@ PP_API void pp_par2_proc_destroy(pp_par2_proc* p) {
   if (p->s_copy) cudaStreamSynchronize(p->s_copy);
   for (auto& a : p->areas) {
     if (a.d_in) cudaFree(a.d_in);
+    if (a.d_ck) cudaFree(a.d_ck);
     if (a.h_in) cudaFreeHost(a.h_in);
     if (a.d_coeff) cudaFree(a.d_coeff);
     if (a.d_aexp) cudaFree(a.d_aexp);
     if (a.done) cudaEventDestroy(a.done);
   }
   if (p->d_out) cudaFree(p->d_out);
+  if (p->d_out_ck) cudaFree(p->d_out_ck);
   if (p->d_valid) cudaFree(p->d_valid);
   if (p->copied) cudaEventDestroy(p->copied);
   if (p->s_copy) cudaStreamDestroy(p->s_copy);
@@ -953,8 +959,11 @@ PP_API int pp_par2_proc_set_current_slice_size(pp_par2_proc* p, size_t size) {
 static int proc_ensure_out(pp_par2_proc* p) {
   size_t need = p->row * std::max<size_t>(1, p->exps.size());
   if (p->d_valid) cudaFree(p->d_valid);
+  if (p->d_out_ck) cudaFree(p->d_out_ck);
   p->d_valid = nullptr;
-  if (cudaMalloc(&p->d_valid, sizeof(int) * std::max<size_t>(1, p->exps.size())) != cudaSuccess) {
+  p->d_out_ck = nullptr;
+  if (cudaMalloc(&p->d_valid, sizeof(int) * std::max<size_t>(1, p->exps.size())) != cudaSuccess ||
+      cudaMalloc(&p->d_out_ck, (size_t)16 * std::max<size_t>(1, p->exps.size())) != cudaSuccess) {
     cudaGetLastError();
     return set_err(p->ctx, PP_ERR_NO_MEMORY, "checksum flags");
   }
@@ -1036,13 +1045,15 @@ static int proc_submit(pp_par2_proc* p) {
                                    cudaMemcpyHostToDevice, p->s_copy));
   CUDA_TRY(p->ctx, cudaEventRecord(p->copied, p->s_copy));
   CUDA_TRY(p->ctx, cudaStreamWaitEvent(p->s_comp, p->copied, 0));
-  // attach each row's memory checksum, then multiply-accumulate data and
-  // checksum blocks together
-  const size_t ck = proc_ck_off(p);
-  CUDA_TRY(p->ctx, launch_par2_cksum(a.d_in, p->row, a.count, ck, a.d_in + ck, p->row, nullptr, p->s_comp));
-  CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_in, p->row, a.count, ck + 16, a.d_coeff, p->batch,
+  // each row's memory checksum, then the products of the data rows and of
+  // the checksum rows (the second launch reuses the expanded coefficient tiles)
+  CUDA_TRY(p->ctx, launch_par2_cksum(a.d_in, p->row, a.count, p->cur_size, a.d_ck, 16, nullptr, p->s_comp));
+  CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_in, p->row, a.count, p->cur_size, a.d_coeff, p->batch,
                                n_out, p->d_out, p->row, p->has_output, p->ctx->sms, a.d_aexp, p->ctx->d_status,
                                p->s_comp));
+  CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_ck, 16, a.count, 16, a.d_coeff, p->batch, n_out,
+                               p->d_out_ck, 16, p->has_output, p->ctx->sms, a.d_aexp, p->ctx->d_status, p->s_comp,
+                               true));
   p->checked = false;
   CUDA_TRY(p->ctx, cudaEventRecord(a.done, p->s_comp));
   a.active = true;
@@ -1127,8 +1138,8 @@ PP_API int pp_par2_proc_get_output(pp_par2_proc* p, unsigned index, void* output
   } else if (!p->checked) {
     // verify every output's carried checksum against its data once
     // (finish_packed_cksum, gf16/controller_cpu.cpp:423-443)
-    const size_t ck = proc_ck_off(p);
-    CUDA_TRY(p->ctx, launch_par2_cksum(p->d_out, p->row, n_out, ck, p->d_out + ck, p->row, p->d_valid, p->s_copy));
+    CUDA_TRY(p->ctx, launch_par2_cksum(p->d_out, p->row, n_out, p->cur_size, p->d_out_ck, 16, p->d_valid,
+                                       p->s_copy));
     p->valid.assign(n_out, 0);
     CUDA_TRY(p->ctx, cudaMemcpyAsync(p->valid.data(), p->d_valid, sizeof(int) * n_out, cudaMemcpyDeviceToHost,
                                      p->s_copy));
