@@ -46,20 +46,30 @@ namespace pp {
 namespace tc16 {
 using namespace pp::tc;
 
-constexpr int kWords = 512;                 // words per CTA
 constexpr int kStageIn = 8;                 // inputs per stage
-constexpr int kABytes = 128 * 128;          // A tile: 128 rows x 128 B
-constexpr int kBBytes = kWords * 128;       // B tile: 512 rows x 128 B
-constexpr int kRawBytes = kStageIn * kWords * 2;
+constexpr int kABytes = 128 * 128;          // A tile of one output group: 128 rows x 128 B
 constexpr int kThreads = 320;
 constexpr int kExp = 256;  // expander / epilogue threads (warps 2-9)
-constexpr int kLd = 4;                             // load ring depth (A tile + raw rows)
-constexpr int kBs = 2;                             // B tile ring depth
-constexpr int kOffA = 0;
-constexpr int kOffB = kLd * kABytes;               // 64 KiB
-constexpr int kOffRaw = kOffB + kBs * kBBytes;     // 192 KiB
-constexpr int kOffBar = kOffRaw + kLd * kRawBytes; // 224 KiB
-constexpr int kSmemBytes = kOffBar + 256 + 1024;   // + barriers + alignment slack
+
+// Tile shape by output groups per CTA (KG): KG = 1 -> 8 outputs x 512 words;
+// KG = 2 -> 16 outputs x 256 words, two MMA accumulators of N = 256 sharing
+// each B tile, which halves the B tile built per output.  Either way the
+// accumulator fills TMEM (128 lanes x 512 columns).
+template <int KG>
+struct Shape {
+  static constexpr int kLd = 4;                       // load ring depth (A tiles + raw rows)
+  static constexpr int kBs = 2;                       // B tile ring depth
+  static constexpr int kWords = KG == 2 ? 256 : 512;  // words per CTA
+  static constexpr int kAStage = KG * kABytes;        // A bytes per stage
+  static constexpr int kBBytes = kWords * 128;        // B tile: kWords rows x 128 B
+  static constexpr int kRawBytes = kStageIn * kWords * 2;
+  static constexpr int kOffA = 0;
+  static constexpr int kOffB = kLd * kAStage;
+  static constexpr int kOffRaw = kOffB + kBs * kBBytes;
+  static constexpr int kOffBar = kOffRaw + kLd * kRawBytes;
+  static constexpr int kSmemBytes = kOffBar + 256 + 1024;  // + barriers + alignment slack
+};
+static_assert(Shape<1>::kSmemBytes <= 227 * 1024 && Shape<2>::kSmemBytes <= 227 * 1024, "shared memory");
 
 // instruction descriptor: D int32, A/B unsigned 8-bit, both K-major,
 // N = 256, M = 128
@@ -121,8 +131,13 @@ k_gf16_tc_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigne
 // One CTA per work item of the job table (tc_batch.h): the item fixes the
 // job, the output group, the word tile and the stage range; mode 0 stores,
 // 1 XORs into the output, 2 XORs atomically (the job is split over CTAs).
+template <int KG>
 __global__ void __launch_bounds__(kThreads, 1)
 k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ status) {
+  using S = Shape<KG>;
+  constexpr int kWords = S::kWords, kBBytes = S::kBBytes, kRawBytes = S::kRawBytes, kAStage = S::kAStage;
+  constexpr int kOffA = S::kOffA, kOffB = S::kOffB, kOffRaw = S::kOffRaw, kOffBar = S::kOffBar;
+  constexpr int kLd = S::kLd, kBs = S::kBs;
   const TcSeg sg = tc_item(&batch, blockIdx.x);
   const Gf16TcJob J = pinned_job(batch.job[sg.job]);
   const uint8_t* __restrict__ in = J.in;
@@ -163,7 +178,7 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
   volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 8 * NBARS + 8);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const unsigned g = (unsigned)(sg.tile % J.groups);  // output group
+  const unsigned g = (unsigned)(sg.tile % J.groups) * KG;  // first output group of the CTA
   const size_t w0 = (size_t)(sg.tile / J.groups) * kWords;
   const unsigned st_begin = sg.st0;
   const unsigned nst = sg.st1 - sg.st0;
@@ -206,8 +221,11 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
           }
         }
         const unsigned st = st_begin + k;
-        mbar_expect_tx(BAR(A_FULL + sl), kABytes);
-        bulk_g2s(sA + sl * kABytes, a_exp + ((size_t)g * n_stages_total + st) * kABytes, kABytes, BAR(A_FULL + sl));
+        mbar_expect_tx(BAR(A_FULL + sl), kAStage);
+#pragma unroll
+        for (int gg = 0; gg < KG; gg++)
+          bulk_g2s(sA + sl * kAStage + gg * kABytes, a_exp + ((size_t)(g + gg) * n_stages_total + st) * kABytes,
+                   kABytes, BAR(A_FULL + sl));
         const unsigned i0 = st * kStageIn;
         const unsigned ni = min((unsigned)kStageIn, n_in - i0);
         mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
@@ -238,8 +256,11 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
         for (int kk = 0; kk < 4; kk++) {
 #pragma unroll
           for (int nn = 0; nn < 2; nn++) {
-            mma_i8(tmem + nn * 256, sw128_desc(sA + sl * kABytes + 32 * kk),
-                   sw128_desc(sB + bs * kBBytes + nn * (256 * 128) + 32 * kk), kIdesc, (k > 0 || kk > 0) ? 1u : 0u);
+            // KG = 1: two word halves of one group; KG = 2: one word tile of two groups
+            const uint32_t a_off = KG == 2 ? nn * kABytes : 0;
+            const uint32_t b_off = KG == 2 ? 0 : nn * (256 * 128);
+            mma_i8(tmem + nn * 256, sw128_desc(sA + sl * kAStage + a_off + 32 * kk),
+                   sw128_desc(sB + bs * kBBytes + b_off + 32 * kk), kIdesc, (k > 0 || kk > 0) ? 1u : 0u);
           }
         }
         mma_commit(BAR(A_EMPTY + sl));
@@ -252,8 +273,47 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
     }
   } else {
     // ------------------------------------------------------------ expanders
-    const int e = threadIdx.x - 64;  // 0..255: word pair n = 2e, 2e+1 of the tile
-    const unsigned n = 2 * e;
+    const int e = threadIdx.x - 64;  // 0..255
+    if constexpr (KG == 2) {
+      // one word row per thread: row n = e holds the 8 inputs' words, shifted by j
+      const unsigned n = e;
+      const bool odd_tail = (slice_bytes & 1) && (w0 + kWords >= total_words);
+      const unsigned last_word = (unsigned)(total_words - 1 - w0);
+      uint32_t mask = n < words_valid ? 0xFFFFu : 0u;
+      if (odd_tail && n == last_word) mask &= 0x00FFu;
+      const uint32_t rowA = (n >> 3) * 1024 + (n & 7) * 128, rA = n & 7;
+      for (unsigned k = 0; k < nst; k++) {
+        const unsigned sl = k % kLd, bs = k % kBs;
+        if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
+          *err = 1;
+          break;
+        }
+        const unsigned i0 = (st_begin + k) * kStageIn;
+        const unsigned ni = min((unsigned)kStageIn, n_in - i0);
+        const uint8_t* raw = raw_p + sl * kRawBytes;
+        uint32_t v[kStageIn];
+#pragma unroll
+        for (int ii = 0; ii < kStageIn; ii++)
+          v[ii] = (unsigned)ii < ni ? (*reinterpret_cast<const uint16_t*>(raw + ii * (kWords * 2) + 2 * n) & mask) : 0u;
+        mbar_arrive(BAR(RAW_EMPTY + sl));
+        if (k >= (unsigned)kBs && !mbar_wait(BAR(B_EMPTY + bs), (k / kBs - 1) & 1)) {
+          *err = 1;
+          break;
+        }
+        uint8_t* bt = b_p + bs * kBBytes;
+        uint32_t pA[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) pA[q] = v[2 * q] | (v[2 * q + 1] << 16);
+        // 8 consecutive threads store 8 rows of one swizzle atom at 8 distinct chunks: conflict-free
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          *reinterpret_cast<uint4*>(bt + rowA + ((j ^ rA) << 4)) =
+              make_uint4(pA[0] >> j, pA[1] >> j, pA[2] >> j, pA[3] >> j);
+        fence_async_smem();
+        mbar_arrive(BAR(B_FULL + bs));
+      }
+    } else {
+    const unsigned n = 2 * e;  // word pair n, n + 1 of the tile
     const bool odd_tail = (slice_bytes & 1) && (w0 + kWords >= total_words);
     const unsigned last_word = (unsigned)(total_words - 1 - w0);
     uint32_t mask = 0;
@@ -307,13 +367,15 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
       fence_async_smem();
       mbar_arrive(BAR(B_FULL + bs));
     }
+    }
     // ------------------------------------------------------------ epilogue
     const bool have = nst > 0 && !*err && mbar_wait(BAR(D_FULL), 0);
     if (nst > 0 && !have) *err = 1;
     tc_fence_after();
     const int q = warp & 3;               // TMEM lane quarter of this warp
     const int chalf = (warp - 2) >> 2;    // columns [256*chalf, 256*chalf + 256)
-    const unsigned o_lo = 8 * g + 2 * q, o_hi = o_lo + 1;
+    // KG = 1: the halves are words 0-255 / 256-511 of one group; KG = 2: two groups
+    const unsigned o_lo = 8 * (g + (KG == 2 ? chalf : 0)) + 2 * q, o_hi = o_lo + 1;
     for (int c = 8 * chalf; c < 8 * chalf + 8; c++) {
       uint32_t r[32];
       if (have) {
@@ -329,7 +391,7 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
         if (lane == j) mine = bal;
       }
       if (!have) continue;
-      const unsigned widx = 32 * c + lane;  // word within the tile
+      const unsigned widx = 32 * (KG == 2 ? c - 8 * chalf : c) + lane;  // word within the tile
       // pair lanes into 32-bit words: even lane holds words widx, widx+1
       const uint32_t nb = __shfl_down_sync(0xFFFFFFFFu, mine, 1);
       if ((lane & 1) || widx >= words_valid) continue;
@@ -395,19 +457,27 @@ cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned
 cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         tc16::kSmemBytes);
+    cudaError_t e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tc16::Shape<1>::kSmemBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc16::Shape<2>::kSmemBytes);
     if (e != cudaSuccess) return e;
     attr = true;
   }
+  // two output groups per CTA when every job's outputs pair up into groups of 16
+  int kg = 2;
+  for (uint32_t j = 0; j < b.n_jobs; j++)
+    if (b.job[j].n_out && b.job[j].slice_bytes && b.job[j].n_in && (b.job[j].n_out + 7) / 8 % 2) kg = 1;
+  const size_t words = kg == 2 ? tc16::Shape<2>::kWords : tc16::Shape<1>::kWords;
   uint32_t m = 0;
   for (uint32_t j = 0; j < b.n_jobs; j++) {
     Gf16TcJob& J = b.job[j];
     if (!J.n_out || !J.slice_bytes) continue;
     J.n_stages = (J.n_in + 7) / 8;
     if (!J.a_stride) J.a_stride = J.n_stages;
-    J.groups = (J.n_out + 7) / 8;
-    const size_t wt = ceil_div((J.slice_bytes + 1) / 2, tc16::kWords);
+    J.groups = (J.n_out + 7) / 8 / (unsigned)kg;  // output tiles of a CTA: groups (kg = 1) or group pairs
+    const size_t wt = ceil_div((J.slice_bytes + 1) / 2, words);
     if (wt > 0xFFFFFFFFu) return cudaErrorInvalidValue;
     J.wt = (uint32_t)wt;
     if (!J.n_in) {
@@ -430,7 +500,10 @@ cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStr
     note_launch();
     if (e != cudaSuccess) return e;
   }
-  tc16::k_gf16_muladd_tc<<<(unsigned)ctas, tc16::kThreads, tc16::kSmemBytes, s>>>(b, d_status);
+  if (kg == 2)
+    tc16::k_gf16_muladd_tc<2><<<(unsigned)ctas, tc16::kThreads, tc16::Shape<2>::kSmemBytes, s>>>(b, d_status);
+  else
+    tc16::k_gf16_muladd_tc<1><<<(unsigned)ctas, tc16::kThreads, tc16::Shape<1>::kSmemBytes, s>>>(b, d_status);
   note_launch();
   return cudaGetLastError();
 }
