@@ -238,6 +238,11 @@ PP_API int pp_gf64_region_2d_muladd_arr(pp_ctx* ctx, uint64_t* const* outs, size
  * gf64/gf64_invert.c:71-75). */
 PP_API int pp_gf64_inverse_batch(pp_ctx* ctx, uint64_t* out, const uint64_t* in, size_t n);
 
+/* dst ^= src over `bytes` bytes (replaces the xor_buffers export,
+ * src/gf64_addon.cc:3216-3265, used to reduce chunked recovery partials).
+ * The caller checks equal lengths (the reference's RangeError). */
+PP_API int pp_xor_buffers(pp_ctx* ctx, void* dst, const void* src, size_t bytes);
+
 /* Allocation-free solve.  No counterpart in the reference: an addition for
  * callers that cannot allocate device memory where they need the repair solve
  * (a device pool owned by another allocator with no headroom, latency-bound

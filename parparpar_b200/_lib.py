@@ -62,7 +62,7 @@ EXPORTS = [
     "pp_server_last_error", "pp_server_destroy",
     "pp_par2_block_hashes", "pp_par3_block_hashes", "pp_par3_assemble_recovery_packets",
     "pp_par2_create_hashed", "pp_par3_create_packets", "pp_par2_memory_checksums", "pp_par3_create_streaming",
-    "pp_par2_recovery_packet_headers",
+    "pp_par2_recovery_packet_headers", "pp_xor_buffers",
 ]
 
 
@@ -147,6 +147,7 @@ _sig("pp_gf64_repair", _I, _P, _P, _SZ, _P, _SZ, _P, _P, _SZ, _U64, _U64, _P)
 _sig("pp_par2_block_hashes", _I, _P, _P, _SZ, _SZ, _SZ, _P, _P)
 _sig("pp_par2_memory_checksums", _I, _P, _P, _SZ, _SZ, _SZ, _P)
 _sig("pp_par2_recovery_packet_headers", _I, _P, _P, _SZ, _SZ, _SZ, _P, _P, _P)
+_sig("pp_xor_buffers", _I, _P, _P, _P, _SZ)
 
 
 class PPStreamStats(ctypes.Structure):

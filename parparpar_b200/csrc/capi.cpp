@@ -2178,4 +2178,30 @@ PP_API int pp_par2_recovery_packet_headers(pp_ctx* ctx, const void* slices, size
   return PP_OK;
 }
 
+PP_API int pp_xor_buffers(pp_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  if (!bytes) return PP_OK;
+  if (!dst || !src) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  const bool d_dev = is_device_ptr(dst), s_dev = is_device_ptr(src);
+  uint8_t* dd = (uint8_t*)dst;
+  const uint8_t* ds = (const uint8_t*)src;
+  if (!d_dev) {
+    dd = (uint8_t*)scratch(ctx, S_OUT, bytes);
+    if (!dd) return set_err(ctx, PP_ERR_NO_MEMORY, "staging");
+    CUDA_TRY(ctx, cudaMemcpyAsync(dd, dst, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (!s_dev) {
+    uint8_t* t = (uint8_t*)scratch(ctx, S_IN, bytes);
+    if (!t) return set_err(ctx, PP_ERR_NO_MEMORY, "staging");
+    CUDA_TRY(ctx, cudaMemcpyAsync(t, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    ds = t;
+  }
+  CUDA_TRY(ctx, launch_xor_bytes(dd, ds, bytes, ctx->stream));
+  if (!d_dev) CUDA_TRY(ctx, cudaMemcpyAsync(dst, dd, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!d_dev || !s_dev) CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PP_OK;
+}
+
 }  // extern "C"

@@ -536,4 +536,38 @@ cudaError_t launch_gf64_solve(uint64_t* d_A, uint64_t* d_rhs, size_t n, size_t B
   return cudaGetLastError();
 }
 
+// dst ^= src over `bytes` bytes (16-byte vectors where both are aligned,
+// bytes otherwise)
+__global__ void k_xor_bytes(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, size_t bytes, bool vec) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t done = 0;
+  if (vec) {
+    const size_t nv = bytes / 16;
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    const uint4* q = reinterpret_cast<const uint4*>(src);
+    for (size_t i = t; i < nv; i += stride) {
+      uint4 a = d[i];
+      const uint4 b = q[i];
+      a.x ^= b.x;
+      a.y ^= b.y;
+      a.z ^= b.z;
+      a.w ^= b.w;
+      d[i] = a;
+    }
+    done = nv * 16;
+  }
+  for (size_t i = done + t; i < bytes; i += stride) dst[i] ^= src[i];
+}
+
+cudaError_t launch_xor_bytes(uint8_t* d_dst, const uint8_t* d_src, size_t bytes, cudaStream_t s) {
+  if (!bytes) return cudaSuccess;
+  const bool vec = ((uintptr_t)d_dst % 16) == 0 && ((uintptr_t)d_src % 16) == 0;
+  const size_t units = vec ? bytes / 16 + 16 : bytes;
+  const unsigned blocks = (unsigned)std::min<size_t>(ceil_div(units, 256), 148 * 8);
+  k_xor_bytes<<<std::max(1u, blocks), 256, 0, s>>>(d_dst, d_src, bytes, vec);
+  note_launch();
+  return cudaGetLastError();
+}
+
 }  // namespace pp

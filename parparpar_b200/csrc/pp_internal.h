@@ -116,6 +116,9 @@ cudaError_t launch_gf64_region_muladd_arr(uint64_t* d_out, const uint64_t* d_in,
 cudaError_t launch_gf64_solve(uint64_t* d_A, uint64_t* d_rhs, size_t n, size_t B, uint64_t* d_fcol,
                               int* d_status, cudaStream_t s);
 
+// dst ^= src over `bytes` bytes (any alignment)
+cudaError_t launch_xor_bytes(uint8_t* d_dst, const uint8_t* d_src, size_t bytes, cudaStream_t s);
+
 // Batched additive FFT, in place (column-major: coefficient c of polynomial
 // b at data[c*ld + b]).
 cudaError_t launch_gf64_fft(uint64_t* d_data, size_t n, size_t batch, size_t ld, bool inverse, cudaStream_t s);

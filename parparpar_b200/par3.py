@@ -464,3 +464,133 @@ def par3_create_streaming(sourcePath, options, callback=None, recovery=None, dat
         callback(None, result)
         return None
     return result
+
+
+# ------------------------------------------------------ remaining N-API exports
+def mul_arr(out, inp, coeff, len_words, n_coeff, ctx=None):
+    """mul_arr export (src/gf64_addon.cc:3021-3150): out[w] = in[w] * coeff[w % n_coeff]."""
+    if any(b is None for b in (out, inp, coeff)):
+        raise TypeError("Requires out, in, coeff, len_words, n_coeff")
+    len_words, n_coeff = _check_int(len_words, "len_words"), _check_int(n_coeff, "n_coeff")
+    if n_coeff <= 0 and len_words > 0:
+        raise ValueError("n_coeff must be positive")
+    if _nbytes(out) < 8 * len_words or _nbytes(inp) < 8 * len_words or _nbytes(coeff) < 8 * n_coeff:
+        raise ValueError("buffer too small")
+    gf64_region_mul_arr(out, inp, coeff, len_words, n_coeff, ctx=ctx)
+
+
+def xor_buffers(dst, src, ctx=None):
+    """xor_buffers export (src/gf64_addon.cc:3216-3265): dst ^= src; equal lengths required."""
+    if dst is None or src is None:
+        raise TypeError("Requires dst and src Buffers")
+    if _nbytes(dst) != _nbytes(src):
+        raise ValueError(f"xor_buffers: dst.length ({_nbytes(dst)}) must equal src.length ({_nbytes(src)})")
+    c = _ctx(ctx)
+    c.check(lib.pp_xor_buffers(c.h, ptr(dst), ptr(src), _nbytes(dst)))
+
+
+def gf64_solve(A, b, n, ctx=None):
+    """gf64_solve export (src/gf64_addon.cc:1127-1230, gf64/gf64_solve.c:39-96):
+    solve A x = b for one right-hand side; A and b are left unchanged.
+    Returns x (numpy uint64, n words) or None if A is singular."""
+    if A is None or b is None:
+        raise TypeError("Requires A, b, and n")
+    n = _check_int(n, "n")
+    Ac = np.array(np.frombuffer(memoryview(A).cast("B"), dtype=np.uint64)[: n * n]) if not hasattr(A, "numel") \
+        else np.array(A.cpu().numpy().view(np.uint64).reshape(-1)[: n * n])
+    bc = np.array(np.frombuffer(memoryview(b).cast("B"), dtype=np.uint64)[:n]) if not hasattr(b, "numel") \
+        else np.array(b.cpu().numpy().view(np.uint64).reshape(-1)[:n])
+    if Ac.size < n * n or bc.size < n:
+        raise ValueError("buffer too small for n")
+    if n == 0:
+        return np.zeros(0, dtype=np.uint64)
+    rhs = bc.reshape(n, 1).copy()
+    if GF64Controller.SolveAndReconstruct(Ac.reshape(n, n), rhs, n, 1) != 0:
+        return None
+    return rhs.reshape(-1)
+
+
+def gf64_info(method=0):
+    """gf64_info export (src/gf64_addon.cc:89-160): the arithmetic method in use."""
+    return {"method": 4, "name": "CUDA sm_100a (tcgen05 int8 bit-matrix)", "alignment": 16}
+
+
+def compute_recovery_streaming(inputBatches, outputBuffer, numInputs, numRecovery, blockSize, firstInput,
+                               firstRecovery, numThreads=0, ctx=None):
+    """compute_recovery_streaming export (src/gf64_addon.cc:2290-2480): the
+    recovery of the concatenation of inputBatches (each a whole number of
+    blocks), one pass per batch accumulating into outputBuffer."""
+    if not isinstance(inputBatches, (list, tuple)):
+        raise TypeError("inputBatches must be an array of Buffers")
+    numInputs, numRecovery = _check_int(numInputs, "numInputs"), _check_int(numRecovery, "numRecovery")
+    blockSize = _check_int(blockSize, "blockSize")
+    if numInputs <= 0 or numRecovery <= 0:
+        raise ValueError("numInputs and numRecovery must be positive")
+    if blockSize <= 0 or blockSize % 8:
+        raise ValueError("blockSize must be positive and a multiple of 8")
+    counts = [_nbytes(bb) // blockSize for bb in inputBatches]
+    if sum(counts) != numInputs or any(_nbytes(bb) % blockSize for bb in inputBatches):
+        raise ValueError("inputBatches must hold numInputs whole blocks")
+    if _nbytes(outputBuffer) < numRecovery * blockSize:
+        raise ValueError("outputBuffer too small for numRecovery * blockSize")
+    off = 0
+    for k, (bb, cnt) in enumerate(zip(inputBatches, counts)):
+        if cnt:
+            GF64Controller.ComputeRecoveryBlocks(bb, cnt, outputBuffer, numRecovery, blockSize // 8,
+                                                 _u64(firstInput) + off, firstRecovery, numThreads, off > 0)
+        off += cnt
+
+
+def get_last_decomposition_path():
+    """get_last_decomposition_path export: the reference's CPU engine reports
+    which input decomposition its last call used; this engine never splits the
+    inputs into host-side decompositions, so it is always 0."""
+    return 0
+
+
+def isAlignedBuffer(buf, alignment=64):
+    """isAlignedBuffer export (src/gf64_addon.cc:2976-3015)."""
+    if buf is None or not (hasattr(buf, "data_ptr") or hasattr(buf, "ctypes")):
+        return False
+    if not isinstance(alignment, (int, np.integer)) or alignment <= 0 or alignment & (alignment - 1):
+        alignment = 64
+    return ptr(buf) % int(alignment) == 0
+
+
+def allocAlignedBuffer(size):
+    """allocAlignedBuffer export: a zeroed, 64-byte aligned host buffer."""
+    size = _check_int(size, "Size")
+    if size <= 0:
+        raise ValueError("Size must be positive")
+    raw = np.zeros(size + 64, dtype=np.uint8)
+    off = (-raw.ctypes.data) % 64
+    return raw[off: off + size]
+
+
+def get_cpu_topology():
+    """get_cpu_topology export (host information; the device engine does not
+    depend on it)."""
+    import os
+    n = os.cpu_count() or 1
+    return {"logicalCpus": n, "groups": 1}
+
+
+def reset_cpu_topology_cache():
+    return None
+
+
+def get_effective_cpu_count():
+    import os
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def reset_effective_cpu_count_cache():
+    return None
+
+
+def Gf64Encoder_create(method=0, ctx=None):
+    return Gf64Encoder(ctx)
+
+
+def Gf64Encoder_destroy(encoder):
+    return None

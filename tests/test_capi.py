@@ -119,3 +119,16 @@ def test_create_streaming_argument_errors():
         par3.par3_create_streaming("x", {"recoverySlices": 1, "blockSize": 60})
     with pytest.raises(TypeError):
         par3.par3_create_streaming("x", {"recoverySlices": 1, "blockSize": 64, "firstInput": 1.5})
+
+
+def test_compute_recovery_argument_errors():
+    """test/par3-native-edge.js error scenarios: numInputs 0, numRecovery 0,
+    blockSize 7 and 0, a numInputs the inputs buffer cannot hold -- all raise
+    before any device work."""
+    from parparpar_b200 import par3
+    x = np.zeros(8, dtype=np.uint64)
+    out = np.zeros(8, dtype=np.uint64)
+    for args in [(0, 1, 8), (1, 0, 8), (1, 1, 7), (1, 1, 0), (2**31 - 1, 1, 8)]:
+        with pytest.raises((ValueError, TypeError)):
+            par3.compute_recovery(x, out, args[0], args[1], args[2], 0, 1)
+    assert par3.isAlignedBuffer(par3.allocAlignedBuffer(100)) and par3.get_last_decomposition_path() == 0
