@@ -129,11 +129,11 @@ def test_native_edge_cases(ctx, oracle):
     one recovery block (output non-zero and not the input), blockSize 8,
     large blocks; deterministic across calls."""
     from parparpar_b200 import par3
-    x = np.array([[0x0123456789ABCDEF]], dtype=np.uint64)
+    x = np.array([[0xDEADBEEFCAFEBABE]], dtype=np.uint64)
     out = np.zeros((1, 1), dtype=np.uint64)
-    par3.compute_recovery(x, out, 1, 1, 8, 0, 1)
+    par3.compute_recovery(x, out, 1, 1, 8, 0, 2, 1)  # fR = 2: coefficient 1/(0 + 2) != 1
     assert out[0, 0] != 0 and out[0, 0] != x[0, 0]
-    assert (out == oracle.gf64_compute_recovery(x, 1, 0, 1)).all()
+    assert (out == oracle.gf64_compute_recovery(x, 1, 0, 2)).all()
     x2 = np.arange(1, 3, dtype=np.uint64).reshape(2, 1)
     a = np.zeros((1, 1), dtype=np.uint64)
     b = np.zeros((1, 1), dtype=np.uint64)
