@@ -706,6 +706,28 @@ def measure_fused(ctx, dev):
     return out
 
 
+def profile_tc(ctx, dev):
+    """The small ncu case of the tensor-core region kernels, 256 MiB of
+    seeded device input each (larger than L2): PAR2 create 8,192 x 32 KiB,
+    R=64, three calls (the third runs with the coefficient tiles resident, so
+    it is the region kernel alone), then PAR3 create 32,768 x 8 KiB, R=8."""
+    import torch
+    from parparpar_b200 import par2, par3
+    g = torch.Generator(device=f"cuda:{dev}")
+    g.manual_seed(1)
+    d = torch.randint(0, 256, (8192, 32768), dtype=torch.uint8, device=f"cuda:{dev}", generator=g)
+    o = torch.zeros((64, 32768), dtype=torch.uint8, device=f"cuda:{dev}")
+    for _ in range(3):
+        par2.par2_create(d, np.arange(8192), list(range(64)), out=o, ctx=ctx)
+        ctx.synchronize()
+    x = d.view(torch.int64).view(32768, 1024)
+    r = torch.zeros((8, 1024), dtype=torch.int64, device=f"cuda:{dev}")
+    par3.GF64Controller.ctx = ctx
+    par3.GF64Controller.ComputeRecoveryBlocks(x, 32768, r, 8, 1024, 0, 32768)
+    ctx.synchronize()
+    print(json.dumps({"profile_tc": "ok"}), flush=True)
+
+
 def profile_hashes(ctx, dev):
     """The small ncu case of the hash kernels: 256 MiB of seeded device data
     (larger than L2) hashed once each way -- PAR2 MD5 + CRC32 of 8,192 x
@@ -772,6 +794,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-hashes", action="store_true",
                     help="one launch of each block-hash kernel on 256 MiB (a small case for ncu), then exit")
+    ap.add_argument("--profile-tc", action="store_true",
+                    help="the small ncu case of the tensor-core region kernels (256 MiB), then exit")
     ap.add_argument("--gf16-kernel", default="auto", choices=["auto", "lut", "tensor"])
     ap.add_argument("--gf64-kernel", default="auto", choices=["auto", "lut", "tensor"])
     args = ap.parse_args()
@@ -807,6 +831,9 @@ def main():
 
     if args.profile_hashes:
         profile_hashes(ctx, local)
+        return
+    if args.profile_tc:
+        profile_tc(ctx, local)
         return
     if args.batched_only:
         print(json.dumps(measure_batched_vs_plain(ctx, timer, args.steps, args.warmup, local)), flush=True)
