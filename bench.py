@@ -126,7 +126,8 @@ def load_bf16_peak():
 # DRAM bytes (read + write) per launch of the dominant kernel, from the ncu
 # captures summarised in profiles/ (the file named after kernel and workload)
 TRAFFIC = {
-    "k_gf16_muladd_tc.par2_create_32768x32KiB_R64": 2465423872 + 10860288,
+    # the 8,192-slice capture (543.1 + 9.5 MB) scaled to the 32,768-slice launch
+    "k_gf16_muladd_tc.par2_create_32768x32KiB_R64": 4 * (543139328 + 9490176),
     "k_gf16_muladd_tc.par2_create_1024x1MiB_R8": 1087907000 + 10907904,
     "k_gf64_matvec_tc.par3_create_131072x8KiB_R8": 1083011000 + 3985664,
 }
