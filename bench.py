@@ -387,7 +387,8 @@ def cpu_baseline_sample(name, budget_s=12.0, threads=0):
         if w["field"] == "hash2":
             if kind == "reference":
                 run = lambda: R.par2_hash_file(inp.reshape(-1), w["s"])
-                what = "HasherInput_Scalar (block MD5+CRC32 and the file MD5 lane)"
+                what = (f"HasherInput_{R.par2_hasher_method()} (the variant the reference selects on this CPU; "
+                        "block MD5+CRC32 and the file MD5 lane)")
             else:
                 run = lambda: orc.par2_block_hashes(inp, w["s"])
                 what = "hashlib MD5 + zlib CRC32"

@@ -332,8 +332,13 @@ class Reference:
         return a
 
     # ---- block hashes -----------------------------------------------------
+    def par2_hasher_method(self) -> str:
+        self.L.ref_par2_hasher_method.restype = ctypes.c_char_p
+        return self.L.ref_par2_hasher_method().decode()
+
     def par2_hash_file(self, data: np.ndarray, slice_size: int):
-        """One file through the reference hasher: (IFSC entries (n, 20), file MD5)."""
+        """One file through the reference hasher (the variant it selects for
+        this CPU): (IFSC entries (n, 20), file MD5)."""
         data = np.ascontiguousarray(data, dtype=np.uint8)
         n = (data.size + slice_size - 1) // slice_size
         ifsc = np.zeros((max(n, 1), 20), dtype=np.uint8)

@@ -16,7 +16,8 @@
 //   region ops   : gf64_region_* dispatch table (gf64/gf64_global.h:23-37)
 //   FFT          : gf64_addfft64_{fwd,inv}_recursive_scratch
 //                  (gf64/gf64_additive_fft_hqc2026.c:1656,1680)
-//   block hashes : HasherInput_Scalar update / getBlock / end
+//   block hashes : setup_hasher + HasherInput_Create (hasher/hasher.cpp: the
+//                  fastest variant the CPU supports) update / getBlock / end
 //                  (hasher/hasher_input_base.h:44-128), driven like the PAR2
 //                  hasher binding (src/gf.cc:928-1037); blake3_hash
 //                  (hasher/hasher_blake3.h:50)
@@ -30,7 +31,7 @@ extern "C" {
 #include "gf64_additive_fft.h"
 #include "hasher_blake3.h"
 }
-#include "hasher_input_impl.h"
+#include "hasher.h"
 #include <cstdint>
 #include <cstring>
 #include <future>
@@ -219,8 +220,22 @@ void ref_gf64_poly_mul(uint64_t* out, const uint64_t* a, size_t la, const uint64
 // every full slice gets getBlock(md5crc, 0); a trailing partial slice gets
 // getBlock(md5crc, slice - tail) (zero padding); then end() gives the file MD5.
 // ifsc receives ceil(len / slice) 20-byte entries.
+static void ensure_hasher() {
+	static bool done = false;
+	if (!done) {
+		setup_hasher();
+		done = true;
+	}
+}
+
+const char* ref_par2_hasher_method() {
+	ensure_hasher();
+	return hasherInput_methodName();
+}
+
 void ref_par2_hash_file(const uint8_t* data, size_t len, size_t slice, uint8_t* ifsc, uint8_t* file_md5) {
-	IHasherInput* h = HasherInput_Scalar::create();
+	ensure_hasher();
+	IHasherInput* h = HasherInput_Create();
 	size_t pos = 0;
 	while (len - pos >= slice) {
 		h->update(data + pos, slice);

@@ -19,7 +19,8 @@ Fixtures:
   gf64_ops.npz     gf64 mul/inverse pairs, a Cauchy matrix, a matvec, a solve.
   gf64_fft.npz     additive FFT forward/inverse (recursive, Cantor basis).
   hashes.npz       block hashes from the reference's hasher: PAR2 IFSC entries
-                   and file MD5s (HasherInput_Scalar driven like src/gf.cc:928-1037),
+                   and file MD5s (the HasherInput variant setup_hasher selects,
+                   driven like src/gf.cc:928-1037),
                    BLAKE3 digests (hasher/hasher_blake3.c), the PAR3 data-block
                    checksum layout of lib/par3gen.js:1001-1017 and recovery
                    packets laid out as src/gf64_addon.cc:2884-2934, checksummed
