@@ -455,15 +455,15 @@ cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned
 }
 
 cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<uint64_t> attr{0};
+  if (!device_done(attr)) {
     cudaError_t e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          tc16::Shape<1>::kSmemBytes);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc16::Shape<2>::kSmemBytes);
     if (e != cudaSuccess) return e;
-    attr = true;
+    device_mark(attr);
   }
   // two output groups per CTA when every job's outputs pair up into groups of 16
   int kg = 2;

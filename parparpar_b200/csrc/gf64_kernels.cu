@@ -324,10 +324,11 @@ static cudaError_t matvec_common(const uint64_t* d_in, const uint64_t* const* d_
                                  uint64_t* d_out, uint64_t* const* d_out_ptrs, size_t out_stride, bool accumulate,
                                  int sms, cudaStream_t s) {
   if (!n_out || !words) return cudaSuccess;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_gf64_matvec_lut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem);
-    attr_set = true;
+  static std::atomic<uint64_t> attr{0};
+  if (!device_done(attr)) {
+    cudaError_t e = cudaFuncSetAttribute(k_gf64_matvec_lut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMvSmem);
+    if (e != cudaSuccess) return e;
+    device_mark(attr);
   }
   const size_t rt = ceil_div(n_out, kMvR);
   const size_t wt = ceil_div(words, kMvTile);

@@ -312,12 +312,12 @@ static uint64_t tiles64(const Gf64TcJob& j) { return (uint64_t)j.pairs * j.wt; }
 }  // namespace tc64
 
 cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<uint64_t> attr{0};
+  if (!device_done(attr)) {
     cudaError_t e = cudaFuncSetAttribute(tc64::k_gf64_matvec_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          tc64::kSmemBytes);
     if (e != cudaSuccess) return e;
-    attr = true;
+    device_mark(attr);
   }
   // drop empty jobs (nothing to multiply) after zeroing their outputs
   uint32_t m = 0;

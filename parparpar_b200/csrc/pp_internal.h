@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -14,6 +15,19 @@
 struct pp_ctx;
 
 namespace pp {
+
+// One-time setup per device (kernel attributes are set per device): whether
+// the current device's bit is set in `mask`, and setting it.
+inline bool device_done(const std::atomic<uint64_t>& mask) {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d >= 0 && d < 64 && ((mask.load(std::memory_order_acquire) >> d) & 1u);
+}
+inline void device_mark(std::atomic<uint64_t>& mask) {
+  int d = 0;
+  cudaGetDevice(&d);
+  if (d >= 0 && d < 64) mask.fetch_or(1ull << d, std::memory_order_acq_rel);
+}
 
 // Launch counter: every kernel launch issued by this library increments it
 // (reported by pp_ctx_launch_count so callers can account for native work).
