@@ -78,7 +78,7 @@ def bit_macs(w):
     """GF(2) multiply-accumulates of a create: every (input word, output)
     pair is a 16x16 (GF(2^16)) or 64x64 (GF(2^64)) bit-matrix product; the
     tensor-core kernels run exactly these as int8 MACs."""
-    if w["field"] == "gf16":
+    if w["field"] in ("gf16", "gf16_repair"):  # PAR2 repair: the decode product over all N sources
         return (w["n"] * w["s"] // 2) * w["r"] * 256
     if w["field"] == "gf64":
         return (w["n"] * w["s"] // 8) * w["r"] * 4096
@@ -210,6 +210,8 @@ WORKLOADS = {
     "par3_repair_262144x4KiB_R4096_1pct": dict(field="gf64_repair", n=262144, s=4 * 1024, r=2621),
     # forward additive FFT of the same 1 GiB: 1,024 word columns of 131,072 coefficients
     "par3_fft_fwd_131072x8KiB": dict(field="fft", n=131072, s=8 * 1024, r=0),
+    # PAR2 repair: 64 of 32,768 slices lost, restored from the R=64 recovery slices
+    "par2_repair_32768x32KiB_R64_lost64": dict(field="gf16_repair", n=32768, s=32 * 1024, r=64),
     # block hashes over 1 GiB of resident slices / blocks
     "par2_hash_32768x32KiB": dict(field="hash2", n=32768, s=32 * 1024, r=0),
     "par3_hash_131072x8KiB": dict(field="hash3", n=131072, s=8 * 1024, r=0),
@@ -249,6 +251,18 @@ def setup_job(name, dev, seed, ctx):
     g = torch.Generator(device=f"cuda:{dev}")
     g.manual_seed(seed)
     job = dict(w)
+    if w["field"] == "gf16_repair":
+        # the decode's sources: the valid inputs then the recovery slices (the
+        # recovery contents do not change the work); the lost set is seeded
+        n, m = w["n"], w["r"]
+        lost = np.sort(np.random.default_rng(seed).choice(n, m, replace=False))
+        valid = np.ones(n, dtype=bool)
+        valid[lost] = False
+        srcs = torch.randint(0, 256, (n, w["s"]), dtype=torch.uint8, device=f"cuda:{dev}", generator=g)
+        job.update(d_in=srcs, valid=valid, exps=list(range(m)),
+                   d_fac=torch.zeros((m, n), dtype=torch.int16, device=f"cuda:{dev}"),
+                   d_out=torch.zeros((m, w["s"]), dtype=torch.uint8, device=f"cuda:{dev}"))
+        return job
     if w["field"] in HASH_FIELDS:
         d_in = torch.randint(0, 256, (w["n"], w["s"]), dtype=torch.uint8, device=f"cuda:{dev}", generator=g)
         out_bytes = {"hash2": 20, "hash3": 16, "pkt3": 64 + w["s"]}[w["field"]]
@@ -280,6 +294,8 @@ def step_fn(job, ctx):
     from parparpar_b200 import par2, par3
     if job["field"] == "gf16":
         return lambda: par2.par2_create(job["d_in"], job["idx"], job["exps"], out=job["d_out"], ctx=ctx)
+    if job["field"] == "gf16_repair":
+        return lambda: par2_repair_step(job, ctx)
     if job["field"] in HASH_FIELDS:
         return hash_fn(job, job["d_in"], job["d_out"], ctx)
     par3.GF64Controller.ctx = ctx
@@ -292,10 +308,20 @@ def step_fn(job, ctx):
                                                              job["words"], 0, job["n"])
 
 
+def par2_repair_step(job, ctx):
+    """Galois16RecMatrix inversion (factors on the device) + the decode product."""
+    from parparpar_b200 import par2
+    m = par2.Galois16RecMatrix(ctx=ctx)
+    used = list(job["exps"])
+    if not m.Compute(job["valid"], int(job["valid"].sum()), used, out=job["d_fac"]):
+        raise RuntimeError("PAR2 repair matrix not invertible")
+    par2.gf16_muladd(job["d_in"], job["d_fac"], out=job["d_out"], ctx=ctx)
+
+
 def dtype_of(w):
     """Arithmetic type of the path: GF(2^16) symbols, GF(2^64) words, or the
     32-bit words of MD5 / CRC32 / BLAKE3."""
-    return {"gf16": "u16"}.get(w["field"], "u32" if w["field"] in HASH_FIELDS else "u64")
+    return {"gf16": "u16", "gf16_repair": "u16"}.get(w["field"], "u32" if w["field"] in HASH_FIELDS else "u64")
 
 
 def hash_fn(job, src, dst, ctx):
@@ -324,6 +350,8 @@ def dominant_kernel(w, args):
         return "k_gf16_muladd_lut" if args.gf16_kernel == "lut" else "k_gf16_muladd_tc"
     if w["field"] == "fft":
         return "k_fft_*"
+    if w["field"] == "gf16_repair":
+        return "k_gf16_muladd_tc"
     if w["field"] == "hash2":
         return "k_par2_block_hash"
     if w["field"] in ("hash3", "pkt3"):
@@ -340,7 +368,7 @@ def algo_bytes(job):
         return job["n"] * (job["s"] + 16)
     if job["field"] == "pkt3":  # blocks read, packets written
         return job["n"] * (2 * job["s"] + 64)
-    if job["field"] == "gf64_repair":  # (N - n) known blocks + n recovery blocks read, n blocks written
+    if job["field"] in ("gf64_repair", "gf16_repair"):  # (N - n) known + n recovery read, n written
         return (job["n"] + job["r"]) * job["s"]
     return (job["n"] + job["r"]) * job["s"]
 
@@ -401,6 +429,29 @@ def cpu_baseline_sample(name, budget_s=12.0, threads=0):
                     else "oracle packet assembly")
         sample = f"{sub_n} x {w['s']} B of the workload's {w['n']} blocks; {what}; 1 thread"
         cores = 1
+    elif w["field"] == "gf16_repair" and orc.Reference.available():
+        # the reference's Galois16RecMatrix inversion + its coefficient-driven
+        # PAR2 controller decode over a 2,048-byte sub-range of every source
+        R, kind, cores = orc.Reference(), "reference", os.cpu_count() or 1
+        sub = 2048
+        inp = rng.integers(0, 256, (w["n"], sub), dtype=np.uint8)
+        lost = np.sort(rng.choice(w["n"], w["r"], replace=False))
+        valid = np.ones(w["n"], dtype=np.uint8)
+        valid[lost] = 0
+
+        # the inversion's cost does not depend on the slice length, the
+        # decode's is linear in it: time both, scale the decode to full slices
+        t0 = time.perf_counter()
+        ok, f, used = R.par2_invert(valid, list(range(w["r"])), threads=threads)
+        t_inv = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        R.par2_create_coeffs(inp, sub, f, threads=threads)
+        t_dec = time.perf_counter() - t0
+        t_full = t_inv + t_dec * (w["s"] / sub)
+        sample = (f"inversion ({w['r']} lost of {w['n']}, {t_inv:.2f} s) + decode of {w['n']} sources x {sub} B "
+                  f"(a {sub}-byte sub-range of every slice, {t_dec:.3f} s, scaled x{w['s'] // sub} to the slices)")
+        return dict(value=w["n"] * w["s"] / t_full / 1e9, unit="GB/s", cores=cores, kind=kind, sample=sample,
+                    seconds_per_run=t_full, runs=1)
     elif orc.Reference.available():
         R = orc.Reference()
         kind = "reference"
@@ -883,6 +934,12 @@ def main():
         h_in.copy_(job["d_in"])
         h_out = torch.empty(tuple(job["d_out"].shape), dtype=torch.uint8).pin_memory()
         e2e_f = hash_fn(job, h_in, h_out, ctx)
+    elif w["field"] == "gf16_repair":
+        h_in = torch.empty((w["n"], w["s"]), dtype=torch.uint8).pin_memory()
+        h_in.copy_(job["d_in"])
+        h_out = torch.empty((w["r"], w["s"]), dtype=torch.uint8).pin_memory()
+        hjob = dict(job, d_in=h_in, d_out=h_out, d_fac=np.zeros((w["r"], w["n"]), dtype=np.uint16))
+        e2e_f = lambda: par2_repair_step(hjob, ctx)
     elif w["field"] == "gf16":
         h_in = torch.empty((w["n"], w["s"]), dtype=torch.uint8).pin_memory()
         h_in.copy_(job["d_in"])

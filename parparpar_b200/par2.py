@@ -131,9 +131,10 @@ class Galois16RecMatrix:
     def setNumThreads(self, threads: int):  # API parity; the device decides its own parallelism
         pass
 
-    def Compute(self, inputValid, validCount, recovery) -> bool:
+    def Compute(self, inputValid, validCount, recovery, out=None) -> bool:
         """recovery: a Python list, sorted and truncated in place like the
-        reference's std::vector<uint16_t>&."""
+        reference's std::vector<uint16_t>&.  out: optional (m, n) uint16
+        buffer (host or CUDA) for the factors; default a new numpy array."""
         v = np.ascontiguousarray(np.asarray([1 if x else 0 for x in inputValid], dtype=np.uint8))
         n = v.size
         if int(v.sum()) != validCount:
@@ -141,7 +142,7 @@ class Galois16RecMatrix:
         m = n - validCount
         rec = np.ascontiguousarray(np.asarray(recovery, dtype=np.uint16)).copy()
         nrec = ctypes.c_uint(rec.size)
-        f = np.zeros((max(m, 1), n), dtype=np.uint16)
+        f = np.zeros((max(m, 1), n), dtype=np.uint16) if out is None else out
         st = lib.pp_par2_invert(self.ctx.h, ptr(v), n, ptr(rec), ctypes.byref(nrec), ptr(f))
         if st == _lib.PP_ERR_NOT_INVERTIBLE:
             return False
