@@ -338,7 +338,12 @@ def hash_fn(job, src, dst, ctx):
 def kernel_fn(job, ctx):
     """The dominant kernel alone: after the first call the coefficient table
     (PAR2 tiles / PAR3 Cauchy matrix) is resident, so a step is the region
-    kernel (plus, when the job is split over CTAs, a memset of the outputs)."""
+    kernel (plus, when the job is split over CTAs, a memset of the outputs).
+    PAR2 repair: the decode product with the factors of one inversion."""
+    if job["field"] == "gf16_repair":
+        from parparpar_b200 import par2
+        par2_repair_step(job, ctx)
+        return lambda: par2.gf16_muladd(job["d_in"], job["d_fac"], out=job["d_out"], ctx=ctx)
     return step_fn(job, ctx)
 
 

@@ -749,10 +749,18 @@ PP_API int pp_par2_invert(pp_ctx* ctx, const uint8_t* valid, unsigned num_inputs
   std::sort(rec.begin(), rec.end());
   std::vector<uint16_t> logs(num_inputs);
   for (unsigned i = 0; i < num_inputs; i++) logs[i] = gf16h().ilog[i];
+  // The matrix [valid columns | lost columns] is reduced by eliminating on
+  // the lost columns; row operations never mix the two blocks, so the same
+  // pivots (and zero pivots) arise from the m x m lost block B alone.  The
+  // factors are then [B^-1 * valid block | B^-1]: an m x m elimination plus
+  // one region product, instead of m pivot steps over all n columns.
   const size_t ld = (num_inputs + 7) & ~(size_t)7;
+  const size_t ldb = (m + 7) & ~(size_t)7;
   uint16_t* d_mat = (uint16_t*)scratch(ctx, S_D, (size_t)m * ld * 2);
   uint16_t* d_fcol = (uint16_t*)scratch(ctx, S_E, (size_t)m * 2 + 64);
-  if (!d_mat || !d_fcol) return set_err(ctx, PP_ERR_NO_MEMORY, "inversion matrix");
+  uint16_t* d_blk = (uint16_t*)scratch(ctx, S_PKT, (size_t)m * ldb * 2);
+  uint16_t* d_fac = (uint16_t*)scratch(ctx, S_OUT, (size_t)m * ld * 2);
+  if (!d_mat || !d_fcol || !d_blk || !d_fac) return set_err(ctx, PP_ERR_NO_MEMORY, "inversion matrix");
   int* d_status = (int*)((char*)d_fcol + (((size_t)m * 2 + 15) & ~(size_t)15));
   int st;
   const uint16_t* d_logs = to_device(ctx, S_A, logs.data(), num_inputs, &st);
@@ -765,22 +773,33 @@ PP_API int pp_par2_invert(pp_ctx* ctx, const uint8_t* valid, unsigned num_inputs
     if (st) return st;
     CUDA_TRY(ctx, cudaMemsetAsync(d_mat, 0, (size_t)m * ld * 2, ctx->stream));
     CUDA_TRY(ctx, launch_gf16_build_rec_matrix(d_logs, d_col, num_inputs, d_rec, m, d_mat, ld, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(d_blk, ldb * 2, d_mat + vc, ld * 2, (size_t)m * 2, m, cudaMemcpyDeviceToDevice,
+                                    ctx->stream));
     CUDA_TRY(ctx, cudaMemsetAsync(d_status, 0xFF, sizeof(int), ctx->stream));
-    CUDA_TRY(ctx, launch_gf16_invert(d_mat, m, num_inputs, ld, vc, d_fcol, d_status, ctx->stream));
+    CUDA_TRY(ctx, launch_gf16_invert(d_blk, m, m, ldb, 0, d_fcol, d_status, ctx->stream));
     int hs = -1;
     CUDA_TRY(ctx, cudaMemcpyAsync(&hs, d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     if (hs < 0) break;
     rec.erase(rec.begin() + hs);  // PAR2 flaw: drop the recovery row and retry
   }
-  if (is_device_ptr(factors)) {
-    CUDA_TRY(ctx, cudaMemcpy2DAsync(factors, (size_t)num_inputs * 2, d_mat, ld * 2, (size_t)num_inputs * 2, m,
-                                    cudaMemcpyDeviceToDevice, ctx->stream));
-  } else {
-    CUDA_TRY(ctx, cudaMemcpy2DAsync(factors, (size_t)num_inputs * 2, d_mat, ld * 2, (size_t)num_inputs * 2, m,
-                                    cudaMemcpyDeviceToHost, ctx->stream));
+  // factors = [B^-1 * valid block | B^-1]
+  if (vc) {
+    uint8_t* aexp = nullptr;
+    if (use_tensor(ctx->gf16_kernel, m, m)) {
+      aexp = (uint8_t*)scratch(ctx, S_AEXP, gf16_tc_coeff_bytes(m, m));
+      if (!aexp) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficient tiles");
+    }
+    CUDA_TRY(ctx, gf16_region(ctx->gf16_kernel, (const uint8_t*)d_mat, ld * 2, m, (size_t)vc * 2, d_blk, ldb, m,
+                              (uint8_t*)d_fac, ld * 2, false, ctx->sms, aexp, ctx->d_status, ctx->stream));
   }
+  CUDA_TRY(ctx, cudaMemcpy2DAsync(d_fac + vc, ld * 2, d_blk, ldb * 2, (size_t)m * 2, m, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpy2DAsync(factors, (size_t)num_inputs * 2, d_fac, ld * 2, (size_t)num_inputs * 2, m,
+                                  is_device_ptr(factors) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                  ctx->stream));
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (int r = device_status(ctx)) return r;
   memcpy(recovery, rec.data(), m * 2);
   *num_recovery = m;
   return PP_OK;

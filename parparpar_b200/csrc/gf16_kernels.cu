@@ -297,7 +297,7 @@ __global__ void k_gf16_pivot(uint16_t* __restrict__ mat, unsigned m, unsigned nc
   }
   for (unsigned r = threadIdx.x; r < m; r += blockDim.x) fcol[r] = mat[(size_t)r * ld + pc0 + k];
   __syncthreads();
-  const uint16_t ip = gf16_inv(p);
+  const uint16_t ip = gf16_inv_euclid(p);
   for (unsigned c = threadIdx.x; c < ncols; c += blockDim.x) {
     uint16_t v = (c == pc0 + k) ? (uint16_t)1 : rowk[c];
     rowk[c] = gf16_mul(v, ip);
@@ -343,9 +343,48 @@ k_gf16_eliminate(uint16_t* __restrict__ mat, unsigned m, unsigned ncols, size_t 
   *reinterpret_cast<uint4*>(rowr + c0) = make_uint4(bv[0], bv[1], bv[2], bv[3]);
 }
 
+// The whole elimination of an m x m matrix (m <= kInvSmall; row stride ld,
+// 16-byte aligned rows) by one CTA in shared memory: the same steps as
+// k_gf16_pivot + k_gf16_eliminate with pc0 = 0, all m pivots in one launch.
+constexpr unsigned kInvSmall = 128;
+__global__ void __launch_bounds__(1024) k_gf16_invert_small(uint16_t* __restrict__ mat, unsigned m, size_t ld,
+                                                            int* __restrict__ status) {
+  __shared__ uint16_t a[kInvSmall * kInvSmall];
+  __shared__ uint16_t fcol[kInvSmall];
+  const unsigned mm = m * m;
+  for (unsigned e = threadIdx.x; e < mm; e += blockDim.x) a[e] = mat[(size_t)(e / m) * ld + e % m];
+  __syncthreads();
+  for (unsigned k = 0; k < m; k++) {
+    const uint16_t p = a[k * m + k];
+    if (p == 0) {  // uniform across the CTA
+      if (threadIdx.x == 0) *status = (int)k;
+      return;
+    }
+    for (unsigned r = threadIdx.x; r < m; r += blockDim.x) fcol[r] = a[r * m + k];
+    __syncthreads();
+    const uint16_t ip = gf16_inv_euclid(p);
+    for (unsigned c = threadIdx.x; c < m; c += blockDim.x) a[k * m + c] = gf16_mul(c == k ? (uint16_t)1 : a[k * m + c], ip);
+    __syncthreads();
+    for (unsigned e = threadIdx.x; e < mm; e += blockDim.x) {
+      const unsigned r = e / m, c = e % m;
+      const uint16_t f = fcol[r];
+      if (r == k || f == 0) continue;
+      const uint16_t y = gf16_mul(f, a[k * m + c]);
+      a[e] = c == k ? y : (uint16_t)(a[e] ^ y);
+    }
+    __syncthreads();
+  }
+  for (unsigned e = threadIdx.x; e < mm; e += blockDim.x) mat[(size_t)(e / m) * ld + e % m] = a[e];
+}
+
 cudaError_t launch_gf16_invert(uint16_t* d_mat, unsigned m, unsigned ncols, size_t ld, unsigned pc0,
                                uint16_t* d_fcol, int* d_status, cudaStream_t s) {
-  dim3 grid((unsigned)ceil_div(ld, 256 * 8), m);
+  if (pc0 == 0 && ncols == m && m <= kInvSmall) {
+    k_gf16_invert_small<<<1, 1024, 0, s>>>(d_mat, m, ld, d_status);
+    note_launch();
+    return cudaGetLastError();
+  }
+  dim3 grid((unsigned)ceil_div(ncols, 256 * 8), m);
   for (unsigned k = 0; k < m; k++) {
     k_gf16_pivot<<<1, 1024, 0, s>>>(d_mat, m, ncols, ld, pc0, k, d_fcol, d_status);
     k_gf16_eliminate<<<grid, 256, 0, s>>>(d_mat, m, ncols, ld, pc0, k, d_fcol, d_status);

@@ -70,8 +70,10 @@ cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigne
                                   unsigned a_stride = 0);  // 0: the tiles of exactly these n_in inputs
 
 // PAR2 inversion (Gauss-Jordan without pivoting, identity columns in place).
-// d_mat: m rows x ncols (row stride ld elements).  Runs all m pivot steps;
-// d_status[0] receives -1 on success or the first row whose pivot was zero.
+// d_mat: m rows x ncols (row stride ld elements, rows 16-byte aligned).  Runs
+// all m pivot steps; d_status[0] (set to -1 by the caller) receives the first
+// row whose pivot was zero.  A square matrix (pc0 = 0, ncols = m) of at most
+// 128 rows is eliminated by one CTA in one launch.
 cudaError_t launch_gf16_invert(uint16_t* d_mat, unsigned m, unsigned ncols, size_t ld, unsigned pivot_col0,
                                uint16_t* d_fcol, int* d_status, cudaStream_t s);
 

@@ -218,7 +218,9 @@ def test_par2_invert_golden(ctx, golden):
 def test_par2_invert_vs_oracle(ctx, oracle):
     from parparpar_b200 import par2
     rng = np.random.default_rng(21)
-    for n, miss, extra in [(1000, 40, 3), (32768, 8, 0), (257, 257, 1)]:
+    # lost blocks of 3..200 rows: one-CTA elimination (<= 128) and the
+    # multi-launch form (> 128), lookup (< 8) and tensor-core products
+    for n, miss, extra in [(1000, 40, 3), (32768, 8, 0), (257, 257, 1), (50, 3, 0), (3000, 200, 2), (600, 129, 0)]:
         v = np.ones(n, dtype=np.uint8)
         v[rng.choice(n, miss, replace=False)] = 0
         rec = sorted(rng.choice(65535, miss + extra, replace=False).tolist())
