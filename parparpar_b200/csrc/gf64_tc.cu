@@ -37,6 +37,7 @@
 // records an error in *status, drains its copies and MMAs, frees TMEM and
 // returns.
 #include <algorithm>
+#include <cstdlib>
 
 #include "pp_common.cuh"
 #include "pp_internal.h"
@@ -62,6 +63,24 @@ constexpr int kOffRaw = kOffB + kBs * kBBytes;    // 160 KiB
 constexpr int kOffBar = kOffRaw + kLd * kRawBytes;  // 192 KiB
 constexpr int kSmemBytes = kOffBar + 256 + 1024;
 constexpr uint32_t kIdesc = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+
+// Row b of the 64x64 GF(2) matrix of multiplication by c: bit e is bit b of
+// c * x^e (closed form, see the header).
+PP_D uint64_t mul_matrix_row(uint64_t c, unsigned b) {
+  const uint64_t rv = __brevll(c);
+  uint64_t qrow = rv >> (63 - b);
+#pragma unroll
+  for (int si = 0; si < 4; si++) {
+    const int sft = si == 0 ? 0 : si == 1 ? 1 : si == 2 ? 3 : 4;
+    const int d = (int)b - sft;
+    if (d >= 0) {
+      if (d + 1 < 64) qrow ^= rv << (d + 1);
+      if (d <= 2) qrow ^= rv << (d + 61);
+      if (d <= 1) qrow ^= rv << (d + 62);
+    }
+  }
+  return qrow;
+}
 
 // One CTA per work item of the job table (tc_batch.h): the item fixes the
 // job, the output pair, the word tile and the stage range; mode 0 stores,
@@ -200,19 +219,7 @@ k_gf64_matvec_tc(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
       for (unsigned k = 0; k < nst; k++, g++) {
         const unsigned sl = g % kLd, bs = g % kBs;
         const uint64_t c_nxt = coef(k + 1);  // prefetch the next stage's coefficient
-        // row b of the multiplication matrix of c_cur (closed form, see header)
-        const uint64_t rv = __brevll(c_cur);
-        uint64_t qrow = rv >> (63 - a_b);
-#pragma unroll
-        for (int si = 0; si < 4; si++) {
-          const int sft = si == 0 ? 0 : si == 1 ? 1 : si == 2 ? 3 : 4;
-          const int d = (int)a_b - sft;
-          if (d >= 0) {
-            if (d + 1 < 64) qrow ^= rv << (d + 1);
-            if (d <= 2) qrow ^= rv << (d + 61);
-            if (d <= 1) qrow ^= rv << (d + 62);
-          }
-        }
+        const uint64_t qrow = mul_matrix_row(c_cur, a_b);
         const uint32_t qlo = (uint32_t)qrow, qhi = (uint32_t)(qrow >> 32);
         if (*err || !mbar_wait(BAR(RAW_FULL + sl), (g / kLd) & 1)) {
           *err = 1;
@@ -299,6 +306,270 @@ k_gf64_matvec_tc(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
   if (threadIdx.x == 0 && *err) atomicOr(status, 1);
 }
 
+// ---------------------------------------------------------------------------
+// CTA-pair variant (cluster of 2, tcgen05 cta_group::2).  The pair computes
+// 4 outputs (M = 256 rows: rows 0-127 = outputs o0, o0+1 in CTA 0, rows
+// 128-255 = outputs o0+2, o0+3 in CTA 1) x 512 words with two MMAs of N = 256;
+// each MMA takes B columns 0-127 from CTA 0 and 128-255 from CTA 1.  So each
+// CTA builds the A rows of its own 2 outputs (as above) but the B rows of
+// only 256 of the 512 words: per SM, the B tile the builders write and the
+// tensor cores read is half that of the one-CTA kernel for the same work,
+// and shared-memory bandwidth is what limits that kernel.
+//
+// Word mapping: CTA r builds words w0 + 256 r + u, u = 0..255, as B rows
+// u (MMA nn = u / 128 takes rows 128 nn .. 128 nn + 127).  Column c of
+// accumulator nn is therefore word w0 + 256 (c / 128) + 128 nn + c % 128.
+//
+// Pipeline: each CTA copies its own raw rows and builds its own tiles;
+// CTA 1's warp 1 relays "stage built" to CTA 0 (one remote arrive per
+// stage), CTA 0's warp 1 issues the pair MMAs, and its commits arrive on the
+// "stage free", "accumulators ready" and "MMAs done" barriers of both CTAs.
+// All waits are bounded as in the one-CTA kernel; the only unbounded
+// barriers are the two cluster barriers that every thread of both CTAs
+// reaches on every path.
+constexpr int kPHalf = 256;                       // words built per CTA
+constexpr int kPBBytes = kPHalf * 128;            // 32 KiB
+constexpr int kPRawBytes = kStageIn * kPHalf * 8;  // 4 KiB
+// kPLd raw-row stages, kPBs operand stages (ring depths 4-8 x 3-4 measured
+// within 4 % of each other on the 1 GiB R=8 job; the deepest fits 227 KiB)
+constexpr int pair_smem_bytes(int ld, int bs) { return bs * (kABytes + kPBBytes) + ld * kPRawBytes + 256 + 1024; }
+constexpr int kPLd = 8;
+constexpr int kPBs = 4;
+constexpr int kPSmemBytes = pair_smem_bytes(kPLd, kPBs);
+static_assert(kPSmemBytes <= 227 * 1024, "shared memory per CTA");
+constexpr uint32_t kPIdesc = (2u << 4) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
+
+template <int kPLd, int kPBs>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    k_gf64_matvec_tc_pair(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ status) {
+  constexpr int kPOffA = 0;
+  constexpr int kPOffB = kPBs * kABytes;
+  constexpr int kPOffRaw = kPOffB + kPBs * kPBBytes;
+  constexpr int kPOffBar = kPOffRaw + kPLd * kPRawBytes;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t base_s = smem_addr(smem_raw);
+  const uint32_t pad = ((base_s + 1023) & ~1023u) - base_s;
+  uint8_t* smem = smem_raw + pad;
+  const uint32_t sA = base_s + pad + kPOffA, sB = base_s + pad + kPOffB, sRaw = base_s + pad + kPOffRaw;
+  const uint32_t bar0 = smem_addr(smem + kPOffBar);
+  enum {
+    RAW_FULL = 0,
+    RAW_EMPTY = RAW_FULL + kPLd,
+    OPB_FULL = RAW_EMPTY + kPLd,  // this CTA's builders done with stage slot
+    OPR_FULL = OPB_FULL + kPBs,   // CTA 0: CTA 1's builders done (relayed)
+    OP_EMPTY = OPR_FULL + kPBs,
+    D_FULL = OP_EMPTY + kPBs,
+    DONE = D_FULL + 1,
+    NBARS = DONE + 1
+  };
+  static_assert(8 * NBARS + 16 <= 256, "barrier area");
+  auto BAR = [&](int k) { return bar0 + 8u * (uint32_t)k; };
+  volatile uint32_t* tmem_holder = reinterpret_cast<volatile uint32_t*>(smem + kPOffBar + 8 * NBARS);
+  volatile int* err = reinterpret_cast<volatile int*>(smem + kPOffBar + 8 * NBARS + 8);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NBARS; k++) {
+      const bool by_builders = (k >= RAW_EMPTY && k < RAW_EMPTY + kPLd) || (k >= OPB_FULL && k < OPB_FULL + kPBs);
+      mbar_init(BAR(k), by_builders ? (uint32_t)kExp : 1u);
+    }
+    *err = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {  // both CTAs allocate together
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr((const void*)tmem_holder)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // the peer's barriers are initialised before any remote arrive
+  tc_fence_after();
+  const uint32_t tmem = *tmem_holder;
+  const TcSeg sg = tc_item(&batch, blockIdx.x >> 1);
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      uint32_t g = 0;
+      do {  // the pair's one item
+        const Gf64TcJob J = pinned_job(batch.job[sg.job]);
+        const size_t wc = (size_t)(sg.tile / J.pairs) * kWords + (size_t)kPHalf * rank;
+        const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)kPHalf, J.words - wc) : 0u;
+        const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
+        for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
+          const unsigned sl = g % kPLd;
+          if (g >= (uint32_t)kPLd && !mbar_wait(BAR(RAW_EMPTY + sl), (g / kPLd - 1) & 1)) {
+            *err = 1;
+            break;
+          }
+          const unsigned i0 = st * kStageIn;
+          const unsigned ni = raw_copy ? min((unsigned)kStageIn, J.n_in - i0) : 0u;
+          mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
+          for (unsigned ii = 0; ii < ni; ii++) {
+            const uint64_t* row = J.in_ptrs ? J.in_ptrs[i0 + ii] : J.in + (size_t)(i0 + ii) * J.in_stride;
+            bulk_g2s(sRaw + sl * kPRawBytes + ii * (kPHalf * 8), row + wc, raw_copy, BAR(RAW_FULL + sl));
+          }
+        }
+      } while (0);
+      if (*err) {
+        for (uint32_t k = g > (uint32_t)kPLd ? g - kPLd : 0; k < g; k++)
+          mbar_wait(BAR(RAW_FULL + k % kPLd), (k / kPLd) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const unsigned nst = sg.st1 - sg.st0;
+      if (rank == 0) {
+        // -------------------------------------------------------- MMA issuer
+        for (unsigned k = 0; k < nst; k++) {
+          const unsigned bs = k % kPBs;
+          const uint32_t ph = (k / kPBs) & 1;
+          if (*err || !mbar_wait(BAR(OPB_FULL + bs), ph) || !mbar_wait_cluster(BAR(OPR_FULL + bs), ph)) {
+            *err = 1;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int kk = 0; kk < 4; kk++) {
+#pragma unroll
+            for (int nn = 0; nn < 2; nn++) {
+              mma_i8_pair(tmem + nn * 256, sw128_desc(sA + bs * kABytes + 32 * kk),
+                          sw128_desc(sB + bs * kPBBytes + nn * (128 * 128) + 32 * kk), kPIdesc,
+                          (k > 0 || kk > 0) ? 1u : 0u);
+            }
+          }
+          mma_commit_pair(BAR(OP_EMPTY + bs));
+        }
+        if (!*err) mma_commit_pair(BAR(D_FULL));
+        mma_commit_pair(BAR(DONE));
+      } else {
+        // -------------------------------------------------------- relay
+        const uint32_t remote = peer_addr(BAR(OPR_FULL), 0);
+        for (unsigned k = 0; k < nst; k++) {
+          const unsigned bs = k % kPBs;
+          if (*err || !mbar_wait(BAR(OPB_FULL + bs), (k / kPBs) & 1)) {
+            *err = 1;
+            break;
+          }
+          mbar_arrive_remote(remote + 8u * bs);
+        }
+      }
+      // CTA 0's MMAs (which read this CTA's tiles and write its TMEM) have
+      // completed before the tiles and TMEM are released
+      if (!mbar_wait_cluster(BAR(DONE), 0)) *err = 1;
+    }
+  } else {
+    // ------------------------------------------------------------ operand builders
+    const int e = threadIdx.x - 64;  // 0..255
+    // B: word u = e of this CTA's half, row e % 128 of half e / 128
+    const unsigned bm = (unsigned)e & 127;
+    const uint32_t brow = (e >> 7) * (128 * 128) + (bm >> 3) * 1024 + (bm & 7) * 128, br7 = bm & 7;
+    // A: row m, input half ii (adjacent threads alternate ii)
+    const unsigned a_ii = e & 1, a_m = e >> 1, a_oo = a_m >> 6, a_b = a_m & 63;
+    const uint32_t arow_off = (a_m >> 3) * 1024 + (a_m & 7) * 128 + 8 * a_ii, ar7 = a_m & 7;
+    const int q = warp & 3;
+    const int nn_ep = (warp - 2) >> 2;  // epilogue: accumulator
+    uint32_t g = 0;
+    do {  // the pair's one item
+      const Gf64TcJob J = pinned_job(batch.job[sg.job]);
+      const unsigned o0 = 4 * (unsigned)(sg.tile % J.pairs) + 2 * rank;  // this CTA's two outputs
+      const size_t w0 = (size_t)(sg.tile / J.pairs) * kWords;
+      const size_t wc = w0 + (size_t)kPHalf * rank;
+      const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)kPHalf, J.words - wc) : 0u;
+      const bool okB = (unsigned)e < words_valid;
+      const unsigned nst = sg.st1 - sg.st0;
+      auto coef = [&](unsigned k) -> uint64_t {
+        const unsigned o = o0 + a_oo, i = (sg.st0 + k) * kStageIn + a_ii;
+        return (k < nst && o < J.n_out && i < J.n_in) ? J.coeff[(size_t)o * J.ldc + i] : 0ull;
+      };
+      uint64_t c_cur = coef(0);
+      for (unsigned k = 0; k < nst; k++, g++) {
+        const unsigned sl = g % kPLd, bs = g % kPBs;
+        const uint64_t c_nxt = coef(k + 1);
+        const uint64_t qrow = mul_matrix_row(c_cur, a_b);
+        const uint32_t qlo = (uint32_t)qrow, qhi = (uint32_t)(qrow >> 32);
+        if (*err || !mbar_wait(BAR(RAW_FULL + sl), (g / kPLd) & 1)) {
+          *err = 1;
+          break;
+        }
+        const unsigned i0 = (sg.st0 + k) * kStageIn;
+        const unsigned ni = min((unsigned)kStageIn, J.n_in - i0);
+        uint4 x = make_uint4(0, 0, 0, 0);
+        if (okB) {
+          const uint32_t raw = sRaw + sl * kPRawBytes + 8 * (unsigned)e;
+          const uint2 v0 = lds64(raw);
+          x.x = v0.x;
+          x.y = v0.y;
+          if (ni > 1) {
+            const uint2 v1 = lds64(raw + kPHalf * 8);
+            x.z = v1.x;
+            x.w = v1.y;
+          }
+        }
+        mbar_arrive(BAR(RAW_EMPTY + sl));
+        if (g >= (uint32_t)kPBs && !mbar_wait(BAR(OP_EMPTY + bs), (g / kPBs - 1) & 1)) {
+          *err = 1;
+          break;
+        }
+        const uint32_t at = sA + bs * kABytes, bt = sB + bs * kPBBytes;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          sts64(at + arow_off + ((j ^ ar7) << 4), qlo >> j, qhi >> j);
+          sts128(bt + brow + ((j ^ br7) << 4), x.x >> j, x.y >> j, x.z >> j, x.w >> j);
+        }
+        fence_async_smem();
+        mbar_arrive(BAR(OPB_FULL + bs));
+        c_cur = c_nxt;
+      }
+      // ---------------------------------------------------------- epilogue
+      if (*err || !mbar_wait_cluster(BAR(D_FULL), 0)) {
+        *err = 1;
+        break;
+      }
+      tc_fence_after();
+      const unsigned o = o0 + (q >> 1);
+      const unsigned half = q & 1;
+      uint64_t* orow = o < J.n_out ? (J.out_ptrs ? J.out_ptrs[o] : J.out + (size_t)o * J.out_stride) : nullptr;
+      for (int cc = 0; cc < 8; cc++) {
+        uint32_t r[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + 256 * nn_ep + 32 * cc, r);
+        uint32_t mine = 0;
+#pragma unroll
+        for (int jj = 0; jj < 32; jj++) {
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, r[jj] & 1u);
+          if (lane == jj) mine = bal;
+        }
+        const unsigned c = 32 * cc + lane;  // column of accumulator nn_ep
+        const size_t widx = (size_t)kPHalf * (c >> 7) + 128 * nn_ep + (c & 127);
+        if (!orow || w0 + widx >= J.words) continue;
+        uint32_t* dst = reinterpret_cast<uint32_t*>(orow + w0 + widx) + half;
+        if (sg.mode == 2) {
+          if (mine) atomicXor(dst, mine);
+        } else if (sg.mode == 1) {
+          *dst ^= mine;
+        } else {
+          *dst = mine;
+        }
+      }
+      tc_fence_before();
+    } while (0);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // both CTAs are done with TMEM and the peer's barriers
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+  if (threadIdx.x == 0 && *err) atomicOr(status, 1);
+}
+
 // zero rows given by a pointer table (outputs of a non-accumulating job whose
 // tiles are split across CTAs)
 __global__ void k_zero_rows(uint64_t* const* __restrict__ rows, unsigned n_rows, size_t words) {
@@ -311,21 +582,39 @@ static uint64_t tiles64(const Gf64TcJob& j) { return (uint64_t)j.pairs * j.wt; }
 
 }  // namespace tc64
 
+// Pair kernel (two SMs per tile) or one-CTA kernel for a whole table: the
+// pair kernel's tile has 4 outputs, so it is used when no job has fewer than
+// 4 (PARPAR_B200_GF64_PAIR=0 / 1 forces the choice).
+static bool use_pair_kernel(const Gf64TcBatch& b) {
+  static const int forced = [] {
+    const char* v = getenv("PARPAR_B200_GF64_PAIR");
+    return v && *v ? atoi(v) : -1;
+  }();
+  if (forced >= 0) return forced != 0;
+  for (uint32_t j = 0; j < b.n_jobs; j++)
+    if (b.job[j].n_out < 4) return false;
+  return true;
+}
+
 cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s) {
   static std::atomic<uint64_t> attr{0};
   if (!device_done(attr)) {
     cudaError_t e = cudaFuncSetAttribute(tc64::k_gf64_matvec_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          tc64::kSmemBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(tc64::k_gf64_matvec_tc_pair<tc64::kPLd, tc64::kPBs>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, tc64::kPSmemBytes);
     if (e != cudaSuccess) return e;
     device_mark(attr);
   }
+  const bool pair = use_pair_kernel(b);
   // drop empty jobs (nothing to multiply) after zeroing their outputs
   uint32_t m = 0;
   for (uint32_t j = 0; j < b.n_jobs; j++) {
     Gf64TcJob& J = b.job[j];
     if (!J.n_out || !J.words) continue;
     J.n_stages = (J.n_in + tc64::kStageIn - 1) / tc64::kStageIn;
-    J.pairs = (J.n_out + 1) / 2;
+    J.pairs = pair ? (J.n_out + 3) / 4 : (J.n_out + 1) / 2;
     const size_t wt = ceil_div(J.words, tc64::kWords);
     if (wt > 0xFFFFFFFFu) return cudaErrorInvalidValue;
     J.wt = (uint32_t)wt;
@@ -344,8 +633,9 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
   }
   b.n_jobs = m;
   if (!m) return cudaGetLastError();
-  const uint64_t ctas = tc_batch_plan(b, tc64::tiles64, sms);
-  if (ctas > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+  // the plan deals items to SMs, or to SM pairs for the pair kernel
+  const uint64_t items = tc_batch_plan(b, tc64::tiles64, pair ? std::max(1, sms / 2) : sms);
+  if (items > 0x3FFFFFFFull) return cudaErrorInvalidConfiguration;
   for (uint32_t j = 0; j < m; j++) {
     const Gf64TcJob& J = b.job[j];
     if (J.splits == 1 || J.accumulate) continue;
@@ -357,7 +647,11 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     }
     note_launch();
   }
-  tc64::k_gf64_matvec_tc<<<(unsigned)ctas, tc64::kThreads, tc64::kSmemBytes, s>>>(b, d_status);
+  if (pair)
+    tc64::k_gf64_matvec_tc_pair<tc64::kPLd, tc64::kPBs>
+        <<<2 * (unsigned)items, tc64::kThreads, tc64::kPSmemBytes, s>>>(b, d_status);
+  else
+    tc64::k_gf64_matvec_tc<<<(unsigned)items, tc64::kThreads, tc64::kSmemBytes, s>>>(b, d_status);
   note_launch();
   return cudaGetLastError();
 }

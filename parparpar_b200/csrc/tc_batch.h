@@ -56,7 +56,8 @@ struct Gf64TcJob {
   size_t words;
   uint32_t n_in, n_out;
   uint32_t n_stages;                  // ceil(n_in / 2)
-  uint32_t pairs;                     // ceil(n_out / 2)
+  uint32_t pairs;                     // output groups of a tile: ceil(n_out / 2), or
+                                      // ceil(n_out / 4) for the CTA-pair kernel
   uint32_t wt;                        // ceil(words / 512)
   uint32_t accumulate;
   uint32_t splits, per;               // stage range cut into `splits` parts of `per` stages
