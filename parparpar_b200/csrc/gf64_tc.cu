@@ -461,7 +461,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       }
       // CTA 0's MMAs (which read this CTA's tiles and write its TMEM) have
       // completed before the tiles and TMEM are released
-      if (!mbar_wait_cluster(BAR(DONE), 0)) *err = 1;
+      if (!mbar_wait(BAR(DONE), 0)) *err = 1;
     }
   } else {
     // ------------------------------------------------------------ operand builders
@@ -527,7 +527,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         c_cur = c_nxt;
       }
       // ---------------------------------------------------------- epilogue
-      if (*err || !mbar_wait_cluster(BAR(D_FULL), 0)) {
+      if (*err || !mbar_wait(BAR(D_FULL), 0)) {
         *err = 1;
         break;
       }

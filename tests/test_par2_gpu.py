@@ -201,6 +201,31 @@ def test_proc_mixed_host_device_inputs_reused_on_return(kctx, oracle):
     proc.deinit()
 
 
+@pytest.mark.parametrize("n,r,s", [
+    (8, 32, 512), (13, 32, 1000), (9, 29, 200), (40, 64, 333), (17, 64, 8193), (3000, 32, 4096),
+])
+def test_gf16_wide_outputs_vs_oracle(ctx, oracle, n, r, s):
+    """Output counts of 25-64 on the tensor-core kernel (two output groups per
+    CTA): ragged last word tiles, a slice shorter than one tile (200 bytes),
+    odd slices, input counts that are not a multiple of 8, a job split over
+    CTAs (3000 inputs: atomic XOR of partial products) and accumulation."""
+    import parparpar_b200._lib as L
+    from parparpar_b200 import par2
+    rng = np.random.default_rng(n * 7 + r * 11 + s)
+    inp = rng.integers(0, 256, (n, s), dtype=np.uint8)
+    co = rng.integers(0, 65536, (r, n)).astype(np.uint16)
+    exp = oracle.par2_muladd(list(inp), s, co)
+    ctx.set_gf16_kernel(L.PP_GF16_KERNEL_TENSOR)
+    try:
+        assert np.array_equal(par2.gf16_muladd(inp, co, ctx=ctx), exp)
+        base = rng.integers(0, 256, (r, s), dtype=np.uint8)
+        out = base.copy()
+        par2.gf16_muladd(inp, co, out=out, accumulate=True, ctx=ctx)
+        assert np.array_equal(out, exp ^ base)
+    finally:
+        ctx.set_gf16_kernel(L.PP_GF16_KERNEL_AUTO)
+
+
 def test_par2_invert_golden(ctx, golden):
     from parparpar_b200 import par2
     g = golden("par2_invert.npz")
