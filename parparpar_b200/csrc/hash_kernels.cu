@@ -130,18 +130,11 @@ __device__ __forceinline__ uint32_t masked_word(const uint8_t* row, uint64_t o, 
 
 // One thread per slice.  Rows are 16-byte aligned (data and stride).  The
 // message is L bytes: the row's first len bytes, then zeros.
-__global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restrict__ data, size_t stride,
-                                                         size_t n, uint64_t L,
-                                                         const uint64_t* __restrict__ lengths,
-                                                         uint8_t* __restrict__ out) {
-  extern __shared__ uint32_t crc_tab[];
-  crc_tables_init(crc_tab);
-  __syncthreads();
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint32_t* tk = crc_tab + (threadIdx.x % kCrcCopies);
-  const uint8_t* row = data + i * stride;
-  const uint64_t len = lengths ? (lengths[i] < L ? lengths[i] : L) : L;
+// MD5 and / or CRC32 of one slice's message (the row's first len bytes,
+// then zeros up to L bytes); MD5 goes to o20[0..16), CRC32 to o20[16..20).
+template <bool kMd5, bool kCrc>
+__device__ __forceinline__ void par2_slice_hash(const uint8_t* row, uint64_t len, uint64_t L, const uint32_t* tk,
+                                                uint8_t* o20) {
   uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
   uint32_t crc = 0xFFFFFFFFu;
   uint32_t m[16];
@@ -165,55 +158,98 @@ __global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restri
 #pragma unroll
       for (int q = 0; q < 4; q++) nx[q] = __ldg(reinterpret_cast<const uint4*>(row + 64 * (b + 1)) + q);
     }
+    if constexpr (kCrc) {
 #pragma unroll
-    for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
-    md5_block(st, m);
+      for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
+    }
+    if constexpr (kMd5) md5_block(st, m);
   }
   // the rest of the L / 64 whole message blocks: data tail, then zero padding
   const uint64_t nblk = L / 64;
   for (uint64_t b = nfull; b < nblk; b++) {
 #pragma unroll
     for (int w = 0; w < 16; w++) m[w] = masked_word(row, 64 * b + 4 * w, len);
+    if constexpr (kCrc) {
 #pragma unroll
-    for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
-    md5_block(st, m);
+      for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
+    }
+    if constexpr (kMd5) md5_block(st, m);
   }
   // final partial block (L % 64 bytes) with the MD5 padding
   const uint32_t tail = (uint32_t)(L % 64);
   const uint64_t t0 = 64 * nblk;
 #pragma unroll
   for (int w = 0; w < 16; w++) m[w] = (4u * w < tail) ? masked_word(row, t0 + 4 * w, len) : 0u;
+  if constexpr (kCrc) {
 #pragma unroll
-  for (uint32_t w = 0; w < 16; w++) {
-    if (4 * w + 4 <= tail) {
-      crc = crc_word(crc, m[w], tk);
-    } else if (4 * w < tail) {
+    for (uint32_t w = 0; w < 16; w++) {
+      if (4 * w + 4 <= tail) {
+        crc = crc_word(crc, m[w], tk);
+      } else if (4 * w < tail) {
 #pragma unroll
-      for (uint32_t j = 0; j < 3; j++)
-        if (4 * w + j < tail) crc = crc_byte(crc, (m[w] >> (8 * j)) & 255u, tk);
+        for (uint32_t j = 0; j < 3; j++)
+          if (4 * w + j < tail) crc = crc_byte(crc, (m[w] >> (8 * j)) & 255u, tk);
+      }
     }
+    reinterpret_cast<uint32_t*>(o20)[4] = crc ^ 0xFFFFFFFFu;
   }
-  // clear the bytes at and past `tail` in the last partial word, then 0x80
+  if constexpr (kMd5) {
+    // clear the bytes at and past `tail` in the last partial word, then 0x80
 #pragma unroll
-  for (int w = 0; w < 16; w++) {
-    const uint32_t lo = 4u * w;
-    if (lo < tail && tail < lo + 4) m[w] &= (1u << (8 * (tail - lo))) - 1u;
-    if (lo <= tail && tail < lo + 4) m[w] |= 0x80u << (8 * (tail - lo));
-  }
-  if (tail >= 56) {
+    for (int w = 0; w < 16; w++) {
+      const uint32_t lo = 4u * w;
+      if (lo < tail && tail < lo + 4) m[w] &= (1u << (8 * (tail - lo))) - 1u;
+      if (lo <= tail && tail < lo + 4) m[w] |= 0x80u << (8 * (tail - lo));
+    }
+    if (tail >= 56) {
+      md5_block(st, m);
+#pragma unroll
+      for (int w = 0; w < 16; w++) m[w] = 0;
+    }
+    m[14] = (uint32_t)(L << 3);
+    m[15] = (uint32_t)(L >> 29);
     md5_block(st, m);
-#pragma unroll
-    for (int w = 0; w < 16; w++) m[w] = 0;
+    uint32_t* o = reinterpret_cast<uint32_t*>(o20);
+    o[0] = st[0];
+    o[1] = st[1];
+    o[2] = st[2];
+    o[3] = st[3];
   }
-  m[14] = (uint32_t)(L << 3);
-  m[15] = (uint32_t)(L >> 29);
-  md5_block(st, m);
-  uint32_t* o = reinterpret_cast<uint32_t*>(out + 20 * i);
-  o[0] = st[0];
-  o[1] = st[1];
-  o[2] = st[2];
-  o[3] = st[3];
-  o[4] = crc ^ 0xFFFFFFFFu;
+}
+
+__global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restrict__ data, size_t stride,
+                                                         size_t n, uint64_t L,
+                                                         const uint64_t* __restrict__ lengths,
+                                                         uint8_t* __restrict__ out) {
+  extern __shared__ uint32_t crc_tab[];
+  crc_tables_init(crc_tab);
+  __syncthreads();
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t len = lengths ? (lengths[i] < L ? lengths[i] : L) : L;
+  par2_slice_hash<true, true>(data + i * stride, len, L, crc_tab + (threadIdx.x % kCrcCopies), out + 20 * i);
+}
+
+// Few slices (too few threads to fill the GPU): MD5 and CRC32 of a slice in
+// two threads of different warps, so each serial chain runs alone instead of
+// sharing one thread's in-order instruction stream.  The MD5 chain itself
+// (about 2,000 cycles per 64-byte block) then sets the time.  Threads 0-63 of a CTA
+// hash slices 64b .. 64b+63 with MD5, threads 64-127 the same slices with
+// CRC32 (they read the same bytes at about the same time, served by L1/L2).
+__global__ void __launch_bounds__(128) k_par2_block_hash_split(const uint8_t* __restrict__ data, size_t stride,
+                                                               size_t n, uint64_t L,
+                                                               const uint64_t* __restrict__ lengths,
+                                                               uint8_t* __restrict__ out) {
+  extern __shared__ uint32_t crc_tab[];
+  crc_tables_init(crc_tab);
+  __syncthreads();
+  const size_t i = (size_t)blockIdx.x * 64 + (threadIdx.x & 63);
+  if (i >= n) return;
+  const uint64_t len = lengths ? (lengths[i] < L ? lengths[i] : L) : L;
+  if (threadIdx.x < 64)
+    par2_slice_hash<true, false>(data + i * stride, len, L, nullptr, out + 20 * i);
+  else
+    par2_slice_hash<false, true>(data + i * stride, len, L, crc_tab + (threadIdx.x % kCrcCopies), out + 20 * i);
 }
 
 // PAR2 recovery-slice packet headers (lib/par2.js:517-530 getRecoveryHeader;
@@ -627,10 +663,17 @@ cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t 
   if (n == 0) return cudaSuccess;
   const int smem = kCrcWords * 4;
   cudaError_t e = cudaFuncSetAttribute(k_par2_block_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_par2_block_hash_split, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  const unsigned threads = 128;
-  k_par2_block_hash<<<(unsigned)((n + threads - 1) / threads), threads, smem, s>>>(d_data, stride, n, slice,
-                                                                                   d_lengths, d_out);
+  // split MD5 / CRC32 threads for up to 8,192 slices (1 GiB of device data:
+  // 1,024 x 1 MiB 17.40 -> 17.17 ms, 4,096 x 256 KiB 4.36 -> 4.17 ms, 8,192 x
+  // 128 KiB 2.18 -> 1.96 ms; at 32,768 x 32 KiB the one-thread form is
+  // faster, 0.68 vs 1.22 ms, as the ALU pipe is then the limit)
+  if (n <= 8192)
+    k_par2_block_hash_split<<<(unsigned)((n + 63) / 64), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out);
+  else
+    k_par2_block_hash<<<(unsigned)((n + 127) / 128), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out);
   note_launch();
   return cudaGetLastError();
 }
