@@ -282,6 +282,13 @@ PP_API int pp_ctx_create(int device, pp_ctx** out) {
     return PP_ERR_CUDA;
   }
   ctx->stream = ctx->own;
+  if (gf16_exp_table_init(ctx->own) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(ctx->d_status);
+    cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return PP_ERR_CUDA;
+  }
   if (const char* k = getenv("PP_GF16_KERNEL")) {
     if (!strcmp(k, "lut")) ctx->gf16_kernel = PP_GF16_KERNEL_LUT;
     else if (!strcmp(k, "tensor")) ctx->gf16_kernel = PP_GF16_KERNEL_TENSOR;

@@ -34,6 +34,37 @@ PP_D uint16_t gf16_pow2(uint32_t e) {
   return (uint16_t)r;
 }
 
+// 2^k for k = 0..65535 (2^65535 = 2^0): a PAR2 coefficient
+// 2^(L * e mod 65535) is one lookup.  128 KiB per device, filled once per
+// device (pp_ctx_create waits for it; a launch that finds it unfilled fills it
+// first on its own stream).
+// g_gf16_inv[x] = 1/x (0 for x = 0), for the inversion kernels.
+__device__ uint16_t g_gf16_exp[65536];
+__device__ __align__(16) uint16_t g_gf16_inv[65536];
+static std::atomic<uint64_t> g_gf16_exp_ready{0};
+
+__global__ void k_gf16_exp_init() {
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < 65536; k += gridDim.x * blockDim.x) {
+    g_gf16_exp[k] = gf16_pow2(k % 65535u);
+    g_gf16_inv[k] = gf16_inv_euclid((uint16_t)k);
+  }
+}
+
+static cudaError_t exp_table_on(cudaStream_t s) {
+  if (device_done(g_gf16_exp_ready)) return cudaSuccess;
+  k_gf16_exp_init<<<64, 256, 0, s>>>();
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t gf16_exp_table_init(cudaStream_t s) {
+  if (device_done(g_gf16_exp_ready)) return cudaSuccess;
+  cudaError_t e = exp_table_on(s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) device_mark(g_gf16_exp_ready);
+  return e;
+}
+
 __global__ void k_gf16_coeff_matrix(const uint16_t* __restrict__ logs, unsigned n_in,
                                     const uint16_t* __restrict__ exps, unsigned n_out,
                                     uint16_t* __restrict__ coeffs) {
@@ -42,7 +73,7 @@ __global__ void k_gf16_coeff_matrix(const uint16_t* __restrict__ logs, unsigned 
        idx += (size_t)gridDim.x * blockDim.x) {
     unsigned o = (unsigned)(idx / n_in), i = (unsigned)(idx % n_in);
     uint32_t e = (uint32_t)(((uint64_t)logs[i] * exps[o]) % 65535u);
-    coeffs[idx] = gf16_pow2(e);
+    coeffs[idx] = g_gf16_exp[e];
   }
 }
 
@@ -50,6 +81,7 @@ cudaError_t launch_gf16_coeff_matrix(const uint16_t* d_logs, unsigned n_in, cons
                                      unsigned n_out, uint16_t* d_coeffs, cudaStream_t s) {
   size_t total = (size_t)n_in * n_out;
   if (!total) return cudaSuccess;
+  if (cudaError_t e = exp_table_on(s)) return e;
   unsigned blocks = (unsigned)((total + 255) / 256);
   if (blocks > 4096) blocks = 4096;
   k_gf16_coeff_matrix<<<blocks, 256, 0, s>>>(d_logs, n_in, d_exps, n_out, d_coeffs);
@@ -268,7 +300,7 @@ __global__ void k_gf16_build_rec_matrix(const uint16_t* __restrict__ logs, const
        idx += (size_t)gridDim.x * blockDim.x) {
     unsigned r = (unsigned)(idx / n_in), i = (unsigned)(idx % n_in);
     uint32_t e = (uint32_t)(((uint64_t)logs[i] * rec[r]) % 65535u);
-    mat[(size_t)r * ld + col_of[i]] = gf16_pow2(e);
+    mat[(size_t)r * ld + col_of[i]] = g_gf16_exp[e];
   }
 }
 
@@ -277,6 +309,7 @@ cudaError_t launch_gf16_build_rec_matrix(const uint16_t* d_logs, const uint32_t*
                                          cudaStream_t s) {
   size_t total = (size_t)n_in * m;
   if (!total) return cudaSuccess;
+  if (cudaError_t e = exp_table_on(s)) return e;
   unsigned blocks = (unsigned)ceil_div(total, 256);
   if (blocks > 8192) blocks = 8192;
   k_gf16_build_rec_matrix<<<blocks, 256, 0, s>>>(d_logs, d_col_of, n_in, d_rec, m, d_mat, ld);
@@ -346,41 +379,82 @@ k_gf16_eliminate(uint16_t* __restrict__ mat, unsigned m, unsigned ncols, size_t 
 // The whole elimination of an m x m matrix (m <= kInvSmall; row stride ld,
 // 16-byte aligned rows) by one CTA in shared memory: the same steps as
 // k_gf16_pivot + k_gf16_eliminate with pc0 = 0, all m pivots in one launch.
+// The m pivot steps are serial, so each is kept short: the pivot inverse is
+// one load from a shared-memory copy of the inverse table, and row r's update
+// row_r ^= f_r * row_k uses 4-bit split tables of f_r (64 entries from three
+// doublings and XORs) instead of a multiplication per element.
 constexpr unsigned kInvSmall = 128;
-__global__ void __launch_bounds__(1024) k_gf16_invert_small(uint16_t* __restrict__ mat, unsigned m, size_t ld,
-                                                            int* __restrict__ status) {
+constexpr unsigned kInvThreads = 1024;
+constexpr unsigned kInvPer = kInvSmall * kInvSmall / kInvThreads;  // elements per thread, at most
+constexpr int kInvTableBytes = 65536 * 2;                          // inverse table
+constexpr int kInvDynBytes = kInvTableBytes + kInvSmall * 64 * 2;  // + split tables of every row
+__global__ void __launch_bounds__(kInvThreads) k_gf16_invert_small(uint16_t* __restrict__ mat, unsigned m, size_t ld,
+                                                                   int* __restrict__ status) {
+  extern __shared__ __align__(16) uint16_t dyn[];
+  uint16_t* sinv = dyn;                        // 1/x for every x
+  uint16_t* T = dyn + kInvTableBytes / 2;      // T[(r * 4 + q) * 16 + n] = f_r * (n << 4q)
   __shared__ uint16_t a[kInvSmall * kInvSmall];
   __shared__ uint16_t fcol[kInvSmall];
-  const unsigned mm = m * m;
-  for (unsigned e = threadIdx.x; e < mm; e += blockDim.x) a[e] = mat[(size_t)(e / m) * ld + e % m];
+  const unsigned mm = m * m, t = threadIdx.x;
+  for (unsigned x = t; x < 65536 / 8; x += kInvThreads)
+    reinterpret_cast<uint4*>(sinv)[x] = reinterpret_cast<const uint4*>(g_gf16_inv)[x];
+  unsigned rr[kInvPer], cc[kInvPer];  // this thread's elements (row kInvSmall: none)
+#pragma unroll
+  for (unsigned u = 0; u < kInvPer; u++) {
+    const unsigned e = t + kInvThreads * u;
+    rr[u] = e < mm ? e / m : kInvSmall;
+    cc[u] = e < mm ? e % m : 0;
+  }
+  for (unsigned e = t; e < mm; e += kInvThreads) a[e] = mat[(size_t)(e / m) * ld + e % m];
   __syncthreads();
   for (unsigned k = 0; k < m; k++) {
     const uint16_t p = a[k * m + k];
     if (p == 0) {  // uniform across the CTA
-      if (threadIdx.x == 0) *status = (int)k;
+      if (t == 0) *status = (int)k;
       return;
     }
-    for (unsigned r = threadIdx.x; r < m; r += blockDim.x) fcol[r] = a[r * m + k];
+    const uint16_t ip = sinv[p];
+    if (t < m) fcol[t] = a[t * m + k];  // pivot column (its row-k entry is not used)
+    __syncthreads();                    // every read of the pivot precedes the rewrite of row k
+    if (t < m) a[k * m + t] = gf16_mul(t == k ? (uint16_t)1 : a[k * m + t], ip);
+    if (t < 4 * m) {  // split tables of row r = t / 4, nibble q = t % 4
+      const unsigned r = t >> 2, q = t & 3;
+      uint32_t b0 = fcol[r];
+      for (unsigned d = 0; d < 4 * q; d++) b0 = gf16_dbl(b0);
+      const uint32_t b1 = gf16_dbl(b0), b2 = gf16_dbl(b1), b3 = gf16_dbl(b2);
+      uint16_t* tq = T + (r * 4 + q) * 16;
+#pragma unroll
+      for (unsigned n = 0; n < 16; n++)
+        tq[n] = (uint16_t)(((n & 1) ? b0 : 0u) ^ ((n & 2) ? b1 : 0u) ^ ((n & 4) ? b2 : 0u) ^ ((n & 8) ? b3 : 0u));
+    }
     __syncthreads();
-    const uint16_t ip = gf16_inv_euclid(p);
-    for (unsigned c = threadIdx.x; c < m; c += blockDim.x) a[k * m + c] = gf16_mul(c == k ? (uint16_t)1 : a[k * m + c], ip);
-    __syncthreads();
-    for (unsigned e = threadIdx.x; e < mm; e += blockDim.x) {
-      const unsigned r = e / m, c = e % m;
-      const uint16_t f = fcol[r];
-      if (r == k || f == 0) continue;
-      const uint16_t y = gf16_mul(f, a[k * m + c]);
-      a[e] = c == k ? y : (uint16_t)(a[e] ^ y);
+#pragma unroll
+    for (unsigned u = 0; u < kInvPer; u++) {
+      const unsigned r = rr[u], c = cc[u];
+      if (r < m && r != k && fcol[r]) {
+        const uint32_t x = a[k * m + c];
+        const uint16_t* tr = T + r * 64;
+        const uint16_t y = (uint16_t)(tr[x & 15] ^ tr[16 + ((x >> 4) & 15)] ^ tr[32 + ((x >> 8) & 15)] ^ tr[48 + (x >> 12)]);
+        a[r * m + c] = c == k ? y : (uint16_t)(a[r * m + c] ^ y);
+      }
     }
     __syncthreads();
   }
-  for (unsigned e = threadIdx.x; e < mm; e += blockDim.x) mat[(size_t)(e / m) * ld + e % m] = a[e];
+  for (unsigned e = t; e < mm; e += kInvThreads) mat[(size_t)(e / m) * ld + e % m] = a[e];
 }
 
 cudaError_t launch_gf16_invert(uint16_t* d_mat, unsigned m, unsigned ncols, size_t ld, unsigned pc0,
                                uint16_t* d_fcol, int* d_status, cudaStream_t s) {
   if (pc0 == 0 && ncols == m && m <= kInvSmall) {
-    k_gf16_invert_small<<<1, 1024, 0, s>>>(d_mat, m, ld, d_status);
+    static std::atomic<uint64_t> attr{0};
+    if (!device_done(attr)) {
+      cudaError_t e = cudaFuncSetAttribute(k_gf16_invert_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kInvDynBytes);
+      if (e != cudaSuccess) return e;
+      device_mark(attr);
+    }
+    if (cudaError_t e = exp_table_on(s)) return e;
+    k_gf16_invert_small<<<1, kInvThreads, kInvDynBytes, s>>>(d_mat, m, ld, d_status);
     note_launch();
     return cudaGetLastError();
   }

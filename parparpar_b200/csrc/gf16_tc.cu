@@ -83,48 +83,41 @@ PP_D uint32_t spread4(uint32_t n) { return (n * 0x00204081u) & 0x01010101u; }
 // 8s..8s+7) a 16 KiB tile in the smem canonical layout (K-major, 128-byte
 // swizzle): row m = 16*oo + b; chunk j (shift); byte 2*ii + beta within the
 // chunk holds bit b of c[8g+oo][8s+ii] * x^(8*beta + j).
+//
+// With Q_b(c) = the 16-bit mask whose bit e is bit b of c * x^e (row b of the
+// multiplication matrix of c) and P = Q_b(c[2q]) | Q_b(c[2q+1]) << 16, the
+// 32-bit word q of chunk j is (P >> j) & 0x01010101: byte (ii, beta) = bit
+// 8*beta + j of Q_b(c[ii]).
+//
+// One CTA per tile (g, s), thread m builds row m: a warp writes 32 rows =
+// 4 KiB of contiguous memory, so the 16 KiB tile leaves as whole lines.
 __global__ void __launch_bounds__(128)
 k_gf16_tc_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigned n_in, unsigned n_out,
                         unsigned n_stages, uint8_t* __restrict__ a_exp) {
-  const size_t total = (size_t)((n_out + 7) / 8) * n_stages * 8;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const unsigned oo = t & 7;
-    const size_t gs = t >> 3;  // g * n_stages + s
+  const unsigned m = threadIdx.x, oo = m >> 4, b = m & 15;
+  const size_t tiles = (size_t)((n_out + 7) / 8) * n_stages;
+  for (size_t gs = blockIdx.x; gs < tiles; gs += gridDim.x) {  // gs = g * n_stages + s
     const unsigned s = (unsigned)(gs % n_stages), g = (unsigned)(gs / n_stages);
     const unsigned o = 8 * g + oo;
-    uint16_t y[8][16];  // y[ii][e] = c_ii * x^e
+    uint32_t P[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int ii = 0; ii < 8; ii++) {
       const unsigned i = 8 * s + ii;
       uint32_t c = (o < n_out && i < n_in) ? coeffs[(size_t)o * ldc + i] : 0;
+      uint32_t q = 0;  // Q_b(c)
 #pragma unroll
       for (int e = 0; e < 16; e++) {
-        y[ii][e] = (uint16_t)c;
+        q |= ((c >> b) & 1u) << e;
         c = gf16_dbl(c);
       }
+      P[ii >> 1] |= q << (16 * (ii & 1));
     }
-    uint8_t* tile = a_exp + gs * kABytes;
-#pragma unroll 1
-    for (int b = 0; b < 16; b++) {
-      const unsigned m = 16 * oo + b;
+    uint8_t* row = a_exp + gs * kABytes + (m >> 3) * 1024 + (m & 7) * 128;
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        uint32_t w4[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          // bytes 4q..4q+3 = (ii = 2q, beta 0), (2q, 1), (2q+1, 0), (2q+1, 1)
-          uint32_t v = 0;
-#pragma unroll
-          for (int t4 = 0; t4 < 4; t4++) {
-            const int ii = 2 * q + (t4 >> 1), beta = t4 & 1;
-            v |= (uint32_t)((y[ii][8 * beta + j] >> b) & 1u) << (8 * t4);
-          }
-          w4[q] = v;
-        }
-        *reinterpret_cast<uint4*>(tile + (m >> 3) * 1024 + (m & 7) * 128 + ((j ^ (m & 7)) << 4)) =
-            make_uint4(w4[0], w4[1], w4[2], w4[3]);
-      }
-    }
+    for (int j = 0; j < 8; j++)
+      *reinterpret_cast<uint4*>(row + ((j ^ (m & 7)) << 4)) =
+          make_uint4((P[0] >> j) & 0x01010101u, (P[1] >> j) & 0x01010101u, (P[2] >> j) & 0x01010101u,
+                     (P[3] >> j) & 0x01010101u);
   }
 }
 
@@ -446,9 +439,9 @@ size_t gf16_tc_coeff_bytes(unsigned n_in, unsigned n_out) {
 cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned n_in, unsigned n_out,
                                   uint8_t* d_aexp, cudaStream_t s) {
   const unsigned n_stages = (n_in + 7) / 8;
-  const size_t total = (size_t)((n_out + 7) / 8) * n_stages * 8;
-  if (!total) return cudaSuccess;
-  unsigned blocks = (unsigned)std::min<size_t>(ceil_div(total, 128), 148 * 16);
+  const size_t tiles = (size_t)((n_out + 7) / 8) * n_stages;
+  if (!tiles) return cudaSuccess;
+  unsigned blocks = (unsigned)std::min<size_t>(tiles, 148 * 32);
   tc16::k_gf16_tc_expand_coeffs<<<blocks, 128, 0, s>>>(d_coeffs, ldc, n_in, n_out, n_stages, d_aexp);
   note_launch();
   return cudaGetLastError();

@@ -135,7 +135,10 @@ class Galois16RecMatrix:
         """recovery: a Python list, sorted and truncated in place like the
         reference's std::vector<uint16_t>&.  out: optional (m, n) uint16
         buffer (host or CUDA) for the factors; default a new numpy array."""
-        v = np.ascontiguousarray(np.asarray([1 if x else 0 for x in inputValid], dtype=np.uint8))
+        if isinstance(inputValid, np.ndarray) and inputValid.dtype.kind in "biu":
+            v = np.ascontiguousarray(inputValid != 0, dtype=np.uint8)  # vectorised: no per-element Python loop
+        else:
+            v = np.ascontiguousarray(np.asarray([1 if x else 0 for x in inputValid], dtype=np.uint8))
         n = v.size
         if int(v.sum()) != validCount:
             raise ValueError("validCount does not match inputValid")

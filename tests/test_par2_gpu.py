@@ -254,6 +254,10 @@ def test_par2_invert_vs_oracle(ctx, oracle):
         r2 = list(rec)
         assert m.Compute([bool(x) for x in v], int(v.sum()), r2) == ok
         assert r2 == used and np.array_equal(m.factors, f)
+        # the same flags as a numpy array (converted without a Python loop)
+        m2, r3 = par2.Galois16RecMatrix(ctx=ctx), list(rec)
+        assert m2.Compute(v.astype(bool), int(v.sum()), r3) == ok
+        assert r3 == used and (not ok or np.array_equal(m2.factors, f))
 
 
 def test_par2_repair_roundtrip(kctx):
