@@ -510,6 +510,7 @@ static cudaError_t gf16_region(int sel, const uint8_t* din, size_t dstride, unsi
 // c (accumulating from the second chunk on) waits only for that chunk, so the
 // copies overlap the products and the job takes about as long as its copies.
 constexpr unsigned kCopyChunk = 4096;
+constexpr unsigned kCopyTail = 256;
 constexpr size_t kGf16TileBytes = 128 * 128;  // one expanded tile (8 outputs x 8 inputs)
 
 static int ensure_copy_stream(pp_ctx* ctx) {
@@ -593,8 +594,11 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
     CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
     CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
     if (hashes) CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->start_ev, 0));
-    for (unsigned c0 = 0; c0 < n_in; c0 += kCopyChunk) {
-      const unsigned nc = std::min(kCopyChunk, n_in - c0);
+    for (unsigned c0 = 0, nc = 0; c0 < n_in; c0 += nc) {
+      // the last kCopyChunk slices go in halving pieces (down to kCopyTail),
+      // so little product work is left once the final copy has landed
+      const unsigned rest = n_in - c0;
+      nc = rest > kCopyChunk ? kCopyChunk : rest > kCopyTail ? std::max(kCopyTail, (rest / 2 + 7) & ~7u) : rest;
       CUDA_TRY(ctx, cudaMemcpy2DAsync(din + (size_t)c0 * row, row, (const uint8_t*)inputs + (size_t)c0 * in_stride,
                                       in_stride, slice, nc, cudaMemcpyHostToDevice, ctx->copy));
       CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));

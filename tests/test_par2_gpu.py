@@ -301,7 +301,8 @@ def test_par2_create_resident_tables_across_calls(kctx, oracle):
 def test_par2_create_host_inputs_in_overlapped_chunks(kctx, oracle):
     """Host inputs of >= 8192 slices go to the device in chunks of 4096 whose
     copies overlap the products of the previous chunk (each chunk's kernel
-    accumulates); 10,003 slices make a ragged last chunk.  Checked against the
+    accumulates), the last 4096 in halving pieces; 10,003 slices give chunks
+    of 4096, 4096, 912, 456, 256 and a ragged 187.  Checked against the
     oracle for create (first call: scratch tiles; second: resident table) and
     for an accumulating region product."""
     from parparpar_b200 import par2
