@@ -1328,8 +1328,12 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
     }
     CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
     CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
-    for (size_t c0 = 0; c0 < n_in; c0 += chunk) {
-      const size_t nc = std::min(chunk, n_in - c0);
+    const size_t tail = std::max<size_t>(2, chunk / 16);
+    for (size_t c0 = 0, nc = 0; c0 < n_in; c0 += nc) {
+      // the last chunk goes in halving pieces (down to chunk / 16 blocks), so
+      // little product work is left once the final copy has landed
+      const size_t rest = n_in - c0;
+      nc = rest > chunk ? chunk : rest > tail ? std::max(tail, (rest / 2 + 1) & ~(size_t)1) : rest;
       CUDA_TRY(ctx, cudaMemcpyAsync(s + c0 * B, inputs + c0 * B, nc * B * 8, cudaMemcpyHostToDevice, ctx->copy));
       CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
       CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev, 0));
