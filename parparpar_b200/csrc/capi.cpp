@@ -282,7 +282,7 @@ PP_API int pp_ctx_create(int device, pp_ctx** out) {
     return PP_ERR_CUDA;
   }
   ctx->stream = ctx->own;
-  if (gf16_exp_table_init(ctx->own) != cudaSuccess) {
+  if (gf16_exp_table_init(ctx->own) != cudaSuccess || gf16_tc_tables_init(ctx->own) != cudaSuccess) {
     cudaGetLastError();
     cudaFree(ctx->d_status);
     cudaStreamDestroy(ctx->own);

@@ -87,13 +87,40 @@ PP_D uint32_t spread4(uint32_t n) { return (n * 0x00204081u) & 0x01010101u; }
 // With Q_b(c) = the 16-bit mask whose bit e is bit b of c * x^e (row b of the
 // multiplication matrix of c) and P = Q_b(c[2q]) | Q_b(c[2q+1]) << 16, the
 // 32-bit word q of chunk j is (P >> j) & 0x01010101: byte (ii, beta) = bit
-// 8*beta + j of Q_b(c[ii]).
-//
-// One CTA per tile (g, s), thread m builds row m: a warp writes 32 rows =
-// 4 KiB of contiguous memory, so the 16 KiB tile leaves as whole lines.
+// 8*beta + j of Q_b(c[ii]).  Q_b is linear in c, so
+//   Q_b(c) = XOR_q T[q][nibble q of c][b],   T[q][n][b] = Q_b(n << 4q),
+// a 2 KiB table (b fastest: the 16 threads of one coefficient read 32
+// consecutive bytes) filled once per device.
+__device__ __align__(16) uint16_t g_gf16_qtab[4 * 16 * 16];
+static std::atomic<uint64_t> g_qtab_ready{0};
+
+__global__ void k_gf16_qtab_init() {
+  for (unsigned t = threadIdx.x; t < 1024; t += blockDim.x) {
+    const unsigned q = t >> 8, n = (t >> 4) & 15, b = t & 15;
+    uint32_t c = n << (4 * q), v = 0;
+    for (int e = 0; e < 16; e++) {
+      v |= ((c >> b) & 1u) << e;
+      c = gf16_dbl(c);
+    }
+    g_gf16_qtab[t] = (uint16_t)v;
+  }
+}
+
+static cudaError_t qtab_on(cudaStream_t s) {
+  if (device_done(g_qtab_ready)) return cudaSuccess;
+  k_gf16_qtab_init<<<1, 256, 0, s>>>();
+  note_launch();
+  return cudaGetLastError();
+}
+
+// One CTA per tile (g, s), thread m builds row m; each warp store writes
+// 512 contiguous bytes, so the 16 KiB tile leaves as whole lines.
 __global__ void __launch_bounds__(128)
 k_gf16_tc_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigned n_in, unsigned n_out,
                         unsigned n_stages, uint8_t* __restrict__ a_exp) {
+  __shared__ __align__(16) uint16_t T[4 * 16 * 16];
+  reinterpret_cast<uint4*>(T)[threadIdx.x] = reinterpret_cast<const uint4*>(g_gf16_qtab)[threadIdx.x];
+  __syncthreads();
   const unsigned m = threadIdx.x, oo = m >> 4, b = m & 15;
   const size_t tiles = (size_t)((n_out + 7) / 8) * n_stages;
   for (size_t gs = blockIdx.x; gs < tiles; gs += gridDim.x) {  // gs = g * n_stages + s
@@ -103,21 +130,26 @@ k_gf16_tc_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigne
 #pragma unroll
     for (int ii = 0; ii < 8; ii++) {
       const unsigned i = 8 * s + ii;
-      uint32_t c = (o < n_out && i < n_in) ? coeffs[(size_t)o * ldc + i] : 0;
-      uint32_t q = 0;  // Q_b(c)
-#pragma unroll
-      for (int e = 0; e < 16; e++) {
-        q |= ((c >> b) & 1u) << e;
-        c = gf16_dbl(c);
-      }
+      const uint32_t c = (o < n_out && i < n_in) ? coeffs[(size_t)o * ldc + i] : 0;
+      const uint32_t q = (uint32_t)T[((c & 15) << 4) + b] ^ T[256 + (((c >> 4) & 15) << 4) + b] ^
+                         T[512 + (((c >> 8) & 15) << 4) + b] ^ T[768 + ((c >> 12) << 4) + b];  // Q_b(c)
       P[ii >> 1] |= q << (16 * (ii & 1));
     }
-    uint8_t* row = a_exp + gs * kABytes + (m >> 3) * 1024 + (m & 7) * 128;
+    // the warp's 32 rows are 4 KiB of contiguous memory; store k writes its
+    // 512 bytes [512k, 512k + 512): lane L the 16-byte slot L of it, i.e. row
+    // 4k + L/8 of the warp, physical chunk L%8 (logical chunk (L%8) ^ (row%8)),
+    // from the words of the lane that built that row
+    const unsigned lane = m & 31;
+    uint8_t* wbase = a_exp + gs * kABytes + (m >> 5) * 4096;
 #pragma unroll
-    for (int j = 0; j < 8; j++)
-      *reinterpret_cast<uint4*>(row + ((j ^ (m & 7)) << 4)) =
-          make_uint4((P[0] >> j) & 0x01010101u, (P[1] >> j) & 0x01010101u, (P[2] >> j) & 0x01010101u,
-                     (P[3] >> j) & 0x01010101u);
+    for (int k = 0; k < 8; k++) {
+      const unsigned r = 4 * k + (lane >> 3), j = (lane & 7) ^ (r & 7);
+      const uint32_t p0 = __shfl_sync(0xFFFFFFFFu, P[0], r), p1 = __shfl_sync(0xFFFFFFFFu, P[1], r),
+                     p2 = __shfl_sync(0xFFFFFFFFu, P[2], r), p3 = __shfl_sync(0xFFFFFFFFu, P[3], r);
+      *reinterpret_cast<uint4*>(wbase + 512 * k + 16 * lane) =
+          make_uint4((p0 >> j) & 0x01010101u, (p1 >> j) & 0x01010101u, (p2 >> j) & 0x01010101u,
+                     (p3 >> j) & 0x01010101u);
+    }
   }
 }
 
@@ -432,6 +464,14 @@ static uint64_t tiles16(const Gf16TcJob& j) { return (uint64_t)j.groups * j.wt; 
 
 }  // namespace tc16
 
+cudaError_t gf16_tc_tables_init(cudaStream_t s) {
+  if (device_done(tc16::g_qtab_ready)) return cudaSuccess;
+  cudaError_t e = tc16::qtab_on(s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) device_mark(tc16::g_qtab_ready);
+  return e;
+}
+
 size_t gf16_tc_coeff_bytes(unsigned n_in, unsigned n_out) {
   return (size_t)((n_out + 7) / 8) * ((n_in + 7) / 8) * tc16::kABytes;
 }
@@ -441,6 +481,7 @@ cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned
   const unsigned n_stages = (n_in + 7) / 8;
   const size_t tiles = (size_t)((n_out + 7) / 8) * n_stages;
   if (!tiles) return cudaSuccess;
+  if (cudaError_t e = tc16::qtab_on(s)) return e;
   unsigned blocks = (unsigned)std::min<size_t>(tiles, 148 * 32);
   tc16::k_gf16_tc_expand_coeffs<<<blocks, 128, 0, s>>>(d_coeffs, ldc, n_in, n_out, n_stages, d_aexp);
   note_launch();

@@ -46,6 +46,8 @@ int ctx_fail(pp_ctx* c, int code, const char* msg);  // records the message, ret
 // The device table of 2^k in GF(2^16) behind the coefficient kernels:
 // filled on stream s and waited for, once per device (at context creation).
 cudaError_t gf16_exp_table_init(cudaStream_t s);
+// the same for the table behind launch_gf16_tc_expand (gf16_tc.cu)
+cudaError_t gf16_tc_tables_init(cudaStream_t s);
 // coeffs[o*N + i] = 2^(logs[i] * exps[o] mod 65535)   (device buffers)
 cudaError_t launch_gf16_coeff_matrix(const uint16_t* d_logs, unsigned n_in, const uint16_t* d_exps,
                                      unsigned n_out, uint16_t* d_coeffs, cudaStream_t s);
