@@ -594,6 +594,7 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
     CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
     CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
     if (hashes) CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->start_ev, 0));
+    unsigned hashed = 0;  // slices whose hashes are launched
     for (unsigned c0 = 0, nc = 0; c0 < n_in; c0 += nc) {
       // the last kCopyChunk slices go in halving pieces (down to kCopyTail),
       // so little product work is left once the final copy has landed
@@ -603,10 +604,15 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
                                       in_stride, slice, nc, cudaMemcpyHostToDevice, ctx->copy));
       CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
       CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev, 0));
-      if (hashes) {
+      // hashes: one launch per full chunk, one for all the tail pieces (an
+      // MD5 takes as long for 256 slices as for 4,096, its chain being serial
+      // within each slice, so per-piece launches would queue up after the
+      // last copy)
+      if (hashes && (nc == kCopyChunk || c0 + nc == n_in)) {
         CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->copy_ev, 0));
-        CUDA_TRY(ctx, launch_par2_block_hash(din + (size_t)c0 * row, row, nc, slice, nullptr, dh + (size_t)20 * c0,
-                                             ctx->hash));
+        CUDA_TRY(ctx, launch_par2_block_hash(din + (size_t)hashed * row, row, c0 + nc - hashed, slice, nullptr,
+                                             dh + (size_t)20 * hashed, ctx->hash));
+        hashed = c0 + nc;
       }
       CUDA_TRY(ctx, launch_gf16_muladd_tc(din + (size_t)c0 * row, row, nc, slice, aexp + (size_t)(c0 / 8) * kGf16TileBytes,
                                           n_out, dout, ostride, accumulate || c0 > 0, ctx->sms, ctx->d_status,
