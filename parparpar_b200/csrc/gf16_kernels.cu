@@ -394,7 +394,9 @@ __global__ void __launch_bounds__(kInvThreads) k_gf16_invert_small(uint16_t* __r
   uint16_t* sinv = dyn;                        // 1/x for every x
   uint16_t* T = dyn + kInvTableBytes / 2;      // T[(r * 4 + q) * 16 + n] = f_r * (n << 4q)
   __shared__ uint16_t a[kInvSmall * kInvSmall];
-  __shared__ uint16_t fcol[kInvSmall];
+  // pivot columns: col[k & 1][r] = a[r][k] as step k begins (written by the
+  // elimination of step k - 1, so a step needs two barriers, not three)
+  __shared__ uint16_t col[2][kInvSmall];
   const unsigned mm = m * m, t = threadIdx.x;
   for (unsigned x = t; x < 65536 / 8; x += kInvThreads)
     reinterpret_cast<uint4*>(sinv)[x] = reinterpret_cast<const uint4*>(g_gf16_inv)[x];
@@ -405,18 +407,20 @@ __global__ void __launch_bounds__(kInvThreads) k_gf16_invert_small(uint16_t* __r
     rr[u] = e < mm ? e / m : kInvSmall;
     cc[u] = e < mm ? e % m : 0;
   }
-  for (unsigned e = t; e < mm; e += kInvThreads) a[e] = mat[(size_t)(e / m) * ld + e % m];
+  for (unsigned e = t; e < mm; e += kInvThreads) {
+    const uint16_t v = mat[(size_t)(e / m) * ld + e % m];
+    a[e] = v;
+    if (e % m == 0) col[0][e / m] = v;
+  }
   __syncthreads();
   for (unsigned k = 0; k < m; k++) {
-    const uint16_t p = a[k * m + k];
+    const uint16_t* fcol = col[k & 1];
+    uint16_t* fnext = col[(k + 1) & 1];
+    const uint16_t p = fcol[k];
     if (p == 0) {  // uniform across the CTA
       if (t == 0) *status = (int)k;
       return;
     }
-    const uint16_t ip = sinv[p];
-    if (t < m) fcol[t] = a[t * m + k];  // pivot column (its row-k entry is not used)
-    __syncthreads();                    // every read of the pivot precedes the rewrite of row k
-    if (t < m) a[k * m + t] = gf16_mul(t == k ? (uint16_t)1 : a[k * m + t], ip);
     if (t < 4 * m) {  // split tables of row r = t / 4, nibble q = t % 4
       const unsigned r = t >> 2, q = t & 3;
       uint32_t b0 = fcol[r];
@@ -426,16 +430,27 @@ __global__ void __launch_bounds__(kInvThreads) k_gf16_invert_small(uint16_t* __r
 #pragma unroll
       for (unsigned n = 0; n < 16; n++)
         tq[n] = (uint16_t)(((n & 1) ? b0 : 0u) ^ ((n & 2) ? b1 : 0u) ^ ((n & 4) ? b2 : 0u) ^ ((n & 8) ? b3 : 0u));
+    } else if (t < 5 * m) {  // scale row k, the identity column substituted
+      const unsigned c = t - 4 * m;
+      const uint16_t v = gf16_mul(c == k ? (uint16_t)1 : a[k * m + c], sinv[p]);
+      a[k * m + c] = v;
+      if (c == k + 1) fnext[k] = v;  // row k's entry of the next pivot column
     }
     __syncthreads();
 #pragma unroll
     for (unsigned u = 0; u < kInvPer; u++) {
       const unsigned r = rr[u], c = cc[u];
-      if (r < m && r != k && fcol[r]) {
-        const uint32_t x = a[k * m + c];
-        const uint16_t* tr = T + r * 64;
-        const uint16_t y = (uint16_t)(tr[x & 15] ^ tr[16 + ((x >> 4) & 15)] ^ tr[32 + ((x >> 8) & 15)] ^ tr[48 + (x >> 12)]);
-        a[r * m + c] = c == k ? y : (uint16_t)(a[r * m + c] ^ y);
+      if (r < m && r != k) {
+        uint16_t v = a[r * m + c];
+        if (fcol[r]) {
+          const uint32_t x = a[k * m + c];
+          const uint16_t* tr = T + r * 64;
+          const uint16_t y =
+              (uint16_t)(tr[x & 15] ^ tr[16 + ((x >> 4) & 15)] ^ tr[32 + ((x >> 8) & 15)] ^ tr[48 + (x >> 12)]);
+          v = c == k ? y : (uint16_t)(v ^ y);
+          a[r * m + c] = v;
+        }
+        if (c == k + 1) fnext[r] = v;
       }
     }
     __syncthreads();
