@@ -263,14 +263,17 @@ def test_par3_repair_inverse_paths_vs_oracle(kctx, oracle, N, n, B, fI, fR):
     assert np.array_equal(got, rhs)
 
 
-def test_compute_recovery_host_inputs_in_overlapped_chunks(kctx, oracle):
+@pytest.mark.parametrize("N,R", [(16385, 3), (20003, 5)])
+def test_compute_recovery_host_inputs_in_overlapped_chunks(kctx, oracle, N, R):
     """Host inputs of >= two 64 MiB chunks are copied chunk by chunk on a copy
     stream while the previous chunk's product runs (products accumulate from
-    the second chunk on); 16,385 blocks of 8 KiB leave a one-block last chunk.
-    Sampled word ranges of every block against the oracle, plus accumulate."""
+    the second chunk on); the last chunk goes in halving pieces.  16,385
+    blocks of 8 KiB leave a one-block last chunk; 20,003 blocks give 8,192,
+    8,192, 1,810, 904, 512 and 393 (R=5: the SM-pair kernel).  Sampled word
+    ranges of every block against the oracle, plus accumulate."""
     from parparpar_b200 import par3
-    rng = np.random.default_rng(81)
-    N, B, R, fI, fR = 16385, 1024, 3, 5, 20000
+    rng = np.random.default_rng(81 + N)
+    B, fI, fR = 1024, 5, 20000 + N
     data = rng.integers(0, 2**64, (N, B), dtype=np.uint64)
     out = np.zeros((R, B), dtype=np.uint64)
     par3.GF64Controller.ComputeRecoveryBlocks(data, N, out, R, B, fI, fR)
