@@ -943,7 +943,9 @@ def main():
         h_in = torch.empty((w["n"], w["s"]), dtype=torch.uint8).pin_memory()
         h_in.copy_(job["d_in"])
         h_out = torch.empty((w["r"], w["s"]), dtype=torch.uint8).pin_memory()
-        hjob = dict(job, d_in=h_in, d_out=h_out, d_fac=np.zeros((w["r"], w["n"]), dtype=np.uint16))
+        # host slices in, restored slices out; the factors stay on the device
+        # between the inversion and the decode, as a GPU caller keeps them
+        hjob = dict(job, d_in=h_in, d_out=h_out)
         e2e_f = lambda: par2_repair_step(hjob, ctx)
     elif w["field"] == "gf16":
         h_in = torch.empty((w["n"], w["s"]), dtype=torch.uint8).pin_memory()
