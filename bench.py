@@ -734,6 +734,14 @@ def measure_fused(ctx, dev):
     t_plain = med(lambda: par2.par2_create(h_in, idx, exps, out=h_out, ctx=ctx))
     t_hash = med(lambda: par2.par2_create(h_in, idx, exps, out=h_out, hashes=h_hash, ctx=ctx))
     out["par2_create_32768x32KiB_R64"] = {"plain": n * sl / t_plain / 1e9, "with_ifsc_hashes": n * sl / t_hash / 1e9}
+    # few large slices: the hashed create copies column bands of every slice
+    n1, sl1, r1 = 1024, 1 << 20, 8
+    x1 = h_in.view(n1, sl1)
+    o1 = torch.empty((r1, sl1), dtype=torch.uint8).pin_memory()
+    h1 = torch.empty((n1, 20), dtype=torch.uint8).pin_memory()
+    t_plain = med(lambda: par2.par2_create(x1, np.arange(n1), list(range(r1)), out=o1, ctx=ctx))
+    t_hash = med(lambda: par2.par2_create(x1, np.arange(n1), list(range(r1)), out=o1, hashes=h1, ctx=ctx))
+    out["par2_create_1024x1MiB_R8"] = {"plain": n1 * sl1 / t_plain / 1e9, "with_ifsc_hashes": n1 * sl1 / t_hash / 1e9}
     # the PAR3 inputs reuse the same pinned bytes as 131,072 x 8 KiB blocks
     nb, words, R = 131072, 1024, 8
     x = h_in.view(torch.int64).view(nb, words)

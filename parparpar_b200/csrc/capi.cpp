@@ -77,7 +77,7 @@ const Gf16Host& gf16h() {
 }  // namespace
 
 // -------------------------------------------------------------------- ctx
-enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_AEXP, S_HASH, S_HCV, S_PKT, S_STREAM, S_NSLOTS };
+enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_AEXP, S_HASH, S_HCV, S_PKT, S_STREAM, S_HSTATE, S_NSLOTS };
 
 struct CauchyEntry {
   size_t n_in, n_rec;
@@ -511,6 +511,8 @@ static cudaError_t gf16_region(int sel, const uint8_t* din, size_t dstride, unsi
 // copies overlap the products and the job takes about as long as its copies.
 constexpr unsigned kCopyChunk = 4096;
 constexpr unsigned kCopyTail = 256;
+constexpr size_t kBandMinBytes = (size_t)128 << 20;  // column bands for staged inputs of at least this size
+constexpr size_t kBandMinWidth = 4096;               // bytes of every slice per band, at least (multiple of 64)
 constexpr size_t kGf16TileBytes = 128 * 128;  // one expanded tile (8 outputs x 8 inputs)
 
 static int ensure_copy_stream(pp_ctx* ctx) {
@@ -617,6 +619,60 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
       CUDA_TRY(ctx, launch_gf16_muladd_tc(din + (size_t)c0 * row, row, nc, slice, aexp + (size_t)(c0 / 8) * kGf16TileBytes,
                                           n_out, dout, ostride, accumulate || c0 > 0, ctx->sms, ctx->d_status,
                                           ctx->stream, stages));
+    }
+    if (stage_out)
+      CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,
+                                      out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    if (int r = join_hashes()) return r;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return device_status(ctx);
+  }
+  // ---- column bands: host inputs of few large slices with their hashes.
+  // An MD5 chain runs through a whole slice, so hashing after the last copy
+  // would add a full slice's chain (about 17 ms for 1 MiB) to the call.  The
+  // copies go instead as column bands of every slice (bytes [c0, c1) of all
+  // rows, about 64 MiB per band); each band's product (the region product is
+  // column-separable) and the band's MD5 / CRC32 blocks (state carried from
+  // band to band) run as it lands.
+  const size_t band_w = std::max<size_t>(kBandMinWidth, (((size_t)64 << 20) / std::max(1u, n_in)) & ~(size_t)63);
+  if (hashes && !in_dev && n_in < 2 * kCopyChunk && use_tensor(ctx->gf16_kernel, n_in, n_out) &&
+      (size_t)row * n_in >= kBandMinBytes && slice > band_w) {
+    if (int r = ensure_copy_stream(ctx)) return r;
+    uint8_t* din = (uint8_t*)scratch(ctx, S_IN, row * n_in);
+    uint32_t* hst = (uint32_t*)scratch(ctx, S_HSTATE, (size_t)20 * n_in);
+    if (!din || !hst) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", row * n_in);
+    uint8_t* dout = (uint8_t*)outputs;
+    size_t ostride = out_stride;
+    const bool stage_out = !out_dev || !aligned16(outputs, out_stride);
+    if (stage_out) {
+      dout = (uint8_t*)scratch(ctx, S_OUT, row * n_out);
+      if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "output staging (%zu bytes)", row * n_out);
+      ostride = row;
+      if (accumulate)
+        CUDA_TRY(ctx, cudaMemcpy2DAsync(dout, row, outputs, out_stride, slice, n_out,
+                                        out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    }
+    uint8_t* aexp = aexp_ready;
+    if (!aexp) {
+      aexp = (uint8_t*)scratch(ctx, S_AEXP, gf16_tc_coeff_bytes(n_in, n_out));
+      if (!aexp) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficient tiles");
+      CUDA_TRY(ctx, launch_gf16_tc_expand(d_coeffs, ldc, n_in, n_out, aexp, ctx->stream));
+    }
+    CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->start_ev, 0));
+    for (size_t c0 = 0; c0 < slice; c0 += band_w) {
+      const size_t c1 = std::min(slice, c0 + band_w);
+      CUDA_TRY(ctx, cudaMemcpy2DAsync(din + c0, row, (const uint8_t*)inputs + c0, in_stride, c1 - c0, n_in,
+                                      cudaMemcpyHostToDevice, ctx->copy));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
+      CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev, 0));
+      CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->copy_ev, 0));
+      const bool last = c1 == slice;
+      CUDA_TRY(ctx, launch_par2_block_hash_band(din, row, n_in, slice, c0 / 64, last ? slice / 64 : c1 / 64, hst, dh,
+                                                c0 == 0, last, ctx->hash));
+      CUDA_TRY(ctx, launch_gf16_muladd_tc(din + c0, row, n_in, c1 - c0, aexp, n_out, dout + c0, ostride, accumulate,
+                                          ctx->sms, ctx->d_status, ctx->stream));
     }
     if (stage_out)
       CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,

@@ -130,23 +130,18 @@ __device__ __forceinline__ uint32_t masked_word(const uint8_t* row, uint64_t o, 
 
 // One thread per slice.  Rows are 16-byte aligned (data and stride).  The
 // message is L bytes: the row's first len bytes, then zeros.
-// MD5 and / or CRC32 of one slice's message (the row's first len bytes,
-// then zeros up to L bytes); MD5 goes to o20[0..16), CRC32 to o20[16..20).
+// MD5 and / or CRC32 over the whole 64-byte blocks [b0, b1) of a row (all
+// inside the data): 16-byte loads, one block prefetched.
 template <bool kMd5, bool kCrc>
-__device__ __forceinline__ void par2_slice_hash(const uint8_t* row, uint64_t len, uint64_t L, const uint32_t* tk,
-                                                uint8_t* o20) {
-  uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
-  uint32_t crc = 0xFFFFFFFFu;
+__device__ __forceinline__ void hash_full_blocks(const uint8_t* row, uint64_t b0, uint64_t b1, uint32_t st[4],
+                                                 uint32_t& crc, const uint32_t* tk) {
   uint32_t m[16];
-
-  // blocks wholly inside the data: 16-byte loads, one block prefetched
-  const uint64_t nfull = len / 64;
   uint4 nx[4];
-  if (nfull) {
+  if (b0 < b1) {
 #pragma unroll
-    for (int q = 0; q < 4; q++) nx[q] = __ldg(reinterpret_cast<const uint4*>(row) + q);
+    for (int q = 0; q < 4; q++) nx[q] = __ldg(reinterpret_cast<const uint4*>(row + 64 * b0) + q);
   }
-  for (uint64_t b = 0; b < nfull; b++) {
+  for (uint64_t b = b0; b < b1; b++) {
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       m[4 * q] = nx[q].x;
@@ -154,7 +149,7 @@ __device__ __forceinline__ void par2_slice_hash(const uint8_t* row, uint64_t len
       m[4 * q + 2] = nx[q].z;
       m[4 * q + 3] = nx[q].w;
     }
-    if (b + 1 < nfull) {
+    if (b + 1 < b1) {
 #pragma unroll
       for (int q = 0; q < 4; q++) nx[q] = __ldg(reinterpret_cast<const uint4*>(row + 64 * (b + 1)) + q);
     }
@@ -164,7 +159,16 @@ __device__ __forceinline__ void par2_slice_hash(const uint8_t* row, uint64_t len
     }
     if constexpr (kMd5) md5_block(st, m);
   }
-  // the rest of the L / 64 whole message blocks: data tail, then zero padding
+}
+
+// The rest of the message after its first `nfull` whole data blocks: the
+// remaining L / 64 blocks (data tail, then zero padding), the final partial
+// block with the MD5 padding, and the IFSC entry: MD5 to o20[0..16), CRC32
+// to o20[16..20).
+template <bool kMd5, bool kCrc>
+__device__ __forceinline__ void hash_finish(const uint8_t* row, uint64_t len, uint64_t L, uint64_t nfull,
+                                            uint32_t st[4], uint32_t crc, const uint32_t* tk, uint8_t* o20) {
+  uint32_t m[16];
   const uint64_t nblk = L / 64;
   for (uint64_t b = nfull; b < nblk; b++) {
 #pragma unroll
@@ -217,6 +221,17 @@ __device__ __forceinline__ void par2_slice_hash(const uint8_t* row, uint64_t len
   }
 }
 
+// MD5 and / or CRC32 of one slice's message (the row's first len bytes,
+// then zeros up to L bytes).
+template <bool kMd5, bool kCrc>
+__device__ __forceinline__ void par2_slice_hash(const uint8_t* row, uint64_t len, uint64_t L, const uint32_t* tk,
+                                                uint8_t* o20) {
+  uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
+  uint32_t crc = 0xFFFFFFFFu;
+  hash_full_blocks<kMd5, kCrc>(row, 0, len / 64, st, crc, tk);
+  hash_finish<kMd5, kCrc>(row, len, L, len / 64, st, crc, tk, o20);
+}
+
 __global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restrict__ data, size_t stride,
                                                          size_t n, uint64_t L,
                                                          const uint64_t* __restrict__ lengths,
@@ -250,6 +265,49 @@ __global__ void __launch_bounds__(128) k_par2_block_hash_split(const uint8_t* __
     par2_slice_hash<true, false>(data + i * stride, len, L, nullptr, out + 20 * i);
   else
     par2_slice_hash<false, true>(data + i * stride, len, L, crc_tab + (threadIdx.x % kCrcCopies), out + 20 * i);
+}
+
+// Resumable form over column bands (every row L bytes of data): blocks
+// [k0, k1) of every slice, with MD5 and CRC32 in separate warps as above.
+// state[5 i ..] holds slice i's MD5 words and CRC32 register between bands;
+// the first band starts them, the last one (k1 = L / 64) also hashes the
+// final partial block and padding and writes the IFSC entry.  Slices whose
+// bytes arrive band by band are hashed as they land: a band's launch takes
+// as long as its own blocks, not the whole chain of the slice.
+__global__ void __launch_bounds__(128) k_par2_block_hash_band(const uint8_t* __restrict__ data, size_t stride,
+                                                              size_t n, uint64_t L, uint64_t k0, uint64_t k1,
+                                                              uint32_t* __restrict__ state, uint8_t* __restrict__ out,
+                                                              int first, int last) {
+  extern __shared__ uint32_t crc_tab[];
+  crc_tables_init(crc_tab);
+  __syncthreads();
+  const size_t i = (size_t)blockIdx.x * 64 + (threadIdx.x & 63);
+  if (i >= n) return;
+  const uint8_t* row = data + i * stride;
+  uint32_t* S = state + 5 * i;
+  uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
+  uint32_t crc = 0xFFFFFFFFu;
+  if (threadIdx.x < 64) {
+    if (!first) {
+#pragma unroll
+      for (int w = 0; w < 4; w++) st[w] = S[w];
+    }
+    hash_full_blocks<true, false>(row, k0, k1, st, crc, nullptr);
+    if (last) {
+      hash_finish<true, false>(row, L, L, k1, st, crc, nullptr, out + 20 * i);
+    } else {
+#pragma unroll
+      for (int w = 0; w < 4; w++) S[w] = st[w];
+    }
+  } else {
+    const uint32_t* tk = crc_tab + (threadIdx.x % kCrcCopies);
+    if (!first) crc = S[4];
+    hash_full_blocks<false, true>(row, k0, k1, st, crc, tk);
+    if (last)
+      hash_finish<false, true>(row, L, L, k1, st, crc, tk, out + 20 * i);
+    else
+      S[4] = crc;
+  }
 }
 
 // PAR2 recovery-slice packet headers (lib/par2.js:517-530 getRecoveryHeader;
@@ -674,6 +732,19 @@ cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t 
     k_par2_block_hash_split<<<(unsigned)((n + 63) / 64), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out);
   else
     k_par2_block_hash<<<(unsigned)((n + 127) / 128), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_par2_block_hash_band(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
+                                        uint64_t k0, uint64_t k1, uint32_t* d_state, uint8_t* d_out, bool first,
+                                        bool last, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int smem = kCrcWords * 4;
+  cudaError_t e = cudaFuncSetAttribute(k_par2_block_hash_band, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_par2_block_hash_band<<<(unsigned)((n + 63) / 64), 128, smem, s>>>(d_data, stride, n, slice, k0, k1, d_state,
+                                                                      d_out, first ? 1 : 0, last ? 1 : 0);
   note_launch();
   return cudaGetLastError();
 }

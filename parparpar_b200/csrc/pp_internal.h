@@ -151,6 +151,14 @@ cudaError_t launch_gf64_fft(uint64_t* d_data, size_t n, size_t batch, size_t ld,
 cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
                                    const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s);
 
+// The same hashes over column bands of slices that are all `slice` bytes:
+// 64-byte blocks [k0, k1) of every row; d_state (5 words per row) carries the
+// MD5 and CRC32 state from band to band; `first` starts it, `last` (k1 =
+// slice / 64) finishes the message and writes the entries to d_out.
+cudaError_t launch_par2_block_hash_band(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
+                                        uint64_t k0, uint64_t k1, uint32_t* d_state, uint8_t* d_out, bool first,
+                                        bool last, cudaStream_t s);
+
 // BLAKE3 over n messages "prefix || data_i": the prefix is P bytes (32 or 40)
 // made of pre[0..6) (24 bytes), u64le(first_index + i) and, when P == 40,
 // u64le(extra).  The 16-byte truncated digest of message i goes to

@@ -226,6 +226,31 @@ def test_par2_create_hashed_host_inputs(ctx, oracle, rng, n):
 
 
 @gpu
+@pytest.mark.parametrize("n,sl,exps", [(300, 450002, [0, 1, 7, 300] + list(range(9, 21))),
+                                       (64, 2 * 1024 * 1024 + 6, [2, 5, 9, 11, 13, 17, 19, 23])])
+def test_par2_create_hashed_column_bands(ctx, rng, n, sl, exps):
+    """Host inputs of few large slices (>= 128 MiB staged) go to the device as
+    column bands of every slice, each band's product and MD5 / CRC32 blocks
+    running as it lands (the hash state carried from band to band): 300 x
+    450,002 B makes three bands, the last one 2,642 B (odd: a partial final
+    word); 64 x (2 MiB + 6 B) makes bands of 1 MiB, 1 MiB and 6 B (a band
+    with no whole 64-byte block).  The IFSC entries match
+    hashlib / zlib, the recovery slices the create from device-resident inputs
+    (a path without bands, pinned to the oracle elsewhere)."""
+    torch = _torch()
+    from parparpar_b200 import par2
+    data = rng.integers(0, 256, (n, sl), dtype=np.uint8)
+    hashes = np.zeros((n, 20), dtype=np.uint8)
+    out = par2.par2_create(data, np.arange(n), exps, hashes=hashes, ctx=ctx)
+    want = par2_oracle(data, sl)
+    assert (hashes == want).all()
+    d_out = torch.zeros((len(exps), sl), dtype=torch.uint8, device="cuda")
+    par2.par2_create(torch.from_numpy(data).cuda(), np.arange(n), exps, out=d_out, ctx=ctx)
+    ctx.synchronize()
+    assert (out == d_out.cpu().numpy()).all()
+
+
+@gpu
 def test_par2_create_hashed_device_inputs(ctx, rng):
     torch = _torch()
     from parparpar_b200 import par2
