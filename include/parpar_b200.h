@@ -166,6 +166,18 @@ PP_API int pp_par2_proc_end_input(pp_par2_proc* proc);
 /* getOutput(index, output) -> *valid (1 = output passed the integrity check). */
 PP_API int pp_par2_proc_get_output(pp_par2_proc* proc, unsigned index, void* output, int* valid);
 PP_API int pp_par2_proc_discard_output(pp_par2_proc* proc);
+/* Input hashing in the processor's own pass (replaces feeding the same
+ * buffers to HasherInput::update / getBlock(md5crc, zeroPad),
+ * hasher/hasher_input_base.h:104-117, beside the backend's addInput): with
+ * max_inputs > 0, every slice added by input number afterwards gets its IFSC
+ * entry (MD5 || CRC32le of the slice zero-padded to the current slice size)
+ * computed on the device from its staged row, at index input_num (which must
+ * be < max_inputs); decode inputs (add_input_coeffs) are not hashed.
+ * max_inputs = 0 turns it off.  get_input_hashes waits for the submitted
+ * batches and copies entries [0, count) (20 bytes each, host or device
+ * buffer); entries of inputs not added since enabling read as zero. */
+PP_API int pp_par2_proc_set_input_hashes(pp_par2_proc* proc, unsigned max_inputs);
+PP_API int pp_par2_proc_get_input_hashes(pp_par2_proc* proc, uint8_t* out, unsigned count);
 PP_API int pp_par2_proc_free_processing_mem(pp_par2_proc* proc);
 PP_API unsigned pp_par2_proc_input_batch_size(pp_par2_proc* proc);
 PP_API unsigned pp_par2_proc_batches_started(pp_par2_proc* proc);

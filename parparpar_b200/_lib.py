@@ -51,6 +51,7 @@ EXPORTS = [
     "pp_par2_proc_set_recovery_slices", "pp_par2_proc_can_add", "pp_par2_proc_wait_for_add",
     "pp_par2_proc_add_input", "pp_par2_proc_add_input_coeffs", "pp_par2_proc_flush", "pp_par2_proc_end_input",
     "pp_par2_proc_get_output", "pp_par2_proc_discard_output", "pp_par2_proc_free_processing_mem",
+    "pp_par2_proc_set_input_hashes", "pp_par2_proc_get_input_hashes",
     "pp_par2_proc_input_batch_size", "pp_par2_proc_batches_started", "pp_gf64_build_cauchy",
     "pp_gf64_compute_recovery", "pp_gf64_compute_recovery_with_coeff", "pp_gf64_solve_and_reconstruct",
     "pp_gf64_region_mul", "pp_gf64_region_mul_arr", "pp_gf64_region_muladd_arr",
@@ -126,6 +127,8 @@ _sig("pp_par2_proc_flush", _I, _P)
 _sig("pp_par2_proc_end_input", _I, _P)
 _sig("pp_par2_proc_get_output", _I, _P, _U, _P, ctypes.POINTER(_I))
 _sig("pp_par2_proc_discard_output", _I, _P)
+_sig("pp_par2_proc_set_input_hashes", _I, _P, _U)
+_sig("pp_par2_proc_get_input_hashes", _I, _P, _P, _U)
 _sig("pp_par2_proc_free_processing_mem", _I, _P)
 _sig("pp_par2_proc_input_batch_size", _U, _P)
 _sig("pp_par2_proc_batches_started", _U, _P)

@@ -893,6 +893,9 @@ struct pp_par2_proc {
     uint16_t* d_coeff = nullptr;  // [n_out][batch]
     uint8_t* d_aexp = nullptr;    // tensor-core coefficient tiles
     std::vector<uint16_t> h_coeff;
+    std::vector<uint16_t> h_idx;  // input number of each staged row (0xFFFF: not hashed)
+    uint16_t* d_idx = nullptr;
+    unsigned d_idx_n = 0;
     unsigned count = 0;
     cudaEvent_t done = nullptr;
     bool active = false;
@@ -910,6 +913,8 @@ struct pp_par2_proc {
   unsigned batches_started = 0;
   cudaStream_t s_copy = nullptr, s_comp = nullptr;
   cudaEvent_t copied = nullptr;
+  uint8_t* d_hash = nullptr;  // IFSC entries of the staged inputs, by input number
+  unsigned hash_cap = 0;
 };
 
 // host slices of at least this many bytes are copied straight from the
@@ -1004,8 +1009,10 @@ PP_API void pp_par2_proc_destroy(pp_par2_proc* p) {
     if (a.h_in) cudaFreeHost(a.h_in);
     if (a.d_coeff) cudaFree(a.d_coeff);
     if (a.d_aexp) cudaFree(a.d_aexp);
+    if (a.d_idx) cudaFree(a.d_idx);
     if (a.done) cudaEventDestroy(a.done);
   }
+  if (p->d_hash) cudaFree(p->d_hash);
   if (p->d_out) cudaFree(p->d_out);
   if (p->d_out_ck) cudaFree(p->d_out_ck);
   if (p->d_valid) cudaFree(p->d_valid);
@@ -1135,8 +1142,26 @@ static int proc_submit(pp_par2_proc* p) {
   // coefficient block [n_out][batch] (only the first `count` columns are used)
   CUDA_TRY(p->ctx, cudaMemcpyAsync(a.d_coeff, a.h_coeff.data(), (size_t)n_out * p->batch * 2,
                                    cudaMemcpyHostToDevice, p->s_copy));
+  if (p->d_hash) {  // the rows' input numbers, for the IFSC entries
+    if (a.d_idx_n < a.count) {
+      CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_copy));
+      if (a.d_idx) cudaFree(a.d_idx);
+      a.d_idx = nullptr;
+      a.d_idx_n = 0;
+      if (cudaMalloc(&a.d_idx, sizeof(uint16_t) * p->batch_alloc) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(p->ctx, PP_ERR_NO_MEMORY, "hash index table");
+      }
+      a.d_idx_n = p->batch_alloc;
+    }
+    CUDA_TRY(p->ctx, cudaMemcpyAsync(a.d_idx, a.h_idx.data(), sizeof(uint16_t) * a.count, cudaMemcpyHostToDevice,
+                                     p->s_copy));
+  }
   CUDA_TRY(p->ctx, cudaEventRecord(p->copied, p->s_copy));
   CUDA_TRY(p->ctx, cudaStreamWaitEvent(p->s_comp, p->copied, 0));
+  if (p->d_hash)
+    CUDA_TRY(p->ctx, launch_par2_block_hash(a.d_in, p->row, a.count, p->cur_size, nullptr, p->d_hash, p->s_comp,
+                                            a.d_idx));
   // each row's memory checksum, then the products of the data rows and of
   // the checksum rows (the second launch reuses the expanded coefficient tiles)
   CUDA_TRY(p->ctx, launch_par2_cksum(a.d_in, p->row, a.count, p->cur_size, a.d_ck, 16, nullptr, p->s_comp));
@@ -1166,6 +1191,13 @@ static int proc_add(pp_par2_proc* p, const void* buf, size_t size, const uint16_
   if (area_busy(a)) return set_err(p->ctx, PP_ERR_BUSY, "staging area busy");
   const unsigned n_out = (unsigned)p->exps.size();
   const unsigned idx = a.count;
+  if (p->d_hash) {
+    if (!coeffs && input_num >= p->hash_cap)
+      return set_err(p->ctx, PP_ERR_INVALID_ARG, "input number %u beyond the %u-entry input hash table",
+                     (unsigned)input_num, p->hash_cap);
+    if (a.h_idx.size() < p->batch_alloc) a.h_idx.resize(p->batch_alloc);
+    a.h_idx[idx] = coeffs ? (uint16_t)0xFFFF : input_num;  // decode inputs are not hashed
+  }
   for (unsigned o = 0; o < n_out; o++)
     a.h_coeff[(size_t)o * p->batch + idx] = coeffs ? coeffs[o] : gf16h().coeff(input_num, p->exps[o]);
   if (size && (size >= kProcDirectBytes || !a.h_in || is_device_ptr(buf))) {
@@ -1242,6 +1274,34 @@ PP_API int pp_par2_proc_get_output(pp_par2_proc* p, unsigned index, void* output
   CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_copy));
   if (valid) *valid = p->has_output ? p->valid[index] : 1;
   return PP_OK;
+}
+
+PP_API int pp_par2_proc_set_input_hashes(pp_par2_proc* p, unsigned max_inputs) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  if (max_inputs > 32768) return set_err(p->ctx, PP_ERR_INVALID_ARG, "max_inputs > 32768");
+  bind(p->ctx);
+  CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_comp));
+  if (p->d_hash) cudaFree(p->d_hash);
+  p->d_hash = nullptr;
+  p->hash_cap = 0;
+  if (!max_inputs) return PP_OK;
+  if (cudaMalloc(&p->d_hash, (size_t)20 * max_inputs) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(p->ctx, PP_ERR_NO_MEMORY, "input hash table");
+  }
+  CUDA_TRY(p->ctx, cudaMemset(p->d_hash, 0, (size_t)20 * max_inputs));
+  p->hash_cap = max_inputs;
+  return PP_OK;
+}
+
+PP_API int pp_par2_proc_get_input_hashes(pp_par2_proc* p, uint8_t* out, unsigned count) {
+  if (!p || (count && !out)) return PP_ERR_INVALID_ARG;
+  if (!p->d_hash) return set_err(p->ctx, PP_ERR_INVALID_ARG, "input hashing is not enabled");
+  if (count > p->hash_cap) return set_err(p->ctx, PP_ERR_INVALID_ARG, "count beyond the input hash table");
+  bind(p->ctx);
+  CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_comp));
+  CUDA_TRY(p->ctx, cudaMemcpy(out, p->d_hash, (size_t)20 * count, cudaMemcpyDefault));
+  return device_status(p->ctx);
 }
 
 PP_API int pp_par2_proc_discard_output(pp_par2_proc* p) {

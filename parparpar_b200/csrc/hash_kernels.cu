@@ -232,17 +232,21 @@ __device__ __forceinline__ void par2_slice_hash(const uint8_t* row, uint64_t len
   hash_finish<kMd5, kCrc>(row, len, L, len / 64, st, crc, tk, o20);
 }
 
+// idx (optional): row i's entry goes to out + 20 * idx[i]; 0xFFFF: not hashed
 __global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restrict__ data, size_t stride,
                                                          size_t n, uint64_t L,
                                                          const uint64_t* __restrict__ lengths,
-                                                         uint8_t* __restrict__ out) {
+                                                         uint8_t* __restrict__ out,
+                                                         const uint16_t* __restrict__ idx) {
   extern __shared__ uint32_t crc_tab[];
   crc_tables_init(crc_tab);
   __syncthreads();
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const size_t o = idx ? idx[i] : i;
+  if (idx && o == 0xFFFF) return;
   const uint64_t len = lengths ? (lengths[i] < L ? lengths[i] : L) : L;
-  par2_slice_hash<true, true>(data + i * stride, len, L, crc_tab + (threadIdx.x % kCrcCopies), out + 20 * i);
+  par2_slice_hash<true, true>(data + i * stride, len, L, crc_tab + (threadIdx.x % kCrcCopies), out + 20 * o);
 }
 
 // Few slices (too few threads to fill the GPU): MD5 and CRC32 of a slice in
@@ -254,17 +258,20 @@ __global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restri
 __global__ void __launch_bounds__(128) k_par2_block_hash_split(const uint8_t* __restrict__ data, size_t stride,
                                                                size_t n, uint64_t L,
                                                                const uint64_t* __restrict__ lengths,
-                                                               uint8_t* __restrict__ out) {
+                                                               uint8_t* __restrict__ out,
+                                                               const uint16_t* __restrict__ idx) {
   extern __shared__ uint32_t crc_tab[];
   crc_tables_init(crc_tab);
   __syncthreads();
   const size_t i = (size_t)blockIdx.x * 64 + (threadIdx.x & 63);
   if (i >= n) return;
+  const size_t o = idx ? idx[i] : i;
+  if (idx && o == 0xFFFF) return;
   const uint64_t len = lengths ? (lengths[i] < L ? lengths[i] : L) : L;
   if (threadIdx.x < 64)
-    par2_slice_hash<true, false>(data + i * stride, len, L, nullptr, out + 20 * i);
+    par2_slice_hash<true, false>(data + i * stride, len, L, nullptr, out + 20 * o);
   else
-    par2_slice_hash<false, true>(data + i * stride, len, L, crc_tab + (threadIdx.x % kCrcCopies), out + 20 * i);
+    par2_slice_hash<false, true>(data + i * stride, len, L, crc_tab + (threadIdx.x % kCrcCopies), out + 20 * o);
 }
 
 // Resumable form over column bands (every row L bytes of data): blocks
@@ -717,7 +724,7 @@ uint32_t gf16_pow2(uint64_t e) {
 }  // namespace
 
 cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
-                                   const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s) {
+                                   const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s, const uint16_t* d_idx) {
   if (n == 0) return cudaSuccess;
   const int smem = kCrcWords * 4;
   cudaError_t e = cudaFuncSetAttribute(k_par2_block_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -729,9 +736,11 @@ cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t 
   // 128 KiB 2.18 -> 1.96 ms; at 32,768 x 32 KiB the one-thread form is
   // faster, 0.68 vs 1.22 ms, as the ALU pipe is then the limit)
   if (n <= 8192)
-    k_par2_block_hash_split<<<(unsigned)((n + 63) / 64), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out);
+    k_par2_block_hash_split<<<(unsigned)((n + 63) / 64), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out,
+                                                                         d_idx);
   else
-    k_par2_block_hash<<<(unsigned)((n + 127) / 128), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out);
+    k_par2_block_hash<<<(unsigned)((n + 127) / 128), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out,
+                                                                     d_idx);
   note_launch();
   return cudaGetLastError();
 }

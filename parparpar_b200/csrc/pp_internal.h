@@ -147,9 +147,11 @@ cudaError_t launch_gf64_fft(uint64_t* d_data, size_t n, size_t batch, size_t ld,
 // ------------------------------------------------------------ block hashes
 // PAR2 input-slice checksums: out[20*i..] = MD5 || CRC32le of the first
 // min(lengths[i], slice) bytes of row i followed by zeros up to slice bytes
-// (lengths NULL: every row is slice bytes).  Rows 16-byte aligned.
+// (lengths NULL: every row is slice bytes).  Rows 16-byte aligned.  d_idx
+// (optional): row i's entry goes to d_out + 20 * d_idx[i], none for 0xFFFF.
 cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t n, uint64_t slice,
-                                   const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s);
+                                   const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s,
+                                   const uint16_t* d_idx = nullptr);
 
 // The same hashes over column bands of slices that are all `slice` bytes:
 // 64-byte blocks [k0, k1) of every row; d_state (5 words per row) carries the

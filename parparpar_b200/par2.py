@@ -212,6 +212,20 @@ class PAR2ProcCUDA:
     def discardOutput(self):
         self._chk(lib.pp_par2_proc_discard_output(self.h))
 
+    def setInputHashes(self, maxInputs: int):
+        """Hash every slice added by input number from now on (IFSC entries:
+        MD5 || CRC32le of the slice zero-padded to the slice size), on the
+        device, in the processor's own pass; 0 turns it off."""
+        self._chk(lib.pp_par2_proc_set_input_hashes(self.h, maxInputs))
+
+    def getInputHashes(self, count: int, out=None):
+        """Entries [0, count) as a (count, 20) uint8 array (or into `out`,
+        host or CUDA), after the submitted batches finish."""
+        if out is None:
+            out = np.zeros((count, 20), dtype=np.uint8)
+        self._chk(lib.pp_par2_proc_get_input_hashes(self.h, ptr(out), count))
+        return out
+
     def freeProcessingMem(self):
         self._chk(lib.pp_par2_proc_free_processing_mem(self.h))
 

@@ -167,6 +167,51 @@ def test_proc_batches_and_reuse(kctx, oracle):
     proc.deinit()
 
 
+def test_proc_input_hashes_in_its_own_pass(kctx, oracle):
+    """setInputHashes: the processor hashes every slice it stages (IFSC entry:
+    MD5 || CRC32le of the slice zero-padded to the slice size) at its input
+    number -- full host slices over 256 KiB (copied straight to the device),
+    short host slices (staged through pinned rows, zero-padded), a CUDA
+    input, inputs added out of order, several batches, decode inputs left
+    unhashed, and entries of numbers never added reading zero."""
+    import torch
+    from parparpar_b200 import par2
+    from oracle import par2_block_hashes
+    rng = np.random.default_rng(91)
+    S, n, R = 300_000, 23, 3
+    sizes = [S if i % 3 else int(rng.integers(1, S)) for i in range(n)]
+    data = np.zeros((n, S), dtype=np.uint8)
+    for i, sz in enumerate(sizes):
+        data[i, :sz] = rng.integers(0, 256, sz, dtype=np.uint8)
+    proc = par2.PAR2ProcCUDA(S, 2, 4, ctx=kctx)
+    proc.setRecoverySlices(R, [0, 1, 2])
+    proc.setInputHashes(n + 5)
+    order = list(rng.permutation(n))
+    for k, i in enumerate(order):
+        proc.waitForAdd()
+        buf = torch.from_numpy(data[i, :sizes[i]].copy()).cuda() if i == 5 else data[i, :sizes[i]]
+        proc.addInput(buf, sizes[i], int(i), flush=(k == 10))
+    proc.endInput()
+    got = proc.getInputHashes(n + 5)
+    assert np.array_equal(got[:n], par2_block_hashes(data, S))
+    assert not got[n:].any()
+    exp = oracle.par2_muladd(list(data), S, oracle.par2_coeff_matrix(range(n), [0, 1, 2]))
+    for o in range(R):
+        out = np.zeros(S, dtype=np.uint8)
+        assert proc.getOutput(o, out)
+        assert np.array_equal(out, exp[o])
+    # decode inputs (explicit coefficients) add no entries
+    proc.discardOutput()
+    proc.setInputHashes(4)
+    co = rng.integers(1, 65536, (2, R)).astype(np.uint16)
+    for i in range(2):
+        proc.waitForAdd()
+        proc.addInput(data[i], S, co[i])
+    proc.endInput()
+    assert not proc.getInputHashes(4).any()
+    proc.deinit()
+
+
 def test_proc_mixed_host_device_inputs_reused_on_return(kctx, oracle):
     """Host inputs are staged in pinned rows and copied per batch, device
     inputs are copied at once; mixed in one batch, each buffer overwritten as
