@@ -80,6 +80,9 @@ def test_null_context_is_rejected():
     import parparpar_b200._lib as L
     assert L.lib.pp_gf64_compute_recovery(None, None, 1, None, 1, 1, 0, 1, 0, 0) == L.PP_ERR_INVALID_ARG
     assert L.lib.pp_par2_create(None, None, 0, 0, 0, None, None, 0, None, 0) == L.PP_ERR_INVALID_ARG
+    # processor input hashing: a null processor is rejected before any device work
+    assert L.lib.pp_par2_proc_set_input_hashes(None, 4) == L.PP_ERR_INVALID_ARG
+    assert L.lib.pp_par2_proc_get_input_hashes(None, None, 0) == L.PP_ERR_INVALID_ARG
 
 
 def test_assemble_recovery_packets_argument_errors():
