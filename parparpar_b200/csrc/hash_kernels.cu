@@ -221,18 +221,98 @@ __device__ __forceinline__ void hash_finish(const uint8_t* row, uint64_t len, ui
   }
 }
 
+// MD5 and / or CRC32 of one slice's message (the whole-slice kernels keep
+// this single body: the band kernel below uses the split helpers above).
 // MD5 and / or CRC32 of one slice's message (the row's first len bytes,
-// then zeros up to L bytes).
+// then zeros up to L bytes); MD5 goes to o20[0..16), CRC32 to o20[16..20).
 template <bool kMd5, bool kCrc>
 __device__ __forceinline__ void par2_slice_hash(const uint8_t* row, uint64_t len, uint64_t L, const uint32_t* tk,
                                                 uint8_t* o20) {
   uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
   uint32_t crc = 0xFFFFFFFFu;
-  hash_full_blocks<kMd5, kCrc>(row, 0, len / 64, st, crc, tk);
-  hash_finish<kMd5, kCrc>(row, len, L, len / 64, st, crc, tk, o20);
+  uint32_t m[16];
+
+  // blocks wholly inside the data: 16-byte loads, one block prefetched
+  const uint64_t nfull = len / 64;
+  uint4 nx[4];
+  if (nfull) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) nx[q] = __ldg(reinterpret_cast<const uint4*>(row) + q);
+  }
+  for (uint64_t b = 0; b < nfull; b++) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      m[4 * q] = nx[q].x;
+      m[4 * q + 1] = nx[q].y;
+      m[4 * q + 2] = nx[q].z;
+      m[4 * q + 3] = nx[q].w;
+    }
+    if (b + 1 < nfull) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) nx[q] = __ldg(reinterpret_cast<const uint4*>(row + 64 * (b + 1)) + q);
+    }
+    if constexpr (kCrc) {
+#pragma unroll
+      for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
+    }
+    if constexpr (kMd5) md5_block(st, m);
+  }
+  // the rest of the L / 64 whole message blocks: data tail, then zero padding
+  const uint64_t nblk = L / 64;
+  for (uint64_t b = nfull; b < nblk; b++) {
+#pragma unroll
+    for (int w = 0; w < 16; w++) m[w] = masked_word(row, 64 * b + 4 * w, len);
+    if constexpr (kCrc) {
+#pragma unroll
+      for (int w = 0; w < 16; w++) crc = crc_word(crc, m[w], tk);
+    }
+    if constexpr (kMd5) md5_block(st, m);
+  }
+  // final partial block (L % 64 bytes) with the MD5 padding
+  const uint32_t tail = (uint32_t)(L % 64);
+  const uint64_t t0 = 64 * nblk;
+#pragma unroll
+  for (int w = 0; w < 16; w++) m[w] = (4u * w < tail) ? masked_word(row, t0 + 4 * w, len) : 0u;
+  if constexpr (kCrc) {
+#pragma unroll
+    for (uint32_t w = 0; w < 16; w++) {
+      if (4 * w + 4 <= tail) {
+        crc = crc_word(crc, m[w], tk);
+      } else if (4 * w < tail) {
+#pragma unroll
+        for (uint32_t j = 0; j < 3; j++)
+          if (4 * w + j < tail) crc = crc_byte(crc, (m[w] >> (8 * j)) & 255u, tk);
+      }
+    }
+    reinterpret_cast<uint32_t*>(o20)[4] = crc ^ 0xFFFFFFFFu;
+  }
+  if constexpr (kMd5) {
+    // clear the bytes at and past `tail` in the last partial word, then 0x80
+#pragma unroll
+    for (int w = 0; w < 16; w++) {
+      const uint32_t lo = 4u * w;
+      if (lo < tail && tail < lo + 4) m[w] &= (1u << (8 * (tail - lo))) - 1u;
+      if (lo <= tail && tail < lo + 4) m[w] |= 0x80u << (8 * (tail - lo));
+    }
+    if (tail >= 56) {
+      md5_block(st, m);
+#pragma unroll
+      for (int w = 0; w < 16; w++) m[w] = 0;
+    }
+    m[14] = (uint32_t)(L << 3);
+    m[15] = (uint32_t)(L >> 29);
+    md5_block(st, m);
+    uint32_t* o = reinterpret_cast<uint32_t*>(o20);
+    o[0] = st[0];
+    o[1] = st[1];
+    o[2] = st[2];
+    o[3] = st[3];
+  }
 }
 
-// idx (optional): row i's entry goes to out + 20 * idx[i]; 0xFFFF: not hashed
+// kIdx: row i's entry goes to out + 20 * idx[i] (0xFFFF: not hashed); the
+// variant without it is the plain whole-slice kernel
+template <bool kIdx>
 __global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restrict__ data, size_t stride,
                                                          size_t n, uint64_t L,
                                                          const uint64_t* __restrict__ lengths,
@@ -243,8 +323,11 @@ __global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restri
   __syncthreads();
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const size_t o = idx ? idx[i] : i;
-  if (idx && o == 0xFFFF) return;
+  size_t o = i;
+  if constexpr (kIdx) {
+    o = idx[i];
+    if (o == 0xFFFF) return;
+  }
   const uint64_t len = lengths ? (lengths[i] < L ? lengths[i] : L) : L;
   par2_slice_hash<true, true>(data + i * stride, len, L, crc_tab + (threadIdx.x % kCrcCopies), out + 20 * o);
 }
@@ -255,6 +338,7 @@ __global__ void __launch_bounds__(128) k_par2_block_hash(const uint8_t* __restri
 // (about 2,000 cycles per 64-byte block) then sets the time.  Threads 0-63 of a CTA
 // hash slices 64b .. 64b+63 with MD5, threads 64-127 the same slices with
 // CRC32 (they read the same bytes at about the same time, served by L1/L2).
+template <bool kIdx>
 __global__ void __launch_bounds__(128) k_par2_block_hash_split(const uint8_t* __restrict__ data, size_t stride,
                                                                size_t n, uint64_t L,
                                                                const uint64_t* __restrict__ lengths,
@@ -265,8 +349,11 @@ __global__ void __launch_bounds__(128) k_par2_block_hash_split(const uint8_t* __
   __syncthreads();
   const size_t i = (size_t)blockIdx.x * 64 + (threadIdx.x & 63);
   if (i >= n) return;
-  const size_t o = idx ? idx[i] : i;
-  if (idx && o == 0xFFFF) return;
+  size_t o = i;
+  if constexpr (kIdx) {
+    o = idx[i];
+    if (o == 0xFFFF) return;
+  }
   const uint64_t len = lengths ? (lengths[i] < L ? lengths[i] : L) : L;
   if (threadIdx.x < 64)
     par2_slice_hash<true, false>(data + i * stride, len, L, nullptr, out + 20 * o);
@@ -727,20 +814,24 @@ cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t 
                                    const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s, const uint16_t* d_idx) {
   if (n == 0) return cudaSuccess;
   const int smem = kCrcWords * 4;
-  cudaError_t e = cudaFuncSetAttribute(k_par2_block_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_par2_block_hash_split, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaSuccess;
+  for (auto f : {k_par2_block_hash<false>, k_par2_block_hash<true>, k_par2_block_hash_split<false>,
+                 k_par2_block_hash_split<true>})
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   // split MD5 / CRC32 threads for up to 8,192 slices (1 GiB of device data:
   // 1,024 x 1 MiB 17.40 -> 17.17 ms, 4,096 x 256 KiB 4.36 -> 4.17 ms, 8,192 x
   // 128 KiB 2.18 -> 1.96 ms; at 32,768 x 32 KiB the one-thread form is
   // faster, 0.68 vs 1.22 ms, as the ALU pipe is then the limit)
-  if (n <= 8192)
-    k_par2_block_hash_split<<<(unsigned)((n + 63) / 64), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out,
-                                                                         d_idx);
+  const unsigned gs = (unsigned)((n + 63) / 64), g1 = (unsigned)((n + 127) / 128);
+  if (n <= 8192 && d_idx)
+    k_par2_block_hash_split<true><<<gs, 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out, d_idx);
+  else if (n <= 8192)
+    k_par2_block_hash_split<false><<<gs, 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out, nullptr);
+  else if (d_idx)
+    k_par2_block_hash<true><<<g1, 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out, d_idx);
   else
-    k_par2_block_hash<<<(unsigned)((n + 127) / 128), 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out,
-                                                                     d_idx);
+    k_par2_block_hash<false><<<g1, 128, smem, s>>>(d_data, stride, n, slice, d_lengths, d_out, nullptr);
   note_launch();
   return cudaGetLastError();
 }
