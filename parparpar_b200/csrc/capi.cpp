@@ -1291,6 +1291,10 @@ PP_API int pp_par2_proc_set_input_hashes(pp_par2_proc* p, unsigned max_inputs) {
   }
   CUDA_TRY(p->ctx, cudaMemset(p->d_hash, 0, (size_t)20 * max_inputs));
   p->hash_cap = max_inputs;
+  // rows already staged in the open batch were added without an entry
+  auto& a = p->areas[p->cur];
+  if (a.h_idx.size() < p->batch_alloc) a.h_idx.resize(p->batch_alloc);
+  for (unsigned i = 0; i < a.count; i++) a.h_idx[i] = 0xFFFF;
   return PP_OK;
 }
 

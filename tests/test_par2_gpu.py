@@ -209,6 +209,20 @@ def test_proc_input_hashes_in_its_own_pass(kctx, oracle):
         proc.addInput(data[i], S, co[i])
     proc.endInput()
     assert not proc.getInputHashes(4).any()
+    # hashing switched on with a batch half staged: only the later inputs get entries
+    proc.discardOutput()
+    proc.setInputHashes(0)
+    for i in range(2):
+        proc.waitForAdd()
+        proc.addInput(data[i], S, i)
+    proc.setInputHashes(10)
+    for i in range(2, 4):
+        proc.waitForAdd()
+        proc.addInput(data[i], S, i)
+    proc.endInput()
+    got = proc.getInputHashes(10)
+    assert not got[:2].any() and not got[4:].any()
+    assert np.array_equal(got[2:4], par2_block_hashes(data[2:4], S))
     proc.deinit()
 
 
