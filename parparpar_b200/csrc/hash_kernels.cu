@@ -814,11 +814,15 @@ cudaError_t launch_par2_block_hash(const uint8_t* d_data, size_t stride, size_t 
                                    const uint64_t* d_lengths, uint8_t* d_out, cudaStream_t s, const uint16_t* d_idx) {
   if (n == 0) return cudaSuccess;
   const int smem = kCrcWords * 4;
-  cudaError_t e = cudaSuccess;
-  for (auto f : {k_par2_block_hash<false>, k_par2_block_hash<true>, k_par2_block_hash_split<false>,
-                 k_par2_block_hash_split<true>})
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return e;
+  static std::atomic<uint64_t> attr{0};
+  if (!device_done(attr)) {
+    cudaError_t e = cudaSuccess;
+    for (auto f : {k_par2_block_hash<false>, k_par2_block_hash<true>, k_par2_block_hash_split<false>,
+                   k_par2_block_hash_split<true>})
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    device_mark(attr);
+  }
   // split MD5 / CRC32 threads for up to 8,192 slices (1 GiB of device data:
   // 1,024 x 1 MiB 17.40 -> 17.17 ms, 4,096 x 256 KiB 4.36 -> 4.17 ms, 8,192 x
   // 128 KiB 2.18 -> 1.96 ms; at 32,768 x 32 KiB the one-thread form is
@@ -841,8 +845,12 @@ cudaError_t launch_par2_block_hash_band(const uint8_t* d_data, size_t stride, si
                                         bool last, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   const int smem = kCrcWords * 4;
-  cudaError_t e = cudaFuncSetAttribute(k_par2_block_hash_band, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return e;
+  static std::atomic<uint64_t> attr{0};
+  if (!device_done(attr)) {
+    cudaError_t e = cudaFuncSetAttribute(k_par2_block_hash_band, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    device_mark(attr);
+  }
   k_par2_block_hash_band<<<(unsigned)((n + 63) / 64), 128, smem, s>>>(d_data, stride, n, slice, k0, k1, d_state,
                                                                       d_out, first ? 1 : 0, last ? 1 : 0);
   note_launch();
