@@ -166,6 +166,16 @@ PP_API int pp_par2_proc_end_input(pp_par2_proc* proc);
 /* getOutput(index, output) -> *valid (1 = output passed the integrity check). */
 PP_API int pp_par2_proc_get_output(pp_par2_proc* proc, unsigned index, void* output, int* valid);
 PP_API int pp_par2_proc_discard_output(pp_par2_proc* proc);
+/* Device address of recovery slice `index` in the processor's output area
+ * (rows of the slice size rounded up to 16 bytes; the recovery data once
+ * end_input has returned).  No counterpart in the reference, whose output
+ * area is host memory that getOutput unpacks (gf16/controller_cpu.cpp:423-443):
+ * a caller that consumes recovery slices on the device (packet MD5, a copy to
+ * another device) reads them here in place.  Valid until the next
+ * set_recovery_slices, free_processing_mem or destroy.  Writing through it
+ * before the first get_output of a job makes get_output report the slices so
+ * changed invalid (their memory checksum no longer matches). */
+PP_API int pp_par2_proc_output_ptr(pp_par2_proc* proc, unsigned index, void** dev_ptr);
 /* Input hashing in the processor's own pass (replaces feeding the same
  * buffers to HasherInput::update / getBlock(md5crc, zeroPad),
  * hasher/hasher_input_base.h:104-117, beside the backend's addInput): with
@@ -181,6 +191,15 @@ PP_API int pp_par2_proc_get_input_hashes(pp_par2_proc* proc, uint8_t* out, unsig
 PP_API int pp_par2_proc_free_processing_mem(pp_par2_proc* proc);
 PP_API unsigned pp_par2_proc_input_batch_size(pp_par2_proc* proc);
 PP_API unsigned pp_par2_proc_batches_started(pp_par2_proc* proc);
+/* Staging areas whose device work has finished, counted in submission order
+ * (the PAR2ProcCPU counterpart is the compute thread's _queueProc notify,
+ * gf16/controller_cpu.cpp:520-530, that drives progressCb).  wait_batches
+ * blocks until at least `count` batches have finished (PP_ERR_TIMEOUT after
+ * a minute); it waits on host-side state only, so a watcher thread may call
+ * it while the owning thread keeps adding inputs -- the libuv backend shim
+ * reports finished batches to PAR2Proc::onBackendProcess this way. */
+PP_API unsigned pp_par2_proc_batches_done(pp_par2_proc* proc);
+PP_API int pp_par2_proc_wait_batches(pp_par2_proc* proc, unsigned count);
 
 /* ============================================================ PAR3 / GF64 */
 
@@ -255,13 +274,36 @@ PP_API int pp_gf64_inverse_batch(pp_ctx* ctx, uint64_t* out, const uint64_t* in,
  * The caller checks equal lengths (the reference's RangeError). */
 PP_API int pp_xor_buffers(pp_ctx* ctx, void* dst, const void* src, size_t bytes);
 
+/* ---- One job over several GPUs ------------------------------------------
+ * Each context (one per GPU) computes a contiguous byte range
+ * [range_begin[i], range_end[i]) of every slice / block and writes the same
+ * range of the outputs, with no data exchanged between devices: the split
+ * PAR2Proc makes over its backends (gf16/controller.cpp:42-84, ranges checked
+ * by the rule of checkBackendAllocation: no gaps or overlaps, starts on 16-bit
+ * words, an odd size only for the range that ends the slice) and the Fenger
+ * path's word ranges (src/par3_engine_fenger.cc:266-290; PAR3 ranges on 8-byte
+ * words, 16 bytes keeps the tensor-core path's aligned rows).  Buffers are
+ * host memory or device memory of every context's own GPU (a device buffer of
+ * another GPU -> PP_ERR_INVALID_ARG).  Each range runs on its own host
+ * thread; the call returns when every range is done.  Arguments otherwise as
+ * pp_par2_create / pp_gf64_compute_recovery (create: fI, fR; no accumulate). */
+PP_API int pp_par2_create_split(pp_ctx* const* ctxs, const size_t* range_begin, const size_t* range_end,
+                                unsigned n_ranges, const void* inputs, size_t input_stride, unsigned num_inputs,
+                                size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps,
+                                unsigned num_outputs, void* outputs, size_t output_stride);
+PP_API int pp_gf64_compute_recovery_split(pp_ctx* const* ctxs, const size_t* range_begin, const size_t* range_end,
+                                          unsigned n_ranges, const uint64_t* inputs, size_t num_inputs,
+                                          uint64_t* recovery, size_t num_recovery, size_t block_size64,
+                                          uint64_t first_input, uint64_t first_recovery);
+
 /* Allocation-free solve.  No counterpart in the reference: an addition for
  * callers that cannot allocate device memory where they need the repair solve
  * (a device pool owned by another allocator with no headroom, latency-bound
  * loops that cannot take cudaMalloc's device-wide synchronisation, services
  * that must not fail for lack of memory after start-up).
  * Same result and return codes as pp_gf64_solve_and_reconstruct, but: A and
- * rhs must be device memory; work is enqueued on `cuda_stream` (NULL = the
+ * rhs must be device memory of the current device (or managed memory; other
+ * pointers -> PP_ERR_INVALID_ARG before any work is enqueued); work is enqueued on `cuda_stream` (NULL = the
  * legacy default stream) and the call waits for it; nothing is allocated.
  * Working storage is a fixed array inside the library (about 32 KiB, held on
  * every GPU that loads the library until exit), so n is limited to

@@ -3,6 +3,9 @@
 ``Oracle`` wraps ``oracle/liboracle.so`` (the C restatement, gf_oracle.c).
 ``Reference`` wraps ``oracle/_ref/libppref.so`` (the reference's own sources
 compiled by oracle/Makefile; present only where it was built).
+``Shim`` wraps ``oracle/_ref/libppshim.so``: the reference's PAR2Proc front
+controller driving the CUDA backend shim (parparpar_b200/shim), alone or
+beside the reference's PAR2ProcCPU.
 
 Only the tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 leg import this module, and only as the checker / the timed CPU baseline.
@@ -18,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libppref.so")
+SHIM_SO = os.path.join(HERE, "_ref", "libppshim.so")
 
 _P = ctypes.c_void_p
 _SZ = ctypes.c_size_t
@@ -29,11 +33,20 @@ def _ptr(a: np.ndarray):
     return _P(a.ctypes.data)
 
 
+def reference_dir():
+    """The reference source tree: $PP_REFERENCE_DIR, else a checkout named
+    `reference` beside this repository; None when neither exists."""
+    ref = os.environ.get("PP_REFERENCE_DIR") or os.path.join(os.path.dirname(HERE), "..", "reference")
+    ref = os.path.abspath(ref)
+    return ref if os.path.isdir(ref) else None
+
+
 def build(ref: bool = False) -> None:
     """Compile the oracle (and, when asked and the sources exist, oracle/_ref)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir(os.environ.get("PP_REFERENCE_DIR", "/root/reference")):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+    src = reference_dir() if ref else None
+    if src:
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={src}"], check=True)
 
 
 class Oracle:
@@ -369,3 +382,58 @@ class Reference:
         self.L.ref_par3_assemble_recovery_packets(_ptr(recovery), _SZ(n), _SZ(bs), _ptr(sid), _U64(first_index),
                                                   _ptr(out))
         return out
+
+
+class Shim:
+    """PAR2Proc (the reference's controller) over PAR2ProcCUDA: byte range
+    [0, split) of every slice on the reference's PAR2ProcCPU, [split, slice)
+    on the GPU (split 0: the GPU alone; split = slice: the CPU alone)."""
+
+    def __init__(self, path: str = SHIM_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.L = ctypes.CDLL(path)
+
+    @staticmethod
+    def available(path: str = SHIM_SO) -> bool:
+        return os.path.exists(path)
+
+    def par2_create(self, inputs: np.ndarray, slice_size: int, input_idx, exps, split: int, last_size=None,
+                    device: int = 0, threads: int = 0) -> tuple[np.ndarray, int]:
+        """Returns (outputs, status): status 1 = every output valid, 0 = an
+        output failed its memory checksum, < 0 = a set-up error."""
+        inputs = np.ascontiguousarray(inputs, dtype=np.uint8)
+        n = inputs.shape[0]
+        idx = np.ascontiguousarray(np.asarray(input_idx, dtype=np.uint16))
+        ex = np.ascontiguousarray(np.asarray(exps, dtype=np.uint16))
+        out = np.zeros((ex.size, slice_size), dtype=np.uint8)
+        st = self.L.shim_par2_create(_ptr(inputs), ctypes.c_uint(n), _SZ(slice_size),
+                                     _SZ(slice_size if last_size is None else last_size), _ptr(idx), _ptr(ex),
+                                     ctypes.c_uint(ex.size), _ptr(out), _SZ(split), ctypes.c_int(device),
+                                     ctypes.c_int(threads))
+        return out, st
+
+    def par2_create_coeffs(self, inputs: np.ndarray, slice_size: int, coeffs: np.ndarray, split: int,
+                           device: int = 0, threads: int = 0) -> tuple[np.ndarray, int]:
+        """coeffs: (R, N) as the region product takes them."""
+        inputs = np.ascontiguousarray(inputs, dtype=np.uint8)
+        n = inputs.shape[0]
+        r = coeffs.shape[0]
+        col = np.ascontiguousarray(coeffs.T.astype(np.uint16))
+        out = np.zeros((r, slice_size), dtype=np.uint8)
+        st = self.L.shim_par2_create_coeffs(_ptr(inputs), ctypes.c_uint(n), _SZ(slice_size), _ptr(col),
+                                            ctypes.c_uint(r), _ptr(out), _SZ(split), ctypes.c_int(device),
+                                            ctypes.c_int(threads))
+        return out, st
+
+    def par2_resize_then_create(self, inputs: np.ndarray, first_size: int, slice_size: int, input_idx, exps,
+                                device: int = 0) -> tuple[np.ndarray, int]:
+        inputs = np.ascontiguousarray(inputs, dtype=np.uint8)
+        n = inputs.shape[0]
+        idx = np.ascontiguousarray(np.asarray(input_idx, dtype=np.uint16))
+        ex = np.ascontiguousarray(np.asarray(exps, dtype=np.uint16))
+        out = np.zeros((ex.size, slice_size), dtype=np.uint8)
+        st = self.L.shim_par2_resize_then_create(_ptr(inputs), ctypes.c_uint(n), _SZ(first_size), _SZ(slice_size),
+                                                 _ptr(idx), _ptr(ex), ctypes.c_uint(ex.size), _ptr(out),
+                                                 ctypes.c_int(device))
+        return out, st

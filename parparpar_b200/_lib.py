@@ -50,9 +50,11 @@ EXPORTS = [
     "pp_par2_invert", "pp_par2_proc_create", "pp_par2_proc_destroy", "pp_par2_proc_set_current_slice_size",
     "pp_par2_proc_set_recovery_slices", "pp_par2_proc_can_add", "pp_par2_proc_wait_for_add",
     "pp_par2_proc_add_input", "pp_par2_proc_add_input_coeffs", "pp_par2_proc_flush", "pp_par2_proc_end_input",
-    "pp_par2_proc_get_output", "pp_par2_proc_discard_output", "pp_par2_proc_free_processing_mem",
+    "pp_par2_proc_get_output", "pp_par2_proc_discard_output", "pp_par2_proc_output_ptr",
+    "pp_par2_proc_free_processing_mem",
     "pp_par2_proc_set_input_hashes", "pp_par2_proc_get_input_hashes",
-    "pp_par2_proc_input_batch_size", "pp_par2_proc_batches_started", "pp_gf64_build_cauchy",
+    "pp_par2_proc_input_batch_size", "pp_par2_proc_batches_started", "pp_par2_proc_batches_done",
+    "pp_par2_proc_wait_batches", "pp_gf64_build_cauchy",
     "pp_gf64_compute_recovery", "pp_gf64_compute_recovery_with_coeff", "pp_gf64_solve_and_reconstruct",
     "pp_gf64_region_mul", "pp_gf64_region_mul_arr", "pp_gf64_region_muladd_arr",
     "pp_gf64_region_coupled_muladd_arr", "pp_gf64_region_fused_output_muladd_arr",
@@ -63,7 +65,7 @@ EXPORTS = [
     "pp_server_last_error", "pp_server_destroy",
     "pp_par2_block_hashes", "pp_par3_block_hashes", "pp_par3_assemble_recovery_packets",
     "pp_par2_create_hashed", "pp_par3_create_packets", "pp_par2_memory_checksums", "pp_par3_create_streaming",
-    "pp_par2_recovery_packet_headers", "pp_xor_buffers",
+    "pp_par2_recovery_packet_headers", "pp_xor_buffers", "pp_par2_create_split", "pp_gf64_compute_recovery_split",
 ]
 
 
@@ -127,13 +129,18 @@ _sig("pp_par2_proc_flush", _I, _P)
 _sig("pp_par2_proc_end_input", _I, _P)
 _sig("pp_par2_proc_get_output", _I, _P, _U, _P, ctypes.POINTER(_I))
 _sig("pp_par2_proc_discard_output", _I, _P)
+_sig("pp_par2_proc_output_ptr", _I, _P, _U, ctypes.POINTER(_P))
 _sig("pp_par2_proc_set_input_hashes", _I, _P, _U)
 _sig("pp_par2_proc_get_input_hashes", _I, _P, _P, _U)
 _sig("pp_par2_proc_free_processing_mem", _I, _P)
 _sig("pp_par2_proc_input_batch_size", _U, _P)
 _sig("pp_par2_proc_batches_started", _U, _P)
+_sig("pp_par2_proc_batches_done", _U, _P)
+_sig("pp_par2_proc_wait_batches", _I, _P, _U)
 _sig("pp_gf64_build_cauchy", _I, _P, _P, _SZ, _SZ, _U64, _U64)
 _sig("pp_gf64_compute_recovery", _I, _P, _P, _SZ, _P, _SZ, _SZ, _U64, _U64, _I, _I)
+_sig("pp_par2_create_split", _I, _P, _P, _P, _U, _P, _SZ, _U, _SZ, _P, _P, _U, _P, _SZ)
+_sig("pp_gf64_compute_recovery_split", _I, _P, _P, _P, _U, _P, _SZ, _P, _SZ, _SZ, _U64, _U64)
 _sig("pp_gf64_compute_recovery_with_coeff", _I, _P, _P, _SZ, _P, _SZ, _SZ, _P, _I)
 _sig("pp_gf64_solve_and_reconstruct", _I, _P, _P, _P, _SZ, _SZ)
 _sig("pp_gf64_region_mul", _I, _P, _P, _P, _SZ, _U64)

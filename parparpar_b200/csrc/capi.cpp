@@ -15,6 +15,7 @@
 #include <atomic>
 #include <cerrno>
 #include <chrono>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -915,7 +916,22 @@ struct pp_par2_proc {
   cudaEvent_t copied = nullptr;
   uint8_t* d_hash = nullptr;  // IFSC entries of the staged inputs, by input number
   unsigned hash_cap = 0;
+  // batches whose device work has finished: counted by a host function queued
+  // behind each batch's kernels, waited for without touching CUDA
+  std::mutex done_mu;
+  std::condition_variable done_cv;
+  unsigned batches_done = 0;
 };
+
+// host function queued on the compute stream after each batch (no CUDA calls)
+static void CUDART_CB proc_batch_finished(void* arg) {
+  auto* p = static_cast<pp_par2_proc*>(arg);
+  {
+    std::lock_guard<std::mutex> g(p->done_mu);
+    p->batches_done++;
+  }
+  p->done_cv.notify_all();
+}
 
 // host slices of at least this many bytes are copied straight from the
 // caller's buffer (one DMA beats a host memcpy into the pinned rows)
@@ -1173,6 +1189,7 @@ static int proc_submit(pp_par2_proc* p) {
                                true));
   p->checked = false;
   CUDA_TRY(p->ctx, cudaEventRecord(a.done, p->s_comp));
+  CUDA_TRY(p->ctx, cudaLaunchHostFunc(p->s_comp, proc_batch_finished, p));
   a.active = true;
   a.count = 0;
   p->has_output = true;
@@ -1273,6 +1290,30 @@ PP_API int pp_par2_proc_get_output(pp_par2_proc* p, unsigned index, void* output
                                    p->s_copy));
   CUDA_TRY(p->ctx, cudaStreamSynchronize(p->s_copy));
   if (valid) *valid = p->has_output ? p->valid[index] : 1;
+  return PP_OK;
+}
+
+PP_API unsigned pp_par2_proc_batches_done(pp_par2_proc* p) {
+  if (!p) return 0;
+  std::lock_guard<std::mutex> g(p->done_mu);
+  return p->batches_done;
+}
+
+PP_API int pp_par2_proc_wait_batches(pp_par2_proc* p, unsigned count) {
+  if (!p) return PP_ERR_INVALID_ARG;
+  std::unique_lock<std::mutex> g(p->done_mu);
+  // bounded: a batch that has not finished within a minute is reported, not waited for
+  if (!p->done_cv.wait_for(g, std::chrono::seconds(60), [&] { return p->batches_done >= count; }))
+    return PP_ERR_TIMEOUT;
+  return PP_OK;
+}
+
+PP_API int pp_par2_proc_output_ptr(pp_par2_proc* p, unsigned index, void** dev_ptr) {
+  if (!p || !dev_ptr) return PP_ERR_INVALID_ARG;
+  *dev_ptr = nullptr;
+  if (index >= p->exps.size()) return set_err(p->ctx, PP_ERR_INVALID_ARG, "output index out of range");
+  if (!p->d_out) return set_err(p->ctx, PP_ERR_INVALID_ARG, "no output area");
+  *dev_ptr = p->d_out + (size_t)index * p->row;
   return PP_OK;
 }
 
@@ -1414,12 +1455,27 @@ static cudaError_t gf64_region(pp_ctx* ctx, const uint64_t* din, const uint64_t*
 // chunk), run on the hash stream beside the products; hcv = its chaining-value
 // scratch, sized for the whole input.  The hash work is joined into the
 // context's stream before return.
+// in_ld / out_ld: row strides of the caller's blocks in words (0 = B, the
+// reference's contiguous layout); a word range of every block is a view with
+// the full block length as its stride.
 static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, uint64_t* recovery, size_t n_rec,
                             size_t B, const uint64_t* d_coeff, bool accumulate, const B3Job* hj = nullptr,
-                            uint32_t* hcv = nullptr) {
+                            uint32_t* hcv = nullptr, size_t in_ld = 0, size_t out_ld = 0) {
+  if (!in_ld) in_ld = B;
+  if (!out_ld) out_ld = B;
+  if (hj && in_ld != B) return set_err(ctx, PP_ERR_INVALID_ARG, "block hashes need whole blocks");
   const bool in_dev = is_device_ptr(inputs);
   const bool out_dev = is_device_ptr(recovery);
   const uint64_t* din = inputs;
+  // host <-> staging copies of [rows, B words] views with the caller's strides
+  auto h2d_rows = [&](uint64_t* dst, const uint64_t* src, size_t ld, size_t rows, cudaStream_t st) {
+    return ld == B ? cudaMemcpyAsync(dst, src, rows * B * 8, cudaMemcpyHostToDevice, st)
+                   : cudaMemcpy2DAsync(dst, B * 8, src, ld * 8, B * 8, rows, cudaMemcpyHostToDevice, st);
+  };
+  auto d2h_rows = [&](uint64_t* dst, size_t ld, const uint64_t* src, size_t rows, cudaStream_t st) {
+    return ld == B ? cudaMemcpyAsync(dst, src, rows * B * 8, cudaMemcpyDeviceToHost, st)
+                   : cudaMemcpy2DAsync(dst, ld * 8, src, B * 8, B * 8, rows, cudaMemcpyDeviceToHost, st);
+  };
   if (hj)
     if (int r = ensure_hash_stream(ctx)) return r;
   auto hash_rows = [&](const uint64_t* rows, size_t first, size_t count) -> cudaError_t {
@@ -1446,11 +1502,12 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
     uint64_t* s = (uint64_t*)scratch(ctx, S_IN, n_in * B * 8);
     if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", n_in * B * 8);
     uint64_t* dout = recovery;
+    size_t dout_ld = out_ld;
     if (!out_dev) {
       dout = (uint64_t*)scratch(ctx, S_OUT, n_rec * B * 8);
       if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "output staging");
-      if (accumulate)
-        CUDA_TRY(ctx, cudaMemcpyAsync(dout, recovery, n_rec * B * 8, cudaMemcpyHostToDevice, ctx->stream));
+      dout_ld = B;
+      if (accumulate) CUDA_TRY(ctx, h2d_rows(dout, recovery, out_ld, n_rec, ctx->stream));
     }
     CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
     CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
@@ -1460,26 +1517,28 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
       // little product work is left once the final copy has landed
       const size_t rest = n_in - c0;
       nc = rest > chunk ? chunk : rest > tail ? std::max(tail, (rest / 2 + 1) & ~(size_t)1) : rest;
-      CUDA_TRY(ctx, cudaMemcpyAsync(s + c0 * B, inputs + c0 * B, nc * B * 8, cudaMemcpyHostToDevice, ctx->copy));
+      CUDA_TRY(ctx, h2d_rows(s + c0 * B, inputs + c0 * in_ld, in_ld, nc, ctx->copy));
       CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
       CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_ev, 0));
       if (hj) {
         CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->hash, ctx->copy_ev, 0));
         CUDA_TRY(ctx, hash_rows(s + c0 * B, c0, nc));
       }
-      CUDA_TRY(ctx, gf64_region(ctx, s + c0 * B, nullptr, B, nc, B, d_coeff + c0, n_in, n_rec, dout, nullptr, B,
-                                accumulate || c0 > 0, aligned_rows64(s, B) && aligned_rows64(dout, B)));
+      CUDA_TRY(ctx, gf64_region(ctx, s + c0 * B, nullptr, B, nc, B, d_coeff + c0, n_in, n_rec, dout, nullptr, dout_ld,
+                                accumulate || c0 > 0, aligned_rows64(s, B) && aligned_rows64(dout, dout_ld)));
     }
-    if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(recovery, dout, n_rec * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (!out_dev) CUDA_TRY(ctx, d2h_rows(recovery, out_ld, dout, n_rec, ctx->stream));
     if (int r = join_hash()) return r;
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return device_status(ctx);
   }
+  size_t din_ld = in_ld;
   if (!in_dev) {
     uint64_t* s = (uint64_t*)scratch(ctx, S_IN, n_in * B * 8);
     if (!s) return set_err(ctx, PP_ERR_NO_MEMORY, "input staging (%zu bytes)", n_in * B * 8);
-    CUDA_TRY(ctx, cudaMemcpyAsync(s, inputs, n_in * B * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, h2d_rows(s, inputs, in_ld, n_in, ctx->stream));
     din = s;
+    din_ld = B;
   }
   if (hj) {  // hash the device rows beside the product
     CUDA_TRY(ctx, cudaEventRecord(ctx->staged_ev, ctx->stream));
@@ -1487,15 +1546,16 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
     CUDA_TRY(ctx, hash_rows(din, 0, n_in));
   }
   uint64_t* dout = recovery;
+  size_t dout_ld = out_ld;
   if (!out_dev) {
     dout = (uint64_t*)scratch(ctx, S_OUT, n_rec * B * 8);
     if (!dout) return set_err(ctx, PP_ERR_NO_MEMORY, "output staging");
-    if (accumulate)
-      CUDA_TRY(ctx, cudaMemcpyAsync(dout, recovery, n_rec * B * 8, cudaMemcpyHostToDevice, ctx->stream));
+    dout_ld = B;
+    if (accumulate) CUDA_TRY(ctx, h2d_rows(dout, recovery, out_ld, n_rec, ctx->stream));
   }
-  CUDA_TRY(ctx, gf64_region(ctx, din, nullptr, B, n_in, B, d_coeff, n_in, n_rec, dout, nullptr, B, accumulate,
-                            aligned_rows64(din, B) && aligned_rows64(dout, B)));
-  if (!out_dev) CUDA_TRY(ctx, cudaMemcpyAsync(recovery, dout, n_rec * B * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, gf64_region(ctx, din, nullptr, din_ld, n_in, B, d_coeff, n_in, n_rec, dout, nullptr, dout_ld,
+                            accumulate, aligned_rows64(din, din_ld) && aligned_rows64(dout, dout_ld)));
+  if (!out_dev) CUDA_TRY(ctx, d2h_rows(recovery, out_ld, dout, n_rec, ctx->stream));
   if (int r = join_hash()) return r;
   if (!in_dev || !out_dev) {
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -2365,3 +2425,105 @@ PP_API int pp_xor_buffers(pp_ctx* ctx, void* dst, const void* src, size_t bytes)
 }
 
 }  // extern "C"
+
+// ====================================================== one job, many GPUs
+// A job's slices split by byte range over several contexts (one per GPU),
+// each range computed by its own host thread on its own device: what
+// PAR2Proc does with its backends (gf16/controller.cpp:42-84: every backend
+// takes [offset, offset + size) of every slice) and what the Fenger path does
+// with word ranges (src/par3_engine_fenger.cc:266-290).  No data crosses
+// between devices: each context reads its range of the caller's buffers
+// (host memory, or device memory of that context's own GPU) and writes the
+// same range of the outputs.
+
+// The reference's acceptance rule for a split (PAR2Proc::checkBackendAllocation):
+// the non-empty ranges cover [0, slice) without gaps or overlaps, start on
+// multiples of `unit`, and only the range that ends the slice may have a
+// size that is not a multiple of `unit`.
+static bool split_cover_ok(const size_t* b, const size_t* e, unsigned n, size_t slice, size_t unit) {
+  std::vector<std::pair<size_t, size_t>> r;
+  for (unsigned i = 0; i < n; i++) {
+    if (e[i] < b[i] || e[i] > slice) return false;
+    if (e[i] > b[i]) r.push_back({b[i], e[i]});
+  }
+  std::sort(r.begin(), r.end());
+  size_t pos = 0;
+  for (auto& x : r) {
+    if (x.first != pos || x.first % unit) return false;
+    if ((x.second - x.first) % unit && x.second != slice) return false;
+    pos = x.second;
+  }
+  return pos == slice;
+}
+
+// a context may dereference `p` only if it is host memory or its own device's
+static bool readable_by(const pp_ctx* ctx, const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;  // pageable host memory
+  }
+  if (a.type == cudaMemoryTypeDevice) return a.device == ctx->device;
+  return true;
+}
+
+template <class Fn>
+static int run_split(pp_ctx* const* ctxs, const size_t* b, const size_t* e, unsigned n, Fn fn) {
+  std::vector<int> st(n, PP_OK);
+  std::vector<std::thread> th;
+  for (unsigned i = 0; i < n; i++) {
+    if (e[i] == b[i]) continue;
+    th.emplace_back([&, i] {
+      st[i] = fn(ctxs[i], b[i], e[i]);
+      if (st[i] == PP_OK) st[i] = pp_ctx_synchronize(ctxs[i]);  // device buffers: wait for the range
+    });
+  }
+  for (auto& t : th) t.join();
+  for (unsigned i = 0; i < n; i++)
+    if (st[i] != PP_OK) return st[i];
+  return PP_OK;
+}
+
+PP_API int pp_par2_create_split(pp_ctx* const* ctxs, const size_t* range_begin, const size_t* range_end,
+                                unsigned n_ranges, const void* inputs, size_t input_stride, unsigned num_inputs,
+                                size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps,
+                                unsigned num_outputs, void* outputs, size_t output_stride) {
+  if (!ctxs || !range_begin || !range_end || !n_ranges) return PP_ERR_INVALID_ARG;
+  for (unsigned i = 0; i < n_ranges; i++)
+    if (!ctxs[i]) return PP_ERR_INVALID_ARG;
+  if (!split_cover_ok(range_begin, range_end, n_ranges, slice_bytes, 2))
+    return set_err(ctxs[0], PP_ERR_INVALID_ARG, "ranges do not split the slice on 16-bit words");
+  for (unsigned i = 0; i < n_ranges; i++)
+    if ((num_inputs && !readable_by(ctxs[i], inputs)) || !readable_by(ctxs[i], outputs))
+      return set_err(ctxs[i], PP_ERR_INVALID_ARG, "a device buffer of another GPU");
+  return run_split(ctxs, range_begin, range_end, n_ranges, [&](pp_ctx* c, size_t b, size_t e) {
+    return pp_par2_create(c, (const uint8_t*)inputs + b, input_stride, num_inputs, e - b, input_idx, exps,
+                          num_outputs, (uint8_t*)outputs + b, output_stride);
+  });
+}
+
+PP_API int pp_gf64_compute_recovery_split(pp_ctx* const* ctxs, const size_t* range_begin, const size_t* range_end,
+                                          unsigned n_ranges, const uint64_t* inputs, size_t num_inputs,
+                                          uint64_t* recovery, size_t num_recovery, size_t block_size64,
+                                          uint64_t first_input, uint64_t first_recovery) {
+  if (!ctxs || !range_begin || !range_end || !n_ranges) return PP_ERR_INVALID_ARG;
+  for (unsigned i = 0; i < n_ranges; i++)
+    if (!ctxs[i]) return PP_ERR_INVALID_ARG;
+  if (num_inputs == 0 || num_recovery == 0 || block_size64 == 0) return PP_OK;
+  if (!inputs || !recovery) return set_err(ctxs[0], PP_ERR_INVALID_ARG, "null buffer");
+  // ranges in bytes of a block, on whole words
+  if (!split_cover_ok(range_begin, range_end, n_ranges, block_size64 * 8, 8))
+    return set_err(ctxs[0], PP_ERR_INVALID_ARG, "ranges do not split the block on 8-byte words");
+  for (unsigned i = 0; i < n_ranges; i++)
+    if (!readable_by(ctxs[i], inputs) || !readable_by(ctxs[i], recovery))
+      return set_err(ctxs[i], PP_ERR_INVALID_ARG, "a device buffer of another GPU");
+  return run_split(ctxs, range_begin, range_end, n_ranges, [&](pp_ctx* c, size_t b, size_t e) {
+    std::lock_guard<std::mutex> g(c->mu);
+    if (int r = bind(c)) return r;
+    int st;
+    uint64_t* M = cauchy_get(c, num_inputs, num_recovery, first_input, first_recovery, &st);
+    if (!M) return st;
+    return gf64_matvec_impl(c, inputs + b / 8, num_inputs, recovery + b / 8, num_recovery, (e - b) / 8, M, false,
+                            nullptr, nullptr, block_size64, block_size64);
+  });
+}

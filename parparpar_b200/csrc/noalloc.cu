@@ -68,13 +68,18 @@ int scratch_for_current_device(uint64_t** out) {
   return PP_OK;
 }
 
-bool on_device(const void* p) {
+// True when the kernels launched on device `dev` may dereference p: device
+// memory of that very device, or managed memory.  Device memory of another GPU
+// is refused: the scratch address and every launch belong to the current
+// device, so such a buffer would be read across the link or fault.
+bool on_device(const void* p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace
@@ -84,7 +89,12 @@ extern "C" PP_API int pp_gf64_solve_and_reconstruct_noalloc(uint64_t* A, uint64_
   if (n == 0) return PP_OK;
   if (n > kMaxN) return PP_ERR_TOO_LARGE;
   if (!A || (block_size64 && !rhs)) return PP_ERR_INVALID_ARG;
-  if (!on_device(A) || (block_size64 && !on_device(rhs))) return PP_ERR_INVALID_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return PP_ERR_NO_DEVICE;
+  }
+  if (!on_device(A, dev) || (block_size64 && !on_device(rhs, dev))) return PP_ERR_INVALID_ARG;
   uint64_t* scratch = nullptr;
   if (int st = scratch_for_current_device(&scratch)) return st;
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);

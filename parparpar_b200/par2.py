@@ -212,6 +212,13 @@ class PAR2ProcCUDA:
     def discardOutput(self):
         self._chk(lib.pp_par2_proc_discard_output(self.h))
 
+    def outputDevicePtr(self, index: int) -> int:
+        """Device address of recovery slice `index` in the output area (after
+        endInput), for consumers that read recovery data on the device."""
+        p = ctypes.c_void_p()
+        self._chk(lib.pp_par2_proc_output_ptr(self.h, index, ctypes.byref(p)))
+        return int(p.value)
+
     def setInputHashes(self, maxInputs: int):
         """Hash every slice added by input number from now on (IFSC entries:
         MD5 || CRC32le of the slice zero-padded to the slice size), on the

@@ -47,3 +47,60 @@ def check_ranges(ranges, slice_bytes: int) -> bool:
             return False
         pos = e
     return pos == slice_bytes
+
+
+def _ptr_of(buf):
+    import ctypes
+    if hasattr(buf, "data_ptr"):
+        return ctypes.c_void_p(buf.data_ptr())
+    return ctypes.c_void_p(buf.ctypes.data)
+
+
+def _range_arrays(ranges, contexts):
+    import ctypes
+    n = len(ranges)
+    if len(contexts) != n:
+        raise ValueError("one context per range")
+    ctxs = (ctypes.c_void_p * n)(*[c.h.value for c in contexts])
+    b = (ctypes.c_size_t * n)(*[r[0] for r in ranges])
+    e = (ctypes.c_size_t * n)(*[r[1] for r in ranges])
+    return ctxs, b, e, n
+
+
+def par2_create_split(inputs, input_idx, exps, contexts, ranges=None, out=None):
+    """PAR2 create with byte range r of every slice computed on contexts[r]
+    (pp_par2_create_split): each GPU reads and writes only its range, as
+    PAR2Proc spreads a slice over its backends.  inputs: (N, S) uint8 host
+    array or tensor; ranges default to byte_ranges(S, len(contexts), 2)."""
+    import numpy as np
+    from ._lib import lib
+    n, s = inputs.shape
+    if ranges is None:
+        ranges = byte_ranges(s, len(contexts), 2)
+    idx = np.ascontiguousarray(np.asarray(input_idx, dtype=np.uint16))
+    ex = np.ascontiguousarray(np.asarray(exps, dtype=np.uint16))
+    if out is None:
+        out = np.zeros((ex.size, s), dtype=np.uint8)
+    ctxs, b, e, k = _range_arrays(ranges, contexts)
+    in_stride = inputs.stride(0) if hasattr(inputs, "stride") else inputs.strides[0]
+    out_stride = out.stride(0) if hasattr(out, "stride") else out.strides[0]
+    contexts[0].check(lib.pp_par2_create_split(ctxs, b, e, k, _ptr_of(inputs), in_stride, n, s, _ptr_of(idx),
+                                               _ptr_of(ex), ex.size, _ptr_of(out), out_stride))
+    return out
+
+
+def par3_create_split(inputs, num_recovery, first_input, first_recovery, contexts, ranges=None, out=None):
+    """PAR3 create (Cauchy product) with byte range r of every block on
+    contexts[r] (pp_gf64_compute_recovery_split).  inputs: (N, W) uint64 /
+    int64; ranges default to byte_ranges(8 W, len(contexts), 16)."""
+    import numpy as np
+    from ._lib import lib
+    n, w = inputs.shape
+    if ranges is None:
+        ranges = byte_ranges(8 * w, len(contexts), 16)
+    if out is None:
+        out = np.zeros((num_recovery, w), dtype=np.uint64)
+    ctxs, b, e, k = _range_arrays(ranges, contexts)
+    contexts[0].check(lib.pp_gf64_compute_recovery_split(ctxs, b, e, k, _ptr_of(inputs), n, _ptr_of(out),
+                                                         num_recovery, w, first_input, first_recovery))
+    return out

@@ -6,7 +6,7 @@ own C/C++ hot-path code compiled from its sources).  The fixtures it writes
 are small ``.npz`` files that the tests read; the tests never need the
 reference at run time.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture ...]   (default: all of them)
 
 Fixtures:
   par3_golden.npz  the reference's frozen golden case (test/par3-golden.js:27-98):
@@ -26,6 +26,9 @@ Fixtures:
                    packets laid out as src/gf64_addon.cc:2884-2934, checksummed
                    with the reference's BLAKE3.  Inputs are oracle.pattern_bytes
                    streams, regenerated by the tests from (length, seed).
+  configs.npz      SHA-256 digests of the reference's outputs at benchmark
+                   sizes: PAR2 create 256 x 64 KiB, R=8, and the factors of a
+                   32,768-input PAR2 repair with 64 seeded lost slices.
 """
 from __future__ import annotations
 
@@ -215,14 +218,44 @@ def hashes(R: Reference):
     np.savez_compressed(os.path.join(HERE, "hashes.npz"), **d)
 
 
+def configs(R: Reference):
+    """Digests of the reference's outputs at two benchmark configurations:
+    PAR2 create 256 x 64 KiB, R=8 (input numbers 0..255, exponents 0..7) on
+    pattern_bytes data, and the Galois16RecMatrix factors of a PAR2 repair of
+    32,768 inputs with 64 seeded lost slices and recovery exponents 0..63.
+    The outputs themselves (512 KiB, 4 MiB) are not stored: the tests hash
+    what the device computes and compare digests."""
+    import hashlib
+    n, s, r = 256, 65536, 8
+    data = pattern_bytes(n * s, CFG1_SEED).reshape(n, s)
+    out, ok = R.par2_create(data, s, np.arange(n, dtype=np.uint16), list(range(r)), threads=0)
+    d = {"cfg1_seed": np.int64(CFG1_SEED), "cfg1_sha256": np.frombuffer(hashlib.sha256(out.tobytes()).digest(),
+                                                                         dtype=np.uint8),
+         "cfg1_valid": np.int64(ok)}
+    N, m = 32768, 64
+    lost = np.sort(np.random.default_rng(REPAIR_SEED).choice(N, m, replace=False)).astype(np.int64)
+    valid = np.ones(N, dtype=np.uint8)
+    valid[lost] = 0
+    ok, f, used = R.par2_invert(valid, list(range(m)), threads=0)
+    assert ok
+    d.update(repair_lost=lost, repair_used=np.asarray(used, dtype=np.uint16),
+             repair_factors_sha256=np.frombuffer(hashlib.sha256(np.ascontiguousarray(f).tobytes()).digest(),
+                                                 dtype=np.uint8))
+    np.savez_compressed(os.path.join(HERE, "configs.npz"), **d)
+
+
+CFG1_SEED = 0xC0F1
+REPAIR_SEED = 0x5EED
+
+
+GENERATORS = {"hashes": hashes, "par3_golden": par3_golden, "par2_create": par2_create,
+              "par2_invert": par2_invert, "gf64_ops": gf64_ops, "gf64_fft": gf64_fft, "configs": configs}
+
+
 def main():
     R = Reference()
-    hashes(R)
-    par3_golden(R)
-    par2_create(R)
-    par2_invert(R)
-    gf64_ops(R)
-    gf64_fft(R)
+    for name in (sys.argv[1:] or GENERATORS):
+        GENERATORS[name](R)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -124,7 +124,7 @@ def test_create_streaming_argument_errors():
         par3.par3_create_streaming("x", {"recoverySlices": 1, "blockSize": 64, "firstInput": 1.5})
 
 
-def test_compute_recovery_argument_errors():
+def test_compute_recovery_native_edge_errors():
     """test/par3-native-edge.js error scenarios: numInputs 0, numRecovery 0,
     blockSize 7 and 0, a numInputs the inputs buffer cannot hold -- all raise
     before any device work."""

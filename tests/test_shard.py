@@ -2,9 +2,10 @@
 
 The split must satisfy the reference's own acceptance rule for a backend
 split (gf16/controller.cpp:42-84), and the per-rank results must concatenate
-to the single-rank result.  The multi-rank case runs as world-size-2 `gloo`
-processes; each rank computes its byte range of a PAR2 and a PAR3 create with
-the oracle (no GPU), rank 0 gathers and compares with the full oracle result.
+to the single-rank result.  Here, without a GPU, the multi-rank case runs as
+world-size-2 `gloo` processes that compute their byte ranges with the oracle:
+it checks the split arithmetic and the gather.  The same ranks running the
+CUDA library, and the split entry points, are in tests/test_shard_gpu.py.
 """
 import os
 import socket

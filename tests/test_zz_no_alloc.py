@@ -101,3 +101,18 @@ def test_noalloc_solve_rejects_sizes_above_the_limit(ctx):
     h = np.zeros(16, dtype=np.uint64)
     assert L.lib.pp_gf64_solve_and_reconstruct_noalloc(h.ctypes.data, h.ctypes.data, 2, 1, None) == \
         L.PP_ERR_INVALID_ARG
+    # so is a device matrix beside a host right-hand side
+    assert L.lib.pp_gf64_solve_and_reconstruct_noalloc(t.data_ptr(), h.ctypes.data, 2, 1, None) == \
+        L.PP_ERR_INVALID_ARG
+    # buffers on the current device are accepted (a 2 x 2 identity solves to itself)
+    eye = torch.tensor([1, 0, 0, 1], dtype=torch.int64, device="cuda")
+    r = torch.tensor([7, 9], dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    assert L.lib.pp_gf64_solve_and_reconstruct_noalloc(eye.data_ptr(), r.data_ptr(), 2, 1, None) == L.PP_OK
+    assert r.cpu().tolist() == [7, 9]
+    # buffers on another GPU are refused the same way
+    if torch.cuda.device_count() > 1:
+        other = torch.zeros(16, dtype=torch.int64, device="cuda:1")
+        torch.cuda.synchronize(1)
+        assert L.lib.pp_gf64_solve_and_reconstruct_noalloc(other.data_ptr(), other.data_ptr(), 2, 1, None) == \
+            L.PP_ERR_INVALID_ARG
