@@ -130,6 +130,8 @@ TRAFFIC = {
     "k_gf16_muladd_tc.par2_create_32768x32KiB_R64": 4 * (543139328 + 9490176),
     "k_gf16_muladd_tc.par2_create_1024x1MiB_R8": 1087907000 + 10907904,
     "k_gf64_matvec_tc.par3_create_131072x8KiB_R8": 1083011000 + 3985664,
+    # the SM-pair kernel's 32,768-block capture (270.8 + 4.3 MB) scaled to 131,072 blocks
+    "k_gf64_matvec_tc_pair.par3_create_131072x8KiB_R8": 4 * (270800000 + 4300000),
 }
 
 
@@ -361,7 +363,10 @@ def dominant_kernel(w, args):
         return "k_par2_block_hash"
     if w["field"] in ("hash3", "pkt3"):
         return "k_b3_chunks"
-    return "k_gf64_matvec_lut" if args.gf64_kernel == "lut" else "k_gf64_matvec_tc"
+    if args.gf64_kernel == "lut":
+        return "k_gf64_matvec_lut"
+    # the SM-pair kernel runs when every job of the launch has >= 4 outputs
+    return "k_gf64_matvec_tc_pair" if w["r"] >= 4 else "k_gf64_matvec_tc"
 
 
 def algo_bytes(job):
@@ -383,25 +388,69 @@ def input_bytes_of(name):
     return w["n"] * w["s"]  # create: the input slices; repair: known blocks + recovery blocks (N*S)
 
 
-def measure(job, ctx, timer, steps, warmup, peak):
+def timed_steps(ctx, timer, f, steps):
+    """Time `steps` calls of f with CUDA events on the launching stream and,
+    in the same calls, the device time of the region products the library
+    brackets with its own events (pp_ctx_set_kernel_timing).  Returns
+    (ms per step, region ms per launch or None, region launches, library
+    launches)."""
     import parparpar_b200 as pp
+    ctx.kernel_time()  # drop earlier brackets
+    ctx.set_kernel_timing(True)
+    l0 = pp.launch_count()
+    ms = timer.run(f, steps)
+    launches = pp.launch_count() - l0
+    ctx.set_kernel_timing(False)
+    kt, kn = ctx.kernel_time()
+    return ms, (kt / kn if kn else None), kn, launches
+
+
+def kernel_ms_of(job, ctx, timer, steps, kms):
+    """The dominant kernel's time per launch: the library's own brackets in
+    the timed steps when it made any, else (block hashes, FFT) the step's
+    kernel timed alone."""
+    if kms is not None:
+        return kms, "CUDA events around each region product inside the timed steps"
+    kf = kernel_fn(job, ctx)
+    kf()
+    return timer.run(kf, max(3, min(steps, 20))), "the kernel's call timed alone after the timed steps"
+
+
+def measure(job, ctx, timer, steps, warmup, peak):
     f = step_fn(job, ctx)
     for _ in range(warmup):
         f()
     ctx.synchronize()
-    l0 = pp.launch_count()
-    ms = timer.run(f, steps)
-    launches = pp.launch_count() - l0
-    kf = kernel_fn(job, ctx)
-    kf()
-    kms = timer.run(kf, max(3, min(steps, 20)))
+    ms, kms, _, launches = timed_steps(ctx, timer, f, steps)
+    kms, _ = kernel_ms_of(job, ctx, timer, steps, kms)
     achieved = algo_bytes(job) / (kms * 1e-3) / 1e9
     return dict(ms=ms, launches=launches, kernel_ms=kms, achieved=achieved, frac=achieved / peak)
 
 
-def cpu_baseline_sample(name, budget_s=12.0, threads=0):
+def host_isa():
+    """CPU model and the SIMD extensions the reference's kernels pick from."""
+    model, flags = "", set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name") and not model:
+                    model = ln.split(":", 1)[1].strip()
+                elif ln.startswith("flags") and not flags:
+                    flags = set(ln.split(":", 1)[1].split())
+    except OSError:
+        pass
+    ext = [x for x in ("avx2", "avx512f", "avx512bw", "avx512vl", "avx512vbmi", "gfni", "vpclmulqdq", "pclmulqdq")
+           if x in flags]
+    return f"{model}; {' '.join(ext)}".strip("; ")
+
+
+_SAMPLE_INPUTS = {}
+
+
+def cpu_baseline_sample(name, budget_s=12.0, threads=0, full=False):
     """Reference CPU code on a bounded sample of the workload: every slice,
-    a contiguous byte sub-range of each (cost is linear in the slice length)."""
+    a contiguous byte sub-range of each (cost is linear in the slice length),
+    or with full=True (PAR2 create) the whole job once."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     w = WORKLOADS[name]
@@ -461,10 +510,17 @@ def cpu_baseline_sample(name, budget_s=12.0, threads=0):
         R = orc.Reference()
         kind = "reference"
         if w["field"] == "gf16":
-            sub = 2048
-            inp = rng.integers(0, 256, (w["n"], sub), dtype=np.uint8)
+            sub = w["s"] if full else min(2048, w["s"])
+            key = (w["n"], sub)
+            if key not in _SAMPLE_INPUTS:  # generated once per process (1 GiB for the whole job)
+                _SAMPLE_INPUTS.clear()
+                _SAMPLE_INPUTS[key] = rng.integers(0, 256, (w["n"], sub), dtype=np.uint8)
+            inp = _SAMPLE_INPUTS[key]
             run = lambda: R.par2_create(inp, sub, np.arange(w["n"]), list(range(w["r"])), threads=threads)
-            sample = f"{w['n']} slices x {sub} B (a {sub}-byte sub-range of every slice), R={w['r']}"
+            sample = (f"the whole job: {w['n']} slices x {sub} B, R={w['r']}" if sub == w["s"] else
+                      f"{w['n']} slices x {sub} B (a {sub}-byte sub-range of every slice), R={w['r']}")
+            if full:
+                budget_s = 0.0  # one run of the whole job
             nbytes = inp.nbytes
         else:
             sub = 256
@@ -497,8 +553,11 @@ def cpu_baseline_sample(name, budget_s=12.0, threads=0):
         if time.time() > t_end or len(times) >= 5:
             break
     t = statistics.median(times)
-    return dict(value=nbytes / t / 1e9, unit="GB/s", cores=cores, kind=kind, sample=sample,
-                seconds_per_run=t, runs=len(times))
+    out = dict(value=nbytes / t / 1e9, unit="GB/s", cores=cores, kind=kind, sample=sample,
+               seconds_per_run=t, runs=len(times), host=host_isa())
+    if kind == "reference" and w["field"] == "gf16":
+        out["method"] = R.par2_method()  # PAR2ProcCPU::getMethodName() of the GF16_AUTO choice
+    return out
 
 
 def batched_repair_jobs(dev, seed=2024, count=16):
@@ -544,9 +603,26 @@ def measure_batched_vs_plain(ctx, timer, steps, warmup, dev):
     for _ in range(max(1, warmup - 1)):
         plain()
     plain_ms = timer.run(plain, steps)
+
+    def jobs_of(outs):
+        return [B.par3_repair_job(j["d_in"], j["lost"], j["d_rec"], o) for j, o in zip(jobs, outs)]
+
+    # jobs seen once: a fresh plan for this set of erasures (every repair
+    # system's inverse and tables, no graph) plus its one run, wall clock
+    # around synchronised calls -- the same work as one plain pass
+    once = []
+    for _ in range(max(1, steps)):
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        bo = B.Batch(jobs_of(batch_out), graph=False, ctx=ctx)
+        bo.run()
+        ctx.synchronize()
+        once.append((time.perf_counter() - t0) * 1e3)
+        bo.close()
+    incl_create_ms = statistics.median(once)
+    # a resident plan (tuned once, replayed from its CUDA graph)
     t0 = time.perf_counter()
-    b = B.Batch([B.par3_repair_job(j["d_in"], j["lost"], j["d_rec"], o) for j, o in zip(jobs, batch_out)],
-                tune=True, ctx=ctx)
+    b = B.Batch(jobs_of(batch_out), tune=True, ctx=ctx)
     ctx.synchronize()
     create_s = time.perf_counter() - t0
     for _ in range(warmup):
@@ -559,10 +635,16 @@ def measure_batched_vs_plain(ctx, timer, steps, warmup, dev):
     del jobs, plain_out, batch_out
     torch.cuda.empty_cache()
     return {"workload": "par3_repair_batch16_uneven_64MiB-1GiB_4-64KiB_1pct", "unit": "GB/s",
-            "input_bytes": in_bytes, "batched_value": in_bytes / (batch_ms * 1e-3) / 1e9, "batched_ms": batch_ms,
+            "input_bytes": in_bytes,
             "plain_value": in_bytes / (plain_ms * 1e-3) / 1e9, "plain_ms": plain_ms,
-            "batched_over_plain": plain_ms / batch_ms, "batch_graph_launches": launches,
-            "batch_create_s": create_s, "outputs_identical": bool(same)}
+            # equal work: plan creation (inverses, tables, capture) + one run, for jobs seen once
+            "batched_incl_create_value": in_bytes / (incl_create_ms * 1e-3) / 1e9,
+            "batched_incl_create_ms": incl_create_ms,
+            "batched_incl_create_over_plain": plain_ms / incl_create_ms,
+            # resident plan: graph replay of a plan built (and tuned) beforehand
+            "resident_plan_value": in_bytes / (batch_ms * 1e-3) / 1e9, "resident_plan_ms": batch_ms,
+            "resident_plan_over_plain": plain_ms / batch_ms, "resident_plan_create_s_tuned": create_s,
+            "batch_graph_launches": launches, "outputs_identical": bool(same)}
 
 
 def serving_jobs(dev, seed=5, count=32):
@@ -776,7 +858,8 @@ def profile_tc(ctx, dev):
     """The small ncu case of the tensor-core region kernels, 256 MiB of
     seeded device input each (larger than L2): PAR2 create 8,192 x 32 KiB,
     R=64, three calls (the third runs with the coefficient tiles resident, so
-    it is the region kernel alone), then PAR3 create 32,768 x 8 KiB, R=8."""
+    it is the region kernel alone), then PAR3 create 32,768 x 8 KiB, R=8,
+    then PAR2 create 256 x 1 MiB, R=8, three calls."""
     import torch
     from parparpar_b200 import par2, par3
     g = torch.Generator(device=f"cuda:{dev}")
@@ -791,6 +874,12 @@ def profile_tc(ctx, dev):
     par3.GF64Controller.ctx = ctx
     par3.GF64Controller.ComputeRecoveryBlocks(x, 32768, r, 8, 1024, 0, 32768)
     ctx.synchronize()
+    # PAR2 create 256 x 1 MiB, R=8 (one output group: the one-group tile), three calls
+    d8 = d.view(256, 1 << 20)
+    o8 = torch.zeros((8, 1 << 20), dtype=torch.uint8, device=f"cuda:{dev}")
+    for _ in range(3):
+        par2.par2_create(d8, np.arange(256), list(range(8)), out=o8, ctx=ctx)
+        ctx.synchronize()
     print(json.dumps({"profile_tc": "ok"}), flush=True)
 
 
@@ -827,7 +916,9 @@ def run_reference(args, rank):
     import oracle as orc
     times = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline_sample(name, budget_s=0.0)
+        # warm-ups: the sub-range sample (threads, tables, code); timed steps:
+        # the whole job where it runs in seconds (PAR2 create), else the sample
+        r = cpu_baseline_sample(name, budget_s=0.0, full=i >= args.warmup)
         if i >= args.warmup:
             times.append(r)
     val = statistics.median([t["value"] for t in times])
@@ -839,7 +930,8 @@ def run_reference(args, rank):
         "data": "synthetic (seeded uniform random bytes)",
         "config": {"workload": name, "num_inputs": w["n"], "slice_bytes": w["s"], "num_recovery": w["r"]},
         "cpu_baseline": {"value": val, "unit": "GB/s", "cores": times[0]["cores"], "kind": times[0]["kind"],
-                         "sample": times[0]["sample"]},
+                         "sample": times[0]["sample"], "host": times[0].get("host"),
+                         "method": times[0].get("method")},
         "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -920,9 +1012,7 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    l0 = pp.launch_count()
-    ms = timer.run(f, args.steps)
-    launches = pp.launch_count() - l0
+    ms, kms, _, launches = timed_steps(ctx, timer, f, args.steps)
     if dist:
         dist.barrier()
     clocks = sampler.stop()
@@ -933,10 +1023,8 @@ def main():
 
     int8_tops = int8_peak_tops(local)
 
-    # dominant kernel alone, for the roofline
-    kf = kernel_fn(job, ctx)
-    kf()
-    kms = timer.run(kf, max(5, min(args.steps, 20)))
+    # the dominant kernel's launches inside the timed steps, for the roofline
+    kms, kms_how = kernel_ms_of(job, ctx, timer, args.steps, kms)
     achieved = algo_bytes(job) / (kms * 1e-3) / 1e9
 
     # end to end through the public API with pinned host buffers
@@ -992,7 +1080,7 @@ def main():
         "config": {"workload": args.workload, "num_inputs": w["n"], "slice_bytes": w["s"], "num_recovery": w["r"],
                    "exponents": f"0..{w['r'] - 1}", "parallelism": f"replicas x{world} (one job per GPU)",
                    "l2": "inputs (1 GiB) larger than L2; no flush needed"},
-        "roofline": roofline(w, args, achieved, peak, peak_kind, kms, int8_tops),
+        "roofline": dict(roofline(w, args, achieved, peak, peak_kind, kms, int8_tops), kernel_timing=kms_how),
         "e2e": {"value": input_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "host_buffers": "pinned", "matches_device_result": bool(ok)},
         "gpu_launches": int(launches),
@@ -1018,6 +1106,13 @@ def main():
             except Exception as e:  # report, keep the primary line
                 sec.append({"workload": name, "error": str(e)[:200]})
         line["secondary"] = sec
+        # the north-star shapes (1 GiB at R=8) at the top level of the line
+        r8 = {}
+        for e in sec:
+            if e.get("workload") in ("par2_create_1024x1MiB_R8", "par3_create_131072x8KiB_R8") and "value" in e:
+                r8[e["workload"]] = {"gbps": round(e["value"], 1), "hbm_frac_of_measured": round(e["hbm_frac"], 4),
+                                     "kernel_ms": round(e["kernel_ms"], 4)}
+        line["r8"] = r8
 
     if rank == 0 and world == 1 and not args.no_secondary:
         try:
@@ -1035,7 +1130,7 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline_sample(args.workload)
+            line["cpu_baseline"] = cpu_baseline_sample(args.workload, full=True)
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
 

@@ -89,6 +89,15 @@ PP_API const char* pp_ctx_last_error(pp_ctx* ctx);
 PP_API uint64_t pp_launch_count(void);
 /* Drop cached device buffers (scratch, coefficient matrices). */
 PP_API int pp_ctx_free_cache(pp_ctx* ctx);
+/* Kernel timing, for measurement tools (off by default).  With `on` != 0 the
+ * context brackets each region product it issues on its stream for a
+ * device-resident single job (pp_par2_create / pp_gf16_muladd: the region
+ * kernel and its output zeroing; pp_gf64_compute_recovery: the region
+ * kernel) with a pair of CUDA events.  pp_ctx_kernel_time waits for the
+ * bracketed launches, returns their summed device time in ms and their count
+ * since the previous call, and clears them.  No counterpart in the reference. */
+PP_API int pp_ctx_set_kernel_timing(pp_ctx* ctx, int on);
+PP_API int pp_ctx_kernel_time(pp_ctx* ctx, double* ms, uint64_t* launches);
 /* Choose the GF(2^16) region kernel used by this context (PP_GF16_KERNEL_*). */
 PP_API int pp_ctx_set_gf16_kernel(pp_ctx* ctx, int kernel);
 /* Choose the GF(2^64) region kernel used by this context (same constants). */
@@ -488,6 +497,11 @@ typedef struct pp_job {
 
 typedef struct pp_batch pp_batch;
 #define PP_BATCH_TUNE 1
+/* PP_BATCH_NO_GRAPH: for jobs seen once -- creation builds the tables only
+ * (no eager run, no capture, no tuning) and pp_batch_run issues the fused
+ * launches directly, so creation plus one run is the work of running the
+ * jobs once. */
+#define PP_BATCH_NO_GRAPH 2
 PP_API int pp_batch_create(pp_ctx* ctx, const pp_job* jobs, size_t n_jobs, int flags, pp_batch** out);
 PP_API int pp_batch_run(pp_batch* batch);
 /* launches the batch's graph issues per run (kernels and memset/copy nodes) */

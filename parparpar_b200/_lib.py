@@ -45,7 +45,7 @@ PP_GF64_KERNEL_FENGER = 3
 EXPORTS = [
     "pp_version", "pp_status_string", "pp_ctx_create", "pp_ctx_destroy", "pp_ctx_set_stream",
     "pp_ctx_get_stream", "pp_ctx_synchronize", "pp_ctx_last_error", "pp_launch_count", "pp_ctx_free_cache",
-    "pp_ctx_set_gf16_kernel", "pp_ctx_set_gf64_kernel",
+    "pp_ctx_set_gf16_kernel", "pp_ctx_set_gf64_kernel", "pp_ctx_set_kernel_timing", "pp_ctx_kernel_time",
     "pp_par2_coeff", "pp_par2_input_log", "pp_par2_coeff_matrix", "pp_gf16_muladd", "pp_par2_create",
     "pp_par2_invert", "pp_par2_proc_create", "pp_par2_proc_destroy", "pp_par2_proc_set_current_slice_size",
     "pp_par2_proc_set_recovery_slices", "pp_par2_proc_can_add", "pp_par2_proc_wait_for_add",
@@ -138,6 +138,8 @@ _sig("pp_par2_proc_batches_started", _U, _P)
 _sig("pp_par2_proc_batches_done", _U, _P)
 _sig("pp_par2_proc_wait_batches", _I, _P, _U)
 _sig("pp_gf64_build_cauchy", _I, _P, _P, _SZ, _SZ, _U64, _U64)
+_sig("pp_ctx_set_kernel_timing", _I, _P, _I)
+_sig("pp_ctx_kernel_time", _I, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_U64))
 _sig("pp_gf64_compute_recovery", _I, _P, _P, _SZ, _P, _SZ, _SZ, _U64, _U64, _I, _I)
 _sig("pp_par2_create_split", _I, _P, _P, _P, _U, _P, _SZ, _U, _SZ, _P, _P, _U, _P, _SZ)
 _sig("pp_gf64_compute_recovery_split", _I, _P, _P, _P, _U, _P, _SZ, _P, _SZ, _SZ, _U64, _U64)
@@ -177,6 +179,7 @@ PP_JOB_PAR3_CREATE = 2
 PP_JOB_PAR3_REPAIR = 3
 PP_JOB_GF16_MULADD = 4
 PP_BATCH_TUNE = 1
+PP_BATCH_NO_GRAPH = 2
 
 
 class PPJob(ctypes.Structure):
@@ -249,6 +252,17 @@ class Context:
 
     def synchronize(self):
         self.check(lib.pp_ctx_synchronize(self.h))
+
+    def set_kernel_timing(self, on: bool):
+        """Bracket each region product with CUDA events (measurement only)."""
+        self.check(lib.pp_ctx_set_kernel_timing(self.h, 1 if on else 0))
+
+    def kernel_time(self):
+        """(summed device ms, launches) of the bracketed region products since
+        the last call; waits for them."""
+        ms, n = ctypes.c_double(0), _U64(0)
+        self.check(lib.pp_ctx_kernel_time(self.h, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, int(n.value)
 
     def set_stream(self, stream_ptr: int | None):
         self.check(lib.pp_ctx_set_stream(self.h, _P(stream_ptr or 0)))

@@ -14,7 +14,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (PP_BATCH_TUNE, PP_JOB_GF16_MULADD, PP_JOB_PAR2_CREATE, PP_JOB_PAR3_CREATE, PP_JOB_PAR3_REPAIR,
+from ._lib import (PP_BATCH_NO_GRAPH, PP_BATCH_TUNE, PP_JOB_GF16_MULADD, PP_JOB_PAR2_CREATE, PP_JOB_PAR3_CREATE, PP_JOB_PAR3_REPAIR,
                    PPJob, default_context, lib, ptr)
 
 
@@ -103,13 +103,16 @@ def gf16_muladd_job(inputs, coeffs, outputs, slice_bytes=None):
 class Batch:
     """A batch plan over jobs made by the *_job helpers."""
 
-    def __init__(self, jobs, tune=False, ctx=None):
+    def __init__(self, jobs, tune=False, graph=True, ctx=None):
+        """tune: time candidate work splits at creation (resident plans);
+        graph=False: jobs seen once -- build the tables only and issue the
+        fused launches directly at run() (no eager run, no capture)."""
         self.ctx = _ctx(ctx)
         self._keep = [k for _, k in jobs]
         arr = (PPJob * len(jobs))(*[j for j, _ in jobs])
         h = ctypes.c_void_p()
-        self.ctx.check(lib.pp_batch_create(self.ctx.h, arr, len(jobs), PP_BATCH_TUNE if tune else 0,
-                                           ctypes.byref(h)))
+        flags = (PP_BATCH_TUNE if tune and graph else 0) | (0 if graph else PP_BATCH_NO_GRAPH)
+        self.ctx.check(lib.pp_batch_create(self.ctx.h, arr, len(jobs), flags, ctypes.byref(h)))
         self.h = h
 
     @property

@@ -380,6 +380,10 @@ PP_API int pp_batch_create(pp_ctx* ctx, const pp_job* jobs, size_t n_jobs, int f
 
   const int sms = ctx_sms(ctx);
   int* st = ctx_status_word(ctx);
+  if (flags & PP_BATCH_NO_GRAPH) {  // tables only; runs are issued eagerly
+    *out = b;
+    return PP_OK;
+  }
   // one eager run before capture: sets the kernels' attributes and checks
   // every launch of the plan (the outputs are written)
   BTRY(issue(b, s, nullptr), "batch first run");
@@ -411,6 +415,13 @@ PP_API int pp_batch_run(pp_batch* b) {
   pp_ctx* ctx = b->ctx;
   std::lock_guard<std::mutex> g(ctx_mutex(ctx));
   if (cudaSetDevice(b->device) != cudaSuccess) return ctx_fail(ctx, PP_ERR_CUDA, "cudaSetDevice failed");
+  if (!b->exec) {  // PP_BATCH_NO_GRAPH: issue the fused launches directly
+    int n = 0;
+    cudaError_t e = issue(b, ctx_stream(ctx), &n);
+    if (e != cudaSuccess) return ctx_fail(ctx, PP_ERR_CUDA, cudaGetErrorString(e));
+    b->launches = n;
+    return PP_OK;
+  }
   cudaError_t e = cudaGraphLaunch(b->exec, ctx_stream(ctx));
   if (e != cudaSuccess) return ctx_fail(ctx, PP_ERR_CUDA, cudaGetErrorString(e));
   note_launch(b->launches);

@@ -118,8 +118,31 @@ struct pp_ctx {
   cudaEvent_t hash_ev = nullptr, staged_ev = nullptr;
   uint8_t* pinned = nullptr;       // streaming reads: two pinned chunk buffers
   size_t pinned_n = 0;
+  // kernel timing (pp_ctx_set_kernel_timing): event pairs around region products
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> t_pending, t_free;
   std::mutex mu;
 };
+
+// Bracket one region product on the context's stream with CUDA events when
+// kernel timing is on (measurement only; off by default).
+static std::pair<cudaEvent_t, cudaEvent_t>* timing_begin(pp_ctx* ctx) {
+  if (!ctx->timing) return nullptr;
+  std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+  if (!ctx->t_free.empty()) {
+    ev = ctx->t_free.back();
+    ctx->t_free.pop_back();
+  } else if (cudaEventCreate(&ev.first) != cudaSuccess || cudaEventCreate(&ev.second) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  ctx->t_pending.push_back(ev);
+  cudaEventRecord(ev.first, ctx->stream);
+  return &ctx->t_pending.back();
+}
+static void timing_end(pp_ctx* ctx, std::pair<cudaEvent_t, cudaEvent_t>* ev) {
+  if (ev) cudaEventRecord(ev->second, ctx->stream);
+}
 
 static int set_err(pp_ctx* ctx, int code, const char* fmt, ...) {
   if (ctx) {
@@ -141,6 +164,32 @@ static int set_err(pp_ctx* ctx, int code, const char* fmt, ...) {
                      __LINE__);                                                                      \
     }                                                                                                \
   } while (0)
+
+// ---- tracing: with PARPAR_B200_TRACE set (and not "0"), host-side spans of
+// the single-job entry points and of the allocation / synchronisation calls
+// their caches make are written to stderr, one line per span of at least
+// 0.5 ms: "pp-trace <what> <bytes> <ms>".  Off by default (one getenv).
+static bool trace_on() {
+  static const bool on = [] {
+    const char* e = getenv("PARPAR_B200_TRACE");
+    return e && *e && strcmp(e, "0") != 0;
+  }();
+  return on;
+}
+struct TraceSpan {
+  const char* what;
+  size_t bytes;
+  std::chrono::steady_clock::time_point t0;
+  TraceSpan(const char* w, size_t b) : what(w), bytes(b), t0(std::chrono::steady_clock::now()) {}
+  ~TraceSpan() {
+    if (!trace_on()) return;
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (ms >= 0.5) fprintf(stderr, "pp-trace %s %zu %.3f\n", what, bytes, ms);
+  }
+};
+#define PP_TRACE_CAT2(a, b) a##b
+#define PP_TRACE_CAT(a, b) PP_TRACE_CAT2(a, b)
+#define PP_TRACE(what, bytes) TraceSpan PP_TRACE_CAT(pp_span_, __LINE__)(what, bytes)
 
 static int bind(pp_ctx* ctx) {
   cudaError_t e = cudaSetDevice(ctx->device);
@@ -175,7 +224,9 @@ static int device_status(pp_ctx* ctx) {
 static void* scratch(pp_ctx* ctx, Slot s, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (ctx->slot_n[s] >= bytes) return ctx->slot_p[s];
+  PP_TRACE("scratch-grow", bytes);
   if (ctx->slot_p[s]) {
+    PP_TRACE("scratch-free", ctx->slot_n[s]);
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->slot_p[s]);
     ctx->slot_p[s] = nullptr;
@@ -184,6 +235,7 @@ static void* scratch(pp_ctx* ctx, Slot s, size_t bytes) {
   size_t n = bytes + bytes / 8;  // some headroom against regrowth
   n = (n + 255) & ~(size_t)255;
   void* p = nullptr;
+  PP_TRACE("scratch-malloc", n);
   if (cudaMalloc(&p, n) != cudaSuccess) {
     cudaGetLastError();
     if (cudaMalloc(&p, bytes) != cudaSuccess) {
@@ -322,9 +374,40 @@ PP_API int pp_ctx_free_cache(pp_ctx* ctx) {
   return PP_OK;
 }
 
+PP_API int pp_ctx_set_kernel_timing(pp_ctx* ctx, int on) {
+  if (!ctx) return PP_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->timing = on != 0;
+  return PP_OK;
+}
+
+PP_API int pp_ctx_kernel_time(pp_ctx* ctx, double* ms, uint64_t* launches) {
+  if (!ctx || !ms) return PP_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (int r = bind(ctx)) return r;
+  double total = 0;
+  for (auto& ev : ctx->t_pending) {
+    CUDA_TRY(ctx, cudaEventSynchronize(ev.second));
+    float t = 0;
+    CUDA_TRY(ctx, cudaEventElapsedTime(&t, ev.first, ev.second));
+    total += t;
+  }
+  *ms = total;
+  if (launches) *launches = ctx->t_pending.size();
+  ctx->t_free.insert(ctx->t_free.end(), ctx->t_pending.begin(), ctx->t_pending.end());
+  ctx->t_pending.clear();
+  return PP_OK;
+}
+
 PP_API void pp_ctx_destroy(pp_ctx* ctx) {
   if (!ctx) return;
   pp_ctx_free_cache(ctx);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& ev : ctx->t_pending) ctx->t_free.push_back(ev);
+  for (auto& ev : ctx->t_free) {
+    cudaEventDestroy(ev.first);
+    cudaEventDestroy(ev.second);
+  }
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->copy) cudaStreamDestroy(ctx->copy);
   if (ctx->copy_ev) cudaEventDestroy(ctx->copy_ev);
@@ -432,12 +515,14 @@ static int par2_table(pp_ctx* ctx, const uint16_t* input_idx, unsigned n_in, con
   size_t total = e.bytes;
   for (auto& x : ctx->par2) total += x.bytes;
   while (!ctx->par2.empty() && (ctx->par2.size() >= kPar2CacheEntries || total > kPar2CacheBytes)) {
+    PP_TRACE("par2-table-evict", ctx->par2.back().bytes);
     cudaStreamSynchronize(ctx->stream);
     total -= ctx->par2.back().bytes;
     cudaFree(ctx->par2.back().d_coef);
     cudaFree(ctx->par2.back().d_aexp);
     ctx->par2.pop_back();
   }
+  PP_TRACE("par2-table-malloc", e.bytes);
   if (cudaMalloc(&e.d_coef, cbytes) != cudaSuccess || (tbytes && cudaMalloc(&e.d_aexp, tbytes) != cudaSuccess)) {
     cudaGetLastError();
     cudaFree(e.d_coef);
@@ -514,7 +599,7 @@ constexpr unsigned kCopyChunk = 4096;
 constexpr unsigned kCopyTail = 256;
 constexpr size_t kBandMinBytes = (size_t)128 << 20;  // column bands for staged inputs of at least this size
 constexpr size_t kBandMinWidth = 4096;               // bytes of every slice per band, at least (multiple of 64)
-constexpr size_t kGf16TileBytes = 128 * 128;  // one expanded tile (8 outputs x 8 inputs)
+constexpr size_t kGf16TileBytes = 128 * 128;  // one expanded tile (8 outputs x one stage of inputs)
 
 static int ensure_copy_stream(pp_ctx* ctx) {
   if (ctx->copy) return PP_OK;
@@ -592,7 +677,8 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
       if (!aexp) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficient tiles");
       CUDA_TRY(ctx, launch_gf16_tc_expand(d_coeffs, ldc, n_in, n_out, aexp, ctx->stream));
     }
-    const unsigned stages = (n_in + 7) / 8;
+    const unsigned si = gf16_tc_stage_inputs();  // inputs per tile stage (8 int8, 16 FP4)
+    const unsigned stages = (n_in + si - 1) / si;
     // the staging rows are free once earlier work on the context's stream is done
     CUDA_TRY(ctx, cudaEventRecord(ctx->start_ev, ctx->stream));
     CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy, ctx->start_ev, 0));
@@ -602,7 +688,8 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
       // the last kCopyChunk slices go in halving pieces (down to kCopyTail),
       // so little product work is left once the final copy has landed
       const unsigned rest = n_in - c0;
-      nc = rest > kCopyChunk ? kCopyChunk : rest > kCopyTail ? std::max(kCopyTail, (rest / 2 + 7) & ~7u) : rest;
+      // (pieces are multiples of 16 slices: whole tile stages of either operand format)
+      nc = rest > kCopyChunk ? kCopyChunk : rest > kCopyTail ? std::max(kCopyTail, (rest / 2 + 15) & ~15u) : rest;
       CUDA_TRY(ctx, cudaMemcpy2DAsync(din + (size_t)c0 * row, row, (const uint8_t*)inputs + (size_t)c0 * in_stride,
                                       in_stride, slice, nc, cudaMemcpyHostToDevice, ctx->copy));
       CUDA_TRY(ctx, cudaEventRecord(ctx->copy_ev, ctx->copy));
@@ -617,7 +704,7 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
                                              dh + (size_t)20 * hashed, ctx->hash));
         hashed = c0 + nc;
       }
-      CUDA_TRY(ctx, launch_gf16_muladd_tc(din + (size_t)c0 * row, row, nc, slice, aexp + (size_t)(c0 / 8) * kGf16TileBytes,
+      CUDA_TRY(ctx, launch_gf16_muladd_tc(din + (size_t)c0 * row, row, nc, slice, aexp + (size_t)(c0 / si) * kGf16TileBytes,
                                           n_out, dout, ostride, accumulate || c0 > 0, ctx->sms, ctx->d_status,
                                           ctx->stream, stages));
     }
@@ -713,8 +800,10 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
     aexp = (uint8_t*)scratch(ctx, S_AEXP, gf16_tc_coeff_bytes(n_in, n_out));
     if (!aexp) return set_err(ctx, PP_ERR_NO_MEMORY, "coefficient tiles");
   }
+  auto* tev = timing_begin(ctx);
   CUDA_TRY(ctx, gf16_region(ctx->gf16_kernel, din, dstride, n_in, slice, d_coeffs, ldc, n_out, dout, ostride,
                             accumulate, ctx->sms, aexp, ctx->d_status, ctx->stream, aexp_ready != nullptr));
+  timing_end(ctx, tev);
   if (stage_out) {
     CUDA_TRY(ctx, cudaMemcpy2DAsync(outputs, out_stride, dout, row, slice, n_out,
                                     out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
@@ -730,6 +819,7 @@ static int gf16_muladd_impl(pp_ctx* ctx, const void* inputs, size_t in_stride, u
 PP_API int pp_gf16_muladd(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
                           size_t slice_bytes, const uint16_t* coeffs, size_t coeff_stride, unsigned num_outputs,
                           void* outputs, size_t output_stride, int accumulate) {
+  PP_TRACE("call-gf16_muladd", 0);
   if (!ctx) return PP_ERR_INVALID_ARG;
   if (!outputs || (num_inputs && (!inputs || !coeffs))) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
   if (num_inputs && input_stride < slice_bytes) return set_err(ctx, PP_ERR_INVALID_ARG, "input_stride < slice_bytes");
@@ -788,6 +878,7 @@ static int par2_create_impl(pp_ctx* ctx, const void* inputs, size_t input_stride
 PP_API int pp_par2_create(pp_ctx* ctx, const void* inputs, size_t input_stride, unsigned num_inputs,
                           size_t slice_bytes, const uint16_t* input_idx, const uint16_t* exps, unsigned num_outputs,
                           void* outputs, size_t output_stride) {
+  PP_TRACE("call-par2_create", 0);
   return par2_create_impl(ctx, inputs, input_stride, num_inputs, slice_bytes, input_idx, exps, num_outputs, outputs,
                           output_stride, nullptr);
 }
@@ -1380,11 +1471,13 @@ static uint64_t* cauchy_get(pp_ctx* ctx, size_t n_in, size_t n_rec, uint64_t fI,
   }
   // LRU of 8 matrices, as the reference's coefficient cache (src/par3_engine.cc:451-482)
   if (ctx->cauchy.size() >= 8) {
+    PP_TRACE("cauchy-evict", ctx->cauchy.back().n_in * ctx->cauchy.back().n_rec * 8);
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->cauchy.back().d);
     ctx->cauchy.pop_back();
   }
   void* d = nullptr;
+  PP_TRACE("cauchy-malloc", n_in * n_rec * 8);
   if (cudaMalloc(&d, n_in * n_rec * 8) != cudaSuccess) {
     cudaGetLastError();
     // make room: drop every cached matrix and retry once
@@ -1553,8 +1646,10 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
     dout_ld = B;
     if (accumulate) CUDA_TRY(ctx, h2d_rows(dout, recovery, out_ld, n_rec, ctx->stream));
   }
+  auto* tev = timing_begin(ctx);
   CUDA_TRY(ctx, gf64_region(ctx, din, nullptr, din_ld, n_in, B, d_coeff, n_in, n_rec, dout, nullptr, dout_ld,
                             accumulate, aligned_rows64(din, din_ld) && aligned_rows64(dout, dout_ld)));
+  timing_end(ctx, tev);
   if (!out_dev) CUDA_TRY(ctx, d2h_rows(recovery, out_ld, dout, n_rec, ctx->stream));
   if (int r = join_hash()) return r;
   if (!in_dev || !out_dev) {
@@ -1567,6 +1662,7 @@ static int gf64_matvec_impl(pp_ctx* ctx, const uint64_t* inputs, size_t n_in, ui
 PP_API int pp_gf64_compute_recovery(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs, uint64_t* recovery,
                                     size_t num_recovery, size_t block_size64, uint64_t first_input,
                                     uint64_t first_recovery, int accumulate, int kernel) {
+  PP_TRACE("call-gf64_compute_recovery", 0);
   if (!ctx) return PP_ERR_INVALID_ARG;
   if (num_inputs == 0 || num_recovery == 0 || block_size64 == 0) return PP_OK;
   if (!inputs || !recovery) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");
@@ -1830,6 +1926,7 @@ PP_API int pp_gf64_fft_inv(pp_ctx* ctx, uint64_t* data, size_t n, size_t batch, 
 PP_API int pp_gf64_repair(pp_ctx* ctx, const uint64_t* inputs, size_t num_inputs, const uint64_t* missing, size_t n,
                           const uint64_t* recovery, const uint8_t* recovery_present, size_t B, uint64_t first_input,
                           uint64_t first_recovery, uint64_t* restored) {
+  PP_TRACE("call-gf64_repair", 0);
   if (!ctx) return PP_ERR_INVALID_ARG;
   if (n == 0 || B == 0) return PP_OK;
   if (!inputs || !missing || !recovery || !restored) return set_err(ctx, PP_ERR_INVALID_ARG, "null buffer");

@@ -41,6 +41,8 @@
 #include "tc_common.cuh"
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 
 namespace pp {
 namespace tc16 {
@@ -464,6 +466,410 @@ static uint64_t tiles16(const Gf16TcJob& j) { return (uint64_t)j.groups * j.wt; 
 
 }  // namespace tc16
 
+// ============================================================================
+// The same product on the block-scaled FP4 path (tcgen05.mma kind::mxf4).
+//
+// Operands are e2m1 values 0 or 1.0 (nibbles 0x0 / 0x2), two per byte, with
+// every ue8m0 scale factor 1.0 (0x7F), so each MMA adds exact integer counts
+// into fp32 accumulators (counts stay below 16 * 32768 < 2^23).  The parity of
+// a count is read by adding 2^23: the sum's lowest mantissa bit is the count's
+// lowest bit.  Half the operand bytes of the int8 form per GF(2) product and
+// the FP4 rate of the tensor pipe.
+//
+// Bit selection: e2m1 codes are not parities of their value, so each B
+// element must be exactly 0 or 1.0.  Four bits of a word are picked per shift:
+// ((w >> j) & 0x1111) << 1 places bits j, 4+j, 8+j, 12+j of w in nibbles
+// 0..3 as 0x0 / 0x2.  With
+//   A[(o,b)][(j, i, m)] = 1.0 * bit_b(c[o][i] * x^(4m + j))
+//   B[w][(j, i, m)]     = 1.0 * bit_(4m + j)(in_i[w])          (j = 0..3)
+// D[(o,b)][w] counts the terms of bit b of out[o][w].  A stage is 16 inputs:
+// K = 256 elements = one 128-byte (swizzled) row; the 64-element MMA step j
+// covers 32 bytes: inputs 0-7 then 8-15, two u32 words (two inputs) each.
+//
+// CTA tile: KG = 2 -> 16 outputs x 240 words (two accumulators of N = 240,
+// one per output group, sharing each B tile); KG = 1 -> 8 outputs x 480 words
+// (two accumulators of N = 240 on the two halves of the B tile, sharing each
+// A tile).  TMEM: accumulators at columns 0 and 256 (240 each), scale factors
+// in columns 240-255 (A at 240, B at 248).  Warp roles and bounded waits as in
+// the int8 kernel.
+namespace tc16f4 {
+using namespace pp::tc;
+
+constexpr int kStageIn = 16;        // inputs per stage
+constexpr int kABytes = 128 * 128;  // A tile of one output group: 128 rows x 128 B
+constexpr int kThreads = 320;
+constexpr int kExp = 256;
+constexpr int kN = 240;             // words per accumulator
+constexpr uint32_t kSfaCol = 240, kSfbCol = 248;
+
+template <int KG>
+struct Shape {
+  static constexpr int kLd = KG == 2 ? 4 : 3;
+  static constexpr int kBs = 2;
+  static constexpr int kWords = KG == 2 ? kN : 2 * kN;
+  static constexpr int kAStage = KG * kABytes;
+  static constexpr int kBBytes = kWords * 128;
+  static constexpr int kRawBytes = kStageIn * kWords * 2;
+  static constexpr int kOffA = 0;
+  static constexpr int kOffB = kLd * kAStage;
+  static constexpr int kOffRaw = kOffB + kBs * kBBytes;
+  static constexpr int kOffBar = kOffRaw + kLd * kRawBytes;
+  static constexpr int kSmemBytes = kOffBar + 256 + 1024;
+};
+static_assert(Shape<1>::kSmemBytes <= 227 * 1024 && Shape<2>::kSmemBytes <= 227 * 1024, "shared memory");
+static_assert(Shape<1>::kOffB % 1024 == 0 && Shape<2>::kOffB % 1024 == 0 && (kN * 128) % 1024 == 0,
+              "operand tiles start on 1024-byte swizzle atoms");
+
+// instruction descriptor, block-scaled kinds: A/B e2m1 (mxf4 format 1), both
+// K-major, N = 240, scale factors ue8m0, M = 128, dense K = 64
+constexpr uint32_t kIdesc = (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
+
+PP_D void mma_f4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate, uint32_t sfa, uint32_t sfb) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %3, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %6, [%4], [%5], p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(accumulate), "r"(sfa), "r"(sfb), "r"(kIdesc)
+      : "memory");
+}
+
+// nibbles 0x2 where bit (4m + j) of each 16-bit half of p is set
+PP_D uint32_t pick4(uint32_t p, int j) { return ((p >> j) & 0x11111111u) << 1; }
+
+// A tiles: for output group g and stage s (inputs 16s..16s+15) a 16 KiB tile
+// in the canonical K-major 128-byte-swizzled layout: row m = 16*oo + b; the
+// 16-byte chunk 2j + h holds, for inputs 8h..8h+7 (two per 32-bit word), the
+// nibbles 2*bit_(4m+j) of Q_b(c[8g+oo][16s+8h+ii]) (bit e of Q_b(c) = bit b of
+// c * x^e, the nibble table of the int8 expansion).
+__global__ void __launch_bounds__(128)
+k_gf16_f4_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigned n_in, unsigned n_out,
+                        unsigned n_stages, uint8_t* __restrict__ a_exp) {
+  __shared__ __align__(16) uint16_t T[4 * 16 * 16];
+  reinterpret_cast<uint4*>(T)[threadIdx.x] = reinterpret_cast<const uint4*>(tc16::g_gf16_qtab)[threadIdx.x];
+  __syncthreads();
+  const unsigned m = threadIdx.x, oo = m >> 4, b = m & 15;
+  const size_t tiles = (size_t)((n_out + 7) / 8) * n_stages;
+  for (size_t gs = blockIdx.x; gs < tiles; gs += gridDim.x) {  // gs = g * n_stages + s
+    const unsigned s = (unsigned)(gs % n_stages), g = (unsigned)(gs / n_stages);
+    const unsigned o = 8 * g + oo;
+    uint32_t P[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int ii = 0; ii < kStageIn; ii++) {
+      const unsigned i = kStageIn * s + ii;
+      const uint32_t c = (o < n_out && i < n_in) ? coeffs[(size_t)o * ldc + i] : 0;
+      const uint32_t q = (uint32_t)T[((c & 15) << 4) + b] ^ T[256 + (((c >> 4) & 15) << 4) + b] ^
+                         T[512 + (((c >> 8) & 15) << 4) + b] ^ T[768 + ((c >> 12) << 4) + b];  // Q_b(c)
+      P[ii >> 1] |= q << (16 * (ii & 1));
+    }
+    // warp stores of 512 contiguous bytes: lane L writes 16-byte slot L of
+    // store k = row 4k + L/8 of the warp, physical chunk L%8 (logical chunk
+    // (L%8) ^ (row%8) = 2j + h), from the words of the lane that built the row
+    const unsigned lane = m & 31;
+    uint8_t* wbase = a_exp + gs * kABytes + (m >> 5) * 4096;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const unsigned r = 4 * k + (lane >> 3), lc = (lane & 7) ^ (r & 7), j = lc >> 1, h = lc & 1;
+      uint32_t w[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        const uint32_t lo = __shfl_sync(0xFFFFFFFFu, P[t], r), hi = __shfl_sync(0xFFFFFFFFu, P[4 + t], r);
+        w[t] = pick4(h ? hi : lo, (int)j);
+      }
+      *reinterpret_cast<uint4*>(wbase + 512 * k + 16 * lane) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+template <int KG>
+__global__ void __launch_bounds__(kThreads, 1)
+k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ status) {
+  using S = Shape<KG>;
+  constexpr int kWords = S::kWords, kBBytes = S::kBBytes, kRawBytes = S::kRawBytes, kAStage = S::kAStage;
+  constexpr int kOffA = S::kOffA, kOffB = S::kOffB, kOffRaw = S::kOffRaw, kOffBar = S::kOffBar;
+  constexpr int kLd = S::kLd, kBs = S::kBs;
+  const TcSeg sg = tc_item(&batch, blockIdx.x);
+  const Gf16TcJob J = pinned_job(batch.job[sg.job]);
+  const uint8_t* __restrict__ in = J.in;
+  const size_t in_stride = J.in_stride;
+  const unsigned n_in = J.n_in;
+  const size_t slice_bytes = J.slice_bytes;
+  const uint8_t* __restrict__ a_exp = J.a_exp;
+  const unsigned n_stages_total = J.a_stride;
+  const unsigned n_out = J.n_out;
+  uint8_t* __restrict__ out = J.out;
+  const size_t out_stride = J.out_stride;
+  const int mode = sg.mode;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t base_s = smem_addr(smem_raw);
+  const uint32_t pad = ((base_s + 1023) & ~1023u) - base_s;
+  uint8_t* smem = smem_raw + pad;
+  const uint32_t sA = base_s + pad + kOffA, sB = base_s + pad + kOffB, sRaw = base_s + pad + kOffRaw;
+  uint8_t* raw_p = smem + kOffRaw;
+  uint8_t* b_p = smem + kOffB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+  const uint32_t bar0 = smem_addr(bars);
+  enum {
+    A_FULL = 0,
+    RAW_FULL = A_FULL + kLd,
+    A_EMPTY = RAW_FULL + kLd,
+    RAW_EMPTY = A_EMPTY + kLd,
+    B_FULL = RAW_EMPTY + kLd,
+    B_EMPTY = B_FULL + kBs,
+    D_FULL = B_EMPTY + kBs,
+    DONE = D_FULL + 1,
+    NBARS = DONE + 1
+  };
+  static_assert(8 * NBARS + 16 <= 256, "barrier area");
+  auto BAR = [&](int k) { return bar0 + 8u * (uint32_t)k; };
+  volatile uint32_t* tmem_holder = reinterpret_cast<volatile uint32_t*>(smem + kOffBar + 8 * NBARS);
+  volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 8 * NBARS + 8);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned g = (unsigned)(sg.tile % J.groups) * KG;  // first output group of the CTA
+  const size_t w0 = (size_t)(sg.tile / J.groups) * kWords;
+  const unsigned st_begin = sg.st0;
+  const unsigned nst = sg.st1 - sg.st0;
+  const size_t total_words = (slice_bytes + 1) / 2;
+  const unsigned words_valid = (unsigned)min((size_t)kWords, total_words - w0);
+  const size_t tile_bytes_valid = min((size_t)kWords * 2, slice_bytes - 2 * w0);
+  const uint32_t raw_copy = (uint32_t)((tile_bytes_valid + 15) & ~(size_t)15);
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NBARS; k++) {
+      const bool by_expanders = (k >= RAW_EMPTY && k < RAW_EMPTY + kLd) || (k >= B_FULL && k < B_FULL + kBs);
+      mbar_init(BAR(k), by_expanders ? (uint32_t)kExp : 1u);
+    }
+    *err = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr((const void*)tmem_holder)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_holder;
+  if (warp >= 2 && warp < 6) {
+    // scale factors 1.0 (ue8m0 0x7F) in columns 240-255 of this warp's lane quarter
+    const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + kSfaCol;
+    const uint32_t v = 0x7F7F7F7Fu;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(t),
+        "r"(v)
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      unsigned issued = 0;
+      for (unsigned k = 0; k < nst && !*err; k++) {
+        const unsigned sl = k % kLd, use = k / kLd;
+        if (k >= kLd) {
+          if (!mbar_wait(BAR(A_EMPTY + sl), (use - 1) & 1) || !mbar_wait(BAR(RAW_EMPTY + sl), (use - 1) & 1)) {
+            *err = 1;
+            break;
+          }
+        }
+        const unsigned st = st_begin + k;
+        mbar_expect_tx(BAR(A_FULL + sl), kAStage);
+#pragma unroll
+        for (int gg = 0; gg < KG; gg++)
+          bulk_g2s(sA + sl * kAStage + gg * kABytes, a_exp + ((size_t)(g + gg) * n_stages_total + st) * kABytes,
+                   kABytes, BAR(A_FULL + sl));
+        const unsigned i0 = st * kStageIn;
+        const unsigned ni = min((unsigned)kStageIn, n_in - i0);
+        mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
+        for (unsigned ii = 0; ii < ni; ii++)
+          bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 2), in + (size_t)(i0 + ii) * in_stride + 2 * w0, raw_copy,
+                   BAR(RAW_FULL + sl));
+        issued = k + 1;
+      }
+      if (*err) {
+        for (unsigned k = issued > (unsigned)kLd ? issued - kLd : 0; k < issued; k++) {
+          mbar_wait(BAR(A_FULL + k % kLd), (k / kLd) & 1);
+          mbar_wait(BAR(RAW_FULL + k % kLd), (k / kLd) & 1);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t sfa = tmem + kSfaCol, sfb = tmem + kSfbCol;
+      for (unsigned k = 0; k < nst; k++) {
+        const unsigned sl = k % kLd, bs = k % kBs;
+        if (*err || !mbar_wait(BAR(A_FULL + sl), (k / kLd) & 1) || !mbar_wait(BAR(B_FULL + bs), (k / kBs) & 1)) {
+          *err = 1;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+#pragma unroll
+          for (int nn = 0; nn < 2; nn++) {
+            // KG = 2: one word tile, two groups; KG = 1: one group, two word halves
+            const uint32_t a_off = KG == 2 ? nn * kABytes : 0;
+            const uint32_t b_off = KG == 2 ? 0 : nn * (kN * 128);
+            mma_f4(tmem + nn * 256, sw128_desc(sA + sl * kAStage + a_off + 32 * kk),
+                   sw128_desc(sB + bs * kBBytes + b_off + 32 * kk), (k > 0 || kk > 0) ? 1u : 0u, sfa, sfb);
+          }
+        }
+        mma_commit(BAR(A_EMPTY + sl));
+        mma_commit(BAR(B_EMPTY + bs));
+      }
+      if (!*err) mma_commit(BAR(D_FULL));
+      mma_commit(BAR(DONE));
+      if (!mbar_wait(BAR(DONE), 0)) *err = 1;
+    }
+  } else {
+    // ------------------------------------------------------------ expanders
+    const int e = threadIdx.x - 64;  // 0..255
+    const bool odd_tail = (slice_bytes & 1) && (w0 + kWords >= total_words);
+    const unsigned last_word = (unsigned)(total_words - 1 - w0);
+    constexpr int kRows = kWords <= kExp ? 1 : 2;  // word rows per thread
+    for (unsigned k = 0; k < nst; k++) {
+      const unsigned sl = k % kLd, bs = k % kBs;
+      if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
+        *err = 1;
+        break;
+      }
+      const unsigned i0 = (st_begin + k) * kStageIn;
+      const unsigned ni = min((unsigned)kStageIn, n_in - i0);
+      const uint8_t* raw = raw_p + sl * kRawBytes;
+      uint32_t P[kRows][8];
+#pragma unroll
+      for (int rr = 0; rr < kRows; rr++) {
+        const unsigned n = (unsigned)e + rr * kN;  // word row of the tile
+        uint32_t mask = (n < words_valid && e < kN) ? 0xFFFFu : 0u;
+        if (odd_tail && n == last_word) mask &= 0x00FFu;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const uint32_t lo = (unsigned)(2 * q) < ni && e < kN
+                                  ? *reinterpret_cast<const uint16_t*>(raw + (2 * q) * (kWords * 2) + 2 * n) : 0u;
+          const uint32_t hi = (unsigned)(2 * q + 1) < ni && e < kN
+                                  ? *reinterpret_cast<const uint16_t*>(raw + (2 * q + 1) * (kWords * 2) + 2 * n) : 0u;
+          P[rr][q] = (lo & mask) | ((hi & mask) << 16);
+        }
+      }
+      mbar_arrive(BAR(RAW_EMPTY + sl));
+      if (k >= (unsigned)kBs && !mbar_wait(BAR(B_EMPTY + bs), (k / kBs - 1) & 1)) {
+        *err = 1;
+        break;
+      }
+      uint8_t* bt = b_p + bs * kBBytes;
+      if (e < kN) {
+#pragma unroll
+        for (int rr = 0; rr < kRows; rr++) {
+          const unsigned n = (unsigned)e + rr * kN;
+          const uint32_t rowA = (n >> 3) * 1024 + (n & 7) * 128, rA = n & 7;
+          // 8 consecutive threads store 8 rows of one swizzle atom at 8 distinct chunks
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            *reinterpret_cast<uint4*>(bt + rowA + (((2 * j) ^ rA) << 4)) =
+                make_uint4(pick4(P[rr][0], j), pick4(P[rr][1], j), pick4(P[rr][2], j), pick4(P[rr][3], j));
+            *reinterpret_cast<uint4*>(bt + rowA + (((2 * j + 1) ^ rA) << 4)) =
+                make_uint4(pick4(P[rr][4], j), pick4(P[rr][5], j), pick4(P[rr][6], j), pick4(P[rr][7], j));
+          }
+        }
+      }
+      fence_async_smem();
+      mbar_arrive(BAR(B_FULL + bs));
+    }
+    // ------------------------------------------------------------ epilogue
+    const bool have = nst > 0 && !*err && mbar_wait(BAR(D_FULL), 0);
+    if (nst > 0 && !have) *err = 1;
+    tc_fence_after();
+    const int q = warp & 3;             // TMEM lane quarter of this warp
+    const int chalf = (warp - 2) >> 2;  // accumulator 0 (columns 0-239) or 1 (256-495)
+    // KG = 2: accumulator = output group; KG = 1: accumulator = word half
+    const unsigned o_lo = 8 * (g + (KG == 2 ? chalf : 0)) + 2 * q, o_hi = o_lo + 1;
+    const unsigned wbase = KG == 2 ? 0u : (unsigned)chalf * kN;
+    for (int c = 0; c < (kN + 31) / 32; c++) {
+      uint32_t r[32];
+      if (have) {
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + 256 * chalf + 32 * c, r);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++) r[j] = 0;
+      }
+      uint32_t mine = 0;
+#pragma unroll
+      for (int j = 0; j < 32; j++) {
+        // exact count f < 2^23: the lowest mantissa bit of f + 2^23 is f's lowest bit
+        const uint32_t bit = __float_as_uint(__fadd_rn(__uint_as_float(r[j]), 8388608.0f)) & 1u;
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
+        if (lane == j) mine = bal;
+      }
+      if (!have) continue;
+      const unsigned wcol = 32 * c + lane;   // column of the accumulator
+      const unsigned widx = wbase + wcol;    // word within the tile
+      const uint32_t nb = __shfl_down_sync(0xFFFFFFFFu, mine, 1);
+      if ((lane & 1) || wcol >= (unsigned)kN || widx >= words_valid) continue;
+      const size_t wbyte = 2 * (w0 + widx);
+      const size_t nbytes = min((size_t)4, slice_bytes - wbyte);
+#pragma unroll
+      for (int hsel = 0; hsel < 2; hsel++) {
+        const unsigned o = hsel ? o_hi : o_lo;
+        if (o >= n_out) continue;
+        uint32_t val = hsel ? ((mine >> 16) | (nb & 0xFFFF0000u)) : ((mine & 0xFFFFu) | (nb << 16));
+        uint8_t* dst = out + (size_t)o * out_stride + wbyte;
+        if (nbytes >= 4) {
+          if (mode == 2) {
+            if (val) atomicXor(reinterpret_cast<uint32_t*>(dst), val);
+          } else if (mode == 1) {
+            *reinterpret_cast<uint32_t*>(dst) ^= val;
+          } else {
+            *reinterpret_cast<uint32_t*>(dst) = val;
+          }
+        } else {
+          if (mode == 2) {
+            const uint32_t mm = (1u << (8 * nbytes)) - 1u;
+            if (val & mm) atomicXor(reinterpret_cast<uint32_t*>(dst), val & mm);
+          } else {
+            for (size_t bb = 0; bb < nbytes; bb++) {
+              const uint8_t nbv = (uint8_t)(val >> (8 * bb));
+              dst[bb] = mode == 1 ? (uint8_t)(dst[bb] ^ nbv) : nbv;
+            }
+          }
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+  if (threadIdx.x == 0 && *err) atomicOr(status, 1);
+}
+
+}  // namespace tc16f4
+
+// Operand format of the GF(2^16) tensor-core path, fixed for the process at
+// first use: block-scaled FP4 (kind::mxf4, 16 inputs per stage) unless
+// PARPAR_B200_GF16_TC=i8 selects the int8 form (8 inputs per stage).  Every
+// expansion and launch of the process uses the same format, so resident tiles
+// always match the kernel that reads them.
+static bool gf16_tc_use_f4() {
+  static const bool f4 = [] {
+    const char* e = getenv("PARPAR_B200_GF16_TC");
+    return !(e && strcmp(e, "i8") == 0);
+  }();
+  return f4;
+}
+
+unsigned gf16_tc_stage_inputs() { return gf16_tc_use_f4() ? tc16f4::kStageIn : tc16::kStageIn; }
+
 cudaError_t gf16_tc_tables_init(cudaStream_t s) {
   if (device_done(tc16::g_qtab_ready)) return cudaSuccess;
   cudaError_t e = tc16::qtab_on(s);
@@ -473,29 +879,39 @@ cudaError_t gf16_tc_tables_init(cudaStream_t s) {
 }
 
 size_t gf16_tc_coeff_bytes(unsigned n_in, unsigned n_out) {
-  return (size_t)((n_out + 7) / 8) * ((n_in + 7) / 8) * tc16::kABytes;
+  const unsigned si = gf16_tc_stage_inputs();
+  return (size_t)((n_out + 7) / 8) * ((n_in + si - 1) / si) * tc16::kABytes;
 }
 
 cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned n_in, unsigned n_out,
                                   uint8_t* d_aexp, cudaStream_t s) {
-  const unsigned n_stages = (n_in + 7) / 8;
+  const unsigned si = gf16_tc_stage_inputs();
+  const unsigned n_stages = (n_in + si - 1) / si;
   const size_t tiles = (size_t)((n_out + 7) / 8) * n_stages;
   if (!tiles) return cudaSuccess;
   if (cudaError_t e = tc16::qtab_on(s)) return e;
   unsigned blocks = (unsigned)std::min<size_t>(tiles, 148 * 32);
-  tc16::k_gf16_tc_expand_coeffs<<<blocks, 128, 0, s>>>(d_coeffs, ldc, n_in, n_out, n_stages, d_aexp);
+  if (gf16_tc_use_f4())
+    tc16f4::k_gf16_f4_expand_coeffs<<<blocks, 128, 0, s>>>(d_coeffs, ldc, n_in, n_out, n_stages, d_aexp);
+  else
+    tc16::k_gf16_tc_expand_coeffs<<<blocks, 128, 0, s>>>(d_coeffs, ldc, n_in, n_out, n_stages, d_aexp);
   note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStream_t s) {
   static std::atomic<uint64_t> attr{0};
+  const bool f4 = gf16_tc_use_f4();
   if (!device_done(attr)) {
-    cudaError_t e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         tc16::Shape<1>::kSmemBytes);
+    cudaError_t e = f4 ? cudaFuncSetAttribute(tc16f4::k_gf16_muladd_f4<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              tc16f4::Shape<1>::kSmemBytes)
+                       : cudaFuncSetAttribute(tc16::k_gf16_muladd_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              tc16::Shape<1>::kSmemBytes);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(tc16::k_gf16_muladd_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               tc16::Shape<2>::kSmemBytes);
+      e = f4 ? cudaFuncSetAttribute(tc16f4::k_gf16_muladd_f4<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    tc16f4::Shape<2>::kSmemBytes)
+             : cudaFuncSetAttribute(tc16::k_gf16_muladd_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    tc16::Shape<2>::kSmemBytes);
     if (e != cudaSuccess) return e;
     device_mark(attr);
   }
@@ -503,12 +919,14 @@ cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStr
   int kg = 2;
   for (uint32_t j = 0; j < b.n_jobs; j++)
     if (b.job[j].n_out && b.job[j].slice_bytes && b.job[j].n_in && (b.job[j].n_out + 7) / 8 % 2) kg = 1;
-  const size_t words = kg == 2 ? tc16::Shape<2>::kWords : tc16::Shape<1>::kWords;
+  const size_t words = f4 ? (kg == 2 ? tc16f4::Shape<2>::kWords : tc16f4::Shape<1>::kWords)
+                          : (kg == 2 ? tc16::Shape<2>::kWords : tc16::Shape<1>::kWords);
+  const unsigned si = gf16_tc_stage_inputs();
   uint32_t m = 0;
   for (uint32_t j = 0; j < b.n_jobs; j++) {
     Gf16TcJob& J = b.job[j];
     if (!J.n_out || !J.slice_bytes) continue;
-    J.n_stages = (J.n_in + 7) / 8;
+    J.n_stages = (J.n_in + si - 1) / si;
     if (!J.a_stride) J.a_stride = J.n_stages;
     J.groups = (J.n_out + 7) / 8 / (unsigned)kg;  // output tiles of a CTA: groups (kg = 1) or group pairs
     const size_t wt = ceil_div((J.slice_bytes + 1) / 2, words);
@@ -534,7 +952,11 @@ cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStr
     note_launch();
     if (e != cudaSuccess) return e;
   }
-  if (kg == 2)
+  if (f4 && kg == 2)
+    tc16f4::k_gf16_muladd_f4<2><<<(unsigned)ctas, tc16f4::kThreads, tc16f4::Shape<2>::kSmemBytes, s>>>(b, d_status);
+  else if (f4)
+    tc16f4::k_gf16_muladd_f4<1><<<(unsigned)ctas, tc16f4::kThreads, tc16f4::Shape<1>::kSmemBytes, s>>>(b, d_status);
+  else if (kg == 2)
     tc16::k_gf16_muladd_tc<2><<<(unsigned)ctas, tc16::kThreads, tc16::Shape<2>::kSmemBytes, s>>>(b, d_status);
   else
     tc16::k_gf16_muladd_tc<1><<<(unsigned)ctas, tc16::kThreads, tc16::Shape<1>::kSmemBytes, s>>>(b, d_status);

@@ -62,11 +62,14 @@ cudaError_t launch_gf16_muladd(const uint8_t* d_in, size_t in_stride, unsigned n
                                const uint16_t* d_coeffs, size_t ldc, unsigned n_out, uint8_t* d_out,
                                size_t out_stride, bool accumulate, int sms, cudaStream_t s);
 
-// Tensor-core (tcgen05, kind::i8) variant.  launch_gf16_tc_expand builds
+// Tensor-core (tcgen05, kind::mxf4 or kind::i8) variant.  launch_gf16_tc_expand builds
 // the coefficient bit-matrix tiles (gf16_tc_coeff_bytes(n_in, n_out) bytes)
 // that launch_gf16_muladd_tc consumes; *d_status is set nonzero if a bounded
 // device wait timed out.
 size_t gf16_tc_coeff_bytes(unsigned n_in, unsigned n_out);
+// inputs per stage of the tiles (8: int8 operands; 16: block-scaled FP4,
+// the default; fixed for the process)
+unsigned gf16_tc_stage_inputs();
 cudaError_t launch_gf16_tc_expand(const uint16_t* d_coeffs, size_t ldc, unsigned n_in, unsigned n_out,
                                   uint8_t* d_aexp, cudaStream_t s);
 cudaError_t launch_gf16_muladd_tc(const uint8_t* d_in, size_t in_stride, unsigned n_in, size_t slice_bytes,

@@ -89,14 +89,18 @@ def _mixed_jobs(rng):
     return jobs, checks
 
 
-def test_mixed_batch_matches_single_jobs():
+@pytest.mark.parametrize("graph", [True, False])
+def test_mixed_batch_matches_single_jobs(graph):
+    """Replayed from its CUDA graph, or (graph=False, jobs seen once) built
+    without the eager run and capture and issued directly at run()."""
     from parparpar_b200 import batch as B
     import torch
     rng = np.random.default_rng(7)
     jobs, checks = _mixed_jobs(rng)
     torch.cuda.synchronize()  # inputs were written on torch's stream; the library uses its own
-    b = B.Batch(jobs)
-    assert b.launches >= 3
+    b = B.Batch(jobs, graph=graph)
+    if graph:
+        assert b.launches >= 3
     for rep in range(2):  # graph replays
         b.run()
         b.ctx.synchronize()
