@@ -943,7 +943,8 @@ cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStr
   }
   b.n_jobs = m;
   if (!m) return cudaGetLastError();
-  const uint64_t ctas = tc_batch_plan(b, tc16::tiles16, sms);
+  // FP4: at most 16,384 stages (262,144 inputs) per item, so a count stays below 16 * 2^18 < 2^23
+  const uint64_t ctas = tc_batch_plan(b, tc16::tiles16, sms, f4 ? 16384u : 0u);
   if (ctas > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
   for (uint32_t j = 0; j < m; j++) {
     const Gf16TcJob& J = b.job[j];

@@ -38,6 +38,7 @@
 // returns.
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 
 #include "pp_common.cuh"
 #include "pp_internal.h"
@@ -582,6 +583,307 @@ static uint64_t tiles64(const Gf64TcJob& j) { return (uint64_t)j.pairs * j.wt; }
 
 }  // namespace tc64
 
+// ============================================================================
+// The GF(2^64) product on the block-scaled FP4 path (tcgen05.mma kind::mxf4),
+// one CTA per tile.  As in the GF(2^16) FP4 kernel (gf16_tc.cu): e2m1
+// operands 0 / 1.0 (nibbles 0x0 / 0x2), ue8m0 scale factors 1.0, exact fp32
+// counts (an item sums at most 65,536 inputs: counts < 64 * 2^16 = 2^22), the
+// parity read as the lowest mantissa bit of count + 2^23.  Four bits of each
+// 32-bit half of a word are picked per shift:
+//   B[w][(j, ii, half, m)]     = bit (32 half + 4m + j) of x_ii[w]
+//   A[(o,b)][(j, ii, half, m)] = bit (32 half + 4m + j) of Q_{o,ii,b}
+// (Q = row b of the multiplication matrix, the closed form above).  A stage is
+// 4 inputs: K = 256 elements = one 128-byte swizzled row; the 64-element MMA
+// step j covers 32 bytes: inputs 0-1 in its first 16-byte chunk, 2-3 in the
+// second, (lo half, hi half) as two 32-bit words per input.
+//
+// CTA tile: 2 outputs (M = 128) x 480 words (two accumulators of N = 240 on
+// the two halves of the B tile); TMEM columns 0-239 and 256-495, scale
+// factors in 240-255.  Builders (warps 2-9): the A rows of the stage's 4
+// coefficients per output row (two (row, input) pairs per thread) and the B
+// rows of up to two words per thread; then the epilogue.
+namespace tc64f4 {
+using namespace pp::tc;
+PP_D uint64_t mul_matrix_row_f4(uint64_t c, unsigned b) { return tc64::mul_matrix_row(c, b); }
+
+constexpr int kN = 240;
+constexpr int kWords = 2 * kN;
+constexpr int kStageIn = 4;
+constexpr int kABytes = 128 * 128;               // 16 KiB
+constexpr int kBBytes = kWords * 128;            // 60 KiB
+constexpr int kRawBytes = kStageIn * kWords * 8;  // 15 KiB
+constexpr int kLd = 4;
+constexpr int kBs = 2;
+constexpr int kThreads = 320;
+constexpr int kExp = 256;
+constexpr int kOffA = 0;
+constexpr int kOffB = kBs * kABytes;
+constexpr int kOffRaw = kOffB + kBs * kBBytes;
+constexpr int kOffBar = kOffRaw + kLd * kRawBytes;
+constexpr int kSmemBytes = kOffBar + 256 + 1024;
+constexpr uint32_t kMaxStagesPerItem = 16384;  // 65,536 inputs
+constexpr uint32_t kSfaCol = 240, kSfbCol = 248;
+static_assert(kSmemBytes <= 227 * 1024, "shared memory");
+static_assert(kOffB % 1024 == 0 && kBBytes % 1024 == 0 && (kN * 128) % 1024 == 0, "swizzle atoms");
+constexpr uint32_t kIdesc = (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
+
+PP_D void mma_f4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate, uint32_t sfa, uint32_t sfb) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %3, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %6, [%4], [%5], p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(accumulate), "r"(sfa), "r"(sfb), "r"(kIdesc)
+      : "memory");
+}
+PP_D uint32_t pick4(uint32_t p, int j) { return ((p >> j) & 0x11111111u) << 1; }
+
+__global__ void __launch_bounds__(kThreads, 1)
+k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ status) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t base_s = smem_addr(smem_raw);
+  const uint32_t pad = ((base_s + 1023) & ~1023u) - base_s;
+  uint8_t* smem = smem_raw + pad;
+  const uint32_t sA = base_s + pad + kOffA, sB = base_s + pad + kOffB, sRaw = base_s + pad + kOffRaw;
+  const uint32_t bar0 = smem_addr(smem + kOffBar);
+  enum {
+    RAW_FULL = 0,
+    RAW_EMPTY = RAW_FULL + kLd,
+    OP_FULL = RAW_EMPTY + kLd,
+    OP_EMPTY = OP_FULL + kBs,
+    D_FULL = OP_EMPTY + kBs,
+    DONE = D_FULL + 1,
+    NBARS = DONE + 1
+  };
+  static_assert(8 * NBARS + 16 <= 256, "barrier area");
+  auto BAR = [&](int k) { return bar0 + 8u * (uint32_t)k; };
+  volatile uint32_t* tmem_holder = reinterpret_cast<volatile uint32_t*>(smem + kOffBar + 8 * NBARS);
+  volatile int* err = reinterpret_cast<volatile int*>(smem + kOffBar + 8 * NBARS + 8);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NBARS; k++) {
+      const bool by_expanders = (k >= RAW_EMPTY && k < RAW_EMPTY + kLd) || (k >= OP_FULL && k < OP_FULL + kBs);
+      mbar_init(BAR(k), by_expanders ? (uint32_t)kExp : 1u);
+    }
+    *err = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr((const void*)tmem_holder)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_holder;
+  if (warp >= 2 && warp < 6) {
+    // scale factors 1.0 (ue8m0 0x7F) in columns 240-255 of this warp's lane quarter
+    const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + kSfaCol;
+    const uint32_t v = 0x7F7F7F7Fu;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(t),
+        "r"(v)
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const TcSeg sg = tc_item(&batch, blockIdx.x);
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      uint32_t g = 0;
+      do {
+        const Gf64TcJob J = pinned_job(batch.job[sg.job]);
+        const size_t w0 = (size_t)(sg.tile / J.pairs) * kWords;
+        const unsigned words_valid = (unsigned)min((size_t)kWords, J.words - w0);
+        const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
+        for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
+          const unsigned sl = g % kLd;
+          if (g >= (uint32_t)kLd && !mbar_wait(BAR(RAW_EMPTY + sl), (g / kLd - 1) & 1)) {
+            *err = 1;
+            break;
+          }
+          const unsigned i0 = st * kStageIn;
+          const unsigned ni = min((unsigned)kStageIn, J.n_in - i0);
+          mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
+          for (unsigned ii = 0; ii < ni; ii++) {
+            const uint64_t* row = J.in_ptrs ? J.in_ptrs[i0 + ii] : J.in + (size_t)(i0 + ii) * J.in_stride;
+            bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 8), row + w0, raw_copy, BAR(RAW_FULL + sl));
+          }
+        }
+      } while (0);
+      if (*err) {
+        for (uint32_t k = g > (uint32_t)kLd ? g - kLd : 0; k < g; k++)
+          mbar_wait(BAR(RAW_FULL + k % kLd), (k / kLd) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t sfa = tmem + kSfaCol, sfb = tmem + kSfbCol;
+      for (unsigned k = 0; k < sg.st1 - sg.st0; k++) {
+        const unsigned bs = k % kBs;
+        if (*err || !mbar_wait(BAR(OP_FULL + bs), (k / kBs) & 1)) {
+          *err = 1;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+#pragma unroll
+          for (int nn = 0; nn < 2; nn++) {
+            mma_f4(tmem + nn * 256, sw128_desc(sA + bs * kABytes + 32 * kk),
+                   sw128_desc(sB + bs * kBBytes + nn * (kN * 128) + 32 * kk), (k > 0 || kk > 0) ? 1u : 0u, sfa,
+                   sfb);
+          }
+        }
+        mma_commit(BAR(OP_EMPTY + bs));
+      }
+      if (!*err) mma_commit(BAR(D_FULL));
+      mma_commit(BAR(DONE));
+      if (!mbar_wait(BAR(DONE), 0)) *err = 1;
+    }
+  } else {
+    // ------------------------------------------------------------ operand builders
+    const int e = threadIdx.x - 64;  // 0..255
+    // A: row a_m, inputs a_ii and a_ii + 2 (adjacent threads alternate a_ii, so
+    // a 64-bit store phase of 16 threads covers 8 rows x both halves of a chunk)
+    const unsigned a_ii = e & 1, a_m = e >> 1, a_oo = a_m >> 6, a_b = a_m & 63;
+    const uint32_t arow = (a_m >> 3) * 1024 + (a_m & 7) * 128 + 8 * a_ii, ar7 = a_m & 7;
+    const int q = warp & 3;
+    const int chalf = (warp - 2) >> 2;
+    do {
+      const Gf64TcJob J = pinned_job(batch.job[sg.job]);
+      const unsigned o0 = 2 * (unsigned)(sg.tile % J.pairs);
+      const size_t w0 = (size_t)(sg.tile / J.pairs) * kWords;
+      const unsigned words_valid = (unsigned)min((size_t)kWords, J.words - w0);
+      const unsigned nst = sg.st1 - sg.st0;
+      auto coef = [&](unsigned k, unsigned ii) -> uint64_t {
+        const unsigned o = o0 + a_oo, i = (sg.st0 + k) * kStageIn + ii;
+        return (k < nst && o < J.n_out && i < J.n_in) ? J.coeff[(size_t)o * J.ldc + i] : 0ull;
+      };
+      uint64_t c0 = coef(0, a_ii), c1 = coef(0, a_ii + 2);
+      for (unsigned k = 0; k < nst; k++) {
+        const unsigned sl = k % kLd, bs = k % kBs;
+        const uint64_t n0 = coef(k + 1, a_ii), n1 = coef(k + 1, a_ii + 2);  // next stage's coefficients
+        const uint64_t q0 = mul_matrix_row_f4(c0, a_b), q1 = mul_matrix_row_f4(c1, a_b);
+        if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
+          *err = 1;
+          break;
+        }
+        const unsigned i0 = (sg.st0 + k) * kStageIn;
+        const unsigned ni = min((unsigned)kStageIn, J.n_in - i0);
+        // B rows e and e + 240: the 4 inputs' words as (lo, hi) pairs
+        uint32_t xw[2][8];
+#pragma unroll
+        for (int rr = 0; rr < 2; rr++) {
+          const unsigned u = (unsigned)e + rr * kN;
+          const bool ok = e < kN && u < words_valid;
+#pragma unroll
+          for (int ii = 0; ii < kStageIn; ii++) {
+            uint2 v = make_uint2(0, 0);
+            if (ok && (unsigned)ii < ni) v = lds64(sRaw + sl * kRawBytes + ii * (kWords * 8) + 8 * u);
+            xw[rr][2 * ii] = v.x;
+            xw[rr][2 * ii + 1] = v.y;
+          }
+        }
+        mbar_arrive(BAR(RAW_EMPTY + sl));
+        if (k >= (unsigned)kBs && !mbar_wait(BAR(OP_EMPTY + bs), (k / kBs - 1) & 1)) {
+          *err = 1;
+          break;
+        }
+        const uint32_t at = sA + bs * kABytes, bt = sB + bs * kBBytes;
+        const uint32_t q0lo = (uint32_t)q0, q0hi = (uint32_t)(q0 >> 32), q1lo = (uint32_t)q1,
+                       q1hi = (uint32_t)(q1 >> 32);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          // A: input a_ii in chunk 2j, input a_ii + 2 in chunk 2j + 1, at byte 8 a_ii
+          sts64(at + arow + (((2 * j) ^ ar7) << 4), pick4(q0lo, j), pick4(q0hi, j));
+          sts64(at + arow + (((2 * j + 1) ^ ar7) << 4), pick4(q1lo, j), pick4(q1hi, j));
+        }
+        if (e < kN) {
+#pragma unroll
+          for (int rr = 0; rr < 2; rr++) {
+            const unsigned u = (unsigned)e + rr * kN;
+            const uint32_t brow = bt + (u >> 3) * 1024 + (u & 7) * 128, br7 = u & 7;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              sts128(brow + (((2 * j) ^ br7) << 4), pick4(xw[rr][0], j), pick4(xw[rr][1], j), pick4(xw[rr][2], j),
+                     pick4(xw[rr][3], j));
+              sts128(brow + (((2 * j + 1) ^ br7) << 4), pick4(xw[rr][4], j), pick4(xw[rr][5], j),
+                     pick4(xw[rr][6], j), pick4(xw[rr][7], j));
+            }
+          }
+        }
+        fence_async_smem();
+        mbar_arrive(BAR(OP_FULL + bs));
+        c0 = n0;
+        c1 = n1;
+      }
+      // ---------------------------------------------------------- epilogue
+      if (*err || !mbar_wait(BAR(D_FULL), 0)) {
+        *err = 1;
+        break;
+      }
+      tc_fence_after();
+      const unsigned o = o0 + (q >> 1);  // output of these rows
+      const unsigned half = q & 1;       // bits [32*half, 32*half + 32)
+      uint64_t* orow = o < J.n_out ? (J.out_ptrs ? J.out_ptrs[o] : J.out + (size_t)o * J.out_stride) : nullptr;
+      for (int cc = 0; cc < (kN + 31) / 32; cc++) {
+        uint32_t r[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + 256 * chalf + 32 * cc, r);
+        uint32_t mine = 0;
+#pragma unroll
+        for (int jj = 0; jj < 32; jj++) {
+          const uint32_t bit = __float_as_uint(__fadd_rn(__uint_as_float(r[jj]), 8388608.0f)) & 1u;
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
+          if (lane == jj) mine = bal;
+        }
+        const unsigned col = 32 * cc + lane;
+        const unsigned widx = (unsigned)chalf * kN + col;
+        if (!orow || col >= (unsigned)kN || widx >= words_valid) continue;
+        uint32_t* dst = reinterpret_cast<uint32_t*>(orow + w0 + widx) + half;
+        if (sg.mode == 2) {
+          if (mine) atomicXor(dst, mine);
+        } else if (sg.mode == 1) {
+          *dst ^= mine;
+        } else {
+          *dst = mine;
+        }
+      }
+      tc_fence_before();
+    } while (0);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+  if (threadIdx.x == 0 && *err) atomicOr(status, 1);
+}
+
+}  // namespace tc64f4
+
+// GF(2^64) tensor-core path: the FP4 one-CTA kernel unless
+// PARPAR_B200_GF64_TC=i8 selects the int8 kernels (pair / one-CTA); fixed
+// per process for reproducible timings.
+static bool gf64_tc_use_f4() {
+  static const bool f4 = [] {
+    const char* v = getenv("PARPAR_B200_GF64_TC");
+    return !(v && strcmp(v, "i8") == 0);
+  }();
+  return f4;
+}
+
 // Pair kernel (two SMs per tile) or one-CTA kernel for a whole table: the
 // pair kernel's tile has 4 outputs, so it is used when no job has fewer than
 // 4 (PARPAR_B200_GF64_PAIR=0 / 1 forces the choice).
@@ -604,18 +906,24 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(tc64::k_gf64_matvec_tc_pair<tc64::kPLd, tc64::kPBs>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, tc64::kPSmemBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(tc64f4::k_gf64_matvec_f4, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc64f4::kSmemBytes);
     if (e != cudaSuccess) return e;
     device_mark(attr);
   }
-  const bool pair = use_pair_kernel(b);
+  const bool f4 = gf64_tc_use_f4();
+  const bool pair = !f4 && use_pair_kernel(b);
+  const size_t tile_words = f4 ? tc64f4::kWords : tc64::kWords;
+  const unsigned stage_in = f4 ? tc64f4::kStageIn : tc64::kStageIn;
   // drop empty jobs (nothing to multiply) after zeroing their outputs
   uint32_t m = 0;
   for (uint32_t j = 0; j < b.n_jobs; j++) {
     Gf64TcJob& J = b.job[j];
     if (!J.n_out || !J.words) continue;
-    J.n_stages = (J.n_in + tc64::kStageIn - 1) / tc64::kStageIn;
+    J.n_stages = (J.n_in + stage_in - 1) / stage_in;
     J.pairs = pair ? (J.n_out + 3) / 4 : (J.n_out + 1) / 2;
-    const size_t wt = ceil_div(J.words, tc64::kWords);
+    const size_t wt = ceil_div(J.words, tile_words);
     if (wt > 0xFFFFFFFFu) return cudaErrorInvalidValue;
     J.wt = (uint32_t)wt;
     if (!J.n_in) {
@@ -634,7 +942,8 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
   b.n_jobs = m;
   if (!m) return cudaGetLastError();
   // the plan deals items to SMs, or to SM pairs for the pair kernel
-  const uint64_t items = tc_batch_plan(b, tc64::tiles64, pair ? std::max(1, sms / 2) : sms);
+  const uint64_t items = tc_batch_plan(b, tc64::tiles64, pair ? std::max(1, sms / 2) : sms,
+                                      f4 ? tc64f4::kMaxStagesPerItem : 0u);
   if (items > 0x3FFFFFFFull) return cudaErrorInvalidConfiguration;
   for (uint32_t j = 0; j < m; j++) {
     const Gf64TcJob& J = b.job[j];
@@ -647,7 +956,9 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     }
     note_launch();
   }
-  if (pair)
+  if (f4)
+    tc64f4::k_gf64_matvec_f4<<<(unsigned)items, tc64f4::kThreads, tc64f4::kSmemBytes, s>>>(b, d_status);
+  else if (pair)
     tc64::k_gf64_matvec_tc_pair<tc64::kPLd, tc64::kPBs>
         <<<2 * (unsigned)items, tc64::kThreads, tc64::kPSmemBytes, s>>>(b, d_status);
   else

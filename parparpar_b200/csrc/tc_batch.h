@@ -82,8 +82,12 @@ static_assert(sizeof(Gf16TcBatch) < 4000 && sizeof(Gf64TcBatch) < 4000, "job tab
 // pipeline-fill cost.
 constexpr uint64_t kTcItemOverhead = 8;
 
+// max_per: at most this many stages per item (0: no limit) -- an fp32
+// accumulator counts exactly only up to 2^24, so the FP4 kernels bound the
+// inputs one item sums
 template <class Job>
-inline void tc_set_splits(Job& J, uint32_t splits) {
+inline void tc_set_splits(Job& J, uint32_t splits, uint32_t max_per = 0) {
+  if (max_per && splits < (J.n_stages + max_per - 1) / max_per) splits = (J.n_stages + max_per - 1) / max_per;
   if (splits < 1) splits = 1;
   if (splits > J.n_stages) splits = J.n_stages;
   J.per = (J.n_stages + splits - 1) / splits;
@@ -128,7 +132,7 @@ inline uint64_t tc_batch_estimate(TcBatch<Job>& b, uint64_t tiles_of(const Job&)
 // Choose every job's split count (one target item length for the whole
 // table), fill prefix/total and return the grid size (one CTA per item).
 template <class Job>
-inline uint64_t tc_batch_plan(TcBatch<Job>& b, uint64_t tiles_of(const Job&), int sms) {
+inline uint64_t tc_batch_plan(TcBatch<Job>& b, uint64_t tiles_of(const Job&), int sms, uint32_t max_per = 0) {
   const unsigned ctas = (unsigned)(sms > 0 ? sms : 148);
   uint32_t smax = 1;
   for (uint32_t j = 0; j < b.n_jobs; j++) smax = std::max(smax, b.job[j].n_stages);
@@ -138,7 +142,7 @@ inline uint64_t tc_batch_plan(TcBatch<Job>& b, uint64_t tiles_of(const Job&), in
   for (uint32_t d = 1; d <= 256 && !b.q_hint; d++) {
     const uint32_t q = (smax + d - 1) / d;  // target stages per item
     if (d > 1 && q == (smax + d - 2) / (d - 1)) continue;
-    for (uint32_t j = 0; j < b.n_jobs; j++) tc_set_splits(b.job[j], (b.job[j].n_stages + q - 1) / q);
+    for (uint32_t j = 0; j < b.n_jobs; j++) tc_set_splits(b.job[j], (b.job[j].n_stages + q - 1) / q, max_per);
     const uint64_t est = tc_batch_estimate(b, tiles_of, ctas, load);
     if (est < best) {
       best = est;
@@ -148,7 +152,8 @@ inline uint64_t tc_batch_plan(TcBatch<Job>& b, uint64_t tiles_of(const Job&), in
   }
   if (b.q_hint) best_q = b.q_hint;
   b.q_hint = best_q;
-  for (uint32_t j = 0; j < b.n_jobs; j++) tc_set_splits(b.job[j], (b.job[j].n_stages + best_q - 1) / best_q);
+  for (uint32_t j = 0; j < b.n_jobs; j++)
+    tc_set_splits(b.job[j], (b.job[j].n_stages + best_q - 1) / best_q, max_per);
   b.total = 0;
   for (uint32_t j = 0; j < b.n_jobs; j++) {
     b.prefix[j] = b.total;

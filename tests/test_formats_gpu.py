@@ -1,0 +1,68 @@
+"""Both operand formats of the tensor-core region kernels against the oracle.
+
+The GF(2^16) and GF(2^64) tensor-core products run on the block-scaled FP4
+path (tcgen05 kind::mxf4) by default; the int8 path (kind::i8) stays
+selectable per process (PARPAR_B200_GF16_TC=i8, PARPAR_B200_GF64_TC=i8),
+because resident GF(2^16) coefficient tiles are laid out for one format.  The
+rest of the suite exercises the default; this file runs the same parity
+cases in a child process for each format, so both stay bit-exact.  Integer GF
+words: exact comparisons.
+"""
+import os
+import subprocess
+import sys
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+CHILD = r'''
+import sys
+import numpy as np
+sys.path.insert(0, ROOT)
+sys.path.insert(0, ROOT + "/oracle")
+import oracle as orc
+import parparpar_b200 as pp
+import parparpar_b200._lib as L
+from parparpar_b200 import par2, par3
+O = orc.Oracle()
+ctx = pp.Context(0)
+ctx.set_gf16_kernel(L.PP_GF16_KERNEL_TENSOR)
+ctx.set_gf64_kernel(L.PP_GF16_KERNEL_TENSOR)
+par3.GF64Controller.ctx = ctx
+rng = np.random.default_rng(2027)
+# GF(2^16): one-group and two-group tiles, odd slices, ragged stages, an
+# accumulating product, tile edges of both formats (240/256/480/512 words)
+for n, s, r in [(16, 480, 8), (17, 961, 16), (40, 4001, 8), (33, 20000, 16), (300, 8192, 24), (9, 1026, 40)]:
+    data = rng.integers(0, 256, (n, s), dtype=np.uint8)
+    exps = list(range(r))
+    want = O.par2_muladd(list(data), s, O.par2_coeff_matrix(np.arange(n), exps))
+    assert np.array_equal(par2.par2_create(data, np.arange(n), exps, ctx=ctx), want), ("gf16", n, s, r)
+    co = rng.integers(0, 65536, (r, n)).astype(np.uint16)
+    base = rng.integers(0, 256, (r, s), dtype=np.uint8)
+    out = base.copy()
+    par2.gf16_muladd(data, co, out=out, accumulate=True, ctx=ctx)
+    assert np.array_equal(out, base ^ O.par2_muladd(list(data), s, co)), ("gf16 acc", n, s, r)
+# GF(2^64): tile edges (480/512 words), ragged stages, accumulate
+for N, W, R in [(4, 480, 2), (5, 482, 3), (33, 1000, 8), (64, 96, 5), (200, 2048, 16)]:
+    x = rng.integers(0, 2**64, (N, W), dtype=np.uint64)
+    want = O.gf64_compute_recovery(x, R, 0, N)
+    got = np.zeros((R, W), dtype=np.uint64)
+    par3.GF64Controller.ComputeRecoveryBlocks(x, N, got, R, W, 0, N)
+    assert np.array_equal(got, want), ("gf64", N, W, R)
+    acc = rng.integers(0, 2**64, (R, W), dtype=np.uint64)
+    got = acc.copy()
+    par3.GF64Controller.ComputeRecoveryBlocks(x, N, got, R, W, 0, N, accumulate=True)
+    assert np.array_equal(got, acc ^ want), ("gf64 acc", N, W, R)
+print("formats ok")
+'''
+
+
+@pytest.mark.parametrize("fmt", ["f4", "i8"])
+def test_tensor_core_formats_against_the_oracle(fmt):
+    env = dict(os.environ, PARPAR_B200_GF16_TC=fmt, PARPAR_B200_GF64_TC=fmt)
+    code = f"ROOT = {ROOT!r}\n" + CHILD
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "formats ok" in r.stdout, (r.stdout[-2000:], r.stderr[-2000:])
