@@ -786,6 +786,43 @@ def measure_serving(ctx, dev, count=32, seed=5, budget=120 * 10**9):
             "outputs_identical": bool(same)}
 
 
+def measure_fenger_estimate(ctx, timer, dev, dense_ms):
+    """The Fenger route for PAR3 R=1,024 (131,072 inputs) costed from
+    measured device pieces.  Per block word, the reference's interpolation
+    (gf64/gf64_fenger.c:524-590) walks the 17 levels of the subproduct tree;
+    at level l its 2^l nodes each multiply two polynomial pairs of output
+    size n = N / 2^l (the tree polynomials' transforms can be kept, so a
+    product is one forward transform, one pointwise product and one inverse
+    transform of size n).  Measured here on 1,024 words at once: the additive
+    FFT of the 1 GiB array (n = N) and the pointwise GF(2^64) product; a level
+    is charged 2 x (2 FFT x log2(n) / log2(N) + pointwise).  The evaluation
+    on the 1,024-point tree and the final division are left out, so the
+    estimate is a lower bound of the route's device time."""
+    import math
+
+    import torch
+    from parparpar_b200 import par3
+    N, batch = 131072, 1024
+    g = torch.Generator(device=f"cuda:{dev}")
+    g.manual_seed(17)
+    a = torch.randint(-2**63, 2**63 - 1, (N, batch), dtype=torch.int64, device=f"cuda:{dev}", generator=g)
+    b = torch.randint(-2**63, 2**63 - 1, (N, batch), dtype=torch.int64, device=f"cuda:{dev}", generator=g)
+    torch.cuda.synchronize()
+    fft = lambda: par3.gf64_addfft64_fwd(a, N, batch, batch, ctx=ctx)
+    pw = lambda: par3.mul_arr(a, a, b, N * batch, N * batch, ctx=ctx)
+    fft()
+    pw()
+    t_fft = timer.run(fft, 3)
+    t_pw = timer.run(pw, 3)
+    L = int(math.log2(N))
+    est = sum(2 * (2 * t_fft * math.log2(N >> lev) / L + t_pw) for lev in range(L))
+    del a, b
+    torch.cuda.empty_cache()
+    return {"workload": "par3_create_131072x8KiB_R1024 via Fenger (estimate)", "fft_ms_1GiB": t_fft,
+            "pointwise_ms_1GiB": t_pw, "fenger_interp_lower_bound_ms": est, "dense_tensor_core_ms": dense_ms,
+            "fenger_over_dense": est / dense_ms if dense_ms else None}
+
+
 def measure_fused(ctx, dev):
     """End to end with pinned host inputs (1 GiB): each create with and
     without the hashes of its inputs computed in the same pass, and the PAR3
@@ -1113,6 +1150,11 @@ def main():
                 r8[e["workload"]] = {"gbps": round(e["value"], 1), "hbm_frac_of_measured": round(e["hbm_frac"], 4),
                                      "kernel_ms": round(e["kernel_ms"], 4)}
         line["r8"] = r8
+        dense = next((e.get("kernel_ms") for e in sec if e.get("workload") == "par3_create_131072x8KiB_R1024"), None)
+        try:
+            line["fenger_estimate"] = measure_fenger_estimate(ctx, timer, local, dense)
+        except Exception as e:  # report, keep the primary line
+            line["fenger_estimate"] = {"error": str(e)[:200]}
 
     if rank == 0 and world == 1 and not args.no_secondary:
         try:
