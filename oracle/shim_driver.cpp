@@ -47,7 +47,8 @@ struct Procs {
 template <class AddFn>
 int run(size_t slice, size_t split, int device, int threads, unsigned numInputs, unsigned numOutputs,
         const uint16_t* exps, uint8_t* out, AddFn add) {
-	if (split > slice || (split & 1)) return -2;  // the controller splits on 16-bit word boundaries
+	// the controller splits on 16-bit word boundaries (an odd split only at the slice's end)
+	if (split > slice || ((split & 1) && split != slice)) return -2;
 	Procs P(slice, split, device, threads);
 	if (!P.ok) return -3;
 	PAR2Proc par2;

@@ -84,6 +84,7 @@ struct CauchyEntry {
   size_t n_in, n_rec;
   uint64_t fI, fR;
   uint64_t* d;
+  size_t cap;  // bytes of the allocation (a reused buffer may be larger than the matrix)
 };
 
 // Resident PAR2 coefficient table: the coefficient matrix of (input slice
@@ -107,6 +108,7 @@ struct pp_ctx {
   void* slot_p[S_NSLOTS] = {};
   size_t slot_n[S_NSLOTS] = {};
   std::list<CauchyEntry> cauchy;  // LRU, front = most recent
+  std::vector<std::pair<void*, size_t>> cauchy_spare;  // evicted matrices' buffers, reused in stream order
   std::list<Par2Entry> par2;      // LRU, front = most recent
   std::deque<size_t> par2_seen;   // hashes of recent PAR2 keys without a table
   int gf16_kernel = PP_GF16_KERNEL_AUTO;
@@ -225,6 +227,7 @@ static void* scratch(pp_ctx* ctx, Slot s, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (ctx->slot_n[s] >= bytes) return ctx->slot_p[s];
   PP_TRACE("scratch-grow", bytes);
+  const size_t prev_n = ctx->slot_n[s];
   if (ctx->slot_p[s]) {
     PP_TRACE("scratch-free", ctx->slot_n[s]);
     cudaStreamSynchronize(ctx->stream);
@@ -232,7 +235,9 @@ static void* scratch(pp_ctx* ctx, Slot s, size_t bytes) {
     ctx->slot_p[s] = nullptr;
     ctx->slot_n[s] = 0;
   }
-  size_t n = bytes + bytes / 8;  // some headroom against regrowth
+  // headroom against regrowth: at least twice the previous size, so a stream
+  // of growing jobs reallocates (synchronises and frees) O(log) times
+  size_t n = std::max(bytes + bytes / 8, 2 * prev_n);
   n = (n + 255) & ~(size_t)255;
   void* p = nullptr;
   PP_TRACE("scratch-malloc", n);
@@ -366,6 +371,8 @@ PP_API int pp_ctx_free_cache(pp_ctx* ctx) {
   }
   for (auto& e : ctx->cauchy) cudaFree(e.d);
   ctx->cauchy.clear();
+  for (auto& e : ctx->cauchy_spare) cudaFree(e.first);
+  ctx->cauchy_spare.clear();
   for (auto& e : ctx->par2) {
     cudaFree(e.d_coef);
     cudaFree(e.d_aexp);
@@ -1470,21 +1477,48 @@ static uint64_t* cauchy_get(pp_ctx* ctx, size_t n_in, size_t n_rec, uint64_t fI,
     }
   }
   // LRU of 8 matrices, as the reference's coefficient cache (src/par3_engine.cc:451-482)
+  // An evicted matrix's buffer is kept as a spare: the next matrix is built
+  // into it on the same stream, after every kernel that read the old one, so
+  // eviction needs neither a synchronisation nor a free (a free would wait
+  // for the whole device).
   if (ctx->cauchy.size() >= 8) {
-    PP_TRACE("cauchy-evict", ctx->cauchy.back().n_in * ctx->cauchy.back().n_rec * 8);
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(ctx->cauchy.back().d);
+    ctx->cauchy_spare.push_back({ctx->cauchy.back().d, ctx->cauchy.back().cap});
     ctx->cauchy.pop_back();
   }
+  const size_t need = n_in * n_rec * 8;
   void* d = nullptr;
-  PP_TRACE("cauchy-malloc", n_in * n_rec * 8);
-  if (cudaMalloc(&d, n_in * n_rec * 8) != cudaSuccess) {
+  size_t cap = need;
+  {
+    int best = -1;  // the smallest spare that holds the matrix, if it is not more than twice as large
+    for (size_t k = 0; k < ctx->cauchy_spare.size(); k++) {
+      const size_t c = ctx->cauchy_spare[k].second;
+      if (c >= need && c <= 2 * need + (1 << 20) && (best < 0 || c < ctx->cauchy_spare[best].second)) best = (int)k;
+    }
+    if (best >= 0) {
+      d = ctx->cauchy_spare[best].first;
+      cap = ctx->cauchy_spare[best].second;
+      ctx->cauchy_spare.erase(ctx->cauchy_spare.begin() + best);
+    }
+  }
+  if (ctx->cauchy_spare.size() > 4) {  // bounded: release the oldest spares
+    PP_TRACE("cauchy-spare-free", ctx->cauchy_spare.front().second);
+    cudaStreamSynchronize(ctx->stream);
+    while (ctx->cauchy_spare.size() > 4) {
+      cudaFree(ctx->cauchy_spare.front().first);
+      ctx->cauchy_spare.erase(ctx->cauchy_spare.begin());
+    }
+  }
+  PP_TRACE("cauchy-malloc", need);
+  if (!d && cudaMalloc(&d, need) != cudaSuccess) {
     cudaGetLastError();
-    // make room: drop every cached matrix and retry once
+    // make room: drop every cached matrix and spare and retry once
     cudaStreamSynchronize(ctx->stream);
     for (auto& e : ctx->cauchy) cudaFree(e.d);
     ctx->cauchy.clear();
-    if (cudaMalloc(&d, n_in * n_rec * 8) != cudaSuccess) {
+    for (auto& e : ctx->cauchy_spare) cudaFree(e.first);
+    ctx->cauchy_spare.clear();
+    cap = need;
+    if (cudaMalloc(&d, need) != cudaSuccess) {
       cudaGetLastError();
       *st = set_err(ctx, PP_ERR_NO_MEMORY, "Cauchy matrix %zu x %zu", n_rec, n_in);
       return nullptr;
@@ -1496,7 +1530,7 @@ static uint64_t* cauchy_get(pp_ctx* ctx, size_t n_in, size_t n_rec, uint64_t fI,
     *st = set_err(ctx, PP_ERR_CUDA, "Cauchy build: %s", cudaGetErrorString(e));
     return nullptr;
   }
-  ctx->cauchy.push_front({n_in, n_rec, fI, fR, (uint64_t*)d});
+  ctx->cauchy.push_front({n_in, n_rec, fI, fR, (uint64_t*)d, cap});
   return (uint64_t*)d;
 }
 

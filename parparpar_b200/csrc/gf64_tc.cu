@@ -873,13 +873,16 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
 
 }  // namespace tc64f4
 
-// GF(2^64) tensor-core path: the FP4 one-CTA kernel unless
-// PARPAR_B200_GF64_TC=i8 selects the int8 kernels (pair / one-CTA); fixed
-// per process for reproducible timings.
+// GF(2^64) tensor-core path: the int8 kernels (SM pair / one CTA) unless
+// PARPAR_B200_GF64_TC=f4 selects the FP4 one-CTA kernel; fixed per process
+// for reproducible timings.  The int8 SM-pair kernel stays the default: on
+// the 1 GiB PAR3 creates it ran 2.58 ms (R=8) and 348 ms (R=1,024) against
+// 3.46 ms and 435 ms for the FP4 one-CTA kernel, whose builders write the B
+// tile of all 480 words per SM (the pair kernel's CTAs build half of theirs).
 static bool gf64_tc_use_f4() {
   static const bool f4 = [] {
     const char* v = getenv("PARPAR_B200_GF64_TC");
-    return !(v && strcmp(v, "i8") == 0);
+    return v && strcmp(v, "f4") == 0;
   }();
   return f4;
 }

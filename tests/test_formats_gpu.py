@@ -1,11 +1,12 @@
 """Both operand formats of the tensor-core region kernels against the oracle.
 
-The GF(2^16) and GF(2^64) tensor-core products run on the block-scaled FP4
-path (tcgen05 kind::mxf4) by default; the int8 path (kind::i8) stays
-selectable per process (PARPAR_B200_GF16_TC=i8, PARPAR_B200_GF64_TC=i8),
-because resident GF(2^16) coefficient tiles are laid out for one format.  The
-rest of the suite exercises the default; this file runs the same parity
-cases in a child process for each format, so both stay bit-exact.  Integer GF
+Each tensor-core product has two operand formats, block-scaled FP4
+(tcgen05 kind::mxf4) and int8 (kind::i8), chosen per process
+(PARPAR_B200_GF16_TC, PARPAR_B200_GF64_TC = f4 | i8; resident GF(2^16)
+coefficient tiles are laid out for one format).  The defaults are FP4 for
+GF(2^16) and int8 for GF(2^64), and the rest of the suite exercises them;
+this file runs the same parity cases in a child process with both fields on
+each format, so every kernel stays bit-exact.  Integer GF
 words: exact comparisons.
 """
 import os
