@@ -1278,8 +1278,13 @@ static int proc_submit(pp_par2_proc* p) {
                                             a.d_idx));
   // each row's memory checksum, then the products of the data rows and of
   // the checksum rows (the second launch reuses the expanded coefficient tiles)
-  CUDA_TRY(p->ctx, launch_par2_cksum(a.d_in, p->row, a.count, p->cur_size, a.d_ck, 16, nullptr, p->s_comp));
-  CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_in, p->row, a.count, p->cur_size, a.d_coeff, p->batch,
+  // An odd slice's last word is (byte, 0); the product of that word has a
+  // high byte too, which the checksum identity needs, so the internal rows
+  // are multiplied and checksummed over whole words (the staged rows are
+  // zero past the slice; getOutput copies out only the slice's bytes).
+  const size_t len_w = (p->cur_size + 1) & ~(size_t)1;
+  CUDA_TRY(p->ctx, launch_par2_cksum(a.d_in, p->row, a.count, len_w, a.d_ck, 16, nullptr, p->s_comp));
+  CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_in, p->row, a.count, len_w, a.d_coeff, p->batch,
                                n_out, p->d_out, p->row, p->has_output, p->ctx->sms, a.d_aexp, p->ctx->d_status,
                                p->s_comp));
   CUDA_TRY(p->ctx, gf16_region(p->ctx->gf16_kernel, a.d_ck, 16, a.count, 16, a.d_coeff, p->batch, n_out,
@@ -1377,8 +1382,8 @@ PP_API int pp_par2_proc_get_output(pp_par2_proc* p, unsigned index, void* output
   } else if (!p->checked) {
     // verify every output's carried checksum against its data once
     // (finish_packed_cksum, gf16/controller_cpu.cpp:423-443)
-    CUDA_TRY(p->ctx, launch_par2_cksum(p->d_out, p->row, n_out, p->cur_size, p->d_out_ck, 16, p->d_valid,
-                                       p->s_copy));
+    CUDA_TRY(p->ctx, launch_par2_cksum(p->d_out, p->row, n_out, (p->cur_size + 1) & ~(size_t)1, p->d_out_ck, 16,
+                                       p->d_valid, p->s_copy));
     p->valid.assign(n_out, 0);
     CUDA_TRY(p->ctx, cudaMemcpyAsync(p->valid.data(), p->d_valid, sizeof(int) * n_out, cudaMemcpyDeviceToHost,
                                      p->s_copy));

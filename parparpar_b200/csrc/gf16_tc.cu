@@ -502,10 +502,18 @@ constexpr int kExp = 256;
 constexpr int kN = 240;             // words per accumulator
 constexpr uint32_t kSfaCol = 240, kSfbCol = 248;
 
+// ring depths (A tiles + raw rows, B tiles); the two-group tile's can be set
+// at build time for measurements
+#ifndef PP_F4_LD2
+#define PP_F4_LD2 4
+#endif
+#ifndef PP_F4_BS2
+#define PP_F4_BS2 2
+#endif
 template <int KG>
 struct Shape {
-  static constexpr int kLd = KG == 2 ? 4 : 3;
-  static constexpr int kBs = 2;
+  static constexpr int kLd = KG == 2 ? PP_F4_LD2 : 3;
+  static constexpr int kBs = KG == 2 ? PP_F4_BS2 : 2;
   static constexpr int kWords = KG == 2 ? kN : 2 * kN;
   static constexpr int kAStage = KG * kABytes;
   static constexpr int kBBytes = kWords * 128;
@@ -604,8 +612,6 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
   const uint32_t pad = ((base_s + 1023) & ~1023u) - base_s;
   uint8_t* smem = smem_raw + pad;
   const uint32_t sA = base_s + pad + kOffA, sB = base_s + pad + kOffB, sRaw = base_s + pad + kOffRaw;
-  uint8_t* raw_p = smem + kOffRaw;
-  uint8_t* b_p = smem + kOffB;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
   const uint32_t bar0 = smem_addr(bars);
   enum {
@@ -734,7 +740,26 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
     const int e = threadIdx.x - 64;  // 0..255
     const bool odd_tail = (slice_bytes & 1) && (w0 + kWords >= total_words);
     const unsigned last_word = (unsigned)(total_words - 1 - w0);
-    constexpr int kRows = kWords <= kExp ? 1 : 2;  // word rows per thread
+    // KG = 2 (240 words): thread e < 240 builds word row e, 16-bit loads.
+    // KG = 1 (480 words): thread e < 240 builds the adjacent rows 2e, 2e+1 from
+    // one 32-bit load per input (byte permutes split the two words); threads
+    // with bit 2 of e set store their odd row first, so each 128-bit store
+    // phase of 8 threads covers eight distinct rows of a swizzle atom.
+    const unsigned n0 = KG == 2 ? (unsigned)e : 2u * (unsigned)e;
+    const unsigned sw = KG == 2 ? 0u : ((unsigned)e >> 2) & 1u;
+    const bool active = e < kN;
+    uint32_t mask = 0;
+    if (KG == 2) {
+      if (n0 < words_valid) mask = 0xFFFFu;
+      if (odd_tail && n0 == last_word) mask &= 0x00FFu;
+    } else {
+      if (n0 < words_valid) mask = 0xFFFFu;
+      if (n0 + 1 < words_valid) mask |= 0xFFFF0000u;
+      if (odd_tail) {
+        if (n0 == last_word) mask &= 0xFFFF00FFu;
+        else if (n0 + 1 == last_word) mask &= 0x00FFFFFFu;
+      }
+    }
     for (unsigned k = 0; k < nst; k++) {
       const unsigned sl = k % kLd, bs = k % kBs;
       if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
@@ -743,20 +768,24 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
       }
       const unsigned i0 = (st_begin + k) * kStageIn;
       const unsigned ni = min((unsigned)kStageIn, n_in - i0);
-      const uint8_t* raw = raw_p + sl * kRawBytes;
-      uint32_t P[kRows][8];
+      // explicit shared-memory loads (a generic load would resolve its
+      // address space at run time and wait on the long scoreboard)
+      const uint32_t raw = sRaw + sl * kRawBytes;
+      uint32_t P0[8], P1[8];  // row n0 (and n0 + 1): inputs (2q, 2q+1) as the halves of word q
 #pragma unroll
-      for (int rr = 0; rr < kRows; rr++) {
-        const unsigned n = (unsigned)e + rr * kN;  // word row of the tile
-        uint32_t mask = (n < words_valid && e < kN) ? 0xFFFFu : 0u;
-        if (odd_tail && n == last_word) mask &= 0x00FFu;
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const uint32_t lo = (unsigned)(2 * q) < ni && e < kN
-                                  ? *reinterpret_cast<const uint16_t*>(raw + (2 * q) * (kWords * 2) + 2 * n) : 0u;
-          const uint32_t hi = (unsigned)(2 * q + 1) < ni && e < kN
-                                  ? *reinterpret_cast<const uint16_t*>(raw + (2 * q + 1) * (kWords * 2) + 2 * n) : 0u;
-          P[rr][q] = (lo & mask) | ((hi & mask) << 16);
+      for (int q = 0; q < 8; q++) {
+        if (KG == 2) {
+          const uint32_t lo = (unsigned)(2 * q) < ni && active ? lds16(raw + (2 * q) * (kWords * 2) + 2 * n0) : 0u;
+          const uint32_t hi =
+              (unsigned)(2 * q + 1) < ni && active ? lds16(raw + (2 * q + 1) * (kWords * 2) + 2 * n0) : 0u;
+          P0[q] = (lo & mask) | ((hi & mask) << 16);
+          P1[q] = 0;
+        } else {
+          const uint32_t a = (unsigned)(2 * q) < ni && active ? lds32(raw + (2 * q) * (kWords * 2) + 2 * n0) & mask : 0u;
+          const uint32_t b =
+              (unsigned)(2 * q + 1) < ni && active ? lds32(raw + (2 * q + 1) * (kWords * 2) + 2 * n0) & mask : 0u;
+          P0[q] = __byte_perm(a, b, 0x5410);  // word n0 of both inputs
+          P1[q] = __byte_perm(a, b, 0x7632);  // word n0 + 1
         }
       }
       mbar_arrive(BAR(RAW_EMPTY + sl));
@@ -764,19 +793,17 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
         *err = 1;
         break;
       }
-      uint8_t* bt = b_p + bs * kBBytes;
-      if (e < kN) {
+      const uint32_t bt = sB + bs * kBBytes;
+      if (active) {
 #pragma unroll
-        for (int rr = 0; rr < kRows; rr++) {
-          const unsigned n = (unsigned)e + rr * kN;
-          const uint32_t rowA = (n >> 3) * 1024 + (n & 7) * 128, rA = n & 7;
-          // 8 consecutive threads store 8 rows of one swizzle atom at 8 distinct chunks
+        for (int rr = 0; rr < (KG == 2 ? 1 : 2); rr++) {
+          const unsigned n = n0 + (rr ^ sw);
+          const uint32_t* P = (rr ^ sw) ? P1 : P0;
+          const uint32_t row = bt + (n >> 3) * 1024 + (n & 7) * 128, r7 = n & 7;
 #pragma unroll
           for (int j = 0; j < 4; j++) {
-            *reinterpret_cast<uint4*>(bt + rowA + (((2 * j) ^ rA) << 4)) =
-                make_uint4(pick4(P[rr][0], j), pick4(P[rr][1], j), pick4(P[rr][2], j), pick4(P[rr][3], j));
-            *reinterpret_cast<uint4*>(bt + rowA + (((2 * j + 1) ^ rA) << 4)) =
-                make_uint4(pick4(P[rr][4], j), pick4(P[rr][5], j), pick4(P[rr][6], j), pick4(P[rr][7], j));
+            sts128(row + (((2 * j) ^ r7) << 4), pick4(P[0], j), pick4(P[1], j), pick4(P[2], j), pick4(P[3], j));
+            sts128(row + (((2 * j + 1) ^ r7) << 4), pick4(P[4], j), pick4(P[5], j), pick4(P[6], j), pick4(P[7], j));
           }
         }
       }

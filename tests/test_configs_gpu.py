@@ -206,7 +206,7 @@ def test_par2_repair_32768x32KiB_lost64_against_the_reference(ctx, oracle, golde
 
 
 # ------------------------------------------------------ memory checksum flag
-@pytest.mark.parametrize("slice_size", [4096, 4094, 300000])
+@pytest.mark.parametrize("slice_size", [4096, 4094, 4001, 300000])
 def test_proc_valid_is_false_for_a_changed_output_row(ctx, oracle, slice_size):
     """Between the product and the first getOutput one byte of output row 2
     is flipped on the device: getOutput reports that row invalid (and only
