@@ -98,16 +98,14 @@ def roofline(w, args, hbm_achieved, hbm_peak, peak_kind, kms, int8_tops):
            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
            else "fallback 6.65 TB/s"}
     r = {"kernel": kern, "kernel_ms": kms, "traffic": load_traffic(f"{kern}.{args.workload}")}
-    if kern.endswith("_tc"):
+    if kern.endswith(("_tc", "_tc_pair", "_f4")):
         tops = 2 * bit_macs(w) / (kms * 1e-3) / 1e12
-        if int8_tops:
-            peak, kind = int8_tops, "measured here: cuBLASLt dense int8 GEMM 8192^3 (torch._int_mm), best of 10"
-        else:
-            peak, kind = 2 * load_bf16_peak(), "2 x MEASURED_PEAKS.json bf16_tflops (int8 dense rate = 2x bf16)"
+        peak, kind, nominal, nominal_kind = tensor_peak(kern, int8_tops)
+        fmt = "FP4 (e2m1 0/1, block scales 1.0)" if kern.endswith("_f4") else "int8"
         r.update({"bound": "tensor", "achieved": tops, "peak": peak, "unit": "TFLOP/s", "frac": tops / peak,
-                  "peak_kind": kind, "ops": "int8 tensor ops (2 per MAC), one MAC per GF(2) bit product",
-                  "nominal_peak": 4500.0, "frac_of_nominal": tops / 4500.0,
-                  "nominal_kind": "B200 dense int8 tensor rate (NVIDIA's 4.5 POP/s dense figure)", "hbm": hbm})
+                  "peak_kind": kind, "ops": f"{fmt} tensor ops (2 per MAC), one MAC per GF(2) bit product",
+                  "nominal_peak": nominal, "frac_of_nominal": tops / nominal, "nominal_kind": nominal_kind,
+                  "hbm": hbm})
     else:
         r.update({"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
                   "frac": hbm_achieved / hbm_peak, "peak_kind": hbm["peak_kind"]})
@@ -130,6 +128,10 @@ TRAFFIC = {
     "k_gf16_muladd_tc.par2_create_32768x32KiB_R64": 4 * (543139328 + 9490176),
     "k_gf16_muladd_tc.par2_create_1024x1MiB_R8": 1087907000 + 10907904,
     "k_gf64_matvec_tc.par3_create_131072x8KiB_R8": 1083011000 + 3985664,
+    # FP4 GF(2^16) kernel: the 8,192-slice R=64 capture (403.9 + 5.3 MB) and the
+    # 256 x 1 MiB R=8 capture (268.8 + 9.0 MB), each scaled by 4 to the 1 GiB launch
+    "k_gf16_muladd_f4.par2_create_32768x32KiB_R64": 4 * (403939584 + 5251840),
+    "k_gf16_muladd_f4.par2_create_1024x1MiB_R8": 4 * (268794624 + 9036032),
     # the SM-pair kernel's 32,768-block capture (270.8 + 4.3 MB) scaled to 131,072 blocks
     "k_gf64_matvec_tc_pair.par3_create_131072x8KiB_R8": 4 * (270800000 + 4300000),
 }
@@ -353,20 +355,39 @@ def dominant_kernel(w, args):
     """Name of the region kernel the library's dispatch picks for this workload
     (AUTO: tensor cores for >= 8 GF(2^16) inputs, and for 16-byte aligned
     GF(2^64) rows of an even word count)."""
+    gf16_tc = "k_gf16_muladd_tc" if os.environ.get("PARPAR_B200_GF16_TC") == "i8" else "k_gf16_muladd_f4"
     if w["field"] == "gf16":
-        return "k_gf16_muladd_lut" if args.gf16_kernel == "lut" else "k_gf16_muladd_tc"
+        return "k_gf16_muladd_lut" if args.gf16_kernel == "lut" else gf16_tc
     if w["field"] == "fft":
         return "k_fft_*"
     if w["field"] == "gf16_repair":
-        return "k_gf16_muladd_tc"
+        return gf16_tc
     if w["field"] == "hash2":
         return "k_par2_block_hash"
     if w["field"] in ("hash3", "pkt3"):
         return "k_b3_chunks"
     if args.gf64_kernel == "lut":
         return "k_gf64_matvec_lut"
+    if os.environ.get("PARPAR_B200_GF64_TC") == "f4":
+        return "k_gf64_matvec_f4"
     # the SM-pair kernel runs when every job of the launch has >= 4 outputs
     return "k_gf64_matvec_tc_pair" if w["r"] >= 4 else "k_gf64_matvec_tc"
+
+
+def tensor_peak(kern, int8_tops):
+    """(peak TOP/s, how it was obtained, nominal, nominal's source) for a
+    tensor-core region kernel: the FP4 kernels against 4 x the measured dense
+    bf16 GEMM rate (B200's dense FP4 rate is 4x its bf16 rate), the int8
+    kernels against the cuBLASLt int8 GEMM measured in this run (else 2 x
+    bf16)."""
+    if kern.endswith("_f4"):
+        return (4 * load_bf16_peak(), "4 x MEASURED_PEAKS.json bf16_tflops (dense FP4 rate = 4x bf16)", 9000.0,
+                "B200 dense FP4 tensor rate (NVIDIA's 9 PFLOP/s dense figure)")
+    if int8_tops:
+        peak, kind = int8_tops, "measured here: cuBLASLt dense int8 GEMM 8192^3 (torch._int_mm), best of 10"
+    else:
+        peak, kind = 2 * load_bf16_peak(), "2 x MEASURED_PEAKS.json bf16_tflops (int8 dense rate = 2x bf16)"
+    return peak, kind, 4500.0, "B200 dense int8 tensor rate (NVIDIA's 4.5 POP/s dense figure)"
 
 
 def algo_bytes(job):
@@ -1144,8 +1165,11 @@ def main():
                 m = measure(j, ctx, timer, 2 if heavy else 5, 1 if heavy else 3, peak)
                 ent = {"workload": name, "value": input_bytes_of(name) / (m["ms"] * 1e-3) / 1e9,
                        "unit": "GB/s", "ms_per_step": m["ms"], "kernel_ms": m["kernel_ms"], "hbm_frac": m["frac"]}
-                if int8_tops and dominant_kernel(WORKLOADS[name], args).endswith("_tc"):
-                    ent["tensor_frac"] = 2 * bit_macs(WORKLOADS[name]) / (m["kernel_ms"] * 1e-3) / 1e12 / int8_tops
+                kern = dominant_kernel(WORKLOADS[name], args)
+                if kern.endswith(("_tc", "_tc_pair", "_f4")):
+                    ent["kernel"] = kern
+                    ent["tensor_frac"] = (2 * bit_macs(WORKLOADS[name]) / (m["kernel_ms"] * 1e-3) / 1e12 /
+                                          tensor_peak(kern, int8_tops)[0])
                 sec.append(ent)
                 del j
                 torch.cuda.empty_cache()
