@@ -871,6 +871,298 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
   if (threadIdx.x == 0 && *err) atomicOr(status, 1);
 }
 
+// ---------------------------------------------------------------------------
+// FP4 on SM pairs (cluster of 2, tcgen05.mma cta_group::2 kind::mxf4, M = 256):
+// the pair covers 4 outputs (CTA r holds the A rows and the accumulators of
+// outputs o0 + 2r, o0 + 2r + 1) x 480 words (CTA r builds the B rows of words
+// w0 + 240 r + u, u = 0..239); MMA nn takes B rows 120 nn .. 120 nn + 119 of
+// each CTA (N = 240), so column c of accumulator nn is word
+// w0 + 240 (c / 120) + 120 nn + c % 120.  Per SM the B tile is half that of
+// the one-CTA FP4 kernel.  Scale factors 1.0 in TMEM columns 240-255 and
+// 496-511 of both CTAs (A at 240, B at 496).  Pipeline and bounded waits as
+// the int8 pair kernel: CTA 1's warp 1 relays "stage built" to CTA 0, whose
+// warp 1 issues the MMAs and whose commits arrive in both CTAs.
+constexpr int kPN = 240;
+constexpr int kPRowsMma = kPN / 2;               // B rows per CTA per MMA
+constexpr int kPWordsCta = kPN;                  // words built per CTA
+constexpr int kPWords = 2 * kPN;                 // words per pair tile
+constexpr int kPBBytes = kPWordsCta * 128;       // 30 KiB
+constexpr int kPRawBytes = kStageIn * kPWordsCta * 8;  // 7.5 KiB
+constexpr int kPLd = 5;
+constexpr int kPBs = 4;
+constexpr int kPOffA = 0;
+constexpr int kPOffB = kPBs * kABytes;
+constexpr int kPOffRaw = kPOffB + kPBs * kPBBytes;
+constexpr int kPOffBar = kPOffRaw + kPLd * kPRawBytes;
+constexpr int kPSmemBytes = kPOffBar + 256 + 1024;
+constexpr uint32_t kPSfaCol = 240, kPSfbCol = 496;
+static_assert(kPSmemBytes <= 227 * 1024, "shared memory");
+static_assert(kPOffB % 1024 == 0 && kPBBytes % 1024 == 0 && (kPRowsMma * 128) % 1024 == 0, "swizzle atoms");
+constexpr uint32_t kPIdesc =
+    (1u << 7) | (1u << 10) | ((uint32_t)(kPN >> 3) << 17) | (1u << 23) | ((256u >> 4) << 24);
+
+PP_D void mma_f4_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate, uint32_t sfa,
+                      uint32_t sfb) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %3, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::mxf4.block_scale.block32 [%0], %1, %2, %6, [%4], [%5], p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(accumulate), "r"(sfa), "r"(sfb), "r"(kPIdesc)
+      : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    k_gf64_matvec_f4_pair(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ status) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t base_s = smem_addr(smem_raw);
+  const uint32_t pad = ((base_s + 1023) & ~1023u) - base_s;
+  uint8_t* smem = smem_raw + pad;
+  const uint32_t sA = base_s + pad + kPOffA, sB = base_s + pad + kPOffB, sRaw = base_s + pad + kPOffRaw;
+  const uint32_t bar0 = smem_addr(smem + kPOffBar);
+  enum {
+    RAW_FULL = 0,
+    RAW_EMPTY = RAW_FULL + kPLd,
+    OPB_FULL = RAW_EMPTY + kPLd,  // this CTA's builders done with stage slot
+    OPR_FULL = OPB_FULL + kPBs,   // CTA 0: CTA 1's builders done (relayed)
+    OP_EMPTY = OPR_FULL + kPBs,
+    D_FULL = OP_EMPTY + kPBs,
+    DONE = D_FULL + 1,
+    NBARS = DONE + 1
+  };
+  static_assert(8 * NBARS + 16 <= 256, "barrier area");
+  auto BAR = [&](int k) { return bar0 + 8u * (uint32_t)k; };
+  volatile uint32_t* tmem_holder = reinterpret_cast<volatile uint32_t*>(smem + kPOffBar + 8 * NBARS);
+  volatile int* err = reinterpret_cast<volatile int*>(smem + kPOffBar + 8 * NBARS + 8);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NBARS; k++) {
+      const bool by_builders = (k >= RAW_EMPTY && k < RAW_EMPTY + kPLd) || (k >= OPB_FULL && k < OPB_FULL + kPBs);
+      mbar_init(BAR(k), by_builders ? (uint32_t)kExp : 1u);
+    }
+    *err = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {  // both CTAs allocate together
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr((const void*)tmem_holder)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_holder;
+  if (warp >= 2 && warp < 6) {
+    // scale factors 1.0 (ue8m0 0x7F) in columns 240-255 and 496-511 of this warp's lane quarter
+    const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    const uint32_t v = 0x7F7F7F7Fu;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(
+            t + kPSfaCol),
+        "r"(v)
+        : "memory");
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(
+            t + kPSfbCol),
+        "r"(v)
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // the peer's barriers and scale factors are ready before any remote arrive or MMA
+  tc_fence_after();
+  const TcSeg sg = tc_item(&batch, blockIdx.x >> 1);
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      uint32_t g = 0;
+      do {
+        const Gf64TcJob J = pinned_job(batch.job[sg.job]);
+        const size_t wc = (size_t)(sg.tile / J.pairs) * kPWords + (size_t)kPWordsCta * rank;
+        const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)kPWordsCta, J.words - wc) : 0u;
+        const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
+        for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
+          const unsigned sl = g % kPLd;
+          if (g >= (uint32_t)kPLd && !mbar_wait(BAR(RAW_EMPTY + sl), (g / kPLd - 1) & 1)) {
+            *err = 1;
+            break;
+          }
+          const unsigned i0 = st * kStageIn;
+          const unsigned ni = raw_copy ? min((unsigned)kStageIn, J.n_in - i0) : 0u;
+          mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
+          for (unsigned ii = 0; ii < ni; ii++) {
+            const uint64_t* row = J.in_ptrs ? J.in_ptrs[i0 + ii] : J.in + (size_t)(i0 + ii) * J.in_stride;
+            bulk_g2s(sRaw + sl * kPRawBytes + ii * (kPWordsCta * 8), row + wc, raw_copy, BAR(RAW_FULL + sl));
+          }
+        }
+      } while (0);
+      if (*err) {
+        for (uint32_t k = g > (uint32_t)kPLd ? g - kPLd : 0; k < g; k++)
+          mbar_wait(BAR(RAW_FULL + k % kPLd), (k / kPLd) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const unsigned nst = sg.st1 - sg.st0;
+      if (rank == 0) {
+        // -------------------------------------------------------- MMA issuer
+        const uint32_t sfa = tmem + kPSfaCol, sfb = tmem + kPSfbCol;
+        for (unsigned k = 0; k < nst; k++) {
+          const unsigned bs = k % kPBs;
+          const uint32_t ph = (k / kPBs) & 1;
+          if (*err || !mbar_wait(BAR(OPB_FULL + bs), ph) || !mbar_wait_cluster(BAR(OPR_FULL + bs), ph)) {
+            *err = 1;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int kk = 0; kk < 4; kk++) {
+#pragma unroll
+            for (int nn = 0; nn < 2; nn++) {
+              mma_f4_pair(tmem + nn * 256, sw128_desc(sA + bs * kABytes + 32 * kk),
+                          sw128_desc(sB + bs * kPBBytes + nn * (kPRowsMma * 128) + 32 * kk),
+                          (k > 0 || kk > 0) ? 1u : 0u, sfa, sfb);
+            }
+          }
+          mma_commit_pair(BAR(OP_EMPTY + bs));
+        }
+        if (!*err) mma_commit_pair(BAR(D_FULL));
+        mma_commit_pair(BAR(DONE));
+      } else {
+        // -------------------------------------------------------- relay
+        const uint32_t remote = peer_addr(BAR(OPR_FULL), 0);
+        for (unsigned k = 0; k < nst; k++) {
+          const unsigned bs = k % kPBs;
+          if (*err || !mbar_wait(BAR(OPB_FULL + bs), (k / kPBs) & 1)) {
+            *err = 1;
+            break;
+          }
+          mbar_arrive_remote(remote + 8u * bs);
+        }
+      }
+      // CTA 0's MMAs (which read this CTA's tiles and write its TMEM) have
+      // completed before the tiles and TMEM are released
+      if (!mbar_wait(BAR(DONE), 0)) *err = 1;
+    }
+  } else {
+    // ------------------------------------------------------------ operand builders
+    const int e = threadIdx.x - 64;  // 0..255
+    const unsigned a_ii = e & 1, a_m = e >> 1, a_oo = a_m >> 6, a_b = a_m & 63;
+    const uint32_t arow = (a_m >> 3) * 1024 + (a_m & 7) * 128 + 8 * a_ii, ar7 = a_m & 7;
+    const int q = warp & 3;
+    const int nn_ep = (warp - 2) >> 2;  // epilogue: accumulator
+    uint32_t g = 0;
+    do {
+      const Gf64TcJob J = pinned_job(batch.job[sg.job]);
+      const unsigned o0 = 4 * (unsigned)(sg.tile % J.pairs) + 2 * rank;  // this CTA's two outputs
+      const size_t w0 = (size_t)(sg.tile / J.pairs) * kPWords;
+      const size_t wc = w0 + (size_t)kPWordsCta * rank;
+      const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)kPWordsCta, J.words - wc) : 0u;
+      const bool okB = e < kPWordsCta && (unsigned)e < words_valid;
+      const unsigned nst = sg.st1 - sg.st0;
+      auto coef = [&](unsigned k, unsigned ii) -> uint64_t {
+        const unsigned o = o0 + a_oo, i = (sg.st0 + k) * kStageIn + ii;
+        return (k < nst && o < J.n_out && i < J.n_in) ? J.coeff[(size_t)o * J.ldc + i] : 0ull;
+      };
+      uint64_t c0 = coef(0, a_ii), c1 = coef(0, a_ii + 2);
+      for (unsigned k = 0; k < nst; k++, g++) {
+        const unsigned sl = g % kPLd, bs = g % kPBs;
+        const uint64_t n0 = coef(k + 1, a_ii), n1 = coef(k + 1, a_ii + 2);
+        const uint64_t q0 = mul_matrix_row_f4(c0, a_b), q1 = mul_matrix_row_f4(c1, a_b);
+        if (*err || !mbar_wait(BAR(RAW_FULL + sl), (g / kPLd) & 1)) {
+          *err = 1;
+          break;
+        }
+        const unsigned i0 = (sg.st0 + k) * kStageIn;
+        const unsigned ni = min((unsigned)kStageIn, J.n_in - i0);
+        uint32_t xw[8];
+#pragma unroll
+        for (int ii = 0; ii < kStageIn; ii++) {
+          uint2 v = make_uint2(0, 0);
+          if (okB && (unsigned)ii < ni) v = lds64(sRaw + sl * kPRawBytes + ii * (kPWordsCta * 8) + 8 * (unsigned)e);
+          xw[2 * ii] = v.x;
+          xw[2 * ii + 1] = v.y;
+        }
+        mbar_arrive(BAR(RAW_EMPTY + sl));
+        if (g >= (uint32_t)kPBs && !mbar_wait(BAR(OP_EMPTY + bs), (g / kPBs - 1) & 1)) {
+          *err = 1;
+          break;
+        }
+        const uint32_t at = sA + bs * kABytes, bt = sB + bs * kPBBytes;
+        const uint32_t q0lo = (uint32_t)q0, q0hi = (uint32_t)(q0 >> 32), q1lo = (uint32_t)q1,
+                       q1hi = (uint32_t)(q1 >> 32);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          sts64(at + arow + (((2 * j) ^ ar7) << 4), pick4(q0lo, j), pick4(q0hi, j));
+          sts64(at + arow + (((2 * j + 1) ^ ar7) << 4), pick4(q1lo, j), pick4(q1hi, j));
+        }
+        if (e < kPWordsCta) {
+          const unsigned u = (unsigned)e;
+          const uint32_t brow = bt + (u >> 3) * 1024 + (u & 7) * 128, br7 = u & 7;
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            sts128(brow + (((2 * j) ^ br7) << 4), pick4(xw[0], j), pick4(xw[1], j), pick4(xw[2], j), pick4(xw[3], j));
+            sts128(brow + (((2 * j + 1) ^ br7) << 4), pick4(xw[4], j), pick4(xw[5], j), pick4(xw[6], j),
+                   pick4(xw[7], j));
+          }
+        }
+        fence_async_smem();
+        mbar_arrive(BAR(OPB_FULL + bs));
+        c0 = n0;
+        c1 = n1;
+      }
+      // ---------------------------------------------------------- epilogue
+      if (*err || !mbar_wait(BAR(D_FULL), 0)) {
+        *err = 1;
+        break;
+      }
+      tc_fence_after();
+      const unsigned o = o0 + (q >> 1);
+      const unsigned half = q & 1;
+      uint64_t* orow = o < J.n_out ? (J.out_ptrs ? J.out_ptrs[o] : J.out + (size_t)o * J.out_stride) : nullptr;
+      for (int cc = 0; cc < (kPN + 31) / 32; cc++) {
+        uint32_t r[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + 256 * nn_ep + 32 * cc, r);
+        uint32_t mine = 0;
+#pragma unroll
+        for (int jj = 0; jj < 32; jj++) {
+          const uint32_t bit = __float_as_uint(__fadd_rn(__uint_as_float(r[jj]), 8388608.0f)) & 1u;
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, bit);
+          if (lane == jj) mine = bal;
+        }
+        const unsigned c = 32 * cc + lane;  // column of accumulator nn_ep
+        if (!orow || c >= (unsigned)kPN) continue;
+        const size_t widx = (size_t)kPWordsCta * (c / kPRowsMma) + (size_t)kPRowsMma * nn_ep + (c % kPRowsMma);
+        if (w0 + widx >= J.words) continue;
+        uint32_t* dst = reinterpret_cast<uint32_t*>(orow + w0 + widx) + half;
+        if (sg.mode == 2) {
+          if (mine) atomicXor(dst, mine);
+        } else if (sg.mode == 1) {
+          *dst ^= mine;
+        } else {
+          *dst = mine;
+        }
+      }
+      tc_fence_before();
+    } while (0);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // both CTAs are done with TMEM and the peer's barriers
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+  if (threadIdx.x == 0 && *err) atomicOr(status, 1);
+}
+
 }  // namespace tc64f4
 
 // GF(2^64) tensor-core path: the int8 kernels (SM pair / one CTA) unless
@@ -912,12 +1204,15 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(tc64f4::k_gf64_matvec_f4, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc64f4::kSmemBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(tc64f4::k_gf64_matvec_f4_pair, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc64f4::kPSmemBytes);
     if (e != cudaSuccess) return e;
     device_mark(attr);
   }
   const bool f4 = gf64_tc_use_f4();
-  const bool pair = !f4 && use_pair_kernel(b);
-  const size_t tile_words = f4 ? tc64f4::kWords : tc64::kWords;
+  const bool pair = use_pair_kernel(b);
+  const size_t tile_words = f4 ? (pair ? tc64f4::kPWords : tc64f4::kWords) : tc64::kWords;
   const unsigned stage_in = f4 ? tc64f4::kStageIn : tc64::kStageIn;
   // drop empty jobs (nothing to multiply) after zeroing their outputs
   uint32_t m = 0;
@@ -959,7 +1254,9 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     }
     note_launch();
   }
-  if (f4)
+  if (f4 && pair)
+    tc64f4::k_gf64_matvec_f4_pair<<<2 * (unsigned)items, tc64f4::kThreads, tc64f4::kPSmemBytes, s>>>(b, d_status);
+  else if (f4)
     tc64f4::k_gf64_matvec_f4<<<(unsigned)items, tc64f4::kThreads, tc64f4::kSmemBytes, s>>>(b, d_status);
   else if (pair)
     tc64::k_gf64_matvec_tc_pair<tc64::kPLd, tc64::kPBs>
