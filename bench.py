@@ -113,12 +113,17 @@ def roofline(w, args, hbm_achieved, hbm_peak, peak_kind, kms, int8_tops):
 
 
 def load_bf16_peak():
+    """(dense bf16 TFLOP/s, source): the measured burst figure of
+    MEASURED_PEAKS.json, else the fallback 1,590 TFLOP/s."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         with open(p) as f:
-            return float(json.load(f).get("bf16_tflops", 1590.0))
+            v = json.load(f).get("bf16_tflops")
+        if v:
+            return float(v), "MEASURED_PEAKS.json bf16_tflops"
     except Exception:
-        return 1590.0
+        pass
+    return 1590.0, "fallback bf16 1,590 TFLOP/s"
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from the ncu
@@ -380,13 +385,14 @@ def tensor_peak(kern, int8_tops):
     bf16 GEMM rate (B200's dense FP4 rate is 4x its bf16 rate), the int8
     kernels against the cuBLASLt int8 GEMM measured in this run (else 2 x
     bf16)."""
+    bf16, src = load_bf16_peak()
     if kern.endswith("_f4"):
-        return (4 * load_bf16_peak(), "4 x MEASURED_PEAKS.json bf16_tflops (dense FP4 rate = 4x bf16)", 9000.0,
+        return (4 * bf16, f"4 x {src} (dense FP4 rate = 4x bf16)", 9000.0,
                 "B200 dense FP4 tensor rate (NVIDIA's 9 PFLOP/s dense figure)")
     if int8_tops:
         peak, kind = int8_tops, "measured here: cuBLASLt dense int8 GEMM 8192^3 (torch._int_mm), best of 10"
     else:
-        peak, kind = 2 * load_bf16_peak(), "2 x MEASURED_PEAKS.json bf16_tflops (int8 dense rate = 2x bf16)"
+        peak, kind = 2 * bf16, f"2 x {src} (int8 dense rate = 2x bf16)"
     return peak, kind, 4500.0, "B200 dense int8 tensor rate (NVIDIA's 4.5 POP/s dense figure)"
 
 

@@ -39,12 +39,21 @@
 #include "pp_internal.h"
 #include "tc_batch.h"
 #include "tc_common.cuh"
+#include "tma_map.h"
 
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
 
 namespace pp {
+
+// Tensor maps of the jobs' input matrices, entry j for job j of the table: a
+// second __grid_constant__ parameter (the TMA reads the map from parameter
+// space), rows = the job's inputs, boxes of one stage's rows
+struct alignas(64) Gf16TcMaps {
+  CUtensorMap raw[kTcMaxJobs];
+};
+
 namespace tc16 {
 using namespace pp::tc;
 
@@ -72,6 +81,11 @@ struct Shape {
   static constexpr int kSmemBytes = kOffBar + 256 + 1024;  // + barriers + alignment slack
 };
 static_assert(Shape<1>::kSmemBytes <= 227 * 1024 && Shape<2>::kSmemBytes <= 227 * 1024, "shared memory");
+// raw rows arrive as tensor-map boxes of kStageIn rows x kBox bytes: a word
+// tile's 2 * kWords bytes are 2 (KG = 2) or 4 (KG = 1) boxes, box b of a ring
+// slot at b * kBoxStage, row ii of a box at ii * kBox
+constexpr int kBox = 256;
+constexpr int kBoxStage = kStageIn * kBox;
 
 // instruction descriptor: D int32, A/B unsigned 8-bit, both K-major,
 // N = 256, M = 128
@@ -160,15 +174,14 @@ k_gf16_tc_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigne
 // 1 XORs into the output, 2 XORs atomically (the job is split over CTAs).
 template <int KG>
 __global__ void __launch_bounds__(kThreads, 1)
-k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ status) {
+k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, const __grid_constant__ Gf16TcMaps maps,
+                 int* __restrict__ status) {
   using S = Shape<KG>;
   constexpr int kWords = S::kWords, kBBytes = S::kBBytes, kRawBytes = S::kRawBytes, kAStage = S::kAStage;
   constexpr int kOffA = S::kOffA, kOffB = S::kOffB, kOffRaw = S::kOffRaw, kOffBar = S::kOffBar;
   constexpr int kLd = S::kLd, kBs = S::kBs;
   const TcSeg sg = tc_item(&batch, blockIdx.x);
   const Gf16TcJob J = pinned_job(batch.job[sg.job]);
-  const uint8_t* __restrict__ in = J.in;
-  const size_t in_stride = J.in_stride;
   const unsigned n_in = J.n_in;
   const size_t slice_bytes = J.slice_bytes;
   const uint8_t* __restrict__ a_exp = J.a_exp;
@@ -211,9 +224,10 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
   const unsigned nst = sg.st1 - sg.st0;
   const size_t total_words = (slice_bytes + 1) / 2;
   const unsigned words_valid = (unsigned)min((size_t)kWords, total_words - w0);
-  // raw bytes copied per input row (16-byte multiple, inside the padded row)
+  // bytes of the word tile inside the slice
   const size_t tile_bytes_valid = min((size_t)kWords * 2, slice_bytes - 2 * w0);
-  const uint32_t raw_copy = (uint32_t)((tile_bytes_valid + 15) & ~(size_t)15);
+  const unsigned n_box = (unsigned)((tile_bytes_valid + kBox - 1) / kBox);
+  const void* raw_map = &maps.raw[sg.job];
 
   if (threadIdx.x == 0) {
     for (int k = 0; k < NBARS; k++) {
@@ -238,6 +252,7 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
   if (warp == 0) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
+      tma_prefetch_map(raw_map);
       unsigned issued = 0;
       for (unsigned k = 0; k < nst && !*err; k++) {
         const unsigned sl = k % kLd, use = k / kLd;
@@ -253,12 +268,12 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
         for (int gg = 0; gg < KG; gg++)
           bulk_g2s(sA + sl * kAStage + gg * kABytes, a_exp + ((size_t)(g + gg) * n_stages_total + st) * kABytes,
                    kABytes, BAR(A_FULL + sl));
-        const unsigned i0 = st * kStageIn;
-        const unsigned ni = min((unsigned)kStageIn, n_in - i0);
-        mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
-        for (unsigned ii = 0; ii < ni; ii++)
-          bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 2), in + (size_t)(i0 + ii) * in_stride + 2 * w0, raw_copy,
-                   BAR(RAW_FULL + sl));
+        // the stage's rows: one box per kBox bytes of the tile that start
+        // inside the slice (rows past the last input arrive as zeros)
+        mbar_expect_tx(BAR(RAW_FULL + sl), n_box * kBoxStage);
+        for (unsigned b = 0; b < n_box; b++)
+          tma_load_2d(sRaw + sl * kRawBytes + b * kBoxStage, raw_map, (int)(2 * w0) + (int)b * kBox,
+                      (int)(st * kStageIn), BAR(RAW_FULL + sl));
         issued = k + 1;
       }
       // drain: every issued copy lands before the CTA exits
@@ -309,6 +324,7 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
       uint32_t mask = n < words_valid ? 0xFFFFu : 0u;
       if (odd_tail && n == last_word) mask &= 0x00FFu;
       const uint32_t rowA = (n >> 3) * 1024 + (n & 7) * 128, rA = n & 7;
+      const unsigned rb = (2 * n / kBox) * kBoxStage + (2 * n) % kBox;  // word n of row 0 within a ring slot
       for (unsigned k = 0; k < nst; k++) {
         const unsigned sl = k % kLd, bs = k % kBs;
         if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
@@ -321,7 +337,7 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
         uint32_t v[kStageIn];
 #pragma unroll
         for (int ii = 0; ii < kStageIn; ii++)
-          v[ii] = (unsigned)ii < ni ? (*reinterpret_cast<const uint16_t*>(raw + ii * (kWords * 2) + 2 * n) & mask) : 0u;
+          v[ii] = (unsigned)ii < ni ? (*reinterpret_cast<const uint16_t*>(raw + ii * kBox + rb) & mask) : 0u;
         mbar_arrive(BAR(RAW_EMPTY + sl));
         if (k >= (unsigned)kBs && !mbar_wait(BAR(B_EMPTY + bs), (k / kBs - 1) & 1)) {
           *err = 1;
@@ -357,6 +373,7 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
     const unsigned mA = n + sw, mB = n + 1 - sw;
     const uint32_t rowA = (mA >> 3) * 1024 + (mA & 7) * 128, rA = mA & 7;
     const uint32_t rowB = (mB >> 3) * 1024 + (mB & 7) * 128, rB = mB & 7;
+    const unsigned rb = (2 * n / kBox) * kBoxStage + (2 * n) % kBox;  // words n, n+1 of row 0 within a ring slot
     for (unsigned k = 0; k < nst; k++) {
       const unsigned sl = k % kLd, bs = k % kBs;
       if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
@@ -369,7 +386,7 @@ k_gf16_muladd_tc(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
       uint32_t v[kStageIn];
 #pragma unroll
       for (int ii = 0; ii < kStageIn; ii++)
-        v[ii] = (unsigned)ii < ni ? (*reinterpret_cast<const uint32_t*>(raw + ii * (kWords * 2) + 2 * n) & mask) : 0u;
+        v[ii] = (unsigned)ii < ni ? (*reinterpret_cast<const uint32_t*>(raw + ii * kBox + rb) & mask) : 0u;
       mbar_arrive(BAR(RAW_EMPTY + sl));
       if (k >= (unsigned)kBs && !mbar_wait(BAR(B_EMPTY + bs), (k / kBs - 1) & 1)) {
         *err = 1;
@@ -527,6 +544,14 @@ struct Shape {
 static_assert(Shape<1>::kSmemBytes <= 227 * 1024 && Shape<2>::kSmemBytes <= 227 * 1024, "shared memory");
 static_assert(Shape<1>::kOffB % 1024 == 0 && Shape<2>::kOffB % 1024 == 0 && (kN * 128) % 1024 == 0,
               "operand tiles start on 1024-byte swizzle atoms");
+// raw rows arrive as tensor-map boxes of kStageIn rows x kBox bytes: a word
+// tile's 2 * kWords bytes are 2 (KG = 2) or 4 (KG = 1) boxes, box b of a ring
+// slot at b * kBoxStage (a multiple of 128 bytes), row ii of a box at ii * kBox
+constexpr int kBox = 240;
+constexpr int kBoxStage = kStageIn * kBox;
+static_assert(kBoxStage % 128 == 0 && Shape<1>::kOffRaw % 128 == 0 && Shape<2>::kOffRaw % 128 == 0 &&
+                  Shape<1>::kRawBytes % 128 == 0 && Shape<2>::kRawBytes % 128 == 0,
+              "box destinations on 128-byte boundaries");
 
 // instruction descriptor, block-scaled kinds: A/B e2m1 (mxf4 format 1), both
 // K-major, N = 240, scale factors ue8m0, M = 128, dense K = 64
@@ -590,15 +615,14 @@ k_gf16_f4_expand_coeffs(const uint16_t* __restrict__ coeffs, size_t ldc, unsigne
 
 template <int KG>
 __global__ void __launch_bounds__(kThreads, 1)
-k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ status) {
+k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, const __grid_constant__ Gf16TcMaps maps,
+                 int* __restrict__ status) {
   using S = Shape<KG>;
   constexpr int kWords = S::kWords, kBBytes = S::kBBytes, kRawBytes = S::kRawBytes, kAStage = S::kAStage;
   constexpr int kOffA = S::kOffA, kOffB = S::kOffB, kOffRaw = S::kOffRaw, kOffBar = S::kOffBar;
   constexpr int kLd = S::kLd, kBs = S::kBs;
   const TcSeg sg = tc_item(&batch, blockIdx.x);
   const Gf16TcJob J = pinned_job(batch.job[sg.job]);
-  const uint8_t* __restrict__ in = J.in;
-  const size_t in_stride = J.in_stride;
   const unsigned n_in = J.n_in;
   const size_t slice_bytes = J.slice_bytes;
   const uint8_t* __restrict__ a_exp = J.a_exp;
@@ -638,7 +662,8 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
   const size_t total_words = (slice_bytes + 1) / 2;
   const unsigned words_valid = (unsigned)min((size_t)kWords, total_words - w0);
   const size_t tile_bytes_valid = min((size_t)kWords * 2, slice_bytes - 2 * w0);
-  const uint32_t raw_copy = (uint32_t)((tile_bytes_valid + 15) & ~(size_t)15);
+  const unsigned n_box = (unsigned)((tile_bytes_valid + kBox - 1) / kBox);
+  const void* raw_map = &maps.raw[sg.job];
 
   if (threadIdx.x == 0) {
     for (int k = 0; k < NBARS; k++) {
@@ -676,6 +701,7 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
   if (warp == 0) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
+      tma_prefetch_map(raw_map);
       unsigned issued = 0;
       for (unsigned k = 0; k < nst && !*err; k++) {
         const unsigned sl = k % kLd, use = k / kLd;
@@ -691,12 +717,12 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
         for (int gg = 0; gg < KG; gg++)
           bulk_g2s(sA + sl * kAStage + gg * kABytes, a_exp + ((size_t)(g + gg) * n_stages_total + st) * kABytes,
                    kABytes, BAR(A_FULL + sl));
-        const unsigned i0 = st * kStageIn;
-        const unsigned ni = min((unsigned)kStageIn, n_in - i0);
-        mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
-        for (unsigned ii = 0; ii < ni; ii++)
-          bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 2), in + (size_t)(i0 + ii) * in_stride + 2 * w0, raw_copy,
-                   BAR(RAW_FULL + sl));
+        // the stage's rows: one box per kBox bytes of the tile that start
+        // inside the slice (rows past the last input arrive as zeros)
+        mbar_expect_tx(BAR(RAW_FULL + sl), n_box * kBoxStage);
+        for (unsigned b = 0; b < n_box; b++)
+          tma_load_2d(sRaw + sl * kRawBytes + b * kBoxStage, raw_map, (int)(2 * w0) + (int)b * kBox,
+                      (int)(st * kStageIn), BAR(RAW_FULL + sl));
         issued = k + 1;
       }
       if (*err) {
@@ -748,6 +774,7 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
     const unsigned n0 = KG == 2 ? (unsigned)e : 2u * (unsigned)e;
     const unsigned sw = KG == 2 ? 0u : ((unsigned)e >> 2) & 1u;
     const bool active = e < kN;
+    const unsigned rb = (2 * n0 / kBox) * kBoxStage + (2 * n0) % kBox;  // word n0 of row 0 within a ring slot
     uint32_t mask = 0;
     if (KG == 2) {
       if (n0 < words_valid) mask = 0xFFFFu;
@@ -775,15 +802,15 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, int* __restrict__ st
 #pragma unroll
       for (int q = 0; q < 8; q++) {
         if (KG == 2) {
-          const uint32_t lo = (unsigned)(2 * q) < ni && active ? lds16(raw + (2 * q) * (kWords * 2) + 2 * n0) : 0u;
+          const uint32_t lo = (unsigned)(2 * q) < ni && active ? lds16(raw + (2 * q) * kBox + rb) : 0u;
           const uint32_t hi =
-              (unsigned)(2 * q + 1) < ni && active ? lds16(raw + (2 * q + 1) * (kWords * 2) + 2 * n0) : 0u;
+              (unsigned)(2 * q + 1) < ni && active ? lds16(raw + (2 * q + 1) * kBox + rb) : 0u;
           P0[q] = (lo & mask) | ((hi & mask) << 16);
           P1[q] = 0;
         } else {
-          const uint32_t a = (unsigned)(2 * q) < ni && active ? lds32(raw + (2 * q) * (kWords * 2) + 2 * n0) & mask : 0u;
+          const uint32_t a = (unsigned)(2 * q) < ni && active ? lds32(raw + (2 * q) * kBox + rb) & mask : 0u;
           const uint32_t b =
-              (unsigned)(2 * q + 1) < ni && active ? lds32(raw + (2 * q + 1) * (kWords * 2) + 2 * n0) & mask : 0u;
+              (unsigned)(2 * q + 1) < ni && active ? lds32(raw + (2 * q + 1) * kBox + rb) & mask : 0u;
           P0[q] = __byte_perm(a, b, 0x5410);  // word n0 of both inputs
           P1[q] = __byte_perm(a, b, 0x7632);  // word n0 + 1
         }
@@ -970,6 +997,36 @@ cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStr
   }
   b.n_jobs = m;
   if (!m) return cudaGetLastError();
+  // a box's byte column is a 32-bit coordinate: slices of 2 GiB and more run
+  // as separate launches over column bands of 1 GiB (16-byte aligned starts)
+  constexpr size_t kBand = size_t(1) << 30;
+  m = 0;
+  for (uint32_t j = 0; j < b.n_jobs; j++) {
+    const Gf16TcJob J = b.job[j];
+    if (J.slice_bytes < (size_t(1) << 31)) {
+      b.job[m++] = J;
+      continue;
+    }
+    for (size_t c0 = 0; c0 < J.slice_bytes; c0 += kBand) {
+      Gf16TcBatch one{};
+      one.n_jobs = 1;
+      one.job[0] = J;
+      one.job[0].in = J.in + c0;
+      one.job[0].out = J.out + c0;
+      one.job[0].slice_bytes = std::min(kBand, J.slice_bytes - c0);
+      one.job[0].a_stride = J.a_stride;
+      if (cudaError_t e = launch_gf16_tc_batch(one, sms, d_status, s)) return e;
+    }
+  }
+  b.n_jobs = m;
+  if (!m) return cudaGetLastError();
+  Gf16TcMaps maps;
+  for (uint32_t j = 0; j < m; j++) {
+    const Gf16TcJob& J = b.job[j];
+    if (cudaError_t e = tma_encode_rows(&maps.raw[j], J.in, J.slice_bytes, J.n_in, J.in_stride,
+                                        f4 ? tc16f4::kBox : tc16::kBox, si))
+      return e;
+  }
   // FP4: at most 16,384 stages (262,144 inputs) per item, so a count stays below 16 * 2^18 < 2^23
   const uint64_t ctas = tc_batch_plan(b, tc16::tiles16, sms, f4 ? 16384u : 0u);
   if (ctas > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
@@ -981,13 +1038,13 @@ cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStr
     if (e != cudaSuccess) return e;
   }
   if (f4 && kg == 2)
-    tc16f4::k_gf16_muladd_f4<2><<<(unsigned)ctas, tc16f4::kThreads, tc16f4::Shape<2>::kSmemBytes, s>>>(b, d_status);
+    tc16f4::k_gf16_muladd_f4<2><<<(unsigned)ctas, tc16f4::kThreads, tc16f4::Shape<2>::kSmemBytes, s>>>(b, maps, d_status);
   else if (f4)
-    tc16f4::k_gf16_muladd_f4<1><<<(unsigned)ctas, tc16f4::kThreads, tc16f4::Shape<1>::kSmemBytes, s>>>(b, d_status);
+    tc16f4::k_gf16_muladd_f4<1><<<(unsigned)ctas, tc16f4::kThreads, tc16f4::Shape<1>::kSmemBytes, s>>>(b, maps, d_status);
   else if (kg == 2)
-    tc16::k_gf16_muladd_tc<2><<<(unsigned)ctas, tc16::kThreads, tc16::Shape<2>::kSmemBytes, s>>>(b, d_status);
+    tc16::k_gf16_muladd_tc<2><<<(unsigned)ctas, tc16::kThreads, tc16::Shape<2>::kSmemBytes, s>>>(b, maps, d_status);
   else
-    tc16::k_gf16_muladd_tc<1><<<(unsigned)ctas, tc16::kThreads, tc16::Shape<1>::kSmemBytes, s>>>(b, d_status);
+    tc16::k_gf16_muladd_tc<1><<<(unsigned)ctas, tc16::kThreads, tc16::Shape<1>::kSmemBytes, s>>>(b, maps, d_status);
   note_launch();
   return cudaGetLastError();
 }

@@ -80,6 +80,17 @@ PP_D void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) 
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
+// one box of a 2-D tensor map into shared memory (tile mode, no multicast);
+// `map` is the generic address of a CUtensorMap kernel parameter
+// (__grid_constant__), x the byte column (a multiple of 16), y the row
+PP_D void tma_load_2d(uint32_t dst, const void* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(dst),
+      "l"(map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+PP_D void tma_prefetch_map(const void* map) { asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory"); }
 PP_D uint64_t sw128_desc(uint32_t addr) {
   return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
          (2ull << 61);
