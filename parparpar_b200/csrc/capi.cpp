@@ -83,9 +83,18 @@ enum Slot { S_IN = 0, S_OUT, S_COEF, S_A, S_B, S_C, S_D, S_E, S_AEXP, S_HASH, S_
 struct CauchyEntry {
   size_t n_in, n_rec;
   uint64_t fI, fR;
-  uint64_t* d;
-  size_t cap;  // bytes of the allocation (a reused buffer may be larger than the matrix)
+  uint64_t* d;  // from the context's memory pool, in the context stream's order
+  size_t bytes;
 };
+// Resident Cauchy matrices per context: the reference keeps an LRU of 8
+// (src/par3_engine.cc:451-482); on the device the bound is 32 matrices and
+// 16 GiB, so a rotating set of repair shapes (a batch of different jobs run
+// one after another) stays resident instead of being rebuilt every pass.
+constexpr size_t kCauchyEntries = 32;
+constexpr size_t kCauchyBytes = (size_t)16 << 30;
+// Idle memory the context's pool keeps between calls (scratch growth and
+// evicted matrices are recarved from it without driver calls).
+constexpr uint64_t kPoolKeepBytes = (uint64_t)16 << 30;
 
 // Resident PAR2 coefficient table: the coefficient matrix of (input slice
 // numbers, exponents) and, for the tensor-core kernel, its expanded bit-matrix
@@ -108,7 +117,8 @@ struct pp_ctx {
   void* slot_p[S_NSLOTS] = {};
   size_t slot_n[S_NSLOTS] = {};
   std::list<CauchyEntry> cauchy;  // LRU, front = most recent
-  std::vector<std::pair<void*, size_t>> cauchy_spare;  // evicted matrices' buffers, reused in stream order
+  cudaMemPool_t pool = nullptr;   // stream-ordered pool of the scratch slots and Cauchy matrices (first use)
+  cudaEvent_t alloc_ev = nullptr; // orders the side streams against pool allocations and frees
   std::list<Par2Entry> par2;      // LRU, front = most recent
   std::deque<size_t> par2_seen;   // hashes of recent PAR2 keys without a table
   int gf16_kernel = PP_GF16_KERNEL_AUTO;
@@ -223,30 +233,93 @@ static int device_status(pp_ctx* ctx) {
   return PP_OK;
 }
 
+// The context's stream-ordered memory pool, created on first use.  It keeps
+// up to kPoolKeepBytes of freed memory, so buffers that are freed and
+// allocated again (scratch growth, evicted Cauchy matrices) cost no driver
+// call and no synchronisation: a cudaFree of a large buffer waits for the
+// whole device and unmaps its pages, a cudaMalloc maps new ones, tens to
+// hundreds of milliseconds each under load.
+static cudaMemPool_t ctx_pool(pp_ctx* ctx) {
+  if (ctx->pool) return ctx->pool;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = ctx->device;
+  if (cudaMemPoolCreate(&ctx->pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->pool = nullptr;
+    return nullptr;
+  }
+  if (cudaEventCreateWithFlags(&ctx->alloc_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    cudaMemPoolDestroy(ctx->pool);
+    ctx->pool = nullptr;
+    return nullptr;
+  }
+  uint64_t keep = kPoolKeepBytes;
+  cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  return ctx->pool;
+}
+
+// Pool allocations and frees are ordered on the context stream.  The copy and
+// hash streams also touch scratch buffers, so before a free the context
+// stream waits for their work so far (join), and after an allocation they
+// wait for the context stream (follow).
+static void side_streams_join(pp_ctx* ctx) {
+  for (cudaStream_t side : {ctx->copy, ctx->hash}) {
+    if (!side) continue;
+    cudaEventRecord(ctx->alloc_ev, side);
+    cudaStreamWaitEvent(ctx->stream, ctx->alloc_ev, 0);
+  }
+}
+static void side_streams_follow(pp_ctx* ctx) {
+  if (!ctx->alloc_ev) return;
+  cudaEventRecord(ctx->alloc_ev, ctx->stream);
+  for (cudaStream_t side : {ctx->copy, ctx->hash})
+    if (side) cudaStreamWaitEvent(side, ctx->alloc_ev, 0);
+}
+
+static void* pool_alloc(pp_ctx* ctx, size_t n) {
+  cudaMemPool_t pool = ctx_pool(ctx);
+  if (!pool) return nullptr;
+  void* p = nullptr;
+  if (cudaMallocFromPoolAsync(&p, n, pool, ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    // return the pool's idle memory to the device and retry once
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(pool, 0);
+    if (cudaMallocFromPoolAsync(&p, n, pool, ctx->stream) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+  }
+  side_streams_follow(ctx);
+  return p;
+}
+static void pool_free(pp_ctx* ctx, void* p) {
+  if (!p) return;
+  side_streams_join(ctx);
+  cudaFreeAsync(p, ctx->stream);
+}
+
 static void* scratch(pp_ctx* ctx, Slot s, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (ctx->slot_n[s] >= bytes) return ctx->slot_p[s];
   PP_TRACE("scratch-grow", bytes);
   const size_t prev_n = ctx->slot_n[s];
   if (ctx->slot_p[s]) {
-    PP_TRACE("scratch-free", ctx->slot_n[s]);
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(ctx->slot_p[s]);
+    pool_free(ctx, ctx->slot_p[s]);
     ctx->slot_p[s] = nullptr;
     ctx->slot_n[s] = 0;
   }
   // headroom against regrowth: at least twice the previous size, so a stream
-  // of growing jobs reallocates (synchronises and frees) O(log) times
+  // of growing jobs reallocates O(log) times
   size_t n = std::max(bytes + bytes / 8, 2 * prev_n);
   n = (n + 255) & ~(size_t)255;
-  void* p = nullptr;
-  PP_TRACE("scratch-malloc", n);
-  if (cudaMalloc(&p, n) != cudaSuccess) {
-    cudaGetLastError();
-    if (cudaMalloc(&p, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
+  void* p = pool_alloc(ctx, n);
+  if (!p) {
+    p = pool_alloc(ctx, bytes);
+    if (!p) return nullptr;
     n = bytes;
   }
   ctx->slot_p[s] = p;
@@ -365,19 +438,21 @@ PP_API int pp_ctx_free_cache(pp_ctx* ctx) {
   bind(ctx);
   cudaStreamSynchronize(ctx->stream);
   for (int s = 0; s < S_NSLOTS; s++) {
-    if (ctx->slot_p[s]) cudaFree(ctx->slot_p[s]);
+    pool_free(ctx, ctx->slot_p[s]);
     ctx->slot_p[s] = nullptr;
     ctx->slot_n[s] = 0;
   }
-  for (auto& e : ctx->cauchy) cudaFree(e.d);
+  for (auto& e : ctx->cauchy) pool_free(ctx, e.d);
   ctx->cauchy.clear();
-  for (auto& e : ctx->cauchy_spare) cudaFree(e.first);
-  ctx->cauchy_spare.clear();
   for (auto& e : ctx->par2) {
-    cudaFree(e.d_coef);
-    cudaFree(e.d_aexp);
+    pool_free(ctx, e.d_coef);
+    pool_free(ctx, e.d_aexp);
   }
   ctx->par2.clear();
+  if (ctx->pool) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(ctx->pool, 0);
+  }
   return PP_OK;
 }
 
@@ -424,12 +499,22 @@ PP_API void pp_ctx_destroy(pp_ctx* ctx) {
   if (ctx->hash_ev) cudaEventDestroy(ctx->hash_ev);
   if (ctx->staged_ev) cudaEventDestroy(ctx->staged_ev);
   if (ctx->own) cudaStreamDestroy(ctx->own);
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+  if (ctx->alloc_ev) cudaEventDestroy(ctx->alloc_ev);
   delete ctx;
 }
 
 PP_API int pp_ctx_set_stream(pp_ctx* ctx, void* s) {
   if (!ctx) return PP_ERR_INVALID_ARG;
-  ctx->stream = s ? (cudaStream_t)s : ctx->own;
+  cudaStream_t n = s ? (cudaStream_t)s : ctx->own;
+  if (n != ctx->stream && ctx->stream) {
+    // resident buffers are freed and reused in the stream's order: finish
+    // the old stream's work before another stream takes over
+    std::lock_guard<std::mutex> g(ctx->mu);
+    bind(ctx);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  ctx->stream = n;
   return PP_OK;
 }
 PP_API void* pp_ctx_get_stream(pp_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
@@ -521,18 +606,20 @@ static int par2_table(pp_ctx* ctx, const uint16_t* input_idx, unsigned n_in, con
   e.bytes = cbytes + tbytes;
   size_t total = e.bytes;
   for (auto& x : ctx->par2) total += x.bytes;
+  // tables come from the context's pool; an evicted table is freed in the
+  // stream's order, after every kernel that read it
   while (!ctx->par2.empty() && (ctx->par2.size() >= kPar2CacheEntries || total > kPar2CacheBytes)) {
-    PP_TRACE("par2-table-evict", ctx->par2.back().bytes);
-    cudaStreamSynchronize(ctx->stream);
     total -= ctx->par2.back().bytes;
-    cudaFree(ctx->par2.back().d_coef);
-    cudaFree(ctx->par2.back().d_aexp);
+    pool_free(ctx, ctx->par2.back().d_coef);
+    pool_free(ctx, ctx->par2.back().d_aexp);
     ctx->par2.pop_back();
   }
-  PP_TRACE("par2-table-malloc", e.bytes);
-  if (cudaMalloc(&e.d_coef, cbytes) != cudaSuccess || (tbytes && cudaMalloc(&e.d_aexp, tbytes) != cudaSuccess)) {
-    cudaGetLastError();
-    cudaFree(e.d_coef);
+  PP_TRACE("par2-table-alloc", e.bytes);
+  e.d_coef = (uint16_t*)pool_alloc(ctx, cbytes);
+  e.d_aexp = tbytes ? (uint8_t*)pool_alloc(ctx, tbytes) : nullptr;
+  if (!e.d_coef || (tbytes && !e.d_aexp)) {
+    pool_free(ctx, e.d_coef);
+    pool_free(ctx, e.d_aexp);
     return set_err(ctx, PP_ERR_NO_MEMORY, "PAR2 coefficient table (%zu bytes)", e.bytes);
   }
   int r = par2_coeff_matrix_dev(ctx, input_idx, n_in, exps, n_out, e.d_coef);
@@ -541,9 +628,8 @@ static int par2_table(pp_ctx* ctx, const uint16_t* input_idx, unsigned n_in, con
     if (ce != cudaSuccess) r = set_err(ctx, PP_ERR_CUDA, "tile expansion: %s", cudaGetErrorString(ce));
   }
   if (r) {
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(e.d_coef);
-    cudaFree(e.d_aexp);
+    pool_free(ctx, e.d_coef);
+    pool_free(ctx, e.d_aexp);
     return r;
   }
   ctx->par2.push_front(std::move(e));
@@ -616,6 +702,7 @@ static int ensure_copy_stream(pp_ctx* ctx) {
     cudaGetLastError();
     return set_err(ctx, PP_ERR_CUDA, "copy stream");
   }
+  side_streams_follow(ctx);  // after the pool allocations made so far
   return PP_OK;
 }
 
@@ -627,6 +714,7 @@ static int ensure_hash_stream(pp_ctx* ctx) {
     cudaGetLastError();
     return set_err(ctx, PP_ERR_CUDA, "hash stream");
   }
+  side_streams_follow(ctx);  // after the pool allocations made so far
   return PP_OK;
 }
 
@@ -1481,61 +1569,36 @@ static uint64_t* cauchy_get(pp_ctx* ctx, size_t n_in, size_t n_rec, uint64_t fI,
       return ctx->cauchy.front().d;
     }
   }
-  // LRU of 8 matrices, as the reference's coefficient cache (src/par3_engine.cc:451-482)
-  // An evicted matrix's buffer is kept as a spare: the next matrix is built
-  // into it on the same stream, after every kernel that read the old one, so
-  // eviction needs neither a synchronisation nor a free (a free would wait
-  // for the whole device).
-  if (ctx->cauchy.size() >= 8) {
-    ctx->cauchy_spare.push_back({ctx->cauchy.back().d, ctx->cauchy.back().cap});
+  // LRU within kCauchyEntries / kCauchyBytes; matrices come from the
+  // context's pool, an evicted one is freed in the stream's order (after
+  // every kernel that read it)
+  const size_t need = n_in * n_rec * 8;
+  size_t total = need;
+  for (auto& e : ctx->cauchy) total += e.bytes;
+  while (!ctx->cauchy.empty() && (ctx->cauchy.size() >= kCauchyEntries || total > kCauchyBytes)) {
+    total -= ctx->cauchy.back().bytes;
+    pool_free(ctx, ctx->cauchy.back().d);
     ctx->cauchy.pop_back();
   }
-  const size_t need = n_in * n_rec * 8;
-  void* d = nullptr;
-  size_t cap = need;
-  {
-    int best = -1;  // the smallest spare that holds the matrix, if it is not more than twice as large
-    for (size_t k = 0; k < ctx->cauchy_spare.size(); k++) {
-      const size_t c = ctx->cauchy_spare[k].second;
-      if (c >= need && c <= 2 * need + (1 << 20) && (best < 0 || c < ctx->cauchy_spare[best].second)) best = (int)k;
-    }
-    if (best >= 0) {
-      d = ctx->cauchy_spare[best].first;
-      cap = ctx->cauchy_spare[best].second;
-      ctx->cauchy_spare.erase(ctx->cauchy_spare.begin() + best);
-    }
-  }
-  if (ctx->cauchy_spare.size() > 4) {  // bounded: release the oldest spares
-    PP_TRACE("cauchy-spare-free", ctx->cauchy_spare.front().second);
-    cudaStreamSynchronize(ctx->stream);
-    while (ctx->cauchy_spare.size() > 4) {
-      cudaFree(ctx->cauchy_spare.front().first);
-      ctx->cauchy_spare.erase(ctx->cauchy_spare.begin());
-    }
-  }
-  PP_TRACE("cauchy-malloc", need);
-  if (!d && cudaMalloc(&d, need) != cudaSuccess) {
-    cudaGetLastError();
-    // make room: drop every cached matrix and spare and retry once
-    cudaStreamSynchronize(ctx->stream);
-    for (auto& e : ctx->cauchy) cudaFree(e.d);
+  PP_TRACE("cauchy-alloc", need);
+  void* d = pool_alloc(ctx, need);
+  if (!d) {
+    // make room: drop every cached matrix and retry once
+    for (auto& e : ctx->cauchy) pool_free(ctx, e.d);
     ctx->cauchy.clear();
-    for (auto& e : ctx->cauchy_spare) cudaFree(e.first);
-    ctx->cauchy_spare.clear();
-    cap = need;
-    if (cudaMalloc(&d, need) != cudaSuccess) {
-      cudaGetLastError();
+    d = pool_alloc(ctx, need);
+    if (!d) {
       *st = set_err(ctx, PP_ERR_NO_MEMORY, "Cauchy matrix %zu x %zu", n_rec, n_in);
       return nullptr;
     }
   }
   cudaError_t e = launch_gf64_cauchy((uint64_t*)d, n_in, n_rec, fI, fR, n_in, ctx->stream);
   if (e != cudaSuccess) {
-    cudaFree(d);
+    pool_free(ctx, d);
     *st = set_err(ctx, PP_ERR_CUDA, "Cauchy build: %s", cudaGetErrorString(e));
     return nullptr;
   }
-  ctx->cauchy.push_front({n_in, n_rec, fI, fR, (uint64_t*)d, cap});
+  ctx->cauchy.push_front({n_in, n_rec, fI, fR, (uint64_t*)d, need});
   return (uint64_t*)d;
 }
 
