@@ -133,10 +133,11 @@ TRAFFIC = {
     "k_gf16_muladd_tc.par2_create_32768x32KiB_R64": 4 * (543139328 + 9490176),
     "k_gf16_muladd_tc.par2_create_1024x1MiB_R8": 1087907000 + 10907904,
     "k_gf64_matvec_tc.par3_create_131072x8KiB_R8": 1083011000 + 3985664,
-    # FP4 GF(2^16) kernel: the 8,192-slice R=64 capture (403.9 + 5.3 MB) and the
-    # 256 x 1 MiB R=8 capture (268.8 + 9.0 MB), each scaled by 4 to the 1 GiB launch
-    "k_gf16_muladd_f4.par2_create_32768x32KiB_R64": 4 * (403939584 + 5251840),
-    "k_gf16_muladd_f4.par2_create_1024x1MiB_R8": 4 * (268794624 + 9036032),
+    # FP4 GF(2^16) kernel (input rows by tensor-map boxes): the 8,192-slice R=64
+    # capture (404.9 + 4.8 MB) and the 256 x 1 MiB R=8 capture (268.8 + 8.8 MB),
+    # each scaled by 4 to the 1 GiB launch
+    "k_gf16_muladd_f4.par2_create_32768x32KiB_R64": 4 * (404915712 + 4844544),
+    "k_gf16_muladd_f4.par2_create_1024x1MiB_R8": 4 * (268810240 + 8846336),
     # the SM-pair kernel's 32,768-block capture (270.8 + 4.3 MB) scaled to 131,072 blocks
     "k_gf64_matvec_tc_pair.par3_create_131072x8KiB_R8": 4 * (270800000 + 4300000),
 }
