@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import sys
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -235,7 +236,14 @@ def status_string(s: int) -> str:
 
 
 class Context:
-    """One device + stream.  ``check`` turns statuses into ``PPError``."""
+    """One device + stream.  ``check`` turns statuses into ``PPError``.
+
+    The library runs a context's work on its CUDA stream.  From Python that
+    stream follows torch's current stream on the context's device (as a torch
+    operation would), so CUDA tensors produced before a call are ready when
+    its kernels read them and torch work queued after it sees its results;
+    the module functions rebind before every call (``follow_torch``).
+    ``set_stream`` pins an explicit stream instead."""
 
     def __init__(self, device: int = 0):
         h = _P()
@@ -244,6 +252,8 @@ class Context:
             raise PPError(st, status_string(st))
         self.h = h
         self.device = device
+        self._follow = True
+        self._bound = None
 
     def check(self, st: int) -> int:
         if st != PP_OK:
@@ -265,7 +275,31 @@ class Context:
         return ms.value, int(n.value)
 
     def set_stream(self, stream_ptr: int | None):
+        """Pin the context to a CUDA stream (None: its own stream); stops
+        following torch's current stream."""
+        self._follow = False
+        self._bound = None
         self.check(lib.pp_ctx_set_stream(self.h, _P(stream_ptr or 0)))
+
+    def follow_torch(self):
+        """Bind the context to torch's current stream on its device, if torch
+        has initialised CUDA and no stream was pinned (torch's default stream
+        is CUDA's legacy default stream, handle 1 in the C API)."""
+        if not self._follow:
+            return self
+        torch = sys.modules.get("torch")
+        if torch is None:
+            return self
+        try:
+            if not torch.cuda.is_initialized():
+                return self
+            s = int(torch.cuda.current_stream(self.device).cuda_stream) or 1
+        except Exception:
+            return self
+        if s != self._bound:
+            self.check(lib.pp_ctx_set_stream(self.h, _P(s)))
+            self._bound = s
+        return self
 
     def set_gf16_kernel(self, kernel: int):
         """PP_GF16_KERNEL_AUTO / _LUT / _TENSOR"""

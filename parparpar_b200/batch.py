@@ -19,7 +19,7 @@ from ._lib import (PP_BATCH_NO_GRAPH, PP_BATCH_TUNE, PP_JOB_GF16_MULADD, PP_JOB_
 
 
 def _ctx(ctx):
-    return ctx if ctx is not None else default_context()
+    return (ctx if ctx is not None else default_context()).follow_torch()
 
 
 def _rows(t):

@@ -486,19 +486,24 @@ static uint64_t tiles16(const Gf16TcJob& j) { return (uint64_t)j.groups * j.wt; 
 // ============================================================================
 // The same product on the block-scaled FP4 path (tcgen05.mma kind::mxf4).
 //
-// Operands are e2m1 values 0 or 1.0 (nibbles 0x0 / 0x2), two per byte, with
-// every ue8m0 scale factor 1.0 (0x7F), so each MMA adds exact integer counts
-// into fp32 accumulators (counts stay below 16 * 32768 < 2^23).  The parity of
-// a count is read by adding 2^23: the sum's lowest mantissa bit is the count's
-// lowest bit.  Half the operand bytes of the int8 form per GF(2) product and
-// the FP4 rate of the tensor pipe.
+// A operands are e2m1 values 0 or 1.0 (nibbles 0x0 / 0x2), two per byte; B
+// operands are 0 or a power of two, cancelled by the block scale factors
+// (ue8m0), so each MMA adds exact integer counts into fp32 accumulators
+// (counts stay below 16 * 32768 < 2^23).  The parity of a count is read by
+// adding 2^23: the sum's lowest mantissa bit is the count's lowest bit.  Half
+// the operand bytes of the int8 form per GF(2) product and the FP4 rate of
+// the tensor pipe.
 //
-// Bit selection: e2m1 codes are not parities of their value, so each B
-// element must be exactly 0 or 1.0.  Four bits of a word are picked per shift:
-// ((w >> j) & 0x1111) << 1 places bits j, 4+j, 8+j, 12+j of w in nibbles
-// 0..3 as 0x0 / 0x2.  With
+// Bit selection: e2m1 codes are not parities of their value, so a B element
+// must be 0 or one fixed nonzero value per scale block.  Bit j of each nibble
+// of a word, masked in place, is such a value: w & 0x1111 -> 0 / 0.5 (0x1),
+// w & 0x2222 -> 0 / 1.0 (0x2), w & 0x4444 -> 0 / 2.0 (0x4); bit 3 (0x8 is
+// -0) is shifted down first, (w >> 1) & 0x4444 -> 0 / 2.0.  The MMA step j
+// reads only elements of selection j, so its B scale factor 1 / v_j makes
+// every nonzero product exactly 1: 2.0 for j = 0, 1.0 for j = 1, 0.5 for j = 2
+// and 3 (three sets of B scale columns, A scales 1.0).  With
 //   A[(o,b)][(j, i, m)] = 1.0 * bit_b(c[o][i] * x^(4m + j))
-//   B[w][(j, i, m)]     = 1.0 * bit_(4m + j)(in_i[w])          (j = 0..3)
+//   B[w][(j, i, m)]     = v_j * bit_(4m + j)(in_i[w])     (v_j = 0.5, 1, 2, 2)
 // D[(o,b)][w] counts the terms of bit b of out[o][w].  A stage is 16 inputs:
 // K = 256 elements = one 128-byte (swizzled) row; the 64-element MMA step j
 // covers 32 bytes: inputs 0-7 then 8-15, two u32 words (two inputs) each.
@@ -506,9 +511,10 @@ static uint64_t tiles16(const Gf16TcJob& j) { return (uint64_t)j.groups * j.wt; 
 // CTA tile: KG = 2 -> 16 outputs x 240 words (two accumulators of N = 240,
 // one per output group, sharing each B tile); KG = 1 -> 8 outputs x 480 words
 // (two accumulators of N = 240 on the two halves of the B tile, sharing each
-// A tile).  TMEM: accumulators at columns 0 and 256 (240 each), scale factors
-// in columns 240-255 (A at 240, B at 248).  Warp roles and bounded waits as in
-// the int8 kernel.
+// A tile).  TMEM: accumulators at columns 0 and 256 (240 each); scale
+// factors A 1.0 in columns 240-243, B 2.0 in 248-255, 1.0 in 496-503, 0.5 in
+// 504-511 (8-column B sets on 8-column boundaries).  Warp roles and bounded
+// waits as in the int8 kernel.
 namespace tc16f4 {
 using namespace pp::tc;
 
@@ -517,7 +523,8 @@ constexpr int kABytes = 128 * 128;  // A tile of one output group: 128 rows x 12
 constexpr int kThreads = 320;
 constexpr int kExp = 256;
 constexpr int kN = 240;             // words per accumulator
-constexpr uint32_t kSfaCol = 240, kSfbCol = 248;
+// scale-factor columns: A (4 columns), B for selections 0, 1 and 2-3 (8 columns each)
+constexpr uint32_t kSfaCol = 240, kSfb0Col = 248, kSfb1Col = 496, kSfb2Col = 504;
 
 // ring depths (A tiles + raw rows, B tiles); the two-group tile's can be set
 // at build time for measurements
@@ -566,8 +573,13 @@ PP_D void mma_f4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accum
       : "memory");
 }
 
-// nibbles 0x2 where bit (4m + j) of each 16-bit half of p is set
+// A operand: nibbles 0x2 (1.0) where bit (4m + j) of each 16-bit half of p is set
 PP_D uint32_t pick4(uint32_t p, int j) { return ((p >> j) & 0x11111111u) << 1; }
+// selection j of the B operand: nibble m holds bit (4m + j) of p as 0 or v_j
+// (0x1 = 0.5, 0x2 = 1.0, 0x4 = 2.0, 0x4 = 2.0 for j = 0..3)
+PP_D uint32_t sel4(uint32_t p, int j) {
+  return j == 3 ? (p >> 1) & 0x44444444u : p & (0x11111111u << j);
+}
 
 // A tiles: for output group g and stage s (inputs 16s..16s+15) a 16 KiB tile
 // in the canonical K-major 128-byte-swizzled layout: row m = 16*oo + b; the
@@ -685,12 +697,20 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, const __grid_constan
   tc_fence_after();
   const uint32_t tmem = *tmem_holder;
   if (warp >= 2 && warp < 6) {
-    // scale factors 1.0 (ue8m0 0x7F) in columns 240-255 of this warp's lane quarter
-    const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + kSfaCol;
-    const uint32_t v = 0x7F7F7F7Fu;
+    // scale factors (ue8m0: 0x80 = 2.0, 0x7F = 1.0, 0x7E = 0.5) in this warp's
+    // lane quarter: columns 240-255 = A 1.0 (240-243), unused, B 2.0 (248-255);
+    // columns 496-511 = B 1.0 (496-503), B 0.5 (504-511)
+    const uint32_t q = (uint32_t)(32 * (warp & 3)) << 16;
+    const uint32_t two = 0x80808080u, one = 0x7F7F7F7Fu, half = 0x7E7E7E7Eu;
     asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(t),
-        "r"(v)
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%2,%2,%2,%2,%2,%2,%2,%2};" ::"r"(
+            tmem + q + kSfaCol),
+        "r"(one), "r"(two)
+        : "memory");
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%2,%2,%2,%2,%2,%2,%2,%2};" ::"r"(
+            tmem + q + kSfb1Col),
+        "r"(one), "r"(half)
         : "memory");
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
   }
@@ -735,7 +755,7 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, const __grid_constan
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      const uint32_t sfa = tmem + kSfaCol, sfb = tmem + kSfbCol;
+      const uint32_t sfa = tmem + kSfaCol;
       for (unsigned k = 0; k < nst; k++) {
         const unsigned sl = k % kLd, bs = k % kBs;
         if (*err || !mbar_wait(BAR(A_FULL + sl), (k / kLd) & 1) || !mbar_wait(BAR(B_FULL + bs), (k / kBs) & 1)) {
@@ -751,7 +771,8 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, const __grid_constan
             const uint32_t a_off = KG == 2 ? nn * kABytes : 0;
             const uint32_t b_off = KG == 2 ? 0 : nn * (kN * 128);
             mma_f4(tmem + nn * 256, sw128_desc(sA + sl * kAStage + a_off + 32 * kk),
-                   sw128_desc(sB + bs * kBBytes + b_off + 32 * kk), (k > 0 || kk > 0) ? 1u : 0u, sfa, sfb);
+                   sw128_desc(sB + bs * kBBytes + b_off + 32 * kk), (k > 0 || kk > 0) ? 1u : 0u, sfa,
+                   tmem + (kk == 0 ? kSfb0Col : kk == 1 ? kSfb1Col : kSfb2Col));
           }
         }
         mma_commit(BAR(A_EMPTY + sl));
@@ -829,8 +850,8 @@ k_gf16_muladd_f4(const __grid_constant__ Gf16TcBatch batch, const __grid_constan
           const uint32_t row = bt + (n >> 3) * 1024 + (n & 7) * 128, r7 = n & 7;
 #pragma unroll
           for (int j = 0; j < 4; j++) {
-            sts128(row + (((2 * j) ^ r7) << 4), pick4(P[0], j), pick4(P[1], j), pick4(P[2], j), pick4(P[3], j));
-            sts128(row + (((2 * j + 1) ^ r7) << 4), pick4(P[4], j), pick4(P[5], j), pick4(P[6], j), pick4(P[7], j));
+            sts128(row + (((2 * j) ^ r7) << 4), sel4(P[0], j), sel4(P[1], j), sel4(P[2], j), sel4(P[3], j));
+            sts128(row + (((2 * j + 1) ^ r7) << 4), sel4(P[4], j), sel4(P[5], j), sel4(P[6], j), sel4(P[7], j));
           }
         }
       }

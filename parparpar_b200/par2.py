@@ -29,7 +29,7 @@ from ._lib import PP_OK, PPError, default_context, lib, ptr
 
 
 def _ctx(ctx):
-    return ctx if ctx is not None else default_context()
+    return (ctx if ctx is not None else default_context()).follow_torch()
 
 
 def gfmat_coeff(input_block: int, recovery_exp: int) -> int:
@@ -190,6 +190,11 @@ class PAR2ProcCUDA:
         self._chk(lib.pp_par2_proc_wait_for_add(self.h))
 
     def addInput(self, buffer, size: int, inputNumOrCoeffs, flush: bool = False):
+        if getattr(buffer, "is_cuda", False):
+            # the processor copies device slices on its own stream: the
+            # producer of a CUDA tensor (torch's current stream) finishes first
+            import torch
+            torch.cuda.current_stream(buffer.device).synchronize()
         if isinstance(inputNumOrCoeffs, (int, np.integer)):
             self._chk(lib.pp_par2_proc_add_input(self.h, ptr(buffer), size, int(inputNumOrCoeffs), 1 if flush else 0))
         else:

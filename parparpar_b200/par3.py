@@ -29,7 +29,7 @@ from ._lib import PP_OK, PPError, default_context, lib, ptr
 
 
 def _ctx(ctx):
-    return ctx if ctx is not None else default_context()
+    return (ctx if ctx is not None else default_context()).follow_torch()
 
 
 def _u64(x) -> int:

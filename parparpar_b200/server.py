@@ -27,6 +27,12 @@ class Server:
         """Queue a job (a tuple from the batch helpers); returns its ticket.
         The job's buffers are kept referenced until wait() returns."""
         j, keep = job
+        cuda = [b for b in (keep if isinstance(keep, (list, tuple)) else [keep]) if getattr(b, "is_cuda", False)]
+        if cuda:
+            # the server copies and reads device buffers on its own lanes: the
+            # producer of a CUDA tensor (torch's current stream) finishes first
+            import torch
+            torch.cuda.current_stream(cuda[0].device).synchronize()
         t = ctypes.c_uint64()
         st = lib.pp_server_submit(self.h, ctypes.byref(j), ctypes.byref(t))
         if st != PP_OK:

@@ -61,7 +61,7 @@ def _range_arrays(ranges, contexts):
     n = len(ranges)
     if len(contexts) != n:
         raise ValueError("one context per range")
-    ctxs = (ctypes.c_void_p * n)(*[c.h.value for c in contexts])
+    ctxs = (ctypes.c_void_p * n)(*[c.follow_torch().h.value for c in contexts])
     b = (ctypes.c_size_t * n)(*[r[0] for r in ranges])
     e = (ctypes.c_size_t * n)(*[r[1] for r in ranges])
     return ctxs, b, e, n
