@@ -88,20 +88,20 @@ def bit_macs(w):
 
 def roofline(w, args, hbm_achieved, hbm_peak, peak_kind, kms, int8_tops):
     """Roofline of the dominant kernel.  The tensor-core kernels compute each
-    GF product as a dense GF(2) bit-matrix contraction in int8 MMAs, so their
-    binding unit is the int8 tensor pipe: achieved = 2 x bit-MACs / kernel
-    time against the dense int8 GEMM throughput measured in the same run
-    (cuBLASLt); the HBM view of the same launch (algorithmic bytes / time
-    against MEASURED_PEAKS.json) is given beside it."""
+    GF product as a dense GF(2) bit-matrix contraction in FP4 or int8 MMAs,
+    so their binding unit is the tensor pipe: achieved = 2 x bit-MACs /
+    kernel time against the FP4 or int8 dense rate (tensor_peak); the HBM
+    view of the same launch (algorithmic bytes / time against
+    MEASURED_PEAKS.json) is given beside it."""
     kern = dominant_kernel(w, args)
     hbm = {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_achieved / hbm_peak,
            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
            else "fallback 6.65 TB/s"}
     r = {"kernel": kern, "kernel_ms": kms, "traffic": load_traffic(f"{kern}.{args.workload}")}
-    if kern.endswith(("_tc", "_tc_pair", "_f4")):
+    if kern.endswith(("_tc", "_tc_pair", "_f4", "_f4_pair")):
         tops = 2 * bit_macs(w) / (kms * 1e-3) / 1e12
         peak, kind, nominal, nominal_kind = tensor_peak(kern, int8_tops)
-        fmt = "FP4 (e2m1 0/1, block scales 1.0)" if kern.endswith("_f4") else "int8"
+        fmt = "FP4 (e2m1 with block scales, exact counts)" if "_f4" in kern else "int8"
         r.update({"bound": "tensor", "achieved": tops, "peak": peak, "unit": "TFLOP/s", "frac": tops / peak,
                   "peak_kind": kind, "ops": f"{fmt} tensor ops (2 per MAC), one MAC per GF(2) bit product",
                   "nominal_peak": nominal, "frac_of_nominal": tops / nominal, "nominal_kind": nominal_kind,
@@ -138,8 +138,10 @@ TRAFFIC = {
     # each scaled by 4 to the 1 GiB launch
     "k_gf16_muladd_f4.par2_create_32768x32KiB_R64": 4 * (404915712 + 4844544),
     "k_gf16_muladd_f4.par2_create_1024x1MiB_R8": 4 * (268810240 + 8846336),
-    # the SM-pair kernel's 32,768-block capture (270.8 + 4.3 MB) scaled to 131,072 blocks
+    # the SM-pair kernels' 32,768-block captures scaled to 131,072 blocks: int8
+    # (270.8 + 4.3 MB), FP4 (270.8 + 5.4 MB; the input read once, as for int8)
     "k_gf64_matvec_tc_pair.par3_create_131072x8KiB_R8": 4 * (270800000 + 4300000),
+    "k_gf64_matvec_f4_pair.par3_create_131072x8KiB_R8": 4 * (270786304 + 5406464),
 }
 
 
@@ -374,10 +376,14 @@ def dominant_kernel(w, args):
         return "k_b3_chunks"
     if args.gf64_kernel == "lut":
         return "k_gf64_matvec_lut"
-    if os.environ.get("PARPAR_B200_GF64_TC") == "f4":
-        return "k_gf64_matvec_f4"
-    # the SM-pair kernel runs when every job of the launch has >= 4 outputs
-    return "k_gf64_matvec_tc_pair" if w["r"] >= 4 else "k_gf64_matvec_tc"
+    # the SM-pair kernel runs when every job of the launch has >= 4 outputs;
+    # FP4 on SM pairs, int8 on one CTA, unless PARPAR_B200_GF64_TC fixes one
+    pair = w["r"] >= 4
+    fmt = os.environ.get("PARPAR_B200_GF64_TC")
+    f4 = fmt == "f4" or (fmt != "i8" and pair)
+    if f4:
+        return "k_gf64_matvec_f4_pair" if pair else "k_gf64_matvec_f4"
+    return "k_gf64_matvec_tc_pair" if pair else "k_gf64_matvec_tc"
 
 
 def tensor_peak(kern, int8_tops):
@@ -387,7 +393,7 @@ def tensor_peak(kern, int8_tops):
     kernels against the cuBLASLt int8 GEMM measured in this run (else 2 x
     bf16)."""
     bf16, src = load_bf16_peak()
-    if kern.endswith("_f4"):
+    if "_f4" in kern:
         return (4 * bf16, f"4 x {src} (dense FP4 rate = 4x bf16)", 9000.0,
                 "B200 dense FP4 tensor rate (NVIDIA's 9 PFLOP/s dense figure)")
     if int8_tops:
@@ -1176,7 +1182,7 @@ def main():
                 ent = {"workload": name, "value": input_bytes_of(name) / (m["ms"] * 1e-3) / 1e9,
                        "unit": "GB/s", "ms_per_step": m["ms"], "kernel_ms": m["kernel_ms"], "hbm_frac": m["frac"]}
                 kern = dominant_kernel(WORKLOADS[name], args)
-                if kern.endswith(("_tc", "_tc_pair", "_f4")):
+                if kern.endswith(("_tc", "_tc_pair", "_f4", "_f4_pair")):
                     ent["kernel"] = kern
                     ent["tensor_frac"] = (2 * bit_macs(WORKLOADS[name]) / (m["kernel_ms"] * 1e-3) / 1e12 /
                                           tensor_peak(kern, int8_tops)[0])

@@ -585,13 +585,12 @@ static uint64_t tiles64(const Gf64TcJob& j) { return (uint64_t)j.pairs * j.wt; }
 
 // ============================================================================
 // The GF(2^64) product on the block-scaled FP4 path (tcgen05.mma kind::mxf4),
-// one CTA per tile.  As in the GF(2^16) FP4 kernel (gf16_tc.cu): e2m1
-// operands 0 / 1.0 (nibbles 0x0 / 0x2), ue8m0 scale factors 1.0, exact fp32
+// one CTA per tile.  As in the GF(2^16) FP4 kernel (gf16_tc.cu): exact fp32
 // counts (an item sums at most 65,536 inputs: counts < 64 * 2^16 = 2^22), the
-// parity read as the lowest mantissa bit of count + 2^23.  Four bits of each
-// 32-bit half of a word are picked per shift:
-//   B[w][(j, ii, half, m)]     = bit (32 half + 4m + j) of x_ii[w]
-//   A[(o,b)][(j, ii, half, m)] = bit (32 half + 4m + j) of Q_{o,ii,b}
+// parity read as the lowest mantissa bit of count + 2^23.  Selection j of
+// each 32-bit half of a word (bits 4m + j) feeds MMA step j, on both operands:
+//   B[w][(j, ii, half, m)]     = v_j * bit (32 half + 4m + j) of x_ii[w]
+//   A[(o,b)][(j, ii, half, m)] = v_j * bit (32 half + 4m + j) of Q_{o,ii,b}
 // (Q = row b of the multiplication matrix, the closed form above).  A stage is
 // 4 inputs: K = 256 elements = one 128-byte swizzled row; the 64-element MMA
 // step j covers 32 bytes: inputs 0-1 in its first 16-byte chunk, 2-3 in the
@@ -622,7 +621,7 @@ constexpr int kOffRaw = kOffB + kBs * kBBytes;
 constexpr int kOffBar = kOffRaw + kLd * kRawBytes;
 constexpr int kSmemBytes = kOffBar + 256 + 1024;
 constexpr uint32_t kMaxStagesPerItem = 16384;  // 65,536 inputs
-constexpr uint32_t kSfaCol = 240, kSfbCol = 248;
+constexpr uint32_t kSfaCol = 240;
 static_assert(kSmemBytes <= 227 * 1024, "shared memory");
 static_assert(kOffB % 1024 == 0 && kBBytes % 1024 == 0 && (kN * 128) % 1024 == 0, "swizzle atoms");
 constexpr uint32_t kIdesc = (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
@@ -635,7 +634,69 @@ PP_D void mma_f4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accum
       "l"(adesc), "l"(bdesc), "r"(accumulate), "r"(sfa), "r"(sfb), "r"(kIdesc)
       : "memory");
 }
-PP_D uint32_t pick4(uint32_t p, int j) { return ((p >> j) & 0x11111111u) << 1; }
+// Selection j of an operand word, in place: bit j of every nibble (bit 3 moved
+// to bit 2, since e2m1 0x8 is -0), so a nonzero element of MMA step j is v_j =
+// 0.5, 1, 2, 2 (e2m1 0x1, 0x2, 0x4, 0x4) on both operands and a product v_j^2.
+// The B scale factor of step j is 1 / v_j^2 (4, 1, 0.25, 0.25), A's is 1, so
+// every nonzero product adds exactly 1.  TMEM scale columns: A 240-243, B
+// 248-255 (step 0), 496-503 (step 1), 504-511 (steps 2-3); 8-column B sets
+// start on 8-column boundaries.
+PP_D uint32_t sel4(uint32_t p, int j) { return j == 3 ? (p >> 1) & 0x44444444u : p & (0x11111111u << j); }
+PP_D uint32_t sfb_col(int kk) { return kk == 0 ? 248u : kk == 1 ? 496u : 504u; }
+// the scale factors of this warp's TMEM lane quarter (warps 2-5 of a CTA)
+PP_D void fill_scales(uint32_t tmem, int warp) {
+  const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+  const uint32_t four = 0x81818181u, one = 0x7F7F7F7Fu, quarter = 0x7D7D7D7Du;  // ue8m0 4, 1, 0.25
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%2,%2,%2,%2,%2,%2,%2,%2};" ::"r"(t + 240),
+      "r"(one), "r"(four)
+      : "memory");
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%2,%2,%2,%2,%2,%2,%2,%2};" ::"r"(t + 496),
+      "r"(one), "r"(quarter)
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// A rows: builder thread e makes rows b, b + 1 (b = 2 (e % 32)) of the
+// multiplication matrix of coefficient e / 32 of the stage (output e / 128,
+// input (e / 32) % 4): row b by the closed form, row b + 1 from it by one
+// step of Q_{b+1} = ((Q_b ^ [b+1 in {0,1,3,4}] Q_63) << 1) | bit_{b+1}(c),
+// which follows from c x^{e+1} = (c x^e) x mod x^64 + x^4 + x^3 + x + 1.
+PP_D uint64_t mul_matrix_row63(uint64_t c) {  // row 63: the closed form at b = 63
+  const uint64_t rv = __brevll(c);
+  return rv ^ (rv << 63) ^ (rv << 61) ^ (rv << 60);
+}
+struct ARows {
+  unsigned oo, ii, b, ch;
+  uint32_t row0, r70, row1, r71;
+  uint64_t red;
+  PP_D explicit ARows(int e) {
+    const unsigned kc = (unsigned)e >> 5;
+    oo = kc >> 2;
+    ii = kc & 3;
+    b = 2 * ((unsigned)e & 31);
+    const unsigned m0 = 64 * oo + b, m1 = m0 + 1;
+    // input ii sits at chunk 2j + ii / 2, byte 8 (ii % 2) of an A row
+    ch = ii >> 1;
+    row0 = (m0 >> 3) * 1024 + (m0 & 7) * 128 + 8 * (ii & 1);
+    r70 = m0 & 7;
+    row1 = (m1 >> 3) * 1024 + (m1 & 7) * 128 + 8 * (ii & 1);
+    r71 = m1 & 7;
+    red = (b + 1 == 1 || b + 1 == 3) ? ~0ull : 0ull;  // b + 1 in {1, 3}: Q_63 enters
+  }
+  // rows b, b + 1 of coefficient c into the A tile at `at`
+  PP_D void store(uint32_t at, uint64_t c) const {
+    const uint64_t q0 = mul_matrix_row_f4(c, b);
+    const uint64_t q1 = ((q0 ^ (mul_matrix_row63(c) & red)) << 1) | ((c >> (b + 1)) & 1ull);
+    const uint32_t q0lo = (uint32_t)q0, q0hi = (uint32_t)(q0 >> 32), q1lo = (uint32_t)q1, q1hi = (uint32_t)(q1 >> 32);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      sts64(at + row0 + (((2 * j + ch) ^ r70) << 4), sel4(q0lo, j), sel4(q0hi, j));
+      sts64(at + row1 + (((2 * j + ch) ^ r71) << 4), sel4(q1lo, j), sel4(q1hi, j));
+    }
+  }
+};
 
 __global__ void __launch_bounds__(kThreads, 1)
 k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ status) {
@@ -680,16 +741,7 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_holder;
-  if (warp >= 2 && warp < 6) {
-    // scale factors 1.0 (ue8m0 0x7F) in columns 240-255 of this warp's lane quarter
-    const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + kSfaCol;
-    const uint32_t v = 0x7F7F7F7Fu;
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(t),
-        "r"(v)
-        : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-  }
+  if (warp >= 2 && warp < 6) fill_scales(tmem, warp);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -727,7 +779,7 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      const uint32_t sfa = tmem + kSfaCol, sfb = tmem + kSfbCol;
+      const uint32_t sfa = tmem + kSfaCol;
       for (unsigned k = 0; k < sg.st1 - sg.st0; k++) {
         const unsigned bs = k % kBs;
         if (*err || !mbar_wait(BAR(OP_FULL + bs), (k / kBs) & 1)) {
@@ -741,7 +793,7 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
           for (int nn = 0; nn < 2; nn++) {
             mma_f4(tmem + nn * 256, sw128_desc(sA + bs * kABytes + 32 * kk),
                    sw128_desc(sB + bs * kBBytes + nn * (kN * 128) + 32 * kk), (k > 0 || kk > 0) ? 1u : 0u, sfa,
-                   sfb);
+                   tmem + sfb_col(kk));
           }
         }
         mma_commit(BAR(OP_EMPTY + bs));
@@ -753,10 +805,7 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
   } else {
     // ------------------------------------------------------------ operand builders
     const int e = threadIdx.x - 64;  // 0..255
-    // A: row a_m, inputs a_ii and a_ii + 2 (adjacent threads alternate a_ii, so
-    // a 64-bit store phase of 16 threads covers 8 rows x both halves of a chunk)
-    const unsigned a_ii = e & 1, a_m = e >> 1, a_oo = a_m >> 6, a_b = a_m & 63;
-    const uint32_t arow = (a_m >> 3) * 1024 + (a_m & 7) * 128 + 8 * a_ii, ar7 = a_m & 7;
+    const ARows ar(e);
     const int q = warp & 3;
     const int chalf = (warp - 2) >> 2;
     do {
@@ -766,14 +815,13 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
       const unsigned words_valid = (unsigned)min((size_t)kWords, J.words - w0);
       const unsigned nst = sg.st1 - sg.st0;
       auto coef = [&](unsigned k, unsigned ii) -> uint64_t {
-        const unsigned o = o0 + a_oo, i = (sg.st0 + k) * kStageIn + ii;
+        const unsigned o = o0 + ar.oo, i = (sg.st0 + k) * kStageIn + ii;
         return (k < nst && o < J.n_out && i < J.n_in) ? J.coeff[(size_t)o * J.ldc + i] : 0ull;
       };
-      uint64_t c0 = coef(0, a_ii), c1 = coef(0, a_ii + 2);
+      uint64_t c0 = coef(0, ar.ii);
       for (unsigned k = 0; k < nst; k++) {
         const unsigned sl = k % kLd, bs = k % kBs;
-        const uint64_t n0 = coef(k + 1, a_ii), n1 = coef(k + 1, a_ii + 2);  // next stage's coefficients
-        const uint64_t q0 = mul_matrix_row_f4(c0, a_b), q1 = mul_matrix_row_f4(c1, a_b);
+        const uint64_t n0 = coef(k + 1, ar.ii);  // the next stage's coefficient
         if (*err || !mbar_wait(BAR(RAW_FULL + sl), (k / kLd) & 1)) {
           *err = 1;
           break;
@@ -800,14 +848,7 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
           break;
         }
         const uint32_t at = sA + bs * kABytes, bt = sB + bs * kBBytes;
-        const uint32_t q0lo = (uint32_t)q0, q0hi = (uint32_t)(q0 >> 32), q1lo = (uint32_t)q1,
-                       q1hi = (uint32_t)(q1 >> 32);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          // A: input a_ii in chunk 2j, input a_ii + 2 in chunk 2j + 1, at byte 8 a_ii
-          sts64(at + arow + (((2 * j) ^ ar7) << 4), pick4(q0lo, j), pick4(q0hi, j));
-          sts64(at + arow + (((2 * j + 1) ^ ar7) << 4), pick4(q1lo, j), pick4(q1hi, j));
-        }
+        ar.store(at, c0);
         if (e < kN) {
 #pragma unroll
           for (int rr = 0; rr < 2; rr++) {
@@ -815,17 +856,16 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
             const uint32_t brow = bt + (u >> 3) * 1024 + (u & 7) * 128, br7 = u & 7;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-              sts128(brow + (((2 * j) ^ br7) << 4), pick4(xw[rr][0], j), pick4(xw[rr][1], j), pick4(xw[rr][2], j),
-                     pick4(xw[rr][3], j));
-              sts128(brow + (((2 * j + 1) ^ br7) << 4), pick4(xw[rr][4], j), pick4(xw[rr][5], j),
-                     pick4(xw[rr][6], j), pick4(xw[rr][7], j));
+              sts128(brow + (((2 * j) ^ br7) << 4), sel4(xw[rr][0], j), sel4(xw[rr][1], j), sel4(xw[rr][2], j),
+                     sel4(xw[rr][3], j));
+              sts128(brow + (((2 * j + 1) ^ br7) << 4), sel4(xw[rr][4], j), sel4(xw[rr][5], j),
+                     sel4(xw[rr][6], j), sel4(xw[rr][7], j));
             }
           }
         }
         fence_async_smem();
         mbar_arrive(BAR(OP_FULL + bs));
         c0 = n0;
-        c1 = n1;
       }
       // ---------------------------------------------------------- epilogue
       if (*err || !mbar_wait(BAR(D_FULL), 0)) {
@@ -874,18 +914,20 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
 // ---------------------------------------------------------------------------
 // FP4 on SM pairs (cluster of 2, tcgen05.mma cta_group::2 kind::mxf4, M = 256):
 // the pair covers 4 outputs (CTA r holds the A rows and the accumulators of
-// outputs o0 + 2r, o0 + 2r + 1) x 480 words (CTA r builds the B rows of words
-// w0 + 240 r + u, u = 0..239); MMA nn takes B rows 120 nn .. 120 nn + 119 of
-// each CTA (N = 240), so column c of accumulator nn is word
-// w0 + 240 (c / 120) + 120 nn + c % 120.  Per SM the B tile is half that of
-// the one-CTA FP4 kernel.  Scale factors 1.0 in TMEM columns 240-255 and
-// 496-511 of both CTAs (A at 240, B at 496).  Pipeline and bounded waits as
-// the int8 pair kernel: CTA 1's warp 1 relays "stage built" to CTA 0, whose
-// warp 1 issues the MMAs and whose commits arrive in both CTAs.
-constexpr int kPN = 240;
-constexpr int kPRowsMma = kPN / 2;               // B rows per CTA per MMA
-constexpr int kPWordsCta = kPN;                  // words built per CTA
-constexpr int kPWords = 2 * kPN;                 // words per pair tile
+// outputs o0 + 2r, o0 + 2r + 1) x 2N words (CTA r builds the B rows of words
+// w0 + N r + u, u < N); MMA nn takes B rows H nn .. H nn + H - 1 of each CTA
+// (H = N / 2), so column c of accumulator nn is word w0 + N (c / H) + H nn +
+// c % H.  N is chosen per job (Gf64TcJob::n_mma, a multiple of 16 up to 240)
+// so that tiles of 2N words cover the block with little waste (8 KiB blocks:
+// 1,024 words as 3 tiles of 352, not 3 of 480; 4 KiB blocks: 2 of 256).  Per
+// SM the B tile is half that of the one-CTA FP4 kernel.  Operand selections,
+// scale factors (the same columns in both CTAs) and A rows as the one-CTA
+// kernel.  Pipeline and bounded waits as the int8 pair kernel: CTA 1's warp 1
+// relays "stage built" to CTA 0, whose warp 1 issues the MMAs and whose
+// commits arrive in both CTAs.
+constexpr int kPN = 240;                         // largest N
+constexpr int kPWordsCta = kPN;                  // words built per CTA, at most
+constexpr int kPWords = 2 * kPN;                 // words per pair tile, at most
 constexpr int kPBBytes = kPWordsCta * 128;       // 30 KiB
 constexpr int kPRawBytes = kStageIn * kPWordsCta * 8;  // 7.5 KiB
 constexpr int kPLd = 5;
@@ -895,19 +937,30 @@ constexpr int kPOffB = kPBs * kABytes;
 constexpr int kPOffRaw = kPOffB + kPBs * kPBBytes;
 constexpr int kPOffBar = kPOffRaw + kPLd * kPRawBytes;
 constexpr int kPSmemBytes = kPOffBar + 256 + 1024;
-constexpr uint32_t kPSfaCol = 240, kPSfbCol = 496;
+constexpr uint32_t kPSfaCol = 240;
 static_assert(kPSmemBytes <= 227 * 1024, "shared memory");
-static_assert(kPOffB % 1024 == 0 && kPBBytes % 1024 == 0 && (kPRowsMma * 128) % 1024 == 0, "swizzle atoms");
-constexpr uint32_t kPIdesc =
-    (1u << 7) | (1u << 10) | ((uint32_t)(kPN >> 3) << 17) | (1u << 23) | ((256u >> 4) << 24);
+static_assert(kPOffB % 1024 == 0 && kPBBytes % 1024 == 0, "swizzle atoms");
+// instruction descriptor for N (a multiple of 16, so the N/2 B rows of each
+// CTA start on an 8-row swizzle atom)
+PP_D uint32_t pair_idesc(uint32_t n) {
+  return (1u << 7) | (1u << 10) | ((n >> 3) << 17) | (1u << 23) | ((256u >> 4) << 24);
+}
+// N for a job of `words` words: the fewest tiles of at most 2 x 240 words,
+// each as narrow as covers the block
+inline uint32_t pair_n_for(size_t words) {
+  if (!words) return kPN;
+  const size_t t = (words + kPWords - 1) / kPWords;
+  const size_t half = (words + 2 * t - 1) / (2 * t);
+  return (uint32_t)std::min<size_t>(kPN, std::max<size_t>(16, (half + 15) & ~(size_t)15));
+}
 
 PP_D void mma_f4_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate, uint32_t sfa,
-                      uint32_t sfb) {
+                      uint32_t sfb, uint32_t idesc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %3, 0;\n\t"
       "tcgen05.mma.cta_group::2.kind::mxf4.block_scale.block32 [%0], %1, %2, %6, [%4], [%5], p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(accumulate), "r"(sfa), "r"(sfb), "r"(kPIdesc)
+      "l"(adesc), "l"(bdesc), "r"(accumulate), "r"(sfa), "r"(sfb), "r"(idesc)
       : "memory");
 }
 
@@ -956,22 +1009,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_holder;
-  if (warp >= 2 && warp < 6) {
-    // scale factors 1.0 (ue8m0 0x7F) in columns 240-255 and 496-511 of this warp's lane quarter
-    const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
-    const uint32_t v = 0x7F7F7F7Fu;
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(
-            t + kPSfaCol),
-        "r"(v)
-        : "memory");
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(
-            t + kPSfbCol),
-        "r"(v)
-        : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-  }
+  if (warp >= 2 && warp < 6) fill_scales(tmem, warp);
   tc_fence_before();
   __syncthreads();
   cluster_sync();  // the peer's barriers and scale factors are ready before any remote arrive or MMA
@@ -984,8 +1022,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       uint32_t g = 0;
       do {
         const Gf64TcJob J = pinned_job(batch.job[sg.job]);
-        const size_t wc = (size_t)(sg.tile / J.pairs) * kPWords + (size_t)kPWordsCta * rank;
-        const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)kPWordsCta, J.words - wc) : 0u;
+        const unsigned np = J.n_mma;
+        const size_t wc = (size_t)(sg.tile / J.pairs) * (2 * np) + (size_t)np * rank;
+        const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)np, J.words - wc) : 0u;
         const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
         for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
           const unsigned sl = g % kPLd;
@@ -1012,7 +1051,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       const unsigned nst = sg.st1 - sg.st0;
       if (rank == 0) {
         // -------------------------------------------------------- MMA issuer
-        const uint32_t sfa = tmem + kPSfaCol, sfb = tmem + kPSfbCol;
+        const uint32_t sfa = tmem + kPSfaCol;
+        const unsigned np = batch.job[sg.job].n_mma, hp = np / 2;
+        const uint32_t idesc = pair_idesc(np);
         for (unsigned k = 0; k < nst; k++) {
           const unsigned bs = k % kPBs;
           const uint32_t ph = (k / kPBs) & 1;
@@ -1026,8 +1067,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int nn = 0; nn < 2; nn++) {
               mma_f4_pair(tmem + nn * 256, sw128_desc(sA + bs * kABytes + 32 * kk),
-                          sw128_desc(sB + bs * kPBBytes + nn * (kPRowsMma * 128) + 32 * kk),
-                          (k > 0 || kk > 0) ? 1u : 0u, sfa, sfb);
+                          sw128_desc(sB + bs * kPBBytes + nn * (hp * 128) + 32 * kk), (k > 0 || kk > 0) ? 1u : 0u,
+                          sfa, tmem + sfb_col(kk), idesc);
             }
           }
           mma_commit_pair(BAR(OP_EMPTY + bs));
@@ -1053,28 +1094,27 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   } else {
     // ------------------------------------------------------------ operand builders
     const int e = threadIdx.x - 64;  // 0..255
-    const unsigned a_ii = e & 1, a_m = e >> 1, a_oo = a_m >> 6, a_b = a_m & 63;
-    const uint32_t arow = (a_m >> 3) * 1024 + (a_m & 7) * 128 + 8 * a_ii, ar7 = a_m & 7;
+    const ARows ar(e);
     const int q = warp & 3;
     const int nn_ep = (warp - 2) >> 2;  // epilogue: accumulator
     uint32_t g = 0;
     do {
       const Gf64TcJob J = pinned_job(batch.job[sg.job]);
       const unsigned o0 = 4 * (unsigned)(sg.tile % J.pairs) + 2 * rank;  // this CTA's two outputs
-      const size_t w0 = (size_t)(sg.tile / J.pairs) * kPWords;
-      const size_t wc = w0 + (size_t)kPWordsCta * rank;
-      const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)kPWordsCta, J.words - wc) : 0u;
-      const bool okB = e < kPWordsCta && (unsigned)e < words_valid;
+      const unsigned np = J.n_mma, hp = np / 2;
+      const size_t w0 = (size_t)(sg.tile / J.pairs) * (2 * np);
+      const size_t wc = w0 + (size_t)np * rank;
+      const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)np, J.words - wc) : 0u;
+      const bool okB = (unsigned)e < np && (unsigned)e < words_valid;
       const unsigned nst = sg.st1 - sg.st0;
       auto coef = [&](unsigned k, unsigned ii) -> uint64_t {
-        const unsigned o = o0 + a_oo, i = (sg.st0 + k) * kStageIn + ii;
+        const unsigned o = o0 + ar.oo, i = (sg.st0 + k) * kStageIn + ii;
         return (k < nst && o < J.n_out && i < J.n_in) ? J.coeff[(size_t)o * J.ldc + i] : 0ull;
       };
-      uint64_t c0 = coef(0, a_ii), c1 = coef(0, a_ii + 2);
+      uint64_t c0 = coef(0, ar.ii);
       for (unsigned k = 0; k < nst; k++, g++) {
         const unsigned sl = g % kPLd, bs = g % kPBs;
-        const uint64_t n0 = coef(k + 1, a_ii), n1 = coef(k + 1, a_ii + 2);
-        const uint64_t q0 = mul_matrix_row_f4(c0, a_b), q1 = mul_matrix_row_f4(c1, a_b);
+        const uint64_t n0 = coef(k + 1, ar.ii);  // the next stage's coefficient
         if (*err || !mbar_wait(BAR(RAW_FULL + sl), (g / kPLd) & 1)) {
           *err = 1;
           break;
@@ -1095,27 +1135,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           break;
         }
         const uint32_t at = sA + bs * kABytes, bt = sB + bs * kPBBytes;
-        const uint32_t q0lo = (uint32_t)q0, q0hi = (uint32_t)(q0 >> 32), q1lo = (uint32_t)q1,
-                       q1hi = (uint32_t)(q1 >> 32);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          sts64(at + arow + (((2 * j) ^ ar7) << 4), pick4(q0lo, j), pick4(q0hi, j));
-          sts64(at + arow + (((2 * j + 1) ^ ar7) << 4), pick4(q1lo, j), pick4(q1hi, j));
-        }
-        if (e < kPWordsCta) {
+        ar.store(at, c0);
+        if ((unsigned)e < np) {
           const unsigned u = (unsigned)e;
           const uint32_t brow = bt + (u >> 3) * 1024 + (u & 7) * 128, br7 = u & 7;
 #pragma unroll
           for (int j = 0; j < 4; j++) {
-            sts128(brow + (((2 * j) ^ br7) << 4), pick4(xw[0], j), pick4(xw[1], j), pick4(xw[2], j), pick4(xw[3], j));
-            sts128(brow + (((2 * j + 1) ^ br7) << 4), pick4(xw[4], j), pick4(xw[5], j), pick4(xw[6], j),
-                   pick4(xw[7], j));
+            sts128(brow + (((2 * j) ^ br7) << 4), sel4(xw[0], j), sel4(xw[1], j), sel4(xw[2], j), sel4(xw[3], j));
+            sts128(brow + (((2 * j + 1) ^ br7) << 4), sel4(xw[4], j), sel4(xw[5], j), sel4(xw[6], j),
+                   sel4(xw[7], j));
           }
         }
         fence_async_smem();
         mbar_arrive(BAR(OPB_FULL + bs));
         c0 = n0;
-        c1 = n1;
       }
       // ---------------------------------------------------------- epilogue
       if (*err || !mbar_wait(BAR(D_FULL), 0)) {
@@ -1126,7 +1159,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       const unsigned o = o0 + (q >> 1);
       const unsigned half = q & 1;
       uint64_t* orow = o < J.n_out ? (J.out_ptrs ? J.out_ptrs[o] : J.out + (size_t)o * J.out_stride) : nullptr;
-      for (int cc = 0; cc < (kPN + 31) / 32; cc++) {
+      for (int cc = 0; cc < (int)(np + 31) / 32; cc++) {
         uint32_t r[32];
         tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + 256 * nn_ep + 32 * cc, r);
         uint32_t mine = 0;
@@ -1137,8 +1170,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           if (lane == jj) mine = bal;
         }
         const unsigned c = 32 * cc + lane;  // column of accumulator nn_ep
-        if (!orow || c >= (unsigned)kPN) continue;
-        const size_t widx = (size_t)kPWordsCta * (c / kPRowsMma) + (size_t)kPRowsMma * nn_ep + (c % kPRowsMma);
+        if (!orow || c >= np) continue;
+        const size_t widx = (size_t)np * (c / hp) + (size_t)hp * nn_ep + (c % hp);
         if (w0 + widx >= J.words) continue;
         uint32_t* dst = reinterpret_cast<uint32_t*>(orow + w0 + widx) + half;
         if (sg.mode == 2) {
@@ -1165,18 +1198,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 
 }  // namespace tc64f4
 
-// GF(2^64) tensor-core path: the int8 kernels (SM pair / one CTA) unless
-// PARPAR_B200_GF64_TC=f4 selects the FP4 one-CTA kernel; fixed per process
-// for reproducible timings.  The int8 SM-pair kernel stays the default: on
-// the 1 GiB PAR3 creates it ran 2.58 ms (R=8) and 348 ms (R=1,024) against
-// 3.46 ms and 435 ms for the FP4 one-CTA kernel, whose builders write the B
-// tile of all 480 words per SM (the pair kernel's CTAs build half of theirs).
-static bool gf64_tc_use_f4() {
-  static const bool f4 = [] {
+// Operand format of the GF(2^64) tensor-core path (the kernels build their A
+// operand from the coefficients, so it can differ per launch): FP4 on SM
+// pairs, int8 for the one-CTA kernel, unless PARPAR_B200_GF64_TC=f4 or =i8
+// fixes one format for both.  Measured on the 1 GiB PAR3 creates: FP4 pair
+// 2.35 ms (R=8), 250 ms (R=1,024), 832 ms (262,144 x 4 KiB, R=2,621) against
+// the int8 pair's 2.61 / 350 / 899 ms.
+static bool gf64_tc_use_f4(bool pair) {
+  static const int forced = [] {
     const char* v = getenv("PARPAR_B200_GF64_TC");
-    return v && strcmp(v, "f4") == 0;
+    return !v ? -1 : strcmp(v, "f4") == 0 ? 1 : strcmp(v, "i8") == 0 ? 0 : -1;
   }();
-  return f4;
+  return forced >= 0 ? forced != 0 : pair;
 }
 
 // Pair kernel (two SMs per tile) or one-CTA kernel for a whole table: the
@@ -1210,8 +1243,8 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     if (e != cudaSuccess) return e;
     device_mark(attr);
   }
-  const bool f4 = gf64_tc_use_f4();
   const bool pair = use_pair_kernel(b);
+  const bool f4 = gf64_tc_use_f4(pair);
   const size_t tile_words = f4 ? (pair ? tc64f4::kPWords : tc64f4::kWords) : tc64::kWords;
   const unsigned stage_in = f4 ? tc64f4::kStageIn : tc64::kStageIn;
   // drop empty jobs (nothing to multiply) after zeroing their outputs
@@ -1221,7 +1254,8 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     if (!J.n_out || !J.words) continue;
     J.n_stages = (J.n_in + stage_in - 1) / stage_in;
     J.pairs = pair ? (J.n_out + 3) / 4 : (J.n_out + 1) / 2;
-    const size_t wt = ceil_div(J.words, tile_words);
+    J.n_mma = f4 && pair ? tc64f4::pair_n_for(J.words) : 0;  // the FP4 pair's tiles are 2 n_mma words
+    const size_t wt = ceil_div(J.words, J.n_mma ? 2 * (size_t)J.n_mma : tile_words);
     if (wt > 0xFFFFFFFFu) return cudaErrorInvalidValue;
     J.wt = (uint32_t)wt;
     if (!J.n_in) {

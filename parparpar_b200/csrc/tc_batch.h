@@ -61,6 +61,8 @@ struct Gf64TcJob {
   uint32_t wt;                        // ceil(words / 512)
   uint32_t accumulate;
   uint32_t splits, per;               // stage range cut into `splits` parts of `per` stages
+  uint32_t n_mma;                     // FP4 pair kernel: the MMA's N (words per CTA; a tile is 2 n_mma words)
+  uint32_t reserved;
 };
 
 template <class Job>

@@ -4,7 +4,8 @@ Each tensor-core product has two operand formats, block-scaled FP4
 (tcgen05 kind::mxf4) and int8 (kind::i8), chosen per process
 (PARPAR_B200_GF16_TC, PARPAR_B200_GF64_TC = f4 | i8; resident GF(2^16)
 coefficient tiles are laid out for one format).  The defaults are FP4 for
-GF(2^16) and int8 for GF(2^64), and the rest of the suite exercises them;
+GF(2^16) and, for GF(2^64), FP4 on SM pairs (launches whose jobs all have at
+least 4 outputs) and int8 on one CTA; the rest of the suite exercises them;
 this file runs the same parity cases in a child process with both fields on
 each format, so every kernel stays bit-exact.  Integer GF
 words: exact comparisons.
