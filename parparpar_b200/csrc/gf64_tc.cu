@@ -46,6 +46,23 @@
 #include "tc_common.cuh"
 
 namespace pp {
+// Input-row addresses of a stage for the producer thread.  With a pointer
+// table (repair: lost rows point at a zero row) each address is a load from
+// global memory; the producer loads the next stage's addresses while this
+// stage's copies go out, so their latency stays off its path (issued one
+// after another in front of each copy, the loads took longer than a stage).
+template <int S>
+struct StageRows {
+  const uint64_t* p[S];
+  __device__ __forceinline__ void load(const Gf64TcJob& J, unsigned st) {
+#pragma unroll
+    for (int ii = 0; ii < S; ii++) {
+      const unsigned i = st * S + ii;
+      p[ii] = i < J.n_in ? (J.in_ptrs ? J.in_ptrs[i] : J.in + (size_t)i * J.in_stride) : nullptr;
+    }
+  }
+};
+
 namespace tc64 {
 using namespace pp::tc;
 
@@ -140,8 +157,11 @@ k_gf64_matvec_tc(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
         const size_t w0 = (size_t)(sg.tile / J.pairs) * kWords;
         const unsigned words_valid = (unsigned)min((size_t)kWords, J.words - w0);
         const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
+        StageRows<kStageIn> rows, next;
+        rows.load(J, sg.st0);
         for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
           const unsigned sl = g % kLd;
+          next.load(J, st + 1);
           if (g >= (uint32_t)kLd && !mbar_wait(BAR(RAW_EMPTY + sl), (g / kLd - 1) & 1)) {
             *err = 1;
             break;
@@ -150,9 +170,10 @@ k_gf64_matvec_tc(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
           const unsigned ni = min((unsigned)kStageIn, J.n_in - i0);
           mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
           for (unsigned ii = 0; ii < ni; ii++) {
-            const uint64_t* row = J.in_ptrs ? J.in_ptrs[i0 + ii] : J.in + (size_t)(i0 + ii) * J.in_stride;
+            const uint64_t* row = rows.p[ii];
             bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 8), row + w0, raw_copy, BAR(RAW_FULL + sl));
           }
+          rows = next;
         }
       } while (0);
       if (*err) {  // every issued copy lands before the CTA exits
@@ -402,8 +423,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         const size_t wc = (size_t)(sg.tile / J.pairs) * kWords + (size_t)kPHalf * rank;
         const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)kPHalf, J.words - wc) : 0u;
         const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
+        StageRows<kStageIn> rows, next;
+        rows.load(J, sg.st0);
         for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
           const unsigned sl = g % kPLd;
+          next.load(J, st + 1);
           if (g >= (uint32_t)kPLd && !mbar_wait(BAR(RAW_EMPTY + sl), (g / kPLd - 1) & 1)) {
             *err = 1;
             break;
@@ -412,9 +436,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           const unsigned ni = raw_copy ? min((unsigned)kStageIn, J.n_in - i0) : 0u;
           mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
           for (unsigned ii = 0; ii < ni; ii++) {
-            const uint64_t* row = J.in_ptrs ? J.in_ptrs[i0 + ii] : J.in + (size_t)(i0 + ii) * J.in_stride;
+            const uint64_t* row = rows.p[ii];
             bulk_g2s(sRaw + sl * kPRawBytes + ii * (kPHalf * 8), row + wc, raw_copy, BAR(RAW_FULL + sl));
           }
+          rows = next;
         }
       } while (0);
       if (*err) {
@@ -756,8 +781,11 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
         const size_t w0 = (size_t)(sg.tile / J.pairs) * kWords;
         const unsigned words_valid = (unsigned)min((size_t)kWords, J.words - w0);
         const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
+        StageRows<kStageIn> rows, next;
+        rows.load(J, sg.st0);
         for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
           const unsigned sl = g % kLd;
+          next.load(J, st + 1);
           if (g >= (uint32_t)kLd && !mbar_wait(BAR(RAW_EMPTY + sl), (g / kLd - 1) & 1)) {
             *err = 1;
             break;
@@ -766,9 +794,10 @@ k_gf64_matvec_f4(const __grid_constant__ Gf64TcBatch batch, int* __restrict__ st
           const unsigned ni = min((unsigned)kStageIn, J.n_in - i0);
           mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
           for (unsigned ii = 0; ii < ni; ii++) {
-            const uint64_t* row = J.in_ptrs ? J.in_ptrs[i0 + ii] : J.in + (size_t)(i0 + ii) * J.in_stride;
+            const uint64_t* row = rows.p[ii];
             bulk_g2s(sRaw + sl * kRawBytes + ii * (kWords * 8), row + w0, raw_copy, BAR(RAW_FULL + sl));
           }
+          rows = next;
         }
       } while (0);
       if (*err) {
@@ -1026,8 +1055,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         const size_t wc = (size_t)(sg.tile / J.pairs) * (2 * np) + (size_t)np * rank;
         const unsigned words_valid = J.words > wc ? (unsigned)min((size_t)np, J.words - wc) : 0u;
         const uint32_t raw_copy = (uint32_t)(((size_t)words_valid * 8 + 15) & ~(size_t)15);
+        StageRows<kStageIn> rows, next;
+        rows.load(J, sg.st0);
         for (unsigned st = sg.st0; st < sg.st1; st++, g++) {
           const unsigned sl = g % kPLd;
+          next.load(J, st + 1);
           if (g >= (uint32_t)kPLd && !mbar_wait(BAR(RAW_EMPTY + sl), (g / kPLd - 1) & 1)) {
             *err = 1;
             break;
@@ -1036,9 +1068,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           const unsigned ni = raw_copy ? min((unsigned)kStageIn, J.n_in - i0) : 0u;
           mbar_expect_tx(BAR(RAW_FULL + sl), raw_copy * ni);
           for (unsigned ii = 0; ii < ni; ii++) {
-            const uint64_t* row = J.in_ptrs ? J.in_ptrs[i0 + ii] : J.in + (size_t)(i0 + ii) * J.in_stride;
+            const uint64_t* row = rows.p[ii];
             bulk_g2s(sRaw + sl * kPRawBytes + ii * (kPWordsCta * 8), row + wc, raw_copy, BAR(RAW_FULL + sl));
           }
+          rows = next;
         }
       } while (0);
       if (*err) {
