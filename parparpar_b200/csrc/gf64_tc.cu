@@ -683,11 +683,11 @@ PP_D void fill_scales(uint32_t tmem, int warp) {
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
-// A rows: builder thread e makes rows b, b + 1 (b = 2 (e % 32)) of the
-// multiplication matrix of coefficient e / 32 of the stage (output e / 128,
-// input (e / 32) % 4): row b by the closed form, row b + 1 from it by one
-// step of Q_{b+1} = ((Q_b ^ [b+1 in {0,1,3,4}] Q_63) << 1) | bit_{b+1}(c),
-// which follows from c x^{e+1} = (c x^e) x mod x^64 + x^4 + x^3 + x + 1.
+// A rows: builder thread e makes rows b, b + 1 (b = 2 ((e / 4) % 32)) of the
+// multiplication matrix of coefficient (output e / 128, input e % 4) of the
+// stage: row b by the closed form, row b + 1 from it by one step of
+// Q_{b+1} = ((Q_b ^ [b+1 in {0,1,3,4}] Q_63) << 1) | bit_{b+1}(c), which
+// follows from c x^{e+1} = (c x^e) x mod x^64 + x^4 + x^3 + x + 1.
 PP_D uint64_t mul_matrix_row63(uint64_t c) {  // row 63: the closed form at b = 63
   const uint64_t rv = __brevll(c);
   return rv ^ (rv << 63) ^ (rv << 61) ^ (rv << 60);
@@ -697,10 +697,13 @@ struct ARows {
   uint32_t row0, r70, row1, r71;
   uint64_t red;
   PP_D explicit ARows(int e) {
-    const unsigned kc = (unsigned)e >> 5;
-    oo = kc >> 2;
-    ii = kc & 3;
-    b = 2 * ((unsigned)e & 31);
+    // a warp covers the 4 inputs x 8 consecutive row pairs of one output, so
+    // a 64-bit store phase meets every (16-byte slot, half) of a row once or
+    // twice (slot = chunk ^ row % 8, chunk = 2j + input / 2)
+    const unsigned t = (unsigned)e >> 2;
+    ii = (unsigned)e & 3;
+    oo = t >> 5;
+    b = 2 * (t & 31);
     const unsigned m0 = 64 * oo + b, m1 = m0 + 1;
     // input ii sits at chunk 2j + ii / 2, byte 8 (ii % 2) of an A row
     ch = ii >> 1;
