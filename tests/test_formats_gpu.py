@@ -47,8 +47,10 @@ for n, s, r in [(16, 480, 8), (17, 961, 16), (40, 4001, 8), (33, 20000, 16), (30
     out = base.copy()
     par2.gf16_muladd(data, co, out=out, accumulate=True, ctx=ctx)
     assert np.array_equal(out, base ^ O.par2_muladd(list(data), s, co)), ("gf16 acc", n, s, r)
-# GF(2^64): tile edges (480/512 words), ragged stages, accumulate
-for N, W, R in [(4, 480, 2), (5, 482, 3), (33, 1000, 8), (64, 96, 5), (200, 2048, 16)]:
+# GF(2^64): tile edges (480/512 words), ragged stages, accumulate, and the
+# SM pair's per-job MMA width (2 words: N = 16; 16: 16; 512: 128; 1024: 176)
+for N, W, R in [(4, 480, 2), (5, 482, 3), (33, 1000, 8), (64, 96, 5), (200, 2048, 16),
+                (9, 2, 4), (20, 16, 6), (40, 512, 4), (70, 1024, 8)]:
     x = rng.integers(0, 2**64, (N, W), dtype=np.uint64)
     want = O.gf64_compute_recovery(x, R, 0, N)
     got = np.zeros((R, W), dtype=np.uint64)
