@@ -18,6 +18,8 @@
 //       forward (the reference's descending in-place loop)
 //         d[r] ^= d[r + dd], r descending
 //       inverse (ascending)  d[r] ^= d[r + dd]
+//     dd >= polylen / 4, so a forward row takes at most two links:
+//     new d[r] = d[r] ^ d[r + dd] ^ (d[r + 2 dd] if r + 2 dd < polylen).
 //   * butterfly depth d, on bit k = L-1-d, block t = r >> (k+1), twiddle
 //     w = v_{2^d XOR 2t} (v_j = XOR of the Cantor basis vectors at the set
 //     bits of j); forward lo = f[r] ^ w*f[r+h], f[r+h] ^= lo, f[r] = lo;
@@ -27,20 +29,27 @@
 // tree) emits its top phases, then recurses into sched(lb, si) and
 // sched(lb+si, pl-si).  Every phase of sched(lb, pl) XORs rows that differ
 // only in bits [lb, lb+pl) and its condition depends only on those bits, so
-// a subtree acts identically along all other bits, and the two children act
-// on disjoint bit ranges and commute.  Hence:
-//   * a subtree of at most kTileBits bits runs as one tile pass: a CTA loads
-//     the 2^p rows that vary in those bits (stride 2^lb) for 8 polynomials
-//     into shared memory and applies all its phases there;
-//   * the top phases of wider nodes run as global passes, in place, one
-//     thread per chain {r, r+dd, r+2dd, ...} of a column, so every element
-//     is read and written once;
-//   * the butterflies of kTileBits consecutive bits run as one tile pass
-//     (high bits first for the forward transform).
-// For n = 2^17: 9 global conversion passes + 2 conversion tiles + 2
-// butterfly tiles, in place (13 passes over the data).
+// a subtree acts identically along all other bits (a Kronecker factor), and
+// the two children act on disjoint bit ranges and commute.  A butterfly on
+// bit k acts identically along the bits below k.  Hence, all in place:
+//   * class pass: the top phases of the nodes wider than kTileBits bits
+//     (for n <= 2^20: of the root and of its 16-bit child) come first.  They
+//     move data by dd = (2^si - 1) 2^j with si a multiple of 8, all
+//     multiples of m = 255, so the rows congruent to rho mod m are closed
+//     under all of them: one CTA per class and column chunk holds the class
+//     (n / 255 rows) in shared memory and applies every such phase (the
+//     subtrees below are on disjoint bits and commute with them);
+//   * fused tiles: the butterflies run in groups of at most kTileBits
+//     consecutive bits, from the top (no group boundary inside a conversion
+//     subtree); a conversion subtree on bits X commutes with the butterflies
+//     on bits above X, so it runs inside the tile of the group holding X,
+//     before that group's butterflies.  A CTA loads the 2^p rows that vary
+//     in the group's bits (stride 2^lo) for 8 polynomials into shared memory.
+//   The inverse transform runs the same passes in reverse order, each
+//   inverted.  n = 2^17: 1 class pass + 2 fused tiles (3 passes over the data).
 #include <algorithm>
 #include <mutex>
+#include <numeric>
 #include <vector>
 
 #include "pp_common.cuh"
@@ -66,11 +75,52 @@ __device__ uint64_t g_tw[2048];
 
 PP_D uint64_t cantor_v(uint32_t j) { return __ldg(&g_tw[j & 1023]) ^ __ldg(&g_tw[1024 + (j >> 10)]); }
 
+// w * b for one twiddle w and many b: the masked quarters of w's three
+// Karatsuba operands are formed once.  Same products as gf64_mul (32 x 32
+// carry-less products by integer multiplies on every 4th bit, Karatsuba over
+// the halves, then the reduction).
+struct MulByW {
+  uint32_t q[3][4];
+  PP_D static void split(uint32_t* o, uint32_t a) {
+    o[0] = a & 0x11111111u;
+    o[1] = a & 0x22222222u;
+    o[2] = a & 0x44444444u;
+    o[3] = a & 0x88888888u;
+  }
+  PP_D explicit MulByW(uint64_t w) {
+    const uint32_t lo = (uint32_t)w, hi = (uint32_t)(w >> 32);
+    split(q[0], lo);
+    split(q[1], hi);
+    split(q[2], lo ^ hi);
+  }
+  PP_D static uint64_t wide(uint32_t x, uint32_t y) { return (uint64_t)x * y; }
+  PP_D static uint64_t clmul(const uint32_t* a, uint32_t b) {
+    const uint32_t b0 = b & 0x11111111u, b1 = b & 0x22222222u, b2 = b & 0x44444444u, b3 = b & 0x88888888u;
+    const uint64_t z0 = wide(a[0], b0) ^ wide(a[1], b3) ^ wide(a[2], b2) ^ wide(a[3], b1);
+    const uint64_t z1 = wide(a[0], b1) ^ wide(a[1], b0) ^ wide(a[2], b3) ^ wide(a[3], b2);
+    const uint64_t z2 = wide(a[0], b2) ^ wide(a[1], b1) ^ wide(a[2], b0) ^ wide(a[3], b3);
+    const uint64_t z3 = wide(a[0], b3) ^ wide(a[1], b2) ^ wide(a[2], b1) ^ wide(a[3], b0);
+    return (z0 & 0x1111111111111111ull) | (z1 & 0x2222222222222222ull) | (z2 & 0x4444444444444444ull) |
+           (z3 & 0x8888888888888888ull);
+  }
+  PP_D uint64_t mul(uint64_t b) const {
+    const uint32_t bl = (uint32_t)b, bh = (uint32_t)(b >> 32);
+    const uint64_t lo = clmul(q[0], bl), hi = clmul(q[1], bh);
+    const uint64_t mid = clmul(q[2], bl ^ bh) ^ lo ^ hi;
+    return gf64_reduce(hi ^ (mid >> 32), lo ^ (mid << 32));
+  }
+};
+
 constexpr int kTileBits = 9;   // at most 512 rows per tile
 constexpr int kTileCols = 8;   // polynomials per tile (64-byte row segments)
 constexpr int kTileThreads = 256;
-constexpr int kMaxChain = 8;   // dd >= polylen / 4: chains have at most 4 rows
 constexpr int kMaxOps = 32;
+static_assert((1 << (kTileBits - 1)) <= kTileThreads, "one butterfly pair index per thread");
+
+constexpr int kClassThreads = 256;
+constexpr int kClassPer = 17;  // elements per thread
+constexpr uint32_t kClassElems = kClassPer * kClassThreads;  // 4,352 (34 KiB): 2^20 / 255 rows x 1 polynomial
+constexpr int kMaxClassOps = 16;
 
 struct TileOp {
   int32_t kind;  // 0: conversion phase, 1: butterfly
@@ -83,51 +133,74 @@ struct TilePlan {
   TileOp op[kMaxOps];
 };
 
-// One conversion phase over the whole array, in place: one thread per
-// (chain, polynomial); a chain is {base + rho + k*dd} inside one aligned
-// block of polylen rows (n <= 2^20, so chain indices fit 32 bits).
-__global__ void __launch_bounds__(256) k_fft_cvt_chain(uint64_t* __restrict__ d, size_t n, size_t batch, size_t ld,
-                                                       uint32_t polylen, uint32_t dd, uint32_t sl, int inverse,
-                                                       uint32_t col_blocks) {
-  const uint32_t chain = blockIdx.x / col_blocks;
-  const size_t col = (size_t)(blockIdx.x - chain * col_blocks) * blockDim.x + threadIdx.x;
-  if (col >= batch) return;
-  const uint32_t blk = chain / dd;
-  const uint32_t rho = chain - blk * dd;
-  const size_t base = (size_t)blk * polylen + rho;
-  const uint32_t hi = polylen - dd;  // rows [sl, hi) of the block change
-  uint64_t v[kMaxChain];
-  uint32_t K = 0;
+struct ClassOp {
+  uint32_t polylen, dd, sl;
+};
+struct ClassPlan {
+  uint32_t m;          // class modulus (every dd is a multiple)
+  uint32_t cc_log;     // log2 of the polynomials per CTA
+  uint32_t col_tiles;  // column chunks per class
+  uint32_t n_ops;
+  int32_t inverse;
+  ClassOp op[kMaxClassOps];
+};
+
+// The class pass: CTA (rho, column chunk) holds rows rho, rho + m, rho + 2m,
+// ... (J rows) x CC polynomials in shared memory, row-major (element
+// j * CC + c), and applies the phases in order, each from the old values
+// (the two-link closed form).  A partner row r + dd of the class is element
+// (j + dd / m) * CC + c.  n <= 2^20, so row indices fit 32 bits.
+__global__ void __launch_bounds__(kClassThreads) k_fft_cvt_class(uint64_t* __restrict__ d, size_t n, size_t batch,
+                                                                 size_t ld, const __grid_constant__ ClassPlan P) {
+  __shared__ uint64_t s[kClassElems];
+  const uint32_t cl = P.cc_log, CC = 1u << cl;
+  const uint32_t rho = blockIdx.x / P.col_tiles;
+  const size_t col0 = (size_t)(blockIdx.x - rho * P.col_tiles) * CC;
+  const uint32_t J = (uint32_t)((n - rho + P.m - 1) / P.m);
+  const uint32_t E = min(J << cl, kClassElems);  // the host sizes CC so that J * CC fits
+  // consecutive threads read consecutive polynomials of a row
+  for (uint32_t e = threadIdx.x; e < E; e += kClassThreads) {
+    const uint32_t c = e & (CC - 1);
+    const size_t g = rho + (size_t)P.m * (e >> cl);
+    s[e] = col0 + c < batch ? d[g * ld + col0 + c] : 0;
+  }
+  __syncthreads();
+  for (uint32_t oi = 0; oi < P.n_ops; oi++) {
+    const ClassOp op = P.op[oi];
+    const uint32_t q = (op.dd / P.m) << cl;  // partner distance in elements
+    uint64_t nv[kClassPer];
 #pragma unroll
-  for (int k = 0; k < kMaxChain; k++)
-    if (rho + (uint32_t)k * dd < polylen) {
-      v[k] = d[(base + (size_t)k * dd) * ld + col];
-      K = k + 1;
-    }
-  if (!inverse) {
-    // descending: d[r] ^= d[r + dd] with d[r + dd] already updated
-#pragma unroll
-    for (int k = kMaxChain - 2; k >= 0; k--) {
-      const uint32_t r = rho + (uint32_t)k * dd;
-      if ((uint32_t)k + 1 < K && r >= sl && r < hi) {
-        v[k] ^= v[k + 1];
-        d[(base + (size_t)k * dd) * ld + col] = v[k];
+    for (int k = 0; k < kClassPer; k++) {
+      const uint32_t e = threadIdx.x + k * kClassThreads;
+      nv[k] = 0;
+      if (e >= E) continue;
+      const uint32_t r = (rho + P.m * (e >> cl)) & (op.polylen - 1);
+      uint64_t v = s[e];
+      if (r >= op.sl && r + op.dd < op.polylen && e + q < E) {
+        v ^= s[e + q];
+        if (!P.inverse && r + 2 * op.dd < op.polylen && e + 2 * q < E) v ^= s[e + 2 * q];
       }
+      nv[k] = v;
     }
-  } else {
-    // ascending: d[r] ^= d[r + dd] with d[r + dd] not yet updated
+    __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kMaxChain - 1; k++) {
-      const uint32_t r = rho + (uint32_t)k * dd;
-      if ((uint32_t)k + 1 < K && r >= sl && r < hi) d[(base + (size_t)k * dd) * ld + col] = v[k] ^ v[k + 1];
+    for (int k = 0; k < kClassPer; k++) {
+      const uint32_t e = threadIdx.x + k * kClassThreads;
+      if (e < E) s[e] = nv[k];
     }
+    __syncthreads();
+  }
+  for (uint32_t e = threadIdx.x; e < E; e += kClassThreads) {
+    const uint32_t c = e & (CC - 1);
+    if (col0 + c < batch) d[(rho + (size_t)P.m * (e >> cl)) * ld + col0 + c] = s[e];
   }
 }
 
 // A tile pass: 2^p rows varying in bits [lo, lo+p) (the other bits fixed
 // by the tile index) x kTileCols polynomials (the column chunk), in shared
-// memory, column-major with a padded column stride.
-__global__ void __launch_bounds__(kTileThreads) k_fft_tile(uint64_t* __restrict__ d, size_t n, size_t batch,
+// memory, column-major with a padded column stride.  Conversion phases and
+// butterflies in the order of the plan.
+__global__ void __launch_bounds__(kTileThreads, 4) k_fft_tile(uint64_t* __restrict__ d, size_t n, size_t batch,
                                                            size_t ld, const __grid_constant__ TilePlan P) {
   constexpr uint32_t kStride = (1u << kTileBits) + 1;
   constexpr int kPerThread = (1 << kTileBits) * kTileCols / kTileThreads;  // 16
@@ -144,10 +217,14 @@ __global__ void __launch_bounds__(kTileThreads) k_fft_tile(uint64_t* __restrict_
     s[c * kStride + u] = col0 + c < batch ? d[row_of(u) * ld + col0 + c] : 0;
   }
   __syncthreads();
+  // butterflies: one pair index per thread (p <= kTileBits, so T / 2 <= the
+  // thread count), its twiddle shared by the columns the thread takes
+  const uint32_t pr = threadIdx.x & ((T >> 1) - 1);
+  const uint32_t c_first = threadIdx.x >> (p - 1), c_step = kTileThreads >> (p - 1);
   for (uint32_t oi = 0; oi < P.n_ops; oi++) {
     const TileOp op = P.op[oi];
     if (op.kind == 0) {
-      // conversion phase from the old values (at most two links: dd >= polylen / 4)
+      // conversion phase from the old values (at most two links)
       const uint32_t PL = op.a, DD = op.b, SL = op.c, HI = PL - DD;
       uint64_t nv[kPerThread];
 #pragma unroll
@@ -171,22 +248,21 @@ __global__ void __launch_bounds__(kTileThreads) k_fft_tile(uint64_t* __restrict_
         const uint32_t e = threadIdx.x + q * kTileThreads;
         if (e < T * kTileCols) s[(e >> p) * kStride + (e & (T - 1))] = nv[q];
       }
-    } else {
+    } else if (c_first < kTileCols) {
       const uint32_t kl = op.a, kg = op.b, depth = op.c, h = 1u << kl;
-      for (uint32_t e = threadIdx.x; e < (T / 2) * kTileCols; e += kTileThreads) {
-        const uint32_t pr = e & (T / 2 - 1), c = e >> (p - 1);
-        const uint32_t u = ((pr >> kl) << (kl + 1)) | (pr & (h - 1));  // bit kl of u is 0
-        const uint64_t tb = row_of(u) >> (kg + 1);                        // block index of the global row
-        const uint64_t w = cantor_v((1u << depth) ^ (uint32_t)(2 * tb));
+      const uint32_t u = ((pr >> kl) << (kl + 1)) | (pr & (h - 1));  // bit kl of u is 0
+      const uint64_t tb = row_of(u) >> (kg + 1);                        // block index of the global row
+      const MulByW W(cantor_v((1u << depth) ^ (uint32_t)(2 * tb)));
+      for (uint32_t c = c_first; c < kTileCols; c += c_step) {
         uint64_t* col = s + c * kStride;
         const uint64_t a = col[u], b = col[u + h];
         if (!P.inverse) {
-          const uint64_t lo = a ^ gf64_mul(w, b);
+          const uint64_t lo = a ^ W.mul(b);
           col[u] = lo;
           col[u + h] = b ^ lo;
         } else {
           const uint64_t fh = a ^ b;
-          col[u] = a ^ gf64_mul(w, fh);
+          col[u] = a ^ W.mul(fh);
           col[u + h] = fh;
         }
       }
@@ -203,9 +279,13 @@ __global__ void __launch_bounds__(kTileThreads) k_fft_tile(uint64_t* __restrict_
 struct Phase {
   uint32_t polylen, sh, sl;
 };
+struct CvtTile {  // a conversion subtree of at most kTileBits bits
+  uint32_t lb, pl;
+  std::vector<Phase> ph;
+};
 struct Pass {
   bool tile;
-  Phase g;        // global conversion phase
+  ClassPlan cls;  // class pass
   TilePlan plan;  // tile pass
 };
 
@@ -230,35 +310,15 @@ static void sched_inv(int lb, int pl, std::vector<Phase>& out) {
   for (int i = si; i < pl; i++) out.push_back({1u << (i + lb + 1), 1u << (i + lb), 1u << (i + lb - si)});
 }
 
-static Pass tile_pass(uint32_t lo, uint32_t p, uint32_t L, bool inverse) {
-  Pass ps{};
-  ps.tile = true;
-  ps.plan.lo = lo;
-  ps.plan.p = p;
-  ps.plan.L = L;
-  ps.plan.inverse = inverse ? 1 : 0;
-  return ps;
-}
-static void add_cvt_ops(Pass& ps, const std::vector<Phase>& ph, uint32_t lo) {
-  for (const Phase& f : ph) {  // every value of the subtree is a multiple of 2^lo
-    TileOp& o = ps.plan.op[ps.plan.n_ops++];
-    o.kind = 0;
-    o.a = f.polylen >> lo;
-    o.b = (f.sh - f.sl) >> lo;
-    o.c = f.sl >> lo;
-  }
-}
-
-// conversion: global top phases of wide nodes, one tile per narrow subtree
-static void plan_cvt(int lb, int pl, uint32_t L, bool inverse, std::vector<Pass>& out) {
+// The conversion as the top phases of the wide nodes (in their order) and
+// the narrow subtrees.
+static void collect_cvt(int lb, int pl, bool inverse, std::vector<Phase>& wide, std::vector<CvtTile>& tiles) {
   if (pl <= 1) return;
   if (pl <= kTileBits) {
-    std::vector<Phase> ph;
-    if (!inverse) sched_fwd(lb, pl, ph);
-    else sched_inv(lb, pl, ph);
-    Pass ps = tile_pass(lb, pl, L, inverse);
-    add_cvt_ops(ps, ph, lb);
-    out.push_back(ps);
+    CvtTile t{(uint32_t)lb, (uint32_t)pl, {}};
+    if (!inverse) sched_fwd(lb, pl, t.ph);
+    else sched_inv(lb, pl, t.ph);
+    tiles.push_back(std::move(t));
     return;
   }
   const int si = choose_si(pl);
@@ -267,41 +327,83 @@ static void plan_cvt(int lb, int pl, uint32_t L, bool inverse, std::vector<Pass>
     for (int i = pl - 1; i >= si; i--) top.push_back({1u << (i + lb + 1), 1u << (i + lb), 1u << (i + lb - si)});
   else
     for (int i = si; i < pl; i++) top.push_back({1u << (i + lb + 1), 1u << (i + lb), 1u << (i + lb - si)});
-  if (!inverse)
-    for (const Phase& f : top) out.push_back(Pass{false, f, {}});
-  plan_cvt(lb, si, L, inverse, out);
-  plan_cvt(lb + si, pl - si, L, inverse, out);
-  if (inverse)
-    for (const Phase& f : top) out.push_back(Pass{false, f, {}});
+  if (!inverse) wide.insert(wide.end(), top.begin(), top.end());
+  collect_cvt(lb, si, inverse, wide, tiles);
+  collect_cvt(lb + si, pl - si, inverse, wide, tiles);
+  if (inverse) wide.insert(wide.end(), top.begin(), top.end());
 }
 
-// butterflies in groups of kTileBits bits: forward from the top bit down
-static void plan_bfly(uint32_t L, bool inverse, std::vector<Pass>& out) {
-  std::vector<Pass> groups;
-  for (int top = (int)L; top > 0; top -= kTileBits) {
-    const uint32_t lo = (uint32_t)std::max(0, top - kTileBits), p = (uint32_t)top - lo;
-    Pass ps = tile_pass(lo, p, L, inverse);
-    if (!inverse) {
-      for (int k = top - 1; k >= (int)lo; k--) {  // depth d = L-1-k, ascending
-        TileOp& o = ps.plan.op[ps.plan.n_ops++];
-        o.kind = 1;
-        o.a = (uint32_t)k - lo;
-        o.b = (uint32_t)k;
-        o.c = L - 1 - (uint32_t)k;
-      }
-    } else {
-      for (int k = (int)lo; k < top; k++) {  // depth descending
-        TileOp& o = ps.plan.op[ps.plan.n_ops++];
-        o.kind = 1;
-        o.a = (uint32_t)k - lo;
-        o.b = (uint32_t)k;
-        o.c = L - 1 - (uint32_t)k;
-      }
-    }
-    groups.push_back(ps);
+static bool add_op(TilePlan& tp, int32_t kind, uint32_t a, uint32_t b, uint32_t c) {
+  if (tp.n_ops >= (uint32_t)kMaxOps) return false;
+  tp.op[tp.n_ops++] = TileOp{kind, a, b, c};
+  return true;
+}
+// a subtree's phases in the tile's local row units (every value of the
+// subtree is a multiple of 2^lo)
+static bool add_cvt_ops(TilePlan& tp, const CvtTile& t, uint32_t lo) {
+  for (const Phase& f : t.ph)
+    if (!add_op(tp, 0, f.polylen >> lo, (f.sh - f.sl) >> lo, f.sl >> lo)) return false;
+  return true;
+}
+// butterflies of bits [lo, top): forward from the top bit down (depth
+// d = L-1-k ascending), inverse from the bottom bit up
+static bool add_bfly_ops(TilePlan& tp, uint32_t lo, uint32_t top, uint32_t L, bool inverse) {
+  for (uint32_t i = 0; i < top - lo; i++) {
+    const uint32_t k = inverse ? lo + i : top - 1 - i;
+    if (!add_op(tp, 1, k - lo, k, L - 1 - k)) return false;
   }
-  if (inverse) std::reverse(groups.begin(), groups.end());  // low bits first
-  for (auto& g : groups) out.push_back(g);
+  return true;
+}
+
+static bool make_plan(uint32_t L, size_t n, bool inverse, std::vector<Pass>& out) {
+  std::vector<Phase> wide;
+  std::vector<CvtTile> tiles;
+  collect_cvt(0, (int)L, inverse, wide, tiles);
+  // fused tiles, top group first
+  std::vector<Pass> fused;
+  for (uint32_t top = L; top > 0;) {
+    uint32_t lo = top > (uint32_t)kTileBits ? top - kTileBits : 0;
+    for (const CvtTile& t : tiles)
+      if (t.lb < lo && lo < t.lb + t.pl) lo = t.lb + t.pl;  // keep each subtree in one group
+    if (lo >= top) return false;
+    Pass ps{};
+    ps.tile = true;
+    ps.plan.lo = lo;
+    ps.plan.p = top - lo;
+    ps.plan.L = L;
+    ps.plan.inverse = inverse ? 1 : 0;
+    if (inverse && !add_bfly_ops(ps.plan, lo, top, L, true)) return false;
+    for (const CvtTile& t : tiles)
+      if (t.lb >= lo && t.lb + t.pl <= top && !add_cvt_ops(ps.plan, t, lo)) return false;
+    if (!inverse && !add_bfly_ops(ps.plan, lo, top, L, false)) return false;
+    fused.push_back(ps);
+    top = lo;
+  }
+  // the class pass of the wide nodes' phases
+  Pass cls{};
+  if (!wide.empty()) {
+    if (wide.size() > (size_t)kMaxClassOps) return false;
+    uint32_t m = 0;
+    for (const Phase& f : wide) m = std::gcd(m, f.sh - f.sl);
+    const size_t J = (n + m - 1) / m;
+    if (m < 2 || J > kClassElems) return false;
+    uint32_t cc_log = 0;
+    while (cc_log < 3 && (J << (cc_log + 1)) <= kClassElems) cc_log++;
+    cls.tile = false;
+    cls.cls.m = m;
+    cls.cls.cc_log = cc_log;
+    cls.cls.n_ops = (uint32_t)wide.size();
+    cls.cls.inverse = inverse ? 1 : 0;
+    for (size_t i = 0; i < wide.size(); i++) cls.cls.op[i] = ClassOp{wide[i].polylen, wide[i].sh - wide[i].sl, wide[i].sl};
+  }
+  if (!inverse) {
+    if (!wide.empty()) out.push_back(cls);
+    out.insert(out.end(), fused.begin(), fused.end());
+  } else {
+    out.insert(out.end(), fused.rbegin(), fused.rend());
+    if (!wide.empty()) out.push_back(cls);
+  }
+  return true;
 }
 
 // the twiddle tables of the current device (synchronous copy, once per device)
@@ -337,15 +439,8 @@ cudaError_t launch_gf64_fft(uint64_t* d_data, size_t n, size_t batch, size_t ld,
   uint32_t L = 0;
   while (((size_t)1 << L) < n) L++;
   std::vector<Pass> passes;
-  if (!inverse) {
-    plan_cvt(0, (int)L, L, false, passes);
-    plan_bfly(L, false, passes);
-  } else {
-    plan_bfly(L, true, passes);
-    plan_cvt(0, (int)L, L, true, passes);
-  }
+  if (!make_plan(L, n, inverse, passes)) return cudaErrorInvalidValue;
   const unsigned col_tiles = (unsigned)ceil_div(batch, (size_t)kTileCols);
-  const uint32_t col_blocks = (uint32_t)ceil_div(batch, (size_t)256);
   for (Pass& ps : passes) {
     if (ps.tile) {
       const size_t blocks = (n >> ps.plan.p) * col_tiles;
@@ -353,11 +448,10 @@ cudaError_t launch_gf64_fft(uint64_t* d_data, size_t n, size_t batch, size_t ld,
       ps.plan.col_tiles = col_tiles;
       k_fft_tile<<<(unsigned)blocks, kTileThreads, 0, s>>>(d_data, n, batch, ld, ps.plan);
     } else {
-      const uint32_t dd = ps.g.sh - ps.g.sl;
-      const size_t chains = (n / ps.g.polylen) * dd;
-      if (chains * col_blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
-      k_fft_cvt_chain<<<(unsigned)(chains * col_blocks), 256, 0, s>>>(d_data, n, batch, ld, ps.g.polylen, dd,
-                                                                     ps.g.sl, inverse ? 1 : 0, col_blocks);
+      ps.cls.col_tiles = (uint32_t)ceil_div(batch, (size_t)1 << ps.cls.cc_log);
+      const size_t blocks = (size_t)ps.cls.m * ps.cls.col_tiles;
+      if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
+      k_fft_cvt_class<<<(unsigned)blocks, kClassThreads, 0, s>>>(d_data, n, batch, ld, ps.cls);
     }
     note_launch();
   }
