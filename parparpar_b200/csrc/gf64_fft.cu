@@ -146,53 +146,88 @@ struct ClassPlan {
 };
 
 // The class pass: CTA (rho, column chunk) holds rows rho, rho + m, rho + 2m,
-// ... (J rows) x CC polynomials in shared memory, row-major (element
-// j * CC + c), and applies the phases in order, each from the old values
-// (the two-link closed form).  A partner row r + dd of the class is element
-// (j + dd / m) * CC + c.  n <= 2^20, so row indices fit 32 bits.
+// ... (J rows) x CC polynomials in shared memory and applies the phases in
+// order, each from the old values (the two-link closed form).  Row j of the
+// class is CC consecutive words (CC = 8: four 16-byte chunks, chunk x stored
+// at x ^ ((j >> 1) & 3) so that eight consecutive rows cover all banks);
+// its partner r + dd is row j + dd / m.  Global copies: consecutive threads
+// take consecutive polynomials of a row; phases: one row per thread, its
+// condition evaluated once for the row.  n <= 2^20, so row indices fit 32 bits.
+template <int CC>
+struct ClassRow {
+  static constexpr int kChunk = CC >= 2 ? 2 : 1;  // words per shared-memory access
+  static constexpr int kChunks = CC / kChunk;
+  static constexpr int kRowsPer = (kClassElems / CC + kClassThreads - 1) / kClassThreads;
+  PP_D static uint32_t at(uint32_t j, uint32_t x) {  // word index of chunk x of row j
+    return j * CC + (CC == 8 ? (x ^ ((j >> 1) & 3)) : x) * kChunk;
+  }
+};
+
+template <int CC>
 __global__ void __launch_bounds__(kClassThreads) k_fft_cvt_class(uint64_t* __restrict__ d, size_t n, size_t batch,
                                                                  size_t ld, const __grid_constant__ ClassPlan P) {
-  __shared__ uint64_t s[kClassElems];
-  const uint32_t cl = P.cc_log, CC = 1u << cl;
+  using R = ClassRow<CC>;
+  __shared__ __align__(16) uint64_t s[kClassElems];
   const uint32_t rho = blockIdx.x / P.col_tiles;
   const size_t col0 = (size_t)(blockIdx.x - rho * P.col_tiles) * CC;
-  const uint32_t J = (uint32_t)((n - rho + P.m - 1) / P.m);
-  const uint32_t E = min(J << cl, kClassElems);  // the host sizes CC so that J * CC fits
-  // consecutive threads read consecutive polynomials of a row
-  for (uint32_t e = threadIdx.x; e < E; e += kClassThreads) {
-    const uint32_t c = e & (CC - 1);
-    const size_t g = rho + (size_t)P.m * (e >> cl);
-    s[e] = col0 + c < batch ? d[g * ld + col0 + c] : 0;
+  const uint32_t J = min((uint32_t)((n - rho + P.m - 1) / P.m), kClassElems / CC);  // the host sizes CC to fit
+  for (uint32_t e = threadIdx.x; e < J * CC; e += kClassThreads) {
+    const uint32_t j = e / CC, c = e % CC;
+    s[R::at(j, c / R::kChunk) + c % R::kChunk] =
+        col0 + c < batch ? d[(rho + (size_t)P.m * j) * ld + col0 + c] : 0;
   }
   __syncthreads();
   for (uint32_t oi = 0; oi < P.n_ops; oi++) {
     const ClassOp op = P.op[oi];
-    const uint32_t q = (op.dd / P.m) << cl;  // partner distance in elements
-    uint64_t nv[kClassPer];
+    const uint32_t qr = op.dd / P.m;  // partner distance in rows
+    uint64_t nv[R::kRowsPer][CC];
+    bool chg[R::kRowsPer];
 #pragma unroll
-    for (int k = 0; k < kClassPer; k++) {
-      const uint32_t e = threadIdx.x + k * kClassThreads;
-      nv[k] = 0;
-      if (e >= E) continue;
-      const uint32_t r = (rho + P.m * (e >> cl)) & (op.polylen - 1);
-      uint64_t v = s[e];
-      if (r >= op.sl && r + op.dd < op.polylen && e + q < E) {
-        v ^= s[e + q];
-        if (!P.inverse && r + 2 * op.dd < op.polylen && e + 2 * q < E) v ^= s[e + 2 * q];
+    for (int k = 0; k < R::kRowsPer; k++) {
+      const uint32_t j = threadIdx.x + k * kClassThreads;
+      const uint32_t r = (rho + P.m * j) & (op.polylen - 1);
+      chg[k] = j < J && r >= op.sl && r + op.dd < op.polylen && j + qr < J;
+      if (!chg[k]) continue;
+      const bool two = !P.inverse && r + 2 * op.dd < op.polylen && j + 2 * qr < J;
+#pragma unroll
+      for (int x = 0; x < R::kChunks; x++) {
+        if constexpr (R::kChunk == 2) {
+          ulonglong2 v = *reinterpret_cast<const ulonglong2*>(s + R::at(j, x));
+          const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(s + R::at(j + qr, x));
+          v.x ^= a.x;
+          v.y ^= a.y;
+          if (two) {
+            const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(s + R::at(j + 2 * qr, x));
+            v.x ^= b.x;
+            v.y ^= b.y;
+          }
+          nv[k][2 * x] = v.x;
+          nv[k][(2 * x + 1) % CC] = v.y;
+        } else {
+          uint64_t v = s[R::at(j, x)] ^ s[R::at(j + qr, x)];
+          if (two) v ^= s[R::at(j + 2 * qr, x)];
+          nv[k][x] = v;
+        }
       }
-      nv[k] = v;
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kClassPer; k++) {
-      const uint32_t e = threadIdx.x + k * kClassThreads;
-      if (e < E) s[e] = nv[k];
+    for (int k = 0; k < R::kRowsPer; k++) {
+      if (!chg[k]) continue;
+      const uint32_t j = threadIdx.x + k * kClassThreads;
+#pragma unroll
+      for (int x = 0; x < R::kChunks; x++) {
+        if constexpr (R::kChunk == 2)
+          *reinterpret_cast<ulonglong2*>(s + R::at(j, x)) = make_ulonglong2(nv[k][2 * x], nv[k][(2 * x + 1) % CC]);
+        else
+          s[R::at(j, x)] = nv[k][x];
+      }
     }
     __syncthreads();
   }
-  for (uint32_t e = threadIdx.x; e < E; e += kClassThreads) {
-    const uint32_t c = e & (CC - 1);
-    if (col0 + c < batch) d[(rho + (size_t)P.m * (e >> cl)) * ld + col0 + c] = s[e];
+  for (uint32_t e = threadIdx.x; e < J * CC; e += kClassThreads) {
+    const uint32_t j = e / CC, c = e % CC;
+    if (col0 + c < batch) d[(rho + (size_t)P.m * j) * ld + col0 + c] = s[R::at(j, c / R::kChunk) + c % R::kChunk];
   }
 }
 
@@ -200,10 +235,10 @@ __global__ void __launch_bounds__(kClassThreads) k_fft_cvt_class(uint64_t* __res
 // by the tile index) x kTileCols polynomials (the column chunk), in shared
 // memory, column-major with a padded column stride.  Conversion phases and
 // butterflies in the order of the plan.
-__global__ void __launch_bounds__(kTileThreads, 4) k_fft_tile(uint64_t* __restrict__ d, size_t n, size_t batch,
+__global__ void __launch_bounds__(kTileThreads, 3) k_fft_tile(uint64_t* __restrict__ d, size_t n, size_t batch,
                                                            size_t ld, const __grid_constant__ TilePlan P) {
   constexpr uint32_t kStride = (1u << kTileBits) + 1;
-  constexpr int kPerThread = (1 << kTileBits) * kTileCols / kTileThreads;  // 16
+  constexpr int kRowsPerThread = (1 << kTileBits) / kTileThreads;  // 2
   __shared__ uint64_t s[kStride * kTileCols];
   const uint32_t p = P.p, T = 1u << p;
   // column chunk fastest: the CTAs resident together cover whole rows
@@ -224,29 +259,33 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_fft_tile(uint64_t* __restri
   for (uint32_t oi = 0; oi < P.n_ops; oi++) {
     const TileOp op = P.op[oi];
     if (op.kind == 0) {
-      // conversion phase from the old values (at most two links)
+      // conversion phase from the old values (at most two links): one row
+      // per thread, all kTileCols polynomials; only changed rows are stored
       const uint32_t PL = op.a, DD = op.b, SL = op.c, HI = PL - DD;
-      uint64_t nv[kPerThread];
+      uint64_t nv[kRowsPerThread][kTileCols];
+      bool chg[kRowsPerThread];
 #pragma unroll
-      for (int q = 0; q < kPerThread; q++) {
-        const uint32_t e = threadIdx.x + q * kTileThreads;
-        nv[q] = 0;
-        if (e >= T * kTileCols) continue;
-        const uint32_t u = e & (T - 1), c = e >> p;
+      for (int k = 0; k < kRowsPerThread; k++) {
+        const uint32_t u = threadIdx.x + k * kTileThreads;
         const uint32_t r = u & (PL - 1);
-        const uint64_t* col = s + c * kStride;
-        uint64_t v = col[u];
-        if (r >= SL && r < HI) {
-          v ^= col[u + DD];
-          if (!P.inverse && r + 2 * DD < PL) v ^= col[u + 2 * DD];
+        chg[k] = u < T && r >= SL && r < HI;
+        if (!chg[k]) continue;
+        const bool two = !P.inverse && r + 2 * DD < PL;
+#pragma unroll
+        for (int c = 0; c < kTileCols; c++) {
+          const uint64_t* col = s + c * kStride;
+          uint64_t v = col[u] ^ col[u + DD];
+          if (two) v ^= col[u + 2 * DD];
+          nv[k][c] = v;
         }
-        nv[q] = v;
       }
       __syncthreads();
 #pragma unroll
-      for (int q = 0; q < kPerThread; q++) {
-        const uint32_t e = threadIdx.x + q * kTileThreads;
-        if (e < T * kTileCols) s[(e >> p) * kStride + (e & (T - 1))] = nv[q];
+      for (int k = 0; k < kRowsPerThread; k++) {
+        if (!chg[k]) continue;
+        const uint32_t u = threadIdx.x + k * kTileThreads;
+#pragma unroll
+        for (int c = 0; c < kTileCols; c++) s[c * kStride + u] = nv[k][c];
       }
     } else if (c_first < kTileCols) {
       const uint32_t kl = op.a, kg = op.b, depth = op.c, h = 1u << kl;
@@ -451,7 +490,12 @@ cudaError_t launch_gf64_fft(uint64_t* d_data, size_t n, size_t batch, size_t ld,
       ps.cls.col_tiles = (uint32_t)ceil_div(batch, (size_t)1 << ps.cls.cc_log);
       const size_t blocks = (size_t)ps.cls.m * ps.cls.col_tiles;
       if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidConfiguration;
-      k_fft_cvt_class<<<(unsigned)blocks, kClassThreads, 0, s>>>(d_data, n, batch, ld, ps.cls);
+      switch (ps.cls.cc_log) {
+        case 3: k_fft_cvt_class<8><<<(unsigned)blocks, kClassThreads, 0, s>>>(d_data, n, batch, ld, ps.cls); break;
+        case 2: k_fft_cvt_class<4><<<(unsigned)blocks, kClassThreads, 0, s>>>(d_data, n, batch, ld, ps.cls); break;
+        case 1: k_fft_cvt_class<2><<<(unsigned)blocks, kClassThreads, 0, s>>>(d_data, n, batch, ld, ps.cls); break;
+        default: k_fft_cvt_class<1><<<(unsigned)blocks, kClassThreads, 0, s>>>(d_data, n, batch, ld, ps.cls); break;
+      }
     }
     note_launch();
   }
