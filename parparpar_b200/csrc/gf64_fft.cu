@@ -117,9 +117,12 @@ constexpr int kTileThreads = 256;
 constexpr int kMaxOps = 32;
 static_assert((1 << (kTileBits - 1)) <= kTileThreads, "one butterfly pair index per thread");
 
-constexpr int kClassThreads = 256;
-constexpr int kClassPer = 17;  // elements per thread
-constexpr uint32_t kClassElems = kClassPer * kClassThreads;  // 4,352 (34 KiB): 2^20 / 255 rows x 1 polynomial
+constexpr int kClassThreads = 288;  // 9 warps: two rows per thread for the 515-row classes of n = 2^17
+constexpr uint32_t kClassWords = 5376;  // 42 KiB of shared memory: 2^17 / 255 rows x 8 polynomials, 2^20 / 255 x 1
+// words per class row of CC polynomials: the 16-byte chunks of any 8
+// consecutive rows fall on distinct bank groups (row strides of 5, 3 and 1
+// chunks are odd)
+__host__ __device__ constexpr uint32_t class_stride(int CC) { return CC == 8 ? 10 : CC == 4 ? 6 : (uint32_t)CC; }
 constexpr int kMaxClassOps = 16;
 
 struct TileOp {
@@ -148,87 +151,86 @@ struct ClassPlan {
 // The class pass: CTA (rho, column chunk) holds rows rho, rho + m, rho + 2m,
 // ... (J rows) x CC polynomials in shared memory and applies the phases in
 // order, each from the old values (the two-link closed form).  Row j of the
-// class is CC consecutive words (CC = 8: four 16-byte chunks, chunk x stored
-// at x ^ ((j >> 1) & 3) so that eight consecutive rows cover all banks);
-// its partner r + dd is row j + dd / m.  Global copies: consecutive threads
-// take consecutive polynomials of a row; phases: one row per thread, its
-// condition evaluated once for the row.  n <= 2^20, so row indices fit 32 bits.
+// class starts at word j * class_stride(CC); its partner r + dd is row
+// j + dd / m.  Global copies: consecutive threads take consecutive
+// polynomials of a row; phases: one row per thread, its condition evaluated
+// once for the row.  n <= 2^20, so row indices fit 32 bits.
 template <int CC>
-struct ClassRow {
-  static constexpr int kChunk = CC >= 2 ? 2 : 1;  // words per shared-memory access
-  static constexpr int kChunks = CC / kChunk;
-  static constexpr int kRowsPer = (kClassElems / CC + kClassThreads - 1) / kClassThreads;
-  PP_D static uint32_t at(uint32_t j, uint32_t x) {  // word index of chunk x of row j
-    return j * CC + (CC == 8 ? (x ^ ((j >> 1) & 3)) : x) * kChunk;
-  }
-};
-
-template <int CC>
-__global__ void __launch_bounds__(kClassThreads) k_fft_cvt_class(uint64_t* __restrict__ d, size_t n, size_t batch,
+__global__ void __launch_bounds__(kClassThreads, 3) k_fft_cvt_class(uint64_t* __restrict__ d, size_t n, size_t batch,
                                                                  size_t ld, const __grid_constant__ ClassPlan P) {
-  using R = ClassRow<CC>;
-  __shared__ __align__(16) uint64_t s[kClassElems];
+  constexpr uint32_t S = class_stride(CC);
+  constexpr int kChunk = CC >= 2 ? 2 : 1;  // words per shared-memory access
+  constexpr int kChunks = CC / kChunk;
+  constexpr int kRowsPer = (kClassWords / S + kClassThreads - 1) / kClassThreads;
+  constexpr uint32_t kStep = kClassThreads / CC;  // rows per copy step
+  __shared__ __align__(16) uint64_t s[kClassWords];
   const uint32_t rho = blockIdx.x / P.col_tiles;
   const size_t col0 = (size_t)(blockIdx.x - rho * P.col_tiles) * CC;
-  const uint32_t J = min((uint32_t)((n - rho + P.m - 1) / P.m), kClassElems / CC);  // the host sizes CC to fit
-  for (uint32_t e = threadIdx.x; e < J * CC; e += kClassThreads) {
-    const uint32_t j = e / CC, c = e % CC;
-    s[R::at(j, c / R::kChunk) + c % R::kChunk] =
-        col0 + c < batch ? d[(rho + (size_t)P.m * j) * ld + col0 + c] : 0;
+  const uint32_t J = min((uint32_t)((n - rho + P.m - 1) / P.m), kClassWords / S);  // the host sizes CC to fit
+  const uint32_t c = threadIdx.x % CC, j0 = threadIdx.x / CC;
+  const bool col_ok = col0 + c < batch;
+  const size_t g0 = (rho + (size_t)P.m * j0) * ld + col0 + c, gstep = (size_t)P.m * kStep * ld;
+  {
+    size_t gi = g0;
+    // unrolled: several loads in flight per thread
+#pragma unroll 8
+    for (uint32_t j = j0, si = j0 * S + c; j < J; j += kStep, si += kStep * S, gi += gstep) s[si] = col_ok ? d[gi] : 0;
   }
   __syncthreads();
   for (uint32_t oi = 0; oi < P.n_ops; oi++) {
     const ClassOp op = P.op[oi];
     const uint32_t qr = op.dd / P.m;  // partner distance in rows
-    uint64_t nv[R::kRowsPer][CC];
-    bool chg[R::kRowsPer];
+    uint64_t nv[kRowsPer][CC];
+    bool chg[kRowsPer];
 #pragma unroll
-    for (int k = 0; k < R::kRowsPer; k++) {
+    for (int k = 0; k < kRowsPer; k++) {
       const uint32_t j = threadIdx.x + k * kClassThreads;
       const uint32_t r = (rho + P.m * j) & (op.polylen - 1);
       chg[k] = j < J && r >= op.sl && r + op.dd < op.polylen && j + qr < J;
       if (!chg[k]) continue;
       const bool two = !P.inverse && r + 2 * op.dd < op.polylen && j + 2 * qr < J;
+      const uint64_t* a0 = s + j * S;
+      const uint64_t* a1 = a0 + qr * S;
+      const uint64_t* a2 = a1 + qr * S;
 #pragma unroll
-      for (int x = 0; x < R::kChunks; x++) {
-        if constexpr (R::kChunk == 2) {
-          ulonglong2 v = *reinterpret_cast<const ulonglong2*>(s + R::at(j, x));
-          const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(s + R::at(j + qr, x));
-          v.x ^= a.x;
-          v.y ^= a.y;
+      for (int x = 0; x < kChunks; x++) {
+        if constexpr (kChunk == 2) {
+          ulonglong2 v = *reinterpret_cast<const ulonglong2*>(a0 + 2 * x);
+          const ulonglong2 p = *reinterpret_cast<const ulonglong2*>(a1 + 2 * x);
+          v.x ^= p.x;
+          v.y ^= p.y;
           if (two) {
-            const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(s + R::at(j + 2 * qr, x));
-            v.x ^= b.x;
-            v.y ^= b.y;
+            const ulonglong2 q = *reinterpret_cast<const ulonglong2*>(a2 + 2 * x);
+            v.x ^= q.x;
+            v.y ^= q.y;
           }
-          nv[k][2 * x] = v.x;
-          nv[k][(2 * x + 1) % CC] = v.y;
+          nv[k][kChunk * x] = v.x;
+          nv[k][(kChunk * x + 1) % CC] = v.y;
         } else {
-          uint64_t v = s[R::at(j, x)] ^ s[R::at(j + qr, x)];
-          if (two) v ^= s[R::at(j + 2 * qr, x)];
+          uint64_t v = a0[x] ^ a1[x];
+          if (two) v ^= a2[x];
           nv[k][x] = v;
         }
       }
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < R::kRowsPer; k++) {
+    for (int k = 0; k < kRowsPer; k++) {
       if (!chg[k]) continue;
-      const uint32_t j = threadIdx.x + k * kClassThreads;
+      uint64_t* a0 = s + (threadIdx.x + k * kClassThreads) * S;
 #pragma unroll
-      for (int x = 0; x < R::kChunks; x++) {
-        if constexpr (R::kChunk == 2)
-          *reinterpret_cast<ulonglong2*>(s + R::at(j, x)) = make_ulonglong2(nv[k][2 * x], nv[k][(2 * x + 1) % CC]);
+      for (int x = 0; x < kChunks; x++) {
+        if constexpr (kChunk == 2)
+          *reinterpret_cast<ulonglong2*>(a0 + 2 * x) = make_ulonglong2(nv[k][2 * x], nv[k][(2 * x + 1) % CC]);
         else
-          s[R::at(j, x)] = nv[k][x];
+          a0[x] = nv[k][x];
       }
     }
     __syncthreads();
   }
-  for (uint32_t e = threadIdx.x; e < J * CC; e += kClassThreads) {
-    const uint32_t j = e / CC, c = e % CC;
-    if (col0 + c < batch) d[(rho + (size_t)P.m * j) * ld + col0 + c] = s[R::at(j, c / R::kChunk) + c % R::kChunk];
-  }
+  if (!col_ok) return;
+  size_t gi = g0;
+  for (uint32_t j = j0, si = j0 * S + c; j < J; j += kStep, si += kStep * S, gi += gstep) d[gi] = s[si];
 }
 
 // A tile pass: 2^p rows varying in bits [lo, lo+p) (the other bits fixed
@@ -247,6 +249,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_fft_tile(uint64_t* __restri
   const uint64_t low = t & ((1ull << P.lo) - 1), high = t >> P.lo;
   auto row_of = [&](uint32_t u) -> size_t { return low + ((size_t)u << P.lo) + (high << (P.lo + p)); };
   // load: consecutive threads read consecutive polynomials of a row
+#pragma unroll 8
   for (uint32_t e = threadIdx.x; e < T * kTileCols; e += kTileThreads) {
     const uint32_t u = e >> 3, c = e & 7;
     s[c * kStride + u] = col0 + c < batch ? d[row_of(u) * ld + col0 + c] : 0;
@@ -425,9 +428,9 @@ static bool make_plan(uint32_t L, size_t n, bool inverse, std::vector<Pass>& out
     uint32_t m = 0;
     for (const Phase& f : wide) m = std::gcd(m, f.sh - f.sl);
     const size_t J = (n + m - 1) / m;
-    if (m < 2 || J > kClassElems) return false;
-    uint32_t cc_log = 0;
-    while (cc_log < 3 && (J << (cc_log + 1)) <= kClassElems) cc_log++;
+    if (m < 2 || J > kClassWords) return false;
+    uint32_t cc_log = 3;
+    while (cc_log > 0 && J * class_stride(1 << cc_log) > kClassWords) cc_log--;
     cls.tile = false;
     cls.cls.m = m;
     cls.cls.cc_log = cc_log;
