@@ -6,8 +6,9 @@
 // sum of lib/par3gen.js:3892-3960 and SolveAndReconstruct, par3_engine.cc:980).
 //
 // One scheduler thread owns all device work.  Its loop:
-//   1. reap: waves whose completion event has fired release their memory
-//      reservations and table references; their jobs complete.
+//   1. reap: waves whose completion event has fired return their buffers to
+//      the pool and release their memory reservations and table references;
+//      their jobs complete.
 //   2. admit + launch: while a lane (stream) is free and jobs are queued,
 //      take jobs from the head of the queue while their device memory fits
 //      the budget (evicting unused resident tables first) and issue them as
@@ -16,7 +17,7 @@
 //        built once) -> repair systems and their inverses -> one fused
 //        GF(2^16) launch -> one fused GF(2^64) launch (creates and repair
 //        known-input sums) -> one fused GF(2^64) launch (repair restores)
-//        -> copies back to host buffers -> frees -> completion event.
+//        -> copies back to host buffers -> completion event.
 //   3. sleep until a submit, or poll the in-flight events.
 // Waves on different lanes overlap on the device; a job arriving while
 // others run joins the next wave (continuous batching, not a queue that
@@ -95,6 +96,12 @@ struct Wave {
   int* d_words = nullptr;          // device copy
   size_t reserved = 0;
   bool failed = false;             // an API call of the wave's issue failed
+  // staging buffers and temporaries of the wave: returned to the pool only
+  // after the host has seen the wave complete.  Freed in stream order right
+  // after the issue, they could be handed to another lane while this lane's
+  // kernels still read them (observed: the last word tiles of a large PAR3
+  // create read another job's staged bytes when 8 lanes ran concurrently).
+  std::vector<void*> frees;
 };
 
 constexpr int kMaxWords = 64;
@@ -622,10 +629,8 @@ bool launch_one(pp_server* S) {
   }
   note_peak(S);
   w->singular_slot.assign(w->jobs.size(), -1);
-  std::vector<void*> frees;
   const cudaStream_t s = S->lanes[lane];
-  cudaError_t e = issue_wave(S, w, needs, frees);
-  for (void* p : frees) cudaFreeAsync(p, s);
+  cudaError_t e = issue_wave(S, w, needs, w->frees);
   if (e != cudaSuccess) {
     cudaGetLastError();
     S->err = cudaGetErrorString(e);
@@ -657,6 +662,7 @@ bool reap(pp_server* S) {
       finish(S, w->jobs[k], st);
     }
     for (Table* t : w->tables) t->refs--;
+    for (void* p : w->frees) cudaFreeAsync(p, S->lanes[w->lane]);  // the wave's work has completed
     S->used -= w->reserved;
     S->lane_busy[w->lane] = false;
     cudaEventDestroy(w->ev);

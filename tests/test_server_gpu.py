@@ -187,3 +187,61 @@ def test_par2_repair_through_the_server():
     assert srv.wait(srv.submit(B.gf16_muladd_job(_pinned(inputs), m.factors, out))) == 0
     assert np.array_equal(_np(out), data[lost])
     srv.close()
+
+
+def test_large_par3_create_among_concurrent_lanes():
+    """A 283 MB PAR3 create (3,975 blocks of 71,344 bytes, R=413: the last
+    word tile is partial) submitted with 20 other jobs to 8 lanes: every
+    result equals the single-job entry points.  Each wave's staging buffers
+    must stay reserved until the wave has completed; returned to the pool in
+    stream order right after the issue, the large job's last tiles read bytes
+    another lane had staged meanwhile."""
+    import torch
+    from parparpar_b200 import batch as B
+    from parparpar_b200 import par2, par3
+    from parparpar_b200.server import Server
+    rng = np.random.default_rng(34)
+    g = torch.Generator(device="cuda").manual_seed(34)
+
+    def pinned_random(shape, dtype):
+        t = torch.empty(shape, dtype=dtype).pin_memory()
+        n = int(np.prod(shape)) * t.element_size()
+        t.view(-1).view(torch.uint8).copy_(torch.randint(0, 256, (n,), dtype=torch.uint8, device="cuda",
+                                                         generator=g))
+        return t
+
+    jobs = [("par3", pinned_random((3975, 71344 // 8), torch.int64), 413)]
+    for k in range(20):
+        if k % 2:
+            n, sb, r = int(rng.integers(200, 2000)), int(rng.integers(4, 64)) * 1024, int(rng.integers(4, 200))
+            jobs.append(("par2", pinned_random((n, sb), torch.uint8), r))
+        else:
+            n, words, r = int(rng.integers(100, 2000)), int(rng.integers(64, 4096)), int(rng.integers(4, 300))
+            jobs.append(("par3", pinned_random((n, words), torch.int64), r))
+    ctx = par3._ctx(None)
+
+    def out_of(kind, inp, r):
+        return torch.zeros((r, inp.shape[1]), dtype=inp.dtype).pin_memory()
+
+    plain = []
+    for kind, inp, r in jobs:
+        o = out_of(kind, inp, r)
+        if kind == "par2":
+            par2.par2_create(inp, np.arange(inp.shape[0]), np.arange(r, dtype=np.uint16), out=o, ctx=ctx)
+        else:
+            par3.GF64Controller.ctx = ctx
+            par3.GF64Controller.ComputeRecoveryBlocks(inp, inp.shape[0], o, r, inp.shape[1], 0, inp.shape[0])
+        ctx.synchronize()
+        plain.append(o)
+    for rep in range(2):
+        srv = Server(hbm_budget_bytes=120 * 10**9, max_jobs_per_wave=2, lanes=8)
+        outs = [out_of(*j) for j in jobs]
+        tickets = []
+        for (kind, inp, r), o in zip(jobs, outs):
+            job = (B.par2_create_job(inp, np.arange(r, dtype=np.uint16), o) if kind == "par2"
+                   else B.par3_create_job(inp, o, 0, inp.shape[0]))
+            tickets.append(srv.submit(job))
+        assert [srv.wait(t) for t in tickets] == [0] * len(jobs)
+        srv.close()
+        bad = [i for i in range(len(jobs)) if not torch.equal(plain[i], outs[i])]
+        assert not bad, (rep, bad)
