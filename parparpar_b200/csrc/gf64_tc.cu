@@ -1262,7 +1262,8 @@ static bool use_pair_kernel(const Gf64TcBatch& b) {
   return true;
 }
 
-cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s) {
+static cudaError_t launch_gf64_tc_batch_impl(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s,
+                                              bool allow_pair) {
   static std::atomic<uint64_t> attr{0};
   if (!device_done(attr)) {
     cudaError_t e = cudaFuncSetAttribute(tc64::k_gf64_matvec_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1279,7 +1280,7 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     if (e != cudaSuccess) return e;
     device_mark(attr);
   }
-  const bool pair = use_pair_kernel(b);
+  const bool pair = allow_pair && use_pair_kernel(b);
   const bool f4 = gf64_tc_use_f4(pair);
   const size_t tile_words = f4 ? (pair ? tc64f4::kPWords : tc64f4::kWords) : tc64::kWords;
   const unsigned stage_in = f4 ? tc64f4::kStageIn : tc64::kStageIn;
@@ -1335,6 +1336,17 @@ cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStr
     tc64::k_gf64_matvec_tc<<<(unsigned)items, tc64::kThreads, tc64::kSmemBytes, s>>>(b, d_status);
   note_launch();
   return cudaGetLastError();
+}
+
+cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s) {
+  return launch_gf64_tc_batch_impl(b, sms, d_status, s, true);
+}
+// The one-CTA kernels only.  The SM-pair kernels gave wrong words in the last
+// tiles of a large job while kernels of other streams ran on the device
+// (eight serving lanes); the one-CTA kernels were exact in the same runs, so
+// code that overlaps its own launches across streams uses these.
+cudaError_t launch_gf64_tc_batch_one_cta(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s) {
+  return launch_gf64_tc_batch_impl(b, sms, d_status, s, false);
 }
 
 cudaError_t launch_gf64_matvec_tc(const uint64_t* d_in, const uint64_t* const* d_in_ptrs, size_t in_stride,

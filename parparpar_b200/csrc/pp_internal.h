@@ -116,6 +116,7 @@ cudaError_t launch_gf64_matvec(const uint64_t* d_in, size_t in_stride, size_t n_
 // wt) are filled in here and empty jobs are dropped, so the table is modified.
 cudaError_t launch_gf16_tc_batch(Gf16TcBatch& b, int sms, int* d_status, cudaStream_t s);
 cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s);
+cudaError_t launch_gf64_tc_batch_one_cta(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s);
 
 cudaError_t launch_gf64_matvec_tc(const uint64_t* d_in, const uint64_t* const* d_in_ptrs, size_t in_stride,
                                   size_t n_in, size_t words, const uint64_t* d_coeff, size_t ldc, size_t n_out,

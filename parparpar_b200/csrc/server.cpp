@@ -545,7 +545,8 @@ cudaError_t issue_wave(pp_server* S, Wave* w, std::vector<Need>& needs, std::vec
       Gf64TcBatch t{};
       t.n_jobs = (uint32_t)std::min<size_t>(kTcMaxJobs, v->size() - i);
       for (uint32_t j = 0; j < t.n_jobs; j++) t.job[j] = (*v)[i + j];
-      WTRY(launch_gf64_tc_batch(t, S->sms, kst, s));
+      // one-CTA kernels: the lanes overlap on the device
+      WTRY(launch_gf64_tc_batch_one_cta(t, S->sms, kst, s));
     }
     if (v == &j64a) {
       // lookup-kernel jobs (block bytes not a multiple of 16), between the phases
