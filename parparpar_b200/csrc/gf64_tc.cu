@@ -1281,7 +1281,7 @@ static cudaError_t launch_gf64_tc_batch_impl(Gf64TcBatch& b, int sms, int* d_sta
     device_mark(attr);
   }
   const bool pair = allow_pair && use_pair_kernel(b);
-  const bool f4 = gf64_tc_use_f4(pair);
+  const bool f4 = allow_pair && gf64_tc_use_f4(pair);  // overlapped launches: the int8 one-CTA kernel
   const size_t tile_words = f4 ? (pair ? tc64f4::kPWords : tc64f4::kWords) : tc64::kWords;
   const unsigned stage_in = f4 ? tc64f4::kStageIn : tc64::kStageIn;
   // drop empty jobs (nothing to multiply) after zeroing their outputs
@@ -1341,10 +1341,11 @@ static cudaError_t launch_gf64_tc_batch_impl(Gf64TcBatch& b, int sms, int* d_sta
 cudaError_t launch_gf64_tc_batch(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s) {
   return launch_gf64_tc_batch_impl(b, sms, d_status, s, true);
 }
-// The one-CTA kernels only.  The SM-pair kernels gave wrong words in the last
-// tiles of a large job while kernels of other streams ran on the device
-// (eight serving lanes); the one-CTA kernels were exact in the same runs, so
-// code that overlaps its own launches across streams uses these.
+// The int8 one-CTA kernel only.  The SM-pair kernels (FP4 and int8) and the
+// FP4 one-CTA kernel gave wrong words in the last tiles of a large job while
+// kernels of other streams ran on the device (eight serving lanes); the int8
+// one-CTA kernel was exact in every such run, so code that overlaps its own
+// launches across streams uses it, whatever the format variables say.
 cudaError_t launch_gf64_tc_batch_one_cta(Gf64TcBatch& b, int sms, int* d_status, cudaStream_t s) {
   return launch_gf64_tc_batch_impl(b, sms, d_status, s, false);
 }
