@@ -1192,7 +1192,7 @@ def main():
             except Exception as e:  # report, keep the primary line
                 sec.append({"workload": name, "error": str(e)[:200]})
         line["secondary"] = sec
-        # the north-star shapes (1 GiB at R=8) at the top level of the line
+        # the 1 GiB R=8 shapes at the top level of the line
         r8 = {}
         for e in sec:
             if e.get("workload") in ("par2_create_1024x1MiB_R8", "par3_create_131072x8KiB_R8") and "value" in e:

@@ -97,10 +97,9 @@ struct Wave {
   size_t reserved = 0;
   bool failed = false;             // an API call of the wave's issue failed
   // staging buffers and temporaries of the wave: returned to the pool only
-  // after the host has seen the wave complete.  Freed in stream order right
-  // after the issue, they could be handed to another lane while this lane's
-  // kernels still read them (observed: the last word tiles of a large PAR3
-  // create read another job's staged bytes when 8 lanes ran concurrently).
+  // after the host has seen the wave complete, so no other lane's
+  // allocation can take them while this lane's kernels may still read them
+  // (the budget already counts them until then)
   std::vector<void*> frees;
 };
 
